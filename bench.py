@@ -1,0 +1,345 @@
+#!/usr/bin/env python
+"""Benchmark: pixels/s of the Milne-Eddington inversion on B200.
+
+Workload (one "step"): invert the 256x256-pixel, 30-wavelength, PSF-convolved,
+9-free-parameter cube (benchmark configuration 1; Fe I 6173.3354 A, grid
+-350..375 mA in 25 mA steps, Gaussian PSF FWHM 60 mA through the 1 mA table
+route, sigma = 1e-3 noise, <= 50 LM iterations) with the FP32 batched form.
+Synthetic data: seeded atmospheres synthesized by this library's FP64 path.
+
+JSON line (rank 0):
+  value    pixels/s with the cube resident in HBM (CUDA-event time of the
+           inversion kernel; L2 flushed between steps)
+  e2e      pixels/s through the public C ABI with pinned host buffers: the
+           host->device copy of the cube and the device->host copy of models,
+           chi^2 and iterations are inside the timed region
+  plain    the FP64 plain form on the same cube (eigen solve, and Cholesky)
+  roofline FP32-pipe fraction from the frozen flop model
+  cpu_baseline  the reference's own C hot path (oracle/_ref, float build,
+           -O3) on every host core, forked slabs like pmilos' Scatterv
+
+--impl reference: time only the reference's CPU implementation (rank 0).
+Multi-GPU (torchrun): every rank inverts its own cube (weak scaling, replicas:
+pixels are independent, there is no collective on the data path); time is the
+max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "p-milos_b200"))
+
+# ---- frozen flop model (per pixel; counted from the reference statements) ----
+F_VOIGT = 100
+
+
+def flop_model(nl: int, taps: int, K: int, psf: bool, stray: bool):
+    F_syn = nl * (3 * F_VOIGT + 100) + (8 * nl * taps if psf else 0) + (12 * nl if stray else 0)
+    F_rf = 870 * nl + (8 * nl * taps * (K - 1) if psf else 0) + (4 * nl * K if stray else 0)
+    F_ne = 4 * nl * (K * K + 3 * K)
+    F_chi = 20 * nl
+    F_solve = 9 * K ** 3 + 4 * K ** 2
+    return dict(F_syn=F_syn, F_rf=F_rf, F_ne=F_ne, F_chi=F_chi, F_solve=F_solve)
+
+
+def flops(fm, pixels, iterations, accepted):
+    fp32 = pixels * (fm["F_syn"] + fm["F_rf"] + fm["F_ne"] + fm["F_chi"]) + iterations * (
+        fm["F_syn"] + fm["F_chi"]) + accepted * (fm["F_rf"] + fm["F_ne"])
+    fp64 = iterations * fm["F_solve"]
+    return fp32, fp64
+
+
+# ---- clocks sampled during the timed region ----
+class ClockSampler:
+    """nvidia-smi sampling every 100 ms while the timed region runs."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.lines = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=10)
+            except Exception:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        rows = [[x.strip() for x in l.split(",")] for l in self.lines]
+        rows = [r for r in rows if len(r) == 7]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [v for v in (num(r[0]) for r in rows) if v is not None]
+        mx = [v for v in (num(r[1]) for r in rows) if v is not None]
+        pw = [v for v in (num(r[2]) for r in rows) if v is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[3 + k] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "power_w_max": max(pw) if pw else None, "reasons": reasons, "samples": len(rows)}
+
+
+# ---- CPU baseline: the reference's own code on every host core ----
+_W = {}
+
+
+def _cpu_worker_init(lib, lam, lambda0, cq, psf, nterms):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+
+    setup = po.LineSetup(lam, lambda0, cq, psf, nterms)
+    _W["ref"] = po.Reference(setup, lib) if lib.startswith("f") and po.reference_available(lib) else po.Restatement(
+        setup, lib.replace("port_", ""))
+
+
+def _cpu_worker_run(args):
+    obs, guess, fix, noise = args
+    t0 = time.perf_counter()
+    _W["ref"].invert(obs, guess, fix=fix, noise=noise, want_spectra=False)
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(w, obs, sample_pixels: int, cores: int):
+    """Time the reference (oracle/_ref float build, -O3) on `cores` processes,
+    contiguous slabs (pmilos.c:1181-1205).  Returns (pixels/s, info)."""
+    import multiprocessing as mp
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+
+    kind = "reference" if po.reference_available("f32_fast") else "port"
+    lib = "f32_fast" if kind == "reference" else "port_f32"
+    n = min(sample_pixels, obs.shape[0])
+    slabs = np.array_split(obs[:n], cores)
+    noise32 = float(np.float32(np.float32(1.0 / 1000) ** 2))
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores, initializer=_cpu_worker_init,
+                  initargs=(lib, w.lam, w.line.lambda0, w.line.cuantic_dat(), w.psf, w.nterms)) as pool:
+        pool.map(_cpu_worker_run, [(s[:2], w.guess, w.fix, noise32) for s in slabs])  # warm-up
+        t0 = time.perf_counter()
+        per = pool.map(_cpu_worker_run, [(s, w.guess, w.fix, noise32) for s in slabs])
+        wall = time.perf_counter() - t0
+    info = {"kind": kind, "cores": cores, "sample": f"{n} pixels of the workload in {cores} contiguous slabs",
+            "wall_s": round(wall, 3), "max_slab_s": round(max(per), 3)}
+    return n / wall, info
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ---- main ----
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", type=int, default=1)
+    ap.add_argument("--npix", type=int, default=None)
+    ap.add_argument("--cpu-sample", type=int, default=None, help="pixels timed on the CPU baseline")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    import torch
+
+    import pmilos_b200 as pm
+    from pmilos_b200 import workloads
+
+    metric = "pixels/s inverted on 1 B200"
+    w = workloads.config(args.config, npix=args.npix)
+    cfg_desc = {"workload": f"ME inversion, benchmark configuration {args.config}: {w.npix} pixels "
+                            f"({int(np.sqrt(w.npix))}^2) x 4 Stokes x {w.nl} wavelengths, Fe I {w.line.lambda0} A, "
+                            f"PSF FWHM 60 mA, {w.nterms} free parameters, <= {w.miter} LM iterations",
+                "pixels_per_step": w.npix, "nlambda": w.nl, "nterms": w.nterms,
+                "parallelism": f"replicas x{args.gpus}", "l2": "flushed between timed steps (256 MiB write)"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        # the reference's CPU path on the host cores; data synthesized by the oracle port
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle as po
+
+        rng = np.random.default_rng(w.seed)
+        truth = workloads.truth_models(w, rng)
+        cores = host_cores()
+        n = args.cpu_sample or min(w.npix, 1500 * cores)
+        ora = po.Restatement(po.LineSetup(w.lam, w.line.lambda0, w.line.cuantic_dat(), w.psf, w.nterms), "f64")
+        obs = np.array([ora.synth(m, None, fix=w.fix, rf=False)[0] for m in truth[:n]], dtype=np.float32)
+        obs += rng.normal(0, 1e-3, obs.shape).astype(np.float32)
+        vals = []
+        for _ in range(args.warmup + args.steps):
+            v, info = cpu_baseline(w, obs, n, cores)
+            vals.append(v)
+        val = float(np.median(vals[args.warmup:]))
+        print(json.dumps({"metric": metric, "value": val, "unit": "pixels/s", "impl": "reference",
+                          "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": 1000.0 * w.npix / val, "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg_desc,
+                          "cpu_baseline": {"value": val, "unit": "pixels/s", "cores": info["cores"],
+                                           "kind": info["kind"], "sample": info["sample"]},
+                          "e2e": {"value": val, "unit": "pixels/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        return
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    inv32 = pm.Inverter(w.line, w.lam, w.psf, noise=w.noise, fix=w.fix, nterms=w.nterms, precision=pm.PREC_FP32)
+    inv64 = pm.Inverter(w.line, w.lam, w.psf, noise=w.noise, fix=w.fix, nterms=w.nterms, precision=pm.PREC_FP64)
+    rng = np.random.default_rng(w.seed + 1000 * rank)
+    obs = workloads.synthesize(w, inv_fp64=inv64, rng=rng)
+    obs_d = torch.as_tensor(obs, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def step_device(inv):
+        flush.fill_(1)  # L2 flush outside the timed kernel
+        r = inv.invert(obs_d, w.guess, want_spectra=False, want_status=False)
+        s = inv.stats()
+        return r, s
+
+    for _ in range(args.warmup):
+        step_device(inv32)
+    barrier()
+    kms, iters, acc, launches = [], 0, 0, 0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            r, s = step_device(inv32)
+            kms.append(s["kernel_ms"])
+            iters += s["iterations"]
+            acc += s["accepted"]
+            launches += 1
+        barrier()
+    ms = float(np.mean(kms))
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * w.npix / (ms / 1000.0)
+
+    # e2e: host buffers (pinned) through the C ABI; copies inside the timed region
+    e2e_v = None
+    if not args.no_e2e:
+        obs_pinned = torch.from_numpy(obs).pin_memory().numpy()
+        for _ in range(max(1, args.warmup)):
+            inv32.invert(obs_pinned, w.guess, want_spectra=False, want_status=False)
+        e2e_ms = []
+        for _ in range(args.steps):
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            inv32.invert(obs_pinned, w.guess, want_spectra=False, want_status=False)
+            e2e_ms.append(inv32.stats()["total_ms"])
+        e2e_v = world * w.npix / (float(np.mean(e2e_ms)) / 1000.0)
+    h2d = obs.nbytes
+    d2h = w.npix * (11 * 8 + 4 + 4)
+
+    # plain FP64 forms on the same cube (fewer steps: slower)
+    plain = {}
+    if not args.no_plain:
+        for name, solver in (("fp64_eigen", pm.SOLVE_EIGEN), ("fp64_cholesky", pm.SOLVE_CHOLESKY)):
+            with pm.Inverter(w.line, w.lam, w.psf, noise=w.noise, fix=w.fix, nterms=w.nterms,
+                             precision=pm.PREC_FP64, solver=solver) as inv:
+                step_device(inv)
+                t = []
+                for _ in range(max(1, min(2, args.steps))):
+                    t.append(step_device(inv)[1]["kernel_ms"])
+                plain[name] = {"value": w.npix / (float(np.mean(t)) / 1000.0), "unit": "pixels/s",
+                               "ms_per_step": float(np.mean(t))}
+
+    fm = flop_model(w.nl, w.nl, w.nterms, w.psf is not None, w.slight is not None)
+    f32, f64 = flops(fm, w.npix * args.steps, iters, acc)
+    kernel_s = sum(kms) / 1000.0
+    clocks = clk.summary()
+    sm_mhz = clocks.get("sm_mhz") or 1965.0
+    peak_fp32 = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12  # TFLOP/s, FP32 vector pipe at the sampled clock
+    achieved = f32 / kernel_s / 1e12
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    hbm_peak = json.load(open(peaks_path))["hbm_gbs"] if os.path.exists(peaks_path) else 6650.0
+    hbm_bytes = w.npix * args.steps * (16 * w.nl + 11 * 8 + 8)
+    roofline = {"bound": "fp32", "achieved": round(achieved, 3), "peak": round(peak_fp32, 2), "unit": "TFLOP/s",
+                "frac": round(achieved / peak_fp32, 4), "traffic": None,
+                "peak_source": f"148 SMs x 128 FP32 lanes x 2 x sampled SM clock {sm_mhz:.0f} MHz (nominal; no "
+                               "measured FP32-pipe peak in MEASURED_PEAKS.json)",
+                "flops_per_pixel_fp32": round(f32 / (w.npix * args.steps)),
+                "flops_per_pixel_fp64": round(f64 / (w.npix * args.steps)),
+                "iterations_per_pixel": iters / (w.npix * args.steps),
+                "accepted_per_pixel": acc / (w.npix * args.steps),
+                "hbm": {"achieved_gbs": round(hbm_bytes / kernel_s / 1e9, 3), "peak_gbs": hbm_peak,
+                        "frac": round(hbm_bytes / kernel_s / 1e9 / hbm_peak, 6)}}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cores = host_cores()
+        n = args.cpu_sample or min(w.npix, 1500 * cores)
+        v, info = cpu_baseline(w, obs, n, cores)
+        cpu = {"value": v, "unit": "pixels/s", "cores": info["cores"], "kind": info["kind"],
+               "sample": info["sample"]}
+
+    if rank == 0:
+        print(json.dumps({
+            "metric": metric, "value": value, "unit": "pixels/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg_desc,
+            "e2e": {"value": e2e_v, "unit": "pixels/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "plain": plain, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
+            "gpu_launches": launches}), flush=True)
+    inv32.close()
+    inv64.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

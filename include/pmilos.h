@@ -1,0 +1,203 @@
+/*
+ * pmilos.h -- C ABI of libpmilos_b200.so, the B200 (sm_100a) implementation of
+ * P-MILOS's per-pixel Milne-Eddington Stokes inversion.
+ *
+ * The reference inverts one pixel per call of
+ *
+ *   int lm_mils(Cuantic *cuantic, PRECISION *wlines, PRECISION *lambda, int nlambda,
+ *               float *spectro, int nspectro, Init_Model *initModel, REAL *spectra,
+ *               float *chisqrf, REAL *slight, PRECISION toplim, int miter, REAL *weight,
+ *               int *fix, REAL *vSigma, REAL sigma, REAL ilambda,
+ *               int *INSTRUMENTAL_CONVOLUTION, int *iter, REAL ah, int logclambda);
+ *
+ * (milosUtils.h:452-455), preceded by estimacionesClasicas (milosUtils.c:287-452) in
+ * every per-pixel loop of the drivers (milos.c:958-1009, pmilos.c:1256-1336,
+ * :1577-1656, :1851-1930, :2260-2330), with process globals for the line data
+ * (create_cuantic), the PSF taps (G) and NTERMS.  This ABI moves those per-run
+ * constants into a context and inverts whole slabs of pixels per call.
+ *
+ * Conventions
+ *  - Return codes: 0 on success, negative errno-style values on failure (PM_E*).
+ *    Nothing in the library calls exit().
+ *  - Buffers are owned by the caller.  Each call says where its buffers live:
+ *    PM_MEM_HOST (the library copies through its own device staging buffers) or
+ *    PM_MEM_DEVICE (pointers into this GPU's memory; nothing is copied).
+ *  - A context may be used by one host thread at a time; separate contexts are
+ *    independent.  All work of a context is ordered on the stream it was created
+ *    with (NULL = the legacy default stream).
+ *  - Arrays follow the reference's layouts: observed and synthetic profiles are
+ *    [pixel][stokes I,Q,U,V][lambda] float32 (utilsFits.c:248, the order lm_mils
+ *    consumes); response functions are [pixel][stokes][parameter][lambda]
+ *    (me_der.c:243-273); models are pm_model, laid out like Init_Model.
+ */
+#ifndef PMILOS_H
+#define PMILOS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PMILOS_ABI_VERSION 1
+
+/* error codes */
+#define PM_OK 0
+#define PM_EINVAL (-22)   /* bad argument */
+#define PM_ENOMEM (-12)   /* host or device allocation failed */
+#define PM_EIO (-5)       /* CUDA runtime error (see pm_last_error) */
+#define PM_ENODEV (-19)   /* no usable sm_100 device */
+#define PM_ERANGE (-34)   /* size beyond a compiled-in maximum */
+#define PM_ENOTSUP (-95)  /* feature outside this implementation's scope */
+
+/* limits */
+#define PM_NL_MAX 128      /* wavelengths per profile */
+#define PM_NTERMS_MAX 11   /* free parameters */
+#define PM_ZEEMAN_MAX 8    /* Zeeman components per group (pi, sigma_b, sigma_r) */
+
+/* buffer residency */
+#define PM_MEM_HOST 0
+#define PM_MEM_DEVICE 1
+
+/* arithmetic of synthesis, response functions, PSF correlation and normal
+ * equations.  The damped solve and the chi^2 acceptance test are FP64 in both. */
+#define PM_PREC_FP64 0     /* plain form: the FP64 correctness twin of make use_double=yes */
+#define PM_PREC_FP32 1     /* batched form */
+
+/* damped normal-equation solve */
+#define PM_SOLVE_DEFAULT 0   /* EIGEN for FP64, CHOLESKY for FP32 */
+#define PM_SOLVE_EIGEN 1     /* symmetric eigen-decomposition + pseudo-inverse with the
+                                |w| <= 1e-12 cut of mil_svd (milosUtils.c:237-271) */
+#define PM_SOLVE_CHOLESKY 2  /* FP64 Cholesky; exactly-zero rows (fixed parameters) give a
+                                zero step like the pseudo-inverse; a non-positive pivot
+                                falls back to EIGEN for that solve */
+
+/* stray-light modes for pm_invert_batch / pm_synth_batch */
+#define PM_SLIGHT_NONE 0     /* no stray light (slight == NULL) */
+#define PM_SLIGHT_SHARED 1   /* one [4][nlambda] profile for every pixel */
+#define PM_SLIGHT_PER_PIXEL 2/* a [npix][4][nlambda] cube */
+
+/* per-pixel status codes (pm_invert_batch status_out) */
+#define PM_PIX_CONVERGED 0   /* relative chi^2 change < toplim or chi^2 < 1e-4 */
+#define PM_PIX_LAMBDA 1      /* stopped because the LM damping left [1e-25, 1e7] */
+#define PM_PIX_MAXITER 2     /* stopped at miter iterations */
+#define PM_PIX_NFREE (-1)    /* no degrees of freedom (lm_mils returns -1) */
+#define PM_PIX_NONFINITE (-2)/* a non-finite chi^2 or model was produced */
+
+/* Atmosphere model; same field order and types as Init_Model (defines.h:86-98). */
+typedef struct pm_model {
+  double eta0;  /* line-to-continuum absorption ratio */
+  double B;     /* field strength [G] */
+  double vlos;  /* line-of-sight velocity [km/s] */
+  double dopp;  /* Doppler width [A] */
+  double aa;    /* damping */
+  double gm;    /* inclination [deg] */
+  double az;    /* azimuth [deg] */
+  double S0;    /* source function constant */
+  double S1;    /* source function gradient */
+  double mac;   /* macroturbulence [km/s] (must be 0 here) */
+  double alfa;  /* filling factor */
+} pm_model;
+
+/* Spectral line: what create_cuantic (create_cuantic.c:24-294) and wlines[1]
+ * provide to the reference.  Strengths and splittings are per Zeeman group. */
+typedef struct pm_line {
+  double lambda0;   /* line centre [A] (wlines[1]) */
+  int n_pi;         /* components in the pi group (N_PI) */
+  int n_sig;        /* components in each sigma group (N_SIG) */
+  double nup[PM_ZEEMAN_MAX], nub[PM_ZEEMAN_MAX], nur[PM_ZEEMAN_MAX]; /* splittings (Lande units) */
+  double wep[PM_ZEEMAN_MAX], web[PM_ZEEMAN_MAX], wer[PM_ZEEMAN_MAX]; /* strengths */
+  double gl, gu, geff; /* Lande factors */
+  double fo;        /* relative line strength */
+} pm_line;
+
+/* Per-run inversion settings: the control-file fields lm_mils reads
+ * (readConfig.c:420-1023) plus this implementation's precision/solver choice. */
+typedef struct pm_config {
+  int nlambda;            /* 2 .. PM_NL_MAX */
+  const double *lambda;   /* [nlambda] absolute wavelengths [A] (vLambda) */
+  const double *psf;      /* [nlambda] PSF taps centred at nlambda/2 (G), or NULL */
+  double weight[4];       /* Stokes weights (WeightForStokes) */
+  double noise;           /* per-point variance (noise = 1/SN^2; lm_mils' sigma) */
+  double ilambda;         /* initial LM damping (InitialDiagonalElement) */
+  double toplim;          /* relative chi^2 stop (1e-12 in the reference) */
+  int miter;              /* max LM iterations (NumberOfCycles > 0) */
+  int fix[11];            /* 1 = parameter is inverted, reference order (defines.h:245) */
+  int nterms;             /* NTERMS: 9, 10 or 11 */
+  int logclambda;         /* "Diagonal element acceleration" */
+  double mu;              /* heliocentric angle cosine (ah) */
+  int classical_estimates;/* run estimacionesClasicas + NaN fixes before LM */
+  int precision;          /* PM_PREC_FP64 | PM_PREC_FP32 */
+  int solver;             /* PM_SOLVE_* */
+} pm_config;
+
+/* Run statistics of the last pm_invert_batch on a context. */
+typedef struct pm_stats {
+  int64_t pixels;
+  int64_t iterations;     /* summed over pixels */
+  int64_t accepted;       /* LM steps that lowered chi^2 (each re-ran the RFs) */
+  int64_t eigen_fallbacks;/* CHOLESKY solves that fell back to EIGEN */
+  double kernel_ms;       /* device time of the inversion kernel (CUDA events) */
+  double total_ms;        /* device time of the whole call incl. copies */
+} pm_stats;
+
+typedef struct pm_ctx pm_ctx;
+
+/* ---- host-side precompute (no GPU needed) ---- */
+
+/* Zeeman pattern of one line from its quantum numbers, create_cuantic/Cuanten
+ * (create_cuantic.c:60-294); sl, ll, jl / su, lu, ju as readFileCuanticLines
+ * (readConfig.c:24-129) decodes them from a LINES entry. */
+int pm_line_from_quantum(double lambda0, double sl, double ll, double jl, double su, double lu, double ju,
+                         pm_line *out);
+
+/* Gaussian PSF of FWHM [mA] sampled on the grid, fgauss_WL (fgauss.c:79-154). */
+int pm_psf_gaussian(double fwhm_ma, int nlambda, const double *lambda, double *taps_out);
+
+/* PSF read from a tabulated profile (offsets [mA], values), linearly
+ * interpolated on the grid offsets [mA] and normalised, including the
+ * re-centring of milos.c:302-344 / pmilos.c:405-500 and interpolationLinearPSF
+ * (milosUtils.c:684-738). */
+int pm_psf_interpolate(int nsamples, const double *psf_offsets_ma, const double *psf_values, int nlambda,
+                       const double *grid_offsets_ma, double *taps_out);
+
+/* ---- context ---- */
+
+/* Validates cfg, uploads line data, grid and PSF, selects the kernel variant.
+ * stream: a cudaStream_t or NULL. */
+int pm_ctx_create(const pm_line *line, const pm_config *cfg, void *stream, pm_ctx **out);
+int pm_ctx_destroy(pm_ctx *ctx);
+
+/* Invert npix pixels.  Replaces the per-pixel loop of the drivers: for each pixel,
+ * start from *guess, apply the classical estimates if cfg->classical_estimates,
+ * run the LM loop, and store the model, chi^2 and iteration count like
+ * milos.c:998-1006.  best_fit (nullable) receives the profiles of the last
+ * synthesis, as lm_mils leaves them in `spectra`.  status (nullable) receives a
+ * PM_PIX_* code per pixel.  slight follows slight_mode (PM_SLIGHT_*). */
+int pm_invert_batch(pm_ctx *ctx, int64_t npix, const float *spectro, const float *slight, int slight_mode,
+                    const pm_model *guess, pm_model *models_out, float *chisq_out, int *iters_out,
+                    float *best_fit_out, int *status_out, int mem);
+
+/* Forward synthesis (mil_sinrf) and optionally the response functions (me_der)
+ * of npix models, as the reference's synthesis mode (milos.c:601-602) computes
+ * them.  rf_out (nullable) is [npix][4][nterms][nlambda]. */
+int pm_synth_batch(pm_ctx *ctx, int64_t npix, const pm_model *models, const float *slight, int slight_mode,
+                   float *spectra_out, float *rf_out, int mem);
+
+/* Batch-of-one form of lm_mils for hosts that keep their per-pixel loop: inverts
+ * spectro ([4][nlambda], host memory) starting from *init_model (updated in
+ * place); spectra (nullable) gets the last synthesis, *chisqrf and *iter the
+ * results.  Classical estimates follow cfg->classical_estimates.
+ * Returns 1 like lm_mils, -1 when nfree == 0, or a negative PM_E* code. */
+int pm_lm_mils(pm_ctx *ctx, const float *spectro, pm_model *init_model, float *spectra, float *chisqrf,
+               const float *slight, int *iter);
+
+int pm_get_stats(const pm_ctx *ctx, pm_stats *out);
+const char *pm_last_error(void);
+int pm_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,539 @@
+// pm_host.cpp -- host side of libpmilos_b200.so: the C ABI of include/pmilos.h.
+//
+// Responsibilities: per-run precompute that the reference does on the host
+// (Zeeman pattern, PSF taps), validation of the control settings, the context
+// (parameter block, device staging buffers, counters), and the batched entry
+// points that replace the reference's per-pixel loops.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "pm_params.h"
+
+namespace {
+
+thread_local char g_last_error[512] = "";
+
+int fail(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_last_error, sizeof g_last_error, fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  return fail(PM_EIO, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define PM_CUDA(call, what)                       \
+  do {                                            \
+    cudaError_t e_ = (call);                      \
+    if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+  } while (0)
+
+// Device buffer that grows on demand.
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  int ensure(size_t bytes) {
+    if (bytes <= cap) return PM_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) return fail(PM_ENOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+    cap = bytes;
+    return PM_OK;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+}  // namespace
+
+struct pm_ctx {
+  PmParams P;
+  int precision = PM_PREC_FP32;
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  int64_t chunk = 1 << 20;  // pixels per staging chunk in host mode
+  DevBuf spectro, slight, models, chisq, iters, spectra, status, rf, ctr;
+  pm_stats stats{};
+};
+
+// ---------------------------------------------------------------------------
+// Host precompute
+// ---------------------------------------------------------------------------
+
+// Zeeman pattern of an LS-coupled transition (Cuanten, create_cuantic.c:60-294):
+// Lande factors of both levels, then for every pair of magnetic sublevels the
+// component strength (by Delta J and Delta M) and splitting g1 M1 - g2 M2;
+// strengths normalised per group.
+extern "C" int pm_line_from_quantum(double lambda0, double sl, double ll, double jl, double su, double lu,
+                                    double ju, pm_line* out) {
+  if (!out) return fail(PM_EINVAL, "pm_line_from_quantum: out is NULL");
+  if (!(lambda0 > 0) || jl < 0 || ju < 0 || std::fabs(ju - jl) > 1)
+    return fail(PM_EINVAL, "pm_line_from_quantum: invalid line (lambda0=%g, jl=%g, ju=%g)", lambda0, jl, ju);
+  std::memset(out, 0, sizeof *out);
+  const double g1 = (jl != 0) ? (3.0 * jl * (jl + 1) + sl * (sl + 1) - ll * (ll + 1)) / (2 * jl * (jl + 1)) : 0;
+  const double g2 =
+      (ju != 0) ? (3.0 * ju * (ju + 1.0) + su * (su + 1.0) - lu * (lu + 1.0)) / (2.0 * ju * (ju + 1.0)) : 0;
+  const double geff = (g1 + g2) / 2 + (g1 - g2) * (jl * (jl + 1.) - ju * (ju + 1.)) / 4;
+  const int nlo = int(2 * jl + 1), nup = int(2 * ju + 1);
+  const int jj = int(ju - jl);
+  const int n_pi = int(2 * std::min(jl, ju) + 1), n_sig = int(jl + ju);
+  if (n_pi > PM_ZEEMAN_MAX || n_sig > PM_ZEEMAN_MAX || n_sig < 1)
+    return fail(PM_ERANGE, "pm_line_from_quantum: %d pi / %d sigma components exceed %d", n_pi, n_sig,
+                PM_ZEEMAN_MAX);
+  int ip = 0, ib = 0, ir = 0;
+  for (int a = 0; a < nlo; ++a) {
+    const int m1 = a - int(jl);
+    for (int b = 0; b < nup; ++b) {
+      const int m2 = b - int(ju);
+      const int dm = m2 - m1;
+      const double split = g1 * m1 - g2 * m2;
+      if (dm == 0) {
+        out->wep[ip] = (jj == -1) ? jl * jl - m1 * m1 : (jj == 0) ? double(m1 * m1) : (jl + 1) * (jl + 1) - m1 * m1;
+        out->nup[ip++] = split;
+      } else if (dm == 1) {
+        out->web[ib] = (jj == -1)  ? (jl - m1) * (jl - m1 - 1) / 4
+                       : (jj == 0) ? (jl - m1) * (jl + m1 + 1) / 4
+                                   : (jl + m1 + 1) * (jl + m1 + 2) / 4;
+        out->nub[ib++] = split;
+      } else if (dm == -1) {
+        out->wer[ir] = (jj == -1)  ? (jl + m1) * (jl + m1 - 1) / 4
+                       : (jj == 0) ? (jl + m1) * (jl - m1 + 1) / 4
+                                   : (jl - m1 + 1) * (jl - m1 + 2) / 4;
+        out->nur[ir++] = split;
+      }
+    }
+  }
+  if (ip != n_pi || ib != n_sig || ir != n_sig) return fail(PM_EINVAL, "pm_line_from_quantum: inconsistent pattern");
+  double s;
+  s = 0; for (int k = 0; k < n_pi; ++k) s += out->wep[k];
+  for (int k = 0; k < n_pi; ++k) out->wep[k] /= s;
+  s = 0; for (int k = 0; k < n_sig; ++k) s += out->web[k];
+  for (int k = 0; k < n_sig; ++k) out->web[k] /= s;
+  s = 0; for (int k = 0; k < n_sig; ++k) s += out->wer[k];
+  for (int k = 0; k < n_sig; ++k) out->wer[k] /= s;
+  out->lambda0 = lambda0;
+  out->n_pi = n_pi;
+  out->n_sig = n_sig;
+  out->gl = g1;
+  out->gu = g2;
+  out->geff = geff;
+  out->fo = 1.0;
+  return PM_OK;
+}
+
+// fgauss_WL (fgauss.c:79-154): sigma = FWHM * 0.42466090 / 1000 [A], centred on
+// the grid's middle sample lambda[nl/2], sampled at lambda[0] + i * step with
+// step = lambda[1] - lambda[0], normalised to unit sum.
+extern "C" int pm_psf_gaussian(double fwhm_ma, int nlambda, const double* lambda, double* taps_out) {
+  if (nlambda < 2 || !lambda || !taps_out || !(fwhm_ma > 0))
+    return fail(PM_EINVAL, "pm_psf_gaussian: bad arguments");
+  const double sigma = fwhm_ma * 0.42466090 / 1000.0;
+  const double step = lambda[1] - lambda[0], first = lambda[0], central = lambda[nlambda / 2];
+  double cte = 0;
+  for (int i = 0; i < nlambda; ++i) {
+    const double x = first + i * step;
+    const double aux = (x - central) / sigma;
+    const double term = (aux * aux) / 2;
+    taps_out[i] = term < 1e30 ? std::exp(-term) : 0.0;
+    cte += taps_out[i];
+  }
+  for (int i = 0; i < nlambda; ++i) taps_out[i] /= cte;
+  return PM_OK;
+}
+
+// PSF from a tabulated file (readPSFFile + milos.c:302-344 + interpolationLinearPSF
+// milosUtils.c:684-738).  The grid must lie inside the table (integer-truncated
+// comparison); if the grid's zero offset is not its middle sample the table is
+// shifted so that it is (quirk kept: the zero search stops at the first
+// non-leading match); samples are linearly interpolated and normalised.
+extern "C" int pm_psf_interpolate(int nsamples, const double* dl, const double* psf, int nlambda,
+                                  const double* offs, double* taps_out) {
+  if (nsamples < 2 || nlambda < 2 || !dl || !psf || !offs || !taps_out)
+    return fail(PM_EINVAL, "pm_psf_interpolate: bad arguments");
+  if (std::trunc(offs[0]) < std::trunc(dl[0]) || std::trunc(offs[nlambda - 1]) > std::trunc(dl[nsamples - 1]))
+    return fail(PM_EINVAL, "pm_psf_interpolate: PSF table [%g,%g] mA does not cover the grid [%g,%g] mA", dl[0],
+                dl[nsamples - 1], offs[0], offs[nlambda - 1]);
+  int posWL = 0;
+  for (int i = 0; i < nlambda && !posWL; ++i)
+    if (std::fabs(std::trunc(offs[i])) == 0) posWL = i;
+  double offset = 0;
+  const double step = (offs[1] - offs[0]) / 1000.0;
+  if (posWL != nlambda / 2) offset = ((nlambda / 2 - posWL) * step) * 1000;
+  auto interp = [&](double x, double* y) -> bool {
+    if (!(x >= dl[0] && x <= dl[nsamples - 1])) return false;
+    int lo = 0, hi = nsamples - 1;
+    while (hi > lo + 1) {
+      const int mid = (lo + hi) / 2;
+      if (dl[mid] > x) hi = mid; else lo = mid;
+    }
+    const double dx = dl[lo + 1] - dl[lo];
+    *y = dx > 0 ? psf[lo] + (x - dl[lo]) / dx * (psf[lo + 1] - psf[lo]) : 0.0;
+    return true;
+  };
+  for (int i = 0; i < nlambda; ++i) {
+    taps_out[i] = 0.0;
+    const double x = offs[i] - offset;
+    const double lower = (offset >= 0) ? dl[0] : dl[std::min(nlambda, nsamples) - 1];
+    double y;
+    if (x >= lower && interp(x, &y)) taps_out[i] = y;
+  }
+  double cte = 0;
+  for (int i = 0; i < nlambda; ++i) cte += taps_out[i];
+  for (int i = 0; i < nlambda; ++i) taps_out[i] /= cte;
+  return PM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Context
+// ---------------------------------------------------------------------------
+namespace {
+
+int fill_params(const pm_line* L, const pm_config* c, PmParams& P) {
+  std::memset(&P, 0, sizeof P);
+  if (c->nlambda < 2 || c->nlambda > PMK_NL)
+    return fail(PM_ERANGE, "nlambda=%d: this build handles 2..%d wavelengths", c->nlambda, PMK_NL);
+  if (!c->lambda) return fail(PM_EINVAL, "lambda grid is NULL");
+  if (c->nterms != 9 && c->nterms != 10)
+    return fail(PM_ENOTSUP, "nterms=%d: supported are 9 and 10 (10 = filling factor inverted)", c->nterms);
+  if (c->fix[9]) return fail(PM_ENOTSUP, "macroturbulence inversion (fix[9]) is outside this implementation");
+  {
+    // NTERMS = 11 - !fix[10] - (mac == 0 && !fix[9]) (milos.c:152-157)
+    const int expect = 11 - (c->fix[10] ? 0 : 1) - 1;
+    if (expect != c->nterms)
+      return fail(PM_EINVAL, "nterms=%d inconsistent with fix[10]=%d (expected %d)", c->nterms, c->fix[10], expect);
+  }
+  if (c->miter < 0) return fail(PM_EINVAL, "miter=%d", c->miter);
+  if (!(c->noise > 0)) return fail(PM_EINVAL, "noise must be > 0");
+  if (c->precision != PM_PREC_FP32 && c->precision != PM_PREC_FP64) return fail(PM_EINVAL, "precision");
+  if (L->n_pi != 1 || L->n_sig != 1)
+    return fail(PM_ENOTSUP, "only normal Zeeman triplets (N_PI = N_SIG = 1) are compiled in; got %d/%d", L->n_pi,
+                L->n_sig);
+  P.nl = c->nlambda;
+  P.half = c->nlambda / 2;
+  P.K = c->nterms;
+  P.miter = c->miter;
+  P.nfree_base = 4 * c->nlambda - c->nterms;
+  P.logclambda = c->logclambda;
+  P.classical = c->classical_estimates;
+  P.has_psf = c->psf != nullptr;
+  int solver = c->solver;
+  if (solver == PM_SOLVE_DEFAULT) solver = (c->precision == PM_PREC_FP64) ? PM_SOLVE_EIGEN : PM_SOLVE_CHOLESKY;
+  if (solver != PM_SOLVE_EIGEN && solver != PM_SOLVE_CHOLESKY) return fail(PM_EINVAL, "solver=%d", c->solver);
+  P.solver = solver;
+  P.n_pi = L->n_pi;
+  P.n_sig = L->n_sig;
+  for (int i = 0; i < 11; ++i) P.fix[i] = c->fix[i] ? 1 : 0;
+  // FijaACeroDerivadasNoNecesarias (milosUtils.c:199-227)
+  for (int k = 0; k < P.K; ++k) {
+    if (P.K == 10 && k == 9) P.zero_row[k] = (P.fix[9] == 0 && P.fix[10] == 0);
+    else P.zero_row[k] = (P.fix[k] == 0);
+  }
+  P.ff_row = (P.K == 10) ? 9 : -1;
+  P.lambda0 = L->lambda0;
+  for (int i = 0; i < P.nl; ++i) P.dl[i] = c->lambda[i] - L->lambda0;
+  for (int k = 0; k < L->n_pi; ++k) { P.nu[0][k] = L->nup[k]; P.we[0][k] = L->wep[k]; }
+  for (int k = 0; k < L->n_sig; ++k) {
+    P.nu[1][k] = L->nub[k];
+    P.we[1][k] = L->web[k];
+    P.nu[2][k] = -L->nub[L->n_sig - 1 - k];  // mil_sinrf.c:164-166 mirrors the blue splitting
+    P.we[2][k] = L->wer[k];
+  }
+  P.geff = L->geff;
+  P.fo = L->fo;
+  for (int s = 0; s < 4; ++s) P.w[s] = c->weight[s];
+  P.noise = c->noise;
+  P.ilambda = c->ilambda;
+  P.toplim = c->toplim;
+  P.mu = c->mu;
+  if (c->psf) {
+    for (int j = 0; j < P.nl; ++j) {
+      P.taps_d[j] = c->psf[j];
+      P.taps_f[j] = float(c->psf[j]);
+    }
+    for (int t = 0; t < PMK_GC; ++t) {
+      const int j = t - (PMK_NL - 1) + P.half;
+      const double g = (j >= 0 && j < P.nl) ? c->psf[j] : 0.0;
+      P.gc_d[t] = g;
+      P.gc_f[t] = float(g);
+    }
+  }
+  return PM_OK;
+}
+
+void set_guess(PmParams& P, const pm_model* g) {
+  const double* v = reinterpret_cast<const double*>(g);
+  for (int i = 0; i < 11; ++i) P.guess[i] = v[i];
+}
+
+int set_slight(PmParams& P, const float* slight, int mode, int mem) {
+  P.slight_mode = mode;
+  if (mode == PM_SLIGHT_NONE) return PM_OK;
+  if (!slight) return fail(PM_EINVAL, "slight_mode=%d but slight is NULL", mode);
+  if (P.K != 10) return fail(PM_EINVAL, "stray light requires nterms == 10 (filling factor inverted)");
+  if (mode == PM_SLIGHT_SHARED) {
+    std::vector<float> h(4 * P.nl);
+    if (mem == PM_MEM_DEVICE) {
+      cudaError_t e = cudaMemcpy(h.data(), slight, sizeof(float) * 4 * P.nl, cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) return cuda_fail(e, "slight D2H");
+    } else {
+      std::memcpy(h.data(), slight, sizeof(float) * 4 * P.nl);
+    }
+    for (int i = 0; i < 4 * P.nl; ++i) {
+      P.sl_d[i] = h[i];
+      P.sl_f[i] = h[i];
+    }
+    return PM_OK;
+  }
+  if (mode == PM_SLIGHT_PER_PIXEL) return PM_OK;
+  return fail(PM_EINVAL, "slight_mode=%d", mode);
+}
+
+}  // namespace
+
+extern "C" int pm_ctx_create(const pm_line* line, const pm_config* cfg, void* stream, pm_ctx** out) {
+  if (!line || !cfg || !out) return fail(PM_EINVAL, "pm_ctx_create: NULL argument");
+  *out = nullptr;
+  pm_ctx* c = new (std::nothrow) pm_ctx();
+  if (!c) return fail(PM_ENOMEM, "pm_ctx_create: out of host memory");
+  int rc = fill_params(line, cfg, c->P);
+  if (rc != PM_OK) {
+    delete c;
+    return rc;
+  }
+  c->precision = cfg->precision;
+  c->stream = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaGetDevice(&c->device);
+  cudaDeviceProp prop;
+  if (e == cudaSuccess) e = cudaGetDeviceProperties(&prop, c->device);
+  if (e != cudaSuccess) {
+    delete c;
+    return fail(PM_ENODEV, "no CUDA device: %s", cudaGetErrorString(e));
+  }
+  if (prop.major != 10) {
+    delete c;
+    return fail(PM_ENODEV, "device %d is sm_%d%d; this library is built for sm_100a", c->device, prop.major,
+                prop.minor);
+  }
+  c->num_sms = prop.multiProcessorCount;
+  rc = c->ctr.ensure(sizeof(unsigned long long) * PMC_COUNT);
+  if (rc != PM_OK) {
+    delete c;
+    return rc;
+  }
+  *out = c;
+  return PM_OK;
+}
+
+extern "C" int pm_ctx_destroy(pm_ctx* c) {
+  if (!c) return PM_OK;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  else cudaDeviceSynchronize();
+  for (DevBuf* b : {&c->spectro, &c->slight, &c->models, &c->chisq, &c->iters, &c->spectra, &c->status, &c->rf,
+                    &c->ctr})
+    b->release();
+  delete c;
+  return PM_OK;
+}
+
+namespace {
+
+// One launch over n pixels whose buffers are all device pointers.
+int run_invert(pm_ctx* c, PmIO io, float* kernel_ms) {
+  PM_CUDA(cudaMemsetAsync(io.ctr, 0, sizeof(unsigned long long) * PMC_COUNT, c->stream), "counter reset");
+  int rc = pmk_invert(c->P, io, c->precision, c->stream, c->num_sms, kernel_ms);
+  if (rc != PM_OK) return fail(rc, "%s", pmk_last_cuda_error());
+  unsigned long long h[PMC_COUNT];
+  PM_CUDA(cudaMemcpyAsync(h, io.ctr, sizeof h, cudaMemcpyDeviceToHost, c->stream), "counter D2H");
+  PM_CUDA(cudaStreamSynchronize(c->stream), "invert kernel");
+  c->stats.pixels += io.npix;
+  c->stats.iterations += int64_t(h[PMC_ITERS]);
+  c->stats.accepted += int64_t(h[PMC_ACCEPTED]);
+  c->stats.eigen_fallbacks += int64_t(h[PMC_FALLBACK]);
+  return PM_OK;
+}
+
+}  // namespace
+
+extern "C" int pm_invert_batch(pm_ctx* c, int64_t npix, const float* spectro, const float* slight, int slight_mode,
+                               const pm_model* guess, pm_model* models_out, float* chisq_out, int* iters_out,
+                               float* best_fit_out, int* status_out, int mem) {
+  if (!c || !spectro || !guess || !models_out || !chisq_out || !iters_out)
+    return fail(PM_EINVAL, "pm_invert_batch: NULL argument");
+  if (npix < 0) return fail(PM_EINVAL, "pm_invert_batch: npix < 0");
+  if (mem != PM_MEM_HOST && mem != PM_MEM_DEVICE) return fail(PM_EINVAL, "pm_invert_batch: mem=%d", mem);
+  if (guess->mac != 0.0) return fail(PM_ENOTSUP, "macroturbulence (guess.mac > 0) is outside this implementation");
+  c->stats = pm_stats{};
+  if (npix == 0) return PM_OK;
+  set_guess(c->P, guess);
+  int rc = set_slight(c->P, slight, slight_mode, mem);
+  if (rc != PM_OK) return rc;
+  const int nl = c->P.nl;
+  const size_t prof = sizeof(float) * 4 * nl;
+  cudaEvent_t t0, t1;
+  cudaEventCreate(&t0);
+  cudaEventCreate(&t1);
+  cudaEventRecord(t0, c->stream);
+  float kms_total = 0;
+  if (mem == PM_MEM_DEVICE) {
+    PmIO io{};
+    io.npix = npix;
+    io.spectro = spectro;
+    io.slight = slight_mode == PM_SLIGHT_PER_PIXEL ? slight : nullptr;
+    io.models_out = reinterpret_cast<double*>(models_out);
+    io.chisq_out = chisq_out;
+    io.iters_out = iters_out;
+    io.spectra_out = best_fit_out;
+    io.status_out = status_out;
+    io.ctr = static_cast<unsigned long long*>(c->ctr.p);
+    rc = run_invert(c, io, &kms_total);
+  } else {
+    const int64_t chunk = std::min<int64_t>(npix, c->chunk);
+    if ((rc = c->spectro.ensure(prof * chunk)) != PM_OK) return rc;
+    if (slight_mode == PM_SLIGHT_PER_PIXEL && (rc = c->slight.ensure(prof * chunk)) != PM_OK) return rc;
+    if ((rc = c->models.ensure(sizeof(pm_model) * chunk)) != PM_OK) return rc;
+    if ((rc = c->chisq.ensure(sizeof(float) * chunk)) != PM_OK) return rc;
+    if ((rc = c->iters.ensure(sizeof(int) * chunk)) != PM_OK) return rc;
+    if (best_fit_out && (rc = c->spectra.ensure(prof * chunk)) != PM_OK) return rc;
+    if (status_out && (rc = c->status.ensure(sizeof(int) * chunk)) != PM_OK) return rc;
+    pm_stats acc{};
+    for (int64_t p0 = 0; p0 < npix && rc == PM_OK; p0 += chunk) {
+      const int64_t n = std::min(chunk, npix - p0);
+      PM_CUDA(cudaMemcpyAsync(c->spectro.p, spectro + p0 * 4 * nl, prof * n, cudaMemcpyHostToDevice, c->stream),
+              "spectro H2D");
+      if (slight_mode == PM_SLIGHT_PER_PIXEL)
+        PM_CUDA(cudaMemcpyAsync(c->slight.p, slight + p0 * 4 * nl, prof * n, cudaMemcpyHostToDevice, c->stream),
+                "slight H2D");
+      PmIO io{};
+      io.npix = n;
+      io.spectro = static_cast<const float*>(c->spectro.p);
+      io.slight = slight_mode == PM_SLIGHT_PER_PIXEL ? static_cast<const float*>(c->slight.p) : nullptr;
+      io.models_out = static_cast<double*>(c->models.p);
+      io.chisq_out = static_cast<float*>(c->chisq.p);
+      io.iters_out = static_cast<int*>(c->iters.p);
+      io.spectra_out = best_fit_out ? static_cast<float*>(c->spectra.p) : nullptr;
+      io.status_out = status_out ? static_cast<int*>(c->status.p) : nullptr;
+      io.ctr = static_cast<unsigned long long*>(c->ctr.p);
+      float kms = 0;
+      rc = run_invert(c, io, &kms);
+      if (rc != PM_OK) break;
+      kms_total += kms;
+      acc.pixels += c->stats.pixels;
+      acc.iterations += c->stats.iterations;
+      acc.accepted += c->stats.accepted;
+      acc.eigen_fallbacks += c->stats.eigen_fallbacks;
+      c->stats = pm_stats{};
+      PM_CUDA(cudaMemcpyAsync(models_out + p0, c->models.p, sizeof(pm_model) * n, cudaMemcpyDeviceToHost, c->stream),
+              "models D2H");
+      PM_CUDA(cudaMemcpyAsync(chisq_out + p0, c->chisq.p, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream),
+              "chisq D2H");
+      PM_CUDA(cudaMemcpyAsync(iters_out + p0, c->iters.p, sizeof(int) * n, cudaMemcpyDeviceToHost, c->stream),
+              "iters D2H");
+      if (best_fit_out)
+        PM_CUDA(cudaMemcpyAsync(best_fit_out + p0 * 4 * nl, c->spectra.p, prof * n, cudaMemcpyDeviceToHost,
+                                c->stream),
+                "best fit D2H");
+      if (status_out)
+        PM_CUDA(cudaMemcpyAsync(status_out + p0, c->status.p, sizeof(int) * n, cudaMemcpyDeviceToHost, c->stream),
+                "status D2H");
+    }
+    c->stats = acc;
+  }
+  cudaEventRecord(t1, c->stream);
+  cudaEventSynchronize(t1);
+  float tot = 0;
+  cudaEventElapsedTime(&tot, t0, t1);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  c->stats.kernel_ms = kms_total;
+  c->stats.total_ms = tot;
+  if (rc == PM_OK) {
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pm_invert_batch");
+  }
+  return rc;
+}
+
+extern "C" int pm_synth_batch(pm_ctx* c, int64_t npix, const pm_model* models, const float* slight,
+                              int slight_mode, float* spectra_out, float* rf_out, int mem) {
+  if (!c || !models || !spectra_out) return fail(PM_EINVAL, "pm_synth_batch: NULL argument");
+  if (npix < 0) return fail(PM_EINVAL, "pm_synth_batch: npix < 0");
+  if (mem != PM_MEM_HOST && mem != PM_MEM_DEVICE) return fail(PM_EINVAL, "pm_synth_batch: mem=%d", mem);
+  if (npix == 0) return PM_OK;
+  int rc = set_slight(c->P, slight, slight_mode, mem);
+  if (rc != PM_OK) return rc;
+  const int nl = c->P.nl, K = c->P.K;
+  const size_t prof = sizeof(float) * 4 * nl;
+  PmIO io{};
+  io.npix = npix;
+  if (mem == PM_MEM_DEVICE) {
+    io.models_in = reinterpret_cast<const double*>(models);
+    io.slight = slight_mode == PM_SLIGHT_PER_PIXEL ? slight : nullptr;
+    io.spectra_out = spectra_out;
+    io.rf_out = rf_out;
+    rc = pmk_synth(c->P, io, c->precision, c->stream);
+    if (rc != PM_OK) return fail(rc, "%s", pmk_last_cuda_error());
+    PM_CUDA(cudaStreamSynchronize(c->stream), "synth kernel");
+    return PM_OK;
+  }
+  if ((rc = c->models.ensure(sizeof(pm_model) * npix)) != PM_OK) return rc;
+  if ((rc = c->spectra.ensure(prof * npix)) != PM_OK) return rc;
+  if (rf_out && (rc = c->rf.ensure(prof * K * npix)) != PM_OK) return rc;
+  if (slight_mode == PM_SLIGHT_PER_PIXEL && (rc = c->slight.ensure(prof * npix)) != PM_OK) return rc;
+  PM_CUDA(cudaMemcpyAsync(c->models.p, models, sizeof(pm_model) * npix, cudaMemcpyHostToDevice, c->stream),
+          "models H2D");
+  if (slight_mode == PM_SLIGHT_PER_PIXEL)
+    PM_CUDA(cudaMemcpyAsync(c->slight.p, slight, prof * npix, cudaMemcpyHostToDevice, c->stream), "slight H2D");
+  io.models_in = static_cast<const double*>(c->models.p);
+  io.slight = slight_mode == PM_SLIGHT_PER_PIXEL ? static_cast<const float*>(c->slight.p) : nullptr;
+  io.spectra_out = static_cast<float*>(c->spectra.p);
+  io.rf_out = rf_out ? static_cast<float*>(c->rf.p) : nullptr;
+  rc = pmk_synth(c->P, io, c->precision, c->stream);
+  if (rc != PM_OK) return fail(rc, "%s", pmk_last_cuda_error());
+  PM_CUDA(cudaMemcpyAsync(spectra_out, c->spectra.p, prof * npix, cudaMemcpyDeviceToHost, c->stream), "spectra D2H");
+  if (rf_out)
+    PM_CUDA(cudaMemcpyAsync(rf_out, c->rf.p, prof * K * npix, cudaMemcpyDeviceToHost, c->stream), "rf D2H");
+  PM_CUDA(cudaStreamSynchronize(c->stream), "synth kernel");
+  return PM_OK;
+}
+
+extern "C" int pm_lm_mils(pm_ctx* c, const float* spectro, pm_model* init_model, float* spectra, float* chisqrf,
+                          const float* slight, int* iter) {
+  if (!c || !spectro || !init_model || !chisqrf || !iter) return fail(PM_EINVAL, "pm_lm_mils: NULL argument");
+  pm_model out;
+  int it = 0, status = 0;
+  float chi = 0;
+  const int rc = pm_invert_batch(c, 1, spectro, slight, slight ? PM_SLIGHT_SHARED : PM_SLIGHT_NONE, init_model, &out,
+                                 &chi, &it, spectra, &status, PM_MEM_HOST);
+  if (rc != PM_OK) return rc;
+  *init_model = out;
+  *chisqrf = chi;
+  *iter = it;
+  return status == PM_PIX_NFREE ? -1 : 1;
+}
+
+extern "C" int pm_get_stats(const pm_ctx* c, pm_stats* out) {
+  if (!c || !out) return fail(PM_EINVAL, "pm_get_stats: NULL argument");
+  *out = c->stats;
+  return PM_OK;
+}
+
+extern "C" const char* pm_last_error(void) { return g_last_error; }
+extern "C" int pm_abi_version(void) { return PMILOS_ABI_VERSION; }

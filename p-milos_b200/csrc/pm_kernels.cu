@@ -1,0 +1,1078 @@
+// pm_kernels.cu -- sm_100a kernels of the Milne-Eddington inversion.
+//
+// Mapping.  One warp inverts one pixel; lane l owns wavelength l (nl <= 32), so
+// everything the reference does per wavelength in mil_sinrf / me_der runs once
+// per lane with no loop.  A persistent grid pulls pixels from an atomic work
+// counter, so pixels that need 3 or 50 LM iterations retire and refill
+// independently.  Per-warp shared memory holds a transpose buffer for the
+// response functions (lane = wavelength while they are computed, lane = profile
+// while they are correlated with the PSF), the padded synthesis rows for the PSF
+// correlation of the four Stokes profiles, and alpha/beta of the normal
+// equations in FP64.
+//
+// Precision.  R = double is the plain form (every step FP64, the correctness twin
+// of the reference's use_double build); R = float runs synthesis, response
+// functions, PSF correlation and the normal equations in FP32.  The damped solve
+// and the chi^2 acceptance test are FP64 in both.
+//
+// Reference map (file:line of the reference each device function restates):
+//   voigt            fvoigt.c:15-80
+//   synth_lane       mil_sinrf.c:46-285, funcionComponentFor_sinrf :418-449
+//   psf_rows         direct_convolution(_ic) convolution.c:54-121, mil_sinrf.c:387-402
+//   rf_lane          me_der.c:48-312, funcionComponentFor :536-609
+//   rf_correlate     me_der.c:471-496
+//   normal_eq        covarm2 lib.c:71-116, totalParcialf/Matrixf :237-268
+//   chisq            fchisqr lib.c:126-152
+//   solve_*          mil_svd milosUtils.c:237-271
+//   apply_delta      AplicaDelta milosUtils.c:47-115
+//   check_model      check milosUtils.c:118-196
+//   classical        estimacionesClasicas milosUtils.c:287-452 (+ milos.c:976-983)
+//   invert_kernel    lm_mils milosUtils.c:466-635 over the pixel loop of milos.c:958-1009
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+
+#include "pm_params.h"
+
+namespace {
+
+constexpr int NL = PMK_NL;
+constexpr int TRS = NL + 1;  // transpose row stride (odd: conflict-free column reads)
+constexpr double kPi = 3.14159265358979323846264338327950288419716939937510;
+constexpr double kVLight = 2.99792458e+5;
+constexpr double kZeeman = 4.6686411e-13;
+constexpr double kRsqrtPi = 0.5641895836;
+constexpr double kGhostSigma = 1e21;
+constexpr unsigned kFull = 0xffffffffu;
+
+// Hui, Armstrong & Wray (1978) rational approximation of w(z), z = a - i v:
+// numerator degree 6, monic denominator degree 7 (published coefficients).
+__device__ constexpr double kP[7] = {122.607931777104326, 214.382388694706425, 181.928533092181549, 93.155580458138441,
+                          30.180142196210589,  5.912626209773153,   0.564189583562615};
+__device__ constexpr double kQ[7] = {122.60793177387535,  352.730625110963558, 457.334478783897737, 348.703917719495792,
+                          170.354001821091472, 53.992906912940207,  10.479857114260399};
+
+template <typename R>
+__device__ __forceinline__ R taps(const PmParams& P, int j);
+template <>
+__device__ __forceinline__ float taps<float>(const PmParams& P, int j) { return P.taps_f[j]; }
+template <>
+__device__ __forceinline__ double taps<double>(const PmParams& P, int j) { return P.taps_d[j]; }
+template <typename R>
+__device__ __forceinline__ R gcen(const PmParams& P, int t);
+template <>
+__device__ __forceinline__ float gcen<float>(const PmParams& P, int t) { return P.gc_f[t]; }
+template <>
+__device__ __forceinline__ double gcen<double>(const PmParams& P, int t) { return P.gc_d[t]; }
+template <typename R>
+__device__ __forceinline__ R slshared(const PmParams& P, int i);
+template <>
+__device__ __forceinline__ float slshared<float>(const PmParams& P, int i) { return P.sl_f[i]; }
+template <>
+__device__ __forceinline__ double slshared<double>(const PmParams& P, int i) { return P.sl_d[i]; }
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+
+// ---------------------------------------------------------------------------
+// Voigt / Faraday-Voigt: H = Re w, F = Im w / 2 (fvoigt.c:15-80).  Horner in
+// complex arithmetic, then a branch-free Smith (1962) division.
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ __forceinline__ void voigt(R a, R v, R& h, R& f) {
+  const R zr = a, zi = -v;
+  R nr = R(kP[6]) * zr + R(kP[5]);
+  R ni = R(kP[6]) * zi;
+#pragma unroll
+  for (int j = 4; j >= 0; --j) {
+    const R tr = (nr * zr - ni * zi) + R(kP[j]);
+    const R ti = nr * zi + ni * zr;
+    nr = tr;
+    ni = ti;
+  }
+  R dr = zr + R(kQ[6]);
+  R di = zi;
+#pragma unroll
+  for (int j = 5; j >= 0; --j) {
+    const R tr = (dr * zr - di * zi) + R(kQ[j]);
+    const R ti = dr * zi + di * zr;
+    dr = tr;
+    di = ti;
+  }
+  const bool c = fabs(dr) >= fabs(di);
+  const R big = c ? dr : di, small = c ? di : dr;
+  const R x1 = c ? nr : ni, x2 = c ? ni : nr;
+  const R r = small / big;
+  const R inv = R(1) / (big + small * r);
+  const R wr = (x1 + x2 * r) * inv;
+  const R wi = (c ? R(1) : R(-1)) * (x2 - x1 * r) * inv;
+  h = wr;
+  f = wi * R(0.5);
+}
+
+// Per-model terms shared by every wavelength (mil_sinrf.c:84-166, me_der.c:58-63).
+// This build handles the normal Zeeman triplet (one component per group: N_PI =
+// N_SIG = 1, e.g. Fe I 6173 and 6302, 5P1.0-5D0.0); the host rejects multiplets.
+// The FP32 form evaluates these terms in FP32 as well.
+template <typename R>
+struct ModelTerms {
+  R sin_gm, cosi, sinis, cosis, cosis_2, sina, cosa, sinda, cosda, sindi, cosdi, sinis_cosa, sinis_sina;
+  R E0_2, cosi_E0_2, ulos, invLD, A, alf, oma;
+  R zs[3];   // Zeeman splitting per gauss of each group, in Doppler units (nupB/nubB/nurB)
+  R zsB[3];  // the same times B
+  R auxCte;  // d u / d vlos (me_der.c:545)
+  R invE0, sc, ss, cosi_2_E0;  // me_der.c:118-127
+  double E0, B0, B1, ALF;
+};
+
+template <typename R>
+__device__ __forceinline__ void model_terms(const PmParams& P, const double* m, ModelTerms<R>& T) {
+  constexpr bool f32 = sizeof(R) == 4;
+  const int lane = threadIdx.x & 31;
+  T.E0 = m[0] * P.fo;
+  T.B0 = m[7];
+  T.B1 = -(m[8] * P.mu);
+  T.ALF = m[10];
+  T.alf = R(m[10]);
+  T.oma = R(1.0 - m[10]);
+  T.A = R(m[4]);
+  // lane 0 evaluates the inclination, lane 1 the azimuth: one sincos per warp
+  R s, c;
+  if constexpr (f32) {
+    const float CC = float(kPi / 180.0);
+    const float ang = (lane & 1) ? 2.0f * (float(m[6]) * CC) : float(m[5]) * CC;
+    sincosf(ang, &s, &c);
+  } else {
+    const double CC = kPi / 180.0;
+    sincos((lane & 1) ? 2.0 * (m[6] * CC) : m[5] * CC, &s, &c);
+  }
+  T.sin_gm = __shfl_sync(kFull, s, 0);
+  T.cosi = __shfl_sync(kFull, c, 0);
+  T.sina = __shfl_sync(kFull, s, 1);
+  T.cosa = __shfl_sync(kFull, c, 1);
+  T.sinis = T.sin_gm * T.sin_gm;
+  T.cosis = T.cosi * T.cosi;
+  T.cosis_2 = (R(1) + T.cosis) / R(2);
+  const R CCr = R(kPi / 180.0), CC2 = CCr * R(2);
+  T.sinda = T.cosa * CC2;
+  T.cosda = -T.sina * CC2;
+  T.sindi = T.cosi * T.sin_gm * CC2;
+  T.cosdi = -T.sin_gm * CCr;
+  T.sinis_cosa = T.sinis * T.cosa;
+  T.sinis_sina = T.sinis * T.sina;
+  const R LD = R(m[3]), E0 = R(T.E0), l0 = R(P.lambda0);
+  T.E0_2 = E0 / R(2);
+  T.cosi_E0_2 = T.E0_2 * T.cosi;
+  T.invLD = R(1) / LD;
+  T.ulos = (R(m[2]) * l0) / (R(kVLight) * LD);
+  const R parcial = ((l0 * l0) / LD) * R(kZeeman);
+#pragma unroll
+  for (int g = 0; g < 3; ++g) {
+    T.zs[g] = parcial * R(P.nu[g][0]);
+    T.zsB[g] = T.zs[g] * R(m[1]);
+  }
+  T.auxCte = (-l0) / (R(kVLight) * LD);
+  T.invE0 = R(1) / E0;
+  T.sc = E0 * T.sinis_cosa / R(2);
+  T.ss = E0 * T.sinis_sina / R(2);
+  T.cosi_2_E0 = E0 * T.cosi / R(2);
+}
+
+// Everything the response functions need from the synthesis at one wavelength
+// (the reference keeps it in process globals between mil_sinrf and me_der).
+template <typename R>
+struct LaneState {
+  R fi[3], shi[3], uu[3], H[3], F[3];
+  R parcial1, parcial2, parcial3;
+  R etain, etaq, etau, etav, rhoq, rhou, rhov;
+  R etai, etai_2, gp1, gp2, gp3, dt, dti, g4, g5, g6;
+};
+
+// ME synthesis at wavelength offset dl (mil_sinrf.c:117-285): the three Zeeman
+// groups, the propagation matrix, and the Unno-Rachkovsky solution.
+template <typename R>
+__device__ __forceinline__ void synth_lane(const PmParams& P, const ModelTerms<R>& T, double dl, LaneState<R>& s,
+                                           R S[4]) {
+  const R u = R(dl) * T.invLD - T.ulos;
+#pragma unroll
+  for (int g = 0; g < 3; ++g) {
+    const R uu = u - T.zsB[g];
+    R H, F;
+    voigt<R>(T.A, uu, H, F);
+    const R we = R(P.we[g][0]);
+    s.fi[g] = we * H;
+    s.shi[g] = we * F * R(2);
+    s.uu[g] = uu;
+    s.H[g] = H;
+    s.F[g] = F;
+  }
+  s.parcial1 = s.fi[1] + s.fi[2];
+  s.parcial2 = T.E0_2 * (s.fi[0] - s.parcial1 / R(2));
+  s.parcial3 = T.E0_2 * (s.shi[0] - (s.shi[1] + s.shi[2]) / R(2));
+  s.etain = T.E0_2 * (s.fi[0] * T.sinis + s.parcial1 * T.cosis_2);
+  s.etaq = s.parcial2 * T.sinis_cosa;
+  s.etau = s.parcial2 * T.sinis_sina;
+  s.etav = (s.fi[2] - s.fi[1]) * T.cosi_E0_2;
+  s.rhoq = s.parcial3 * T.sinis_cosa;
+  s.rhou = s.parcial3 * T.sinis_sina;
+  s.rhov = (s.shi[2] - s.shi[1]) * T.cosi_E0_2;
+  s.etai = R(1) + s.etain;
+  s.etai_2 = s.etai * s.etai;
+  const R auxq = s.rhoq * s.rhoq, auxu = s.rhou * s.rhou, auxv = s.rhov * s.rhov;
+  s.gp1 = s.etai_2 - s.etaq * s.etaq - s.etau * s.etau - s.etav * s.etav + auxq + auxu + auxv;
+  s.gp3 = s.etai_2 + auxq + auxu + auxv;
+  s.gp2 = s.etaq * s.rhoq + s.etau * s.rhou + s.etav * s.rhov;
+  s.dt = s.etai_2 * s.gp1 - s.gp2 * s.gp2;
+  s.dti = R(1) / s.dt;
+  const R gp4 = s.etai_2 * s.etaq + s.etai * (s.etav * s.rhou - s.etau * s.rhov);
+  const R gp5 = s.etai_2 * s.etau + s.etai * (s.etaq * s.rhov - s.etav * s.rhoq);
+  const R gp6 = s.etai_2 * s.etav + s.etai * (s.etau * s.rhoq - s.etaq * s.rhou);
+  s.g4 = gp4 + s.rhoq * s.gp2;
+  s.g5 = gp5 + s.rhou * s.gp2;
+  s.g6 = gp6 + s.rhov * s.gp2;
+  const R dtiaux = R(s.dti * T.B1);
+  S[0] = R(T.B0 - double(dtiaux * s.etai * s.gp3));
+  S[1] = dtiaux * s.g4;
+  S[2] = dtiaux * s.g5;
+  S[3] = dtiaux * s.g6;
+}
+
+// Per-warp shared memory.
+template <typename R>
+struct WarpSmem {
+  R tr[NL * TRS];      // response functions: [profile][lambda] (transpose buffer)
+  R xs[4][3 * NL];     // padded Stokes rows for the synthesis PSF correlation
+  double ab[PM_NTERMS_MAX * PM_NTERMS_MAX + PM_NTERMS_MAX];  // alpha (K*K) then beta (K)
+  double ev[2][12 * 12];  // eigen solver: A (double-buffered rows reuse ev[1]) and V
+  double rot[12][3];      // per index: partner, c, signed s
+  int pq[6][2];           // the rotated pairs of the current round
+  double delta[PM_NTERMS_MAX];
+};
+
+// PSF correlation of the four synthesized profiles in the lane = wavelength
+// layout: out[k] = sum_j G[j] x[k + j - nl/2] with zero padding; Stokes I
+// correlates Ic - I and returns Ic - result, Ic = max(I[0], I[nl-1])
+// (mil_sinrf.c:387-402, convolution.c:54-121).
+template <typename R>
+__device__ __forceinline__ void psf_rows(const PmParams& P, WarpSmem<R>& sm, int lane, bool valid, R S[4]) {
+  const R i0 = __shfl_sync(kFull, S[0], 0), in = __shfl_sync(kFull, S[0], P.nl - 1);
+  const R ic = (i0 > in) ? i0 : in;
+#pragma unroll
+  for (int s = 0; s < 4; ++s) sm.xs[s][NL + lane] = valid ? (s == 0 ? ic - S[0] : S[s]) : R(0);
+  __syncwarp();
+  const int base = NL + lane - P.half;
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    R acc = 0;
+#pragma unroll
+    for (int j = 0; j < NL; ++j) acc = fma(taps<R>(P, j), sm.xs[s][base + j], acc);
+    S[s] = (s == 0) ? ic - acc : acc;
+  }
+  __syncwarp();
+}
+
+// Synthesis of the model at this lane's wavelength, PSF and stray light included.
+// S gets the final (mixed) profile, Su the profile before the stray-light mix.
+template <typename R>
+__device__ __forceinline__ void synthesize(const PmParams& P, WarpSmem<R>& sm, const double* m,
+                                           const float* sl_pix, int lane, bool valid, ModelTerms<R>& T,
+                                           LaneState<R>& st, R S[4], R Su[4]) {
+  model_terms<R>(P, m, T);
+  synth_lane<R>(P, T, P.dl[valid ? lane : 0], st, S);
+  if (P.has_psf) psf_rows<R>(P, sm, lane, valid, S);
+#pragma unroll
+  for (int s = 0; s < 4; ++s) Su[s] = S[s];
+  if (P.slight_mode != PM_SLIGHT_NONE) {
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      const int idx = s * P.nl + (valid ? lane : 0);
+      const R slv = P.slight_mode == PM_SLIGHT_SHARED ? slshared<R>(P, idx) : R(sl_pix[idx]);
+      S[s] = S[s] * T.alf + slv * T.oma;
+    }
+  }
+}
+
+// Response functions at this lane's wavelength (me_der.c:85-312) written into the
+// transpose buffer: profile p = r*4 + s for rows r = 0..6 (eta0, B, vlos, dopp,
+// a, gamma, azimuth) and r = 7 holding RF row 8 (S1).  Row 7 of the reference
+// (S0: I = 1, Q = U = V = 0) is not convolved and is added in registers later.
+template <typename R>
+__device__ __forceinline__ void rf_lane(const PmParams& P, const ModelTerms<R>& T, const LaneState<R>& st,
+                                        WarpSmem<R>& sm, int lane, bool valid) {
+  R dfi[3][4], dshi[3][4];
+#pragma unroll
+  for (int g = 0; g < 3; ++g) {
+    const R we = R(P.we[g][0]);
+    const R uu = st.uu[g], H = st.H[g], F = st.F[g];
+    const R dH_u = ((R(4) * T.A * F) - (R(2) * uu * H)) * we;
+    const R dF_u = (R(kRsqrtPi) - T.A * H - R(2) * uu * F) * we;
+    const R uun = -uu * T.invLD;
+    dfi[g][0] = dH_u * (-T.zs[g]);
+    dfi[g][1] = dH_u * T.auxCte;
+    dfi[g][2] = dH_u * uun;
+    dfi[g][3] = R(-2) * dF_u;
+    dshi[g][0] = dF_u * (-T.zs[g]);
+    dshi[g][1] = dF_u * T.auxCte;
+    dshi[g][2] = dF_u * uun;
+    dshi[g][3] = dH_u / R(2);
+  }
+  const R invE0 = T.invE0, sc = T.sc, ss = T.ss;
+  const R E0_2 = T.E0_2;
+  const R sindi_cosa = T.sindi * T.cosa, sindi_sina = T.sindi * T.sina;
+  const R cosdi_E0_2 = E0_2 * T.cosdi;
+  const R cosi_2_E0 = T.cosi_2_E0;
+  const R cosis_2_E0_2 = T.cosis_2 * E0_2, sinis_E0_2 = T.sinis * E0_2;
+  const R cosi_cosdi = T.cosi * T.cosdi * E0_2, sindi_E0_2 = T.sindi * E0_2;
+  const R sinis_cosda = T.sinis * T.cosda, sinis_sinda = T.sinis * T.sinda;
+
+  const R dtaux = R(T.B1) / (st.dt * st.dt);
+  const R etai = st.etai, etai_2 = st.etai_2, etaq = st.etaq, etau = st.etau, etav = st.etav;
+  const R rhoq = st.rhoq, rhou = st.rhou, rhov = st.rhov;
+  const R etai_gp3 = etai * st.gp3;
+  const R a2 = R(2) * etai;
+  const R ext1 = a2 * etaq + etav * rhou - etau * rhov;
+  const R ext2 = a2 * etau + etaq * rhov - etav * rhoq;
+  const R ext3 = a2 * etav + etau * rhoq - etaq * rhou;
+  const R ext4 = a2 * st.gp1;
+  R* col = sm.tr + lane;
+#pragma unroll
+  for (int il = 0; il < 7; ++il) {
+    R de, dq, du, dv, rq, ru, rv;
+    if (il == 0) {
+      de = st.etain * invE0; dq = st.etaq * invE0; du = st.etau * invE0; dv = st.etav * invE0;
+      rq = st.rhoq * invE0; ru = st.rhou * invE0; rv = st.rhov * invE0;
+    } else if (il < 5) {
+      const int k = il - 1;
+      const R dfisum = dfi[1][k] + dfi[2][k];
+      const R aux = dfi[0][k] - dfisum / R(2);
+      de = dfi[0][k] * sinis_E0_2 + dfisum * cosis_2_E0_2;
+      dq = aux * sc;
+      du = aux * ss;
+      dv = (dfi[2][k] - dfi[1][k]) * cosi_2_E0;
+      const R auxr = dshi[0][k] - (dshi[1][k] + dshi[2][k]) / R(2);
+      rq = auxr * sc;
+      ru = auxr * ss;
+      rv = (dshi[2][k] - dshi[1][k]) * cosi_2_E0;
+    } else if (il == 5) {
+      de = st.fi[0] * sindi_E0_2 + st.parcial1 * cosi_cosdi;
+      dq = st.parcial2 * sindi_cosa;
+      du = st.parcial2 * sindi_sina;
+      dv = (st.fi[2] - st.fi[1]) * cosdi_E0_2;
+      rq = st.parcial3 * sindi_cosa;
+      ru = st.parcial3 * sindi_sina;
+      rv = (st.shi[2] - st.shi[1]) * cosdi_E0_2;
+    } else {
+      de = 0; dv = 0; rv = 0;
+      dq = st.parcial2 * sinis_cosda;
+      du = st.parcial2 * sinis_sinda;
+      rq = st.parcial3 * sinis_cosda;
+      ru = st.parcial3 * sinis_sinda;
+    }
+    const R dgp1 = R(2) * (etai * de - etaq * dq - etau * du - etav * dv + rhoq * rq + rhou * ru + rhov * rv);
+    const R dgp2 = rhoq * dq + etaq * rq + rhou * du + etau * ru + rhov * dv + etav * rv;
+    const R d_dt = ext4 * de + etai_2 * dgp1 - R(2) * st.gp2 * dgp2;
+    const R dgp3 = R(2) * (etai * de + rhoq * rq + rhou * ru + rhov * rv);
+    R dI = -(((de * st.gp3 + etai * dgp3) * st.dt - d_dt * etai_gp3) * dtaux);
+    const R dgp4 = de * ext1 + etai_2 * dq + etai * (rhou * dv + etav * ru - rhov * du - etau * rv);
+    const R dQ = ((dgp4 + rq * st.gp2 + rhoq * dgp2) * st.dt - d_dt * st.g4) * dtaux;
+    const R dgp5 = de * ext2 + etai_2 * du + etai * (rhov * dq + etaq * rv - rhoq * dv - etav * rq);
+    const R dU = ((dgp5 + ru * st.gp2 + rhou * dgp2) * st.dt - d_dt * st.g5) * dtaux;
+    const R dgp6 = de * ext3 + etai_2 * dv + etai * (rhoq * du + etau * rq - rhou * dq - etaq * ru);
+    R dV = ((dgp6 + rv * st.gp2 + rhov * dgp2) * st.dt - d_dt * st.g6) * dtaux;
+    if (il == 6) { dI = 0; dV = 0; }  // me_der.c:309-312
+    col[(il * 4 + 0) * TRS] = valid ? dI : R(0);
+    col[(il * 4 + 1) * TRS] = valid ? dQ : R(0);
+    col[(il * 4 + 2) * TRS] = valid ? dU : R(0);
+    col[(il * 4 + 3) * TRS] = valid ? dV : R(0);
+  }
+  // S1 (me_der.c:281-298)
+  const R dti_s1 = -(st.dti * R(P.mu));
+  col[(7 * 4 + 0) * TRS] = valid ? -dti_s1 * etai_gp3 : R(0);
+  col[(7 * 4 + 1) * TRS] = valid ? dti_s1 * st.g4 : R(0);
+  col[(7 * 4 + 2) * TRS] = valid ? dti_s1 * st.g5 : R(0);
+  col[(7 * 4 + 3) * TRS] = valid ? dti_s1 * st.g6 : R(0);
+}
+
+// PSF correlation of the 32 response-function profiles, one profile per lane
+// (me_der.c:471-496).  Lane p loads its whole profile into registers and forms
+// out[k] = sum_m x[m] G[m - k + nl/2]; the tap is a compile-time-indexed read of
+// the centred table in the parameter block, i.e. a constant operand of the FMA.
+// Stokes-I rows correlate Ic - x with Ic = max of the row's end points.
+template <typename R>
+__device__ __forceinline__ void rf_correlate(const PmParams& P, WarpSmem<R>& sm, int lane) {
+  __syncwarp();
+  R* row = sm.tr + lane * TRS;
+  R x[NL];
+#pragma unroll
+  for (int m = 0; m < NL; ++m) x[m] = row[m];
+  const bool isI = (lane & 3) == 0;
+  const R e0 = x[0], en = row[P.nl - 1];
+  const R ic = isI ? ((e0 > en) ? e0 : en) : R(0);
+#pragma unroll
+  for (int m = 0; m < NL; ++m) x[m] = (m < P.nl) ? (isI ? ic - x[m] : x[m]) : R(0);
+  R acc[NL];
+#pragma unroll
+  for (int k = 0; k < NL; ++k) acc[k] = 0;
+#pragma unroll
+  for (int m = 0; m < NL; ++m) {
+#pragma unroll
+    for (int k = 0; k < NL; ++k) acc[k] = fma(x[m], gcen<R>(P, m - k + (NL - 1)), acc[k]);
+  }
+#pragma unroll
+  for (int k = 0; k < NL; ++k) row[k] = isI ? ic - acc[k] : acc[k];
+  __syncwarp();
+}
+
+// Reduce N values held by every lane across the warp; afterwards lane l holds
+// the totals of entries [l*N/32, (l+1)*N/32) in v[0 .. N/32).  Recursive halving:
+// 31*N/32 shuffles in total.
+template <typename T, int N>
+__device__ __forceinline__ void transpose_reduce(T (&v)[N], int lane) {
+  static_assert(N % 32 == 0, "N must be a multiple of 32");
+#pragma unroll
+  for (int o = 16, len = N; o > 0; o >>= 1, len >>= 1) {
+    const bool up = (lane & o) != 0;
+    const int half = len / 2;
+#pragma unroll
+    for (int i = 0; i < half; ++i) {
+      const T send = up ? v[i] : v[i + half];
+      const T keep = up ? v[i + half] : v[i];
+      v[i] = keep + __shfl_xor_sync(kFull, send, o);
+    }
+  }
+}
+
+// Response functions at this lane's wavelength after correlation, filling factor
+// and FijaACeroDerivadasNoNecesarias: d[row][stokes] for rows 0..K-1.
+template <typename R, int KT>
+__device__ __forceinline__ void gather_rf(const PmParams& P, const WarpSmem<R>& sm, int lane, bool valid,
+                                          const ModelTerms<R>& T, const R Sff[4], const float* sl_pix,
+                                          R (&d)[KT][4]) {
+  const R* col = sm.tr + lane;
+#pragma unroll
+  for (int r = 0; r < KT; ++r) {
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      R v;
+      if (r < 7) v = col[(r * 4 + s) * TRS];
+      else if (r == 7) v = (s == 0) ? R(1) : R(0);  // S0 (me_der.c:301-306)
+      else if (r == 8) v = col[(7 * 4 + s) * TRS];
+      else v = R(0);
+      d[r][s] = valid ? v : R(0);
+    }
+  }
+  if (P.slight_mode != PM_SLIGHT_NONE) {
+    // me_der.c:499-525: every RF scaled by alpha; the filling-factor row is
+    // S_mag - S_stray, built from the spectrum the caller passes (Sff)
+#pragma unroll
+    for (int r = 0; r < KT; ++r) {
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+        d[r][s] = d[r][s] * T.alf;
+        if (r == P.ff_row) {
+          const int idx = s * P.nl + (valid ? lane : 0);
+          const R slv = P.slight_mode == PM_SLIGHT_SHARED ? slshared<R>(P, idx) : R(sl_pix[idx]);
+          d[r][s] = valid ? Sff[s] - slv : R(0);
+        }
+      }
+    }
+  }
+}
+
+// Normal equations (covarm2): alpha = sum w_s/sigma^2 d_a d_b (upper triangle),
+// beta = sum w_s (S - O)/sigma^2 d_b, reduced over the warp and stored in FP64.
+template <typename R, int KT>
+__device__ __forceinline__ void normal_eq(const PmParams& P, WarpSmem<R>& sm, int lane, const R (&d)[KT][4],
+                                          const R S[4], const float O[4], const R isig[4]) {
+  constexpr int NA = KT * (KT + 1) / 2;
+  constexpr int NV = ((NA + KT + 31) / 32) * 32;
+  R v[NV];
+#pragma unroll
+  for (int i = 0; i < NV; ++i) v[i] = 0;
+  R cw[4], rw[4];
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    cw[s] = R(P.w[s]) * isig[s];
+    rw[s] = R(P.w[s]) * (S[s] - R(O[s])) * isig[s];
+  }
+  int idx = 0;
+#pragma unroll
+  for (int a = 0; a < KT; ++a) {
+#pragma unroll
+    for (int b = a; b < KT; ++b) {
+      R acc = 0;
+#pragma unroll
+      for (int s = 0; s < 4; ++s) acc = fma(d[a][s] * d[b][s], cw[s], acc);
+      v[idx++] = acc;
+    }
+  }
+#pragma unroll
+  for (int b = 0; b < KT; ++b) {
+    R acc = 0;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) acc = fma(rw[s], d[b][s], acc);
+    v[NA + b] = acc;
+  }
+  transpose_reduce<R, NV>(v, lane);
+  constexpr int M = NV / 32;
+  double* red = reinterpret_cast<double*>(sm.tr);  // scratch: the RFs are consumed
+  __syncwarp();
+#pragma unroll
+  for (int i = 0; i < M; ++i) red[lane * M + i] = double(v[i]);
+  __syncwarp();
+  // unpack: full symmetric alpha (K x K) and beta
+  for (int e = lane; e < KT * KT + KT; e += 32) {
+    double val;
+    if (e < KT * KT) {
+      int a = e / KT, b = e % KT;
+      if (a > b) { int t = a; a = b; b = t; }
+      const int u = a * KT - (a * (a - 1)) / 2 + (b - a);
+      val = red[u];
+    } else {
+      val = red[NA + (e - KT * KT)];
+    }
+    sm.ab[e] = val;
+  }
+  __syncwarp();
+}
+
+// chi^2 / nfree (fchisqr), accumulated in FP64.
+template <typename R>
+__device__ __forceinline__ double chisq(const PmParams& P, const R S[4], const float O[4], const R isig[4],
+                                        bool valid, double nfree) {
+  double acc = 0;
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    const R dif = S[s] - R(O[s]);
+    acc += valid ? double(dif * dif) * P.w[s] * double(isig[s]) : 0.0;
+  }
+  return warp_sum(acc) / nfree;
+}
+
+// ---------------------------------------------------------------------------
+// Damped solve.  covar = alpha with the diagonal scaled by (1 + lambda_LM).
+// ---------------------------------------------------------------------------
+
+// Symmetric eigen-decomposition by parallel-ordered Jacobi (round-robin pairs,
+// all K/2 rotations of a round applied at once), then the pseudo-inverse with
+// the absolute 1e-12 eigenvalue cut of mil_svd.  Warp-cooperative; every lane
+// returns delta.
+template <typename R, int KT>
+__device__ void solve_eigen(const PmParams& P, WarpSmem<R>& sm, int lane, double flambda, double (&delta)[KT]) {
+  constexpr int M = (KT + 1) & ~1;  // padded to even; index KT (if any) is a dummy
+  double* A = sm.ev[0];
+  double* V = sm.ev[1];
+  double* A2 = reinterpret_cast<double*>(sm.tr);  // second A buffer
+  for (int e = lane; e < M * M; e += 32) {
+    const int i = e / M, j = e % M;
+    double a = 0;
+    if (i < KT && j < KT) {
+      a = sm.ab[i * KT + j];
+      if (i == j) a *= (1.0 + flambda);
+    }
+    A[e] = a;
+    V[e] = (i == j) ? 1.0 : 0.0;
+  }
+  __syncwarp();
+  for (int sweep = 0; sweep < 24; ++sweep) {
+    double off = 0, dg = 0;
+    for (int e = lane; e < KT * KT; e += 32) {
+      const int i = e / KT, j = e % KT;
+      const double a = A[i * M + j];
+      if (i == j) dg += a * a;
+      else if (i < j) off += a * a;
+    }
+    off = warp_sum(off);
+    dg = warp_sum(dg);
+    if (off == 0.0 || off <= 1e-36 * dg) break;
+    for (int r = 0; r < M - 1; ++r) {
+      // circle method: position 0 fixed, positions 1..M-1 rotate
+      if (lane < M / 2) {
+        const int k = lane;
+        const int pa = (k == 0) ? 0 : ((k - 1 + r) % (M - 1)) + 1;
+        const int pb = ((M - 1 - k - 1 + r) % (M - 1)) + 1;
+        const int p = pa < pb ? pa : pb, q = pa < pb ? pb : pa;
+        double c = 1.0, s = 0.0, t = 0.0;
+        const double apq = (p < KT && q < KT) ? A[p * M + q] : 0.0;
+        if (apq != 0.0) {
+          const double app = A[p * M + p], aqq = A[q * M + q];
+          const double theta = (aqq - app) / (2.0 * apq);
+          t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+          if (!isfinite(t)) t = 0.0;
+          c = rsqrt(t * t + 1.0);
+          s = t * c;
+        }
+        // column p of J: (c at p, -s at q); column q: (s at p, c at q)
+        sm.rot[p][0] = q; sm.rot[p][1] = c; sm.rot[p][2] = -s;
+        sm.rot[q][0] = p; sm.rot[q][1] = c; sm.rot[q][2] = s;
+        sm.pq[k][0] = p; sm.pq[k][1] = q;
+        // exact diagonal update (Rutishauser) stored in the unused slot of delta
+        if (p < KT) sm.delta[p] = A[p * M + p] - t * apq;
+        if (q < KT) sm.delta[q] = A[q * M + q] + t * apq;
+      }
+      __syncwarp();
+      for (int e = lane; e < M * M; e += 32) {
+        const int i = e / M, j = e % M;
+        const int pi = int(sm.rot[i][0]), pj = int(sm.rot[j][0]);
+        const double ci = sm.rot[i][1], si = sm.rot[i][2], cj = sm.rot[j][1], sj = sm.rot[j][2];
+        double a;
+        if (i == j) a = (i < KT) ? sm.delta[i] : 0.0;
+        else if (pi == j) a = 0.0;
+        else
+          a = ci * (cj * A[i * M + j] + sj * A[i * M + pj]) + si * (cj * A[pi * M + j] + sj * A[pi * M + pj]);
+        A2[e] = a;
+      }
+      // V <- V J, one work item per (row, rotated pair): both columns of the pair
+      // are rewritten from their old values by the same lane
+      for (int e = lane; e < M * (M / 2); e += 32) {
+        const int i = e / (M / 2), k = e % (M / 2);
+        const int p = sm.pq[k][0], q = sm.pq[k][1];
+        const double vp = V[i * M + p], vq = V[i * M + q];
+        V[i * M + p] = vp * sm.rot[p][1] + vq * sm.rot[p][2];
+        V[i * M + q] = vq * sm.rot[q][1] + vp * sm.rot[q][2];
+      }
+      __syncwarp();
+      for (int e = lane; e < M * M; e += 32) A[e] = A2[e];
+      __syncwarp();
+    }
+  }
+  // pseudo-inverse: aux_j = (V^T beta)_j / w_j (0 if |w_j| <= 1e-12); delta = V aux
+  const double* beta = sm.ab + KT * KT;
+  if (lane < KT) {
+    double sum = 0;
+    for (int i = 0; i < KT; ++i) sum += beta[i] * V[i * M + lane];
+    const double w = A[lane * M + lane];
+    sm.rot[lane][0] = sum * ((fabs(w) > 1e-12) ? (1.0 / w) : 0.0);
+  }
+  __syncwarp();
+  if (lane < KT) {
+    double sum = 0;
+    for (int j = 0; j < KT; ++j) sum += V[lane * M + j] * sm.rot[j][0];
+    sm.delta[lane] = sum;
+  }
+  __syncwarp();
+#pragma unroll
+  for (int i = 0; i < KT; ++i) delta[i] = sm.delta[i];
+  __syncwarp();
+}
+
+// FP64 Cholesky, computed redundantly by every lane in registers (the matrix is
+// uniform across the warp).  Exactly-zero rows (fixed parameters) get a zero step
+// like the pseudo-inverse would give them.  Returns false on a pivot <= 1e-12.
+template <typename R, int KT>
+__device__ bool solve_cholesky(WarpSmem<R>& sm, double flambda, double (&delta)[KT]) {
+  double L[KT][KT];
+  bool zr[KT];
+#pragma unroll
+  for (int i = 0; i < KT; ++i) {
+    zr[i] = sm.ab[i * KT + i] == 0.0;
+#pragma unroll
+    for (int j = 0; j <= i; ++j) L[i][j] = sm.ab[i * KT + j];
+    L[i][i] *= (1.0 + flambda);
+  }
+  bool ok = true;
+#pragma unroll
+  for (int j = 0; j < KT; ++j) {
+    double d = L[j][j];
+#pragma unroll
+    for (int k = 0; k < j; ++k) d -= L[j][k] * L[j][k];
+    const bool skip = zr[j];
+    ok = ok && (skip || (d > 1e-12 && isfinite(d)));
+    const double rinv = skip ? 0.0 : rsqrt(d);
+    L[j][j] = skip ? 1.0 : d * rinv;
+#pragma unroll
+    for (int i = j + 1; i < KT; ++i) {
+      double a = L[i][j];
+#pragma unroll
+      for (int k = 0; k < j; ++k) a -= L[i][k] * L[j][k];
+      L[i][j] = a * rinv;
+    }
+  }
+  const double* beta = sm.ab + KT * KT;
+  double y[KT];
+#pragma unroll
+  for (int j = 0; j < KT; ++j) {
+    double a = zr[j] ? 0.0 : beta[j];
+#pragma unroll
+    for (int k = 0; k < j; ++k) a -= L[j][k] * y[k];
+    y[j] = a / L[j][j];
+  }
+#pragma unroll
+  for (int j = KT - 1; j >= 0; --j) {
+    double a = y[j];
+#pragma unroll
+    for (int k = j + 1; k < KT; ++k) a -= L[k][j] * delta[k];
+    delta[j] = zr[j] ? 0.0 : a / L[j][j];
+  }
+  return ok;
+}
+
+// AplicaDelta (milosUtils.c:47-115): p <- p - delta for free parameters, with the
+// step on B clamped to +-300 G and on gamma, azimuth to +-30 deg.
+template <int KT>
+__device__ __forceinline__ void apply_delta(const PmParams& P, const double* m, double (&dlt)[KT], double* out) {
+  auto clamp = [](double v, double lim) { return v < -lim ? -lim : (v > lim ? lim : v); };
+  if (P.fix[0]) out[0] = m[0] - dlt[0];
+  if (P.fix[1]) out[1] = m[1] - clamp(dlt[1], 300.0);
+  if (P.fix[2]) out[2] = m[2] - dlt[2];
+  if (P.fix[3]) out[3] = m[3] - dlt[3];
+  if (P.fix[4]) out[4] = m[4] - dlt[4];
+  if (P.fix[5]) out[5] = m[5] - clamp(dlt[5], 30.0);
+  if (P.fix[6]) out[6] = m[6] - clamp(dlt[6], 30.0);
+  if (P.fix[7]) out[7] = m[7] - dlt[7];
+  if (P.fix[8]) out[8] = m[8] - dlt[8];
+  if constexpr (KT == 11) {
+    if (P.fix[9]) out[9] = m[9] - dlt[9];
+    if (P.fix[10]) out[10] = m[10] - dlt[10];
+  } else if constexpr (KT == 10) {
+    if (P.fix[10]) out[10] = m[10] - dlt[9];  // NTERMS == 10: alpha is term 9
+  }
+}
+
+// check (milosUtils.c:118-196).
+__device__ __forceinline__ void check_model(double* m) {
+  if (m[1] < 0) { m[1] = -m[1]; m[5] = 180.0 - m[5]; }
+  if (m[1] > 5000) m[1] = 5000;
+  if (m[5] < 0) m[5] = -m[5];
+  if (m[5] > 180) m[5] = 360.0 - m[5];
+  if (m[6] < 0) m[6] = 180 + m[6];
+  if (m[6] > 180) m[6] = m[6] - 180.0;
+  if (m[0] < 1) m[0] = 1;
+  if (m[0] > 2500) m[0] = 2500;
+  if (m[2] < -20) m[2] = -20;
+  if (m[2] > 20) m[2] = 20;
+  if (m[3] < 0.0001) m[3] = 0.0001;
+  if (m[3] > 0.6) m[3] = 0.6;
+  if (m[4] < 0.0001) m[4] = 0.0001;
+  if (m[4] > 10.0) m[4] = 10.0;
+  if (m[7] < 0.0001) m[7] = 0.0001;
+  if (m[7] > 2.00) m[7] = 2.00;
+  if (m[8] < 0.0001) m[8] = 0.0001;
+  if (m[8] > 2.00) m[8] = 2.00;
+  if (m[9] < 0) m[9] = 0;
+  if (m[9] > 4) m[9] = 4;
+  if (m[10] < 0) m[10] = 0.0;
+  if (m[10] > 1.0) m[10] = 1.0;
+}
+
+// estimacionesClasicas (milosUtils.c:287-452, forInitialUse = 1) followed by the
+// NaN fixes of the drivers (milos.c:976-983).  Sums in FP64 across the warp.
+__device__ void classical(const PmParams& P, const float O[4], int lane, bool valid, double* m) {
+  const int nl = P.nl;
+  const unsigned neg = __ballot_sync(kFull, valid && O[0] < 0.0f);
+  const unsigned validm = (nl >= 32) ? kFull : ((1u << nl) - 1u);
+  // leading and trailing ghost wavelengths (I < 0)
+  const unsigned nonneg = validm & ~neg;
+  if (nonneg == 0) return;  // every intensity negative: no estimate possible
+  const int begin = __ffs(nonneg) - 1;
+  const int end = 32 - __clz(nonneg);  // one past the last non-negative
+  const double Ic = __shfl_sync(kFull, double(O[0]), end - 1);
+  const double dl = valid ? P.dl[lane] : 0.0;
+  const bool in = valid && lane >= begin && lane < end - 1;
+  const bool iv = in && O[0] > -1.0f && O[3] > -1.0f;
+  const double a = iv ? Ic - double(O[0] + O[3]) : 0.0;
+  const double av = iv ? Ic - double(O[0]) : 0.0;
+  const double am = iv ? Ic - double(O[0] - O[3]) : 0.0;
+  const double x = warp_sum(a * dl), y = warp_sum(a);
+  const double xv = warp_sum(av * dl), yv = warp_sum(av);
+  const double xm = warp_sum(am * dl), ym = warp_sum(am);
+  const double lp = fabs(y) > 1e-15 ? x / y : 0.0;
+  const double lmn = fabs(ym) > 1e-15 ? xm / ym : 0.0;
+  const double C = kZeeman * (P.lambda0 * P.lambda0) * P.geff;
+  const double Blos = (1 / C) * ((lp - lmn) / 2);
+  double Vlos = (kVLight / P.lambda0) * ((xv / yv) / 2);
+  const bool iq = in && O[1] > -1.0f && O[2] > -1.0f && O[3] > -1.0f;
+  double gx = 0, gy = 0;
+  if (iq) {
+    const double L = fabs(sqrt(double(O[1]) * O[1] + double(O[2]) * O[2]));
+    const double mm = fabs(4 * dl * L);
+    gx = fabs(double(O[3])) * mm;
+    gy = fabs(double(O[3])) * fabs(double(O[3]));
+  }
+  const double sx = warp_sum(gx);
+  const double sy = warp_sum(gy) * fabs(3 * C * Blos);
+  const double tan_gamma = fabs(sqrt(sx / sy));
+  double gamma_rad = atan(tan_gamma);
+  double gamma = gamma_rad * (180 / kPi);
+  if (gamma >= 85 && gamma <= 90) gamma_rad = 85 * (kPi / 180);
+  if (gamma > 90 && gamma <= 95) gamma_rad = 95 * (kPi / 180);
+  if (Blos < 0) gamma = 180 - gamma;
+  const bool iu = valid && O[2] > -1.0f && O[1] > -1.0f && (fabs(O[2]) > 0.0001f || fabs(O[1]) > 0.0001f);
+  const double su = warp_sum(iu ? double(O[2]) : 0.0), sq = warp_sum(iu ? double(O[1]) : 0.0);
+  double phi = (atan(su / sq) * 180 / kPi) / 2;
+  if (su > 0 && sq > 0) phi = phi;
+  else if (su < 0 && sq > 0) phi = phi + 180;
+  else if (su < 0 && sq < 0) phi = phi + 90;
+  else if (su > 0 && sq < 0) phi = phi + 90;
+  const double B_aux = fabs(Blos / cos(gamma_rad));
+  if (Vlos < -4) Vlos = -4;
+  if (Vlos > 4) Vlos = 4;
+  m[1] = B_aux > 4000 ? 4000 : B_aux;
+  m[2] = Vlos;
+  m[5] = gamma;
+  m[6] = phi;
+  if (isnan(m[1])) m[1] = 1;
+  if (isnan(m[2])) m[2] = 1e-3;
+  if (isnan(m[5])) m[5] = 1;
+  if (isnan(m[6])) m[6] = 1;
+}
+
+// Response functions at the current synthesis -> alpha, beta in shared memory.
+template <typename R, int KT>
+__device__ __forceinline__ void rf_and_normal_eq(const PmParams& P, WarpSmem<R>& sm, int lane, bool valid,
+                                                 const ModelTerms<R>& T, const LaneState<R>& st, const R S[4],
+                                                 const R Sff[4], const float O[4], const R isig[4],
+                                                 const float* sl_pix) {
+  rf_lane<R>(P, T, st, sm, lane, valid);
+  if (P.has_psf) rf_correlate<R>(P, sm, lane);
+  __syncwarp();
+  R d[KT][4];
+  gather_rf<R, KT>(P, sm, lane, valid, T, Sff, sl_pix, d);
+#pragma unroll
+  for (int r = 0; r < KT; ++r)
+    if (P.zero_row[r]) {
+#pragma unroll
+      for (int s = 0; s < 4; ++s) d[r][s] = 0;
+    }
+  normal_eq<R, KT>(P, sm, lane, d, S, O, isig);
+}
+
+// ---------------------------------------------------------------------------
+// Inversion kernel: persistent warps over an atomic pixel queue; lm_mils per
+// pixel (milosUtils.c:466-635).
+// ---------------------------------------------------------------------------
+template <typename R, int KT>
+__global__ void __launch_bounds__(128) invert_kernel(const __grid_constant__ PmParams P, const PmIO io) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  WarpSmem<R>& sm = reinterpret_cast<WarpSmem<R>*>(smem_raw)[warp];
+  for (int e = lane; e < 4 * 3 * NL; e += 32) (&sm.xs[0][0])[e] = R(0);
+  __syncwarp();
+  const bool valid = lane < P.nl;
+  const int li = valid ? lane : 0;
+
+  while (true) {
+    unsigned long long pix = 0;
+    if (lane == 0) pix = atomicAdd(&io.ctr[PMC_NEXT], 1ull);
+    pix = __shfl_sync(kFull, pix, 0);
+    if (pix >= (unsigned long long)io.npix) break;
+    const size_t base = size_t(pix) * 4 * P.nl;
+    const float* sl_pix = (P.slight_mode == PM_SLIGHT_PER_PIXEL) ? io.slight + base : nullptr;
+
+    float O[4];
+    R isig[4];
+    int ghosts = 0;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      O[s] = valid ? io.spectro[base + s * P.nl + lane] : 0.0f;
+      const bool g = valid && O[s] <= -1.0f;
+      ghosts += __popc(__ballot_sync(kFull, g));
+      isig[s] = R(1.0 / (g ? kGhostSigma : P.noise));
+    }
+    double m[11];
+#pragma unroll
+    for (int i = 0; i < 11; ++i) m[i] = P.guess[i];
+    if (P.classical) classical(P, O, lane, valid, m);
+
+    const int nfree = P.nfree_base - ghosts;
+    int status = PM_PIX_MAXITER, iter = 0, accepted = 0, fallbacks = 0;
+    double ochi = 0;
+    ModelTerms<R> T;
+    LaneState<R> st;
+    R S[4], Su[4];
+    if (nfree == 0) {
+      status = PM_PIX_NFREE;
+      iter = -1;
+#pragma unroll
+      for (int s = 0; s < 4; ++s) S[s] = 0;
+    } else {
+      synthesize<R>(P, sm, m, sl_pix, lane, valid, T, st, S, Su);
+      rf_and_normal_eq<R, KT>(P, sm, lane, valid, T, st, S, Su, O, isig, sl_pix);
+      ochi = chisq<R>(P, S, O, isig, valid, double(nfree));
+      const double chi0 = ochi;
+      double flambda = P.ilambda, factor = 1.0;
+      double trial[11];
+#pragma unroll
+      for (int i = 0; i < 11; ++i) trial[i] = m[i];
+      bool stop = false;
+      do {
+        double dlt[KT];
+        bool ok = true;
+        if (P.solver == PM_SOLVE_CHOLESKY) ok = solve_cholesky<R, KT>(sm, flambda, dlt);
+        if (P.solver != PM_SOLVE_CHOLESKY || !ok) {
+          if (P.solver == PM_SOLVE_CHOLESKY) ++fallbacks;
+          solve_eigen<R, KT>(P, sm, lane, flambda, dlt);
+        }
+        apply_delta<KT>(P, m, dlt, trial);
+        check_model(trial);
+        synthesize<R>(P, sm, trial, sl_pix, lane, valid, T, st, S, Su);
+        const double chi = chisq<R>(P, S, O, isig, valid, double(nfree));
+        if ((fabs((ochi - chi) * 100 / chi) < P.toplim) || (chi < 0.0001)) {
+          stop = true;
+          status = PM_PIX_CONVERGED;
+        }
+        if (chi - ochi < 0.) {
+          flambda = flambda / (5.0 * factor);
+#pragma unroll
+          for (int i = 0; i < 11; ++i) m[i] = trial[i];
+          rf_and_normal_eq<R, KT>(P, sm, lane, valid, T, st, S, S, O, isig, sl_pix);
+          ochi = chi;
+          ++accepted;
+        } else {
+          flambda = flambda * 10.0 * factor;
+        }
+        if ((flambda > 1e+7) || (flambda < 1e-25)) {
+          if (!stop) status = PM_PIX_LAMBDA;
+          stop = true;
+        }
+        ++iter;
+        if (P.logclambda) factor = double(log10f(float(chi)) / log10f(float(chi0)));
+      } while (iter < P.miter && !stop);
+      bool finite = isfinite(ochi);
+#pragma unroll
+      for (int i = 0; i < 11; ++i) finite = finite && isfinite(m[i]);
+      if (!finite) status = PM_PIX_NONFINITE;
+    }
+    // outputs
+    if (lane < 11) io.models_out[size_t(pix) * 11 + lane] = m[lane];
+    if (lane == 0) {
+      io.chisq_out[pix] = float(ochi);
+      io.iters_out[pix] = iter;
+      if (io.status_out) io.status_out[pix] = status;
+      atomicAdd(&io.ctr[PMC_ITERS], (unsigned long long)(iter > 0 ? iter : 0));
+      atomicAdd(&io.ctr[PMC_ACCEPTED], (unsigned long long)accepted);
+      if (fallbacks) atomicAdd(&io.ctr[PMC_FALLBACK], (unsigned long long)fallbacks);
+    }
+    if (io.spectra_out && valid) {
+#pragma unroll
+      for (int s = 0; s < 4; ++s) io.spectra_out[base + s * P.nl + lane] = float(S[s]);
+    }
+    (void)li;
+  }
+}
+
+// Synthesis (and response functions) of given models, one warp per model, as the
+// reference's synthesis mode runs mil_sinrf + me_der (milos.c:601-602).
+template <typename R, int KT>
+__global__ void __launch_bounds__(128) synth_kernel(const __grid_constant__ PmParams P, const PmIO io) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  WarpSmem<R>& sm = reinterpret_cast<WarpSmem<R>*>(smem_raw)[warp];
+  for (int e = lane; e < 4 * 3 * NL; e += 32) (&sm.xs[0][0])[e] = R(0);
+  __syncwarp();
+  const bool valid = lane < P.nl;
+  const int64_t nwarps = int64_t(gridDim.x) * (blockDim.x >> 5);
+  for (int64_t pix = int64_t(blockIdx.x) * (blockDim.x >> 5) + warp; pix < io.npix; pix += nwarps) {
+    const size_t base = size_t(pix) * 4 * P.nl;
+    const float* sl_pix = (P.slight_mode == PM_SLIGHT_PER_PIXEL) ? io.slight + base : nullptr;
+    double m[11];
+#pragma unroll
+    for (int i = 0; i < 11; ++i) m[i] = io.models_in[size_t(pix) * 11 + i];
+    ModelTerms<R> T;
+    LaneState<R> st;
+    R S[4], Su[4];
+    synthesize<R>(P, sm, m, sl_pix, lane, valid, T, st, S, Su);
+    if (valid) {
+#pragma unroll
+      for (int s = 0; s < 4; ++s) io.spectra_out[base + s * P.nl + lane] = float(S[s]);
+    }
+    if (io.rf_out) {
+      rf_lane<R>(P, T, st, sm, lane, valid);
+      if (P.has_psf) rf_correlate<R>(P, sm, lane);
+      __syncwarp();
+      R d[KT][4];
+      gather_rf<R, KT>(P, sm, lane, valid, T, Su, sl_pix, d);
+      __syncwarp();
+      if (valid) {
+        const size_t rb = size_t(pix) * 4 * KT * P.nl;
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+#pragma unroll
+          for (int r = 0; r < KT; ++r) io.rf_out[rb + (size_t(s) * KT + r) * P.nl + lane] = float(d[r][s]);
+      }
+    }
+  }
+}
+
+char g_err[256];
+
+template <typename R, int KT>
+int launch_invert(const PmParams& P, const PmIO& io, cudaStream_t st, int num_sms, float* kernel_ms) {
+  const int threads = 128;
+  const size_t smem = sizeof(WarpSmem<R>) * (threads / 32);
+  auto kern = invert_kernel<R, KT>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return snprintf(g_err, sizeof g_err, "%s", cudaGetErrorString(e)), PM_EIO;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+  if (e != cudaSuccess || per_sm < 1) return snprintf(g_err, sizeof g_err, "occupancy: %s", cudaGetErrorString(e)), PM_EIO;
+  int64_t blocks = int64_t(per_sm) * num_sms;
+  const int64_t need = (io.npix + 3) / 4;
+  if (blocks > need) blocks = need > 0 ? need : 1;
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (kernel_ms) {
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, st);
+  }
+  kern<<<unsigned(blocks), threads, smem, st>>>(P, io);
+  e = cudaGetLastError();
+  if (kernel_ms) {
+    cudaEventRecord(b, st);
+    cudaEventSynchronize(b);
+    cudaEventElapsedTime(kernel_ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  }
+  if (e != cudaSuccess) return snprintf(g_err, sizeof g_err, "invert launch: %s", cudaGetErrorString(e)), PM_EIO;
+  return PM_OK;
+}
+
+template <typename R, int KT>
+int launch_synth(const PmParams& P, const PmIO& io, cudaStream_t st) {
+  const int threads = 128;
+  const size_t smem = sizeof(WarpSmem<R>) * (threads / 32);
+  auto kern = synth_kernel<R, KT>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return snprintf(g_err, sizeof g_err, "%s", cudaGetErrorString(e)), PM_EIO;
+  int64_t blocks = (io.npix + 3) / 4;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  if (blocks < 1) blocks = 1;
+  kern<<<unsigned(blocks), threads, smem, st>>>(P, io);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return snprintf(g_err, sizeof g_err, "synth launch: %s", cudaGetErrorString(e)), PM_EIO;
+  return PM_OK;
+}
+
+}  // namespace
+
+int pmk_invert(const PmParams& P, const PmIO& io, int precision, void* stream, int num_sms, float* kernel_ms) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (precision == PM_PREC_FP32) {
+    if (P.K == 9) return launch_invert<float, 9>(P, io, st, num_sms, kernel_ms);
+    if (P.K == 10) return launch_invert<float, 10>(P, io, st, num_sms, kernel_ms);
+  } else {
+    if (P.K == 9) return launch_invert<double, 9>(P, io, st, num_sms, kernel_ms);
+    if (P.K == 10) return launch_invert<double, 10>(P, io, st, num_sms, kernel_ms);
+  }
+  snprintf(g_err, sizeof g_err, "nterms=%d has no compiled kernel", P.K);
+  return PM_ENOTSUP;
+}
+
+int pmk_synth(const PmParams& P, const PmIO& io, int precision, void* stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (precision == PM_PREC_FP32) {
+    if (P.K == 9) return launch_synth<float, 9>(P, io, st);
+    if (P.K == 10) return launch_synth<float, 10>(P, io, st);
+  } else {
+    if (P.K == 9) return launch_synth<double, 9>(P, io, st);
+    if (P.K == 10) return launch_synth<double, 10>(P, io, st);
+  }
+  snprintf(g_err, sizeof g_err, "nterms=%d has no compiled kernel", P.K);
+  return PM_ENOTSUP;
+}
+
+const char* pmk_last_cuda_error() { return g_err; }

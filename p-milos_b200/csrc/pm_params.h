@@ -1,0 +1,73 @@
+// pm_params.h -- launch parameter blocks shared by the host code and the kernels.
+//
+// Everything that is constant for a run (grid, PSF taps, line data, control
+// settings, the initial guess, a shared stray-light profile) travels BY VALUE in
+// the kernel parameter block, i.e. in the constant bank: a tap read with a
+// compile-time index becomes a constant operand of the FMA that uses it, with no
+// load instruction at all.  Per-pixel data travels by pointer in PmIO.
+#pragma once
+#include <stdint.h>
+
+#include "../../include/pmilos.h"
+
+// Wavelengths handled by one warp in this build: one per lane.
+#define PMK_NL 32
+// Centred-tap table length for the profile-per-lane correlation.
+#define PMK_GC (2 * PMK_NL - 1)
+
+struct PmParams {
+  int nl;          // wavelengths
+  int half;        // nl / 2: PSF centre tap (convolution.c:64)
+  int K;           // NTERMS
+  int miter;
+  int nfree_base;  // 4*nl - K (CalculaNfree, lib.c:399-407)
+  int logclambda;
+  int classical;   // estimacionesClasicas before LM
+  int has_psf;
+  int solver;      // PM_SOLVE_EIGEN | PM_SOLVE_CHOLESKY
+  int slight_mode; // PM_SLIGHT_*
+  int want_rf;     // synth kernel: also write response functions
+  int n_pi, n_sig;
+  int fix[11];
+  int zero_row[PM_NTERMS_MAX];  // FijaACeroDerivadasNoNecesarias (milosUtils.c:199-227)
+  int ff_row;      // RF row that holds d/d(filling factor), or -1
+  double lambda0;
+  double dl[PMK_NL];                       // lambda_i - lambda0 [A]
+  double nu[3][PM_ZEEMAN_MAX];             // splittings: 0 = pi (NUP), 1 = blue (NUB), 2 = NUB mirrored
+  double we[3][PM_ZEEMAN_MAX];             // strengths: WEP, WEB, WER
+  double geff, fo;
+  double w[4];
+  double noise, ilambda, toplim, mu;
+  double guess[11];
+  double taps_d[PMK_NL];                   // G[j], zero for j >= nl
+  float taps_f[PMK_NL];
+  double gc_d[PMK_GC];                     // gc[t] = G[t - (PMK_NL-1) + half] inside [0,nl), else 0
+  float gc_f[PMK_GC];
+  double sl_d[4 * PMK_NL];                 // shared stray-light profile [4][nl]
+  float sl_f[4 * PMK_NL];
+};
+
+// Work-queue / statistics counters (device memory, zeroed before each launch).
+enum { PMC_NEXT = 0, PMC_ITERS = 1, PMC_ACCEPTED = 2, PMC_FALLBACK = 3, PMC_COUNT = 4 };
+
+struct PmIO {
+  int64_t npix;
+  const float* spectro;     // [npix][4][nl]
+  const float* slight;      // PM_SLIGHT_PER_PIXEL: [npix][4][nl]
+  const double* models_in;  // synth kernel: [npix][11]
+  double* models_out;       // [npix][11]
+  float* chisq_out;         // [npix]
+  int* iters_out;           // [npix]
+  float* spectra_out;       // [npix][4][nl] (nullable)
+  float* rf_out;            // synth kernel: [npix][4][K][nl] (nullable)
+  int* status_out;          // [npix] (nullable)
+  unsigned long long* ctr;  // PMC_COUNT counters
+};
+
+// Kernel variants compiled into the library.
+enum PmVariant { PMV_FP64 = 0, PMV_FP32 = 1 };
+
+// Host-side launchers (pm_kernels.cu).
+int pmk_invert(const PmParams& P, const PmIO& io, int precision, void* stream, int num_sms, float* kernel_ms);
+int pmk_synth(const PmParams& P, const PmIO& io, int precision, void* stream);
+const char* pmk_last_cuda_error();

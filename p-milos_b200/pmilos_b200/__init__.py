@@ -1,0 +1,357 @@
+"""pmilos_b200 -- Python host interface of libpmilos_b200.so (B200 ME inversion).
+
+The compute path is the CUDA library behind the C ABI of ``include/pmilos.h``;
+this module binds it with ctypes and mirrors the reference's per-run setup:
+
+* ``LineData.from_lines_entry`` / ``line_from_quantum``  -- readFileCuanticLines +
+  create_cuantic (readConfig.c:24-129, create_cuantic.c:24-294)
+* ``grid_from_malla`` -- the wavelength grid of a .grid file (milos.c:176-196)
+* ``psf_gaussian`` / ``psf_from_table`` -- fgauss_WL and the .psf route
+  (fgauss.c:79-154; milos.c:266-344; milosUtils.c:684-738)
+* ``Inverter.invert`` -- the per-pixel loop of milos.c:958-1009 (classical estimates,
+  NaN fixes, lm_mils) over a whole batch
+* ``Inverter.lm_mils`` -- one pixel, same contract as lm_mils (milosUtils.c:466-635)
+* ``Inverter.synth`` -- mil_sinrf + me_der as the synthesis mode runs them
+
+Buffers may be numpy arrays (host memory: the library stages them through the
+GPU) or torch CUDA tensors (device memory: nothing is copied).  There is no CPU
+fallback: without the built library or a B200 every compute call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .files import (grid_from_malla, parse_lines_entry, read_grid_file, read_lines_file, read_model_file,
+                    read_psf_file, read_trol_file)
+
+__all__ = [
+    "MODEL_FIELDS", "PmError", "LineData", "Inverter", "load_library", "line_from_quantum", "psf_gaussian",
+    "psf_from_table", "grid_from_malla", "parse_lines_entry", "read_grid_file", "read_lines_file",
+    "read_model_file", "read_psf_file", "read_trol_file", "PREC_FP64", "PREC_FP32", "SOLVE_DEFAULT",
+    "SOLVE_EIGEN", "SOLVE_CHOLESKY", "SLIGHT_NONE", "SLIGHT_SHARED", "SLIGHT_PER_PIXEL",
+]
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_DIR = os.path.dirname(PKG_DIR)
+LIB_PATH = os.path.join(LIB_DIR, "libpmilos_b200.so")
+
+MODEL_FIELDS = ("eta0", "B", "vlos", "dopp", "aa", "gm", "az", "S0", "S1", "mac", "alfa")
+PREC_FP64, PREC_FP32 = 0, 1
+SOLVE_DEFAULT, SOLVE_EIGEN, SOLVE_CHOLESKY = 0, 1, 2
+SLIGHT_NONE, SLIGHT_SHARED, SLIGHT_PER_PIXEL = 0, 1, 2
+MEM_HOST, MEM_DEVICE = 0, 1
+PIX_CONVERGED, PIX_LAMBDA, PIX_MAXITER, PIX_NFREE, PIX_NONFINITE = 0, 1, 2, -1, -2
+ZMAX = 8
+NL_MAX = 128
+
+# Every symbol include/pmilos.h declares (checked by the CPU test suite).
+EXPORTED_SYMBOLS = (
+    "pm_line_from_quantum", "pm_psf_gaussian", "pm_psf_interpolate", "pm_ctx_create", "pm_ctx_destroy",
+    "pm_invert_batch", "pm_synth_batch", "pm_lm_mils", "pm_get_stats", "pm_last_error", "pm_abi_version",
+)
+
+
+class PmError(RuntimeError):
+    """A negative return code of the C ABI (with pm_last_error's message)."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class _Model(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in MODEL_FIELDS]
+
+
+class _Line(ctypes.Structure):
+    _fields_ = [
+        ("lambda0", ctypes.c_double), ("n_pi", ctypes.c_int), ("n_sig", ctypes.c_int),
+        ("nup", ctypes.c_double * ZMAX), ("nub", ctypes.c_double * ZMAX), ("nur", ctypes.c_double * ZMAX),
+        ("wep", ctypes.c_double * ZMAX), ("web", ctypes.c_double * ZMAX), ("wer", ctypes.c_double * ZMAX),
+        ("gl", ctypes.c_double), ("gu", ctypes.c_double), ("geff", ctypes.c_double), ("fo", ctypes.c_double),
+    ]
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [
+        ("nlambda", ctypes.c_int), ("lambda_", ctypes.POINTER(ctypes.c_double)),
+        ("psf", ctypes.POINTER(ctypes.c_double)), ("weight", ctypes.c_double * 4), ("noise", ctypes.c_double),
+        ("ilambda", ctypes.c_double), ("toplim", ctypes.c_double), ("miter", ctypes.c_int),
+        ("fix", ctypes.c_int * 11), ("nterms", ctypes.c_int), ("logclambda", ctypes.c_int),
+        ("mu", ctypes.c_double), ("classical_estimates", ctypes.c_int), ("precision", ctypes.c_int),
+        ("solver", ctypes.c_int),
+    ]
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [("pixels", ctypes.c_int64), ("iterations", ctypes.c_int64), ("accepted", ctypes.c_int64),
+                ("eigen_fallbacks", ctypes.c_int64), ("kernel_ms", ctypes.c_double), ("total_ms", ctypes.c_double)]
+
+
+_LIB = None
+
+
+def load_library(path: str | None = None):
+    """Load libpmilos_b200.so (raises if it has not been built: there is no fallback)."""
+    global _LIB
+    if _LIB is not None and path is None:
+        return _LIB
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise FileNotFoundError(f"{p} is missing: build it with __graft_entry__.build() (no CPU fallback exists)")
+    L = ctypes.CDLL(p)
+    vp, i64, D, F, I = ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p, ctypes.c_void_p
+    L.pm_line_from_quantum.argtypes = [ctypes.c_double] * 7 + [ctypes.POINTER(_Line)]
+    L.pm_psf_gaussian.argtypes = [ctypes.c_double, ctypes.c_int, D, D]
+    L.pm_psf_interpolate.argtypes = [ctypes.c_int, D, D, ctypes.c_int, D, D]
+    L.pm_ctx_create.argtypes = [ctypes.POINTER(_Line), ctypes.POINTER(_Config), vp, ctypes.POINTER(vp)]
+    L.pm_ctx_destroy.argtypes = [vp]
+    L.pm_invert_batch.argtypes = [vp, i64, F, F, ctypes.c_int, ctypes.POINTER(_Model), vp, vp, vp, vp, vp,
+                                  ctypes.c_int]
+    L.pm_synth_batch.argtypes = [vp, i64, vp, F, ctypes.c_int, vp, vp, ctypes.c_int]
+    L.pm_lm_mils.argtypes = [vp, F, ctypes.POINTER(_Model), vp, ctypes.POINTER(ctypes.c_float), F,
+                             ctypes.POINTER(ctypes.c_int)]
+    L.pm_get_stats.argtypes = [vp, ctypes.POINTER(_Stats)]
+    L.pm_last_error.restype = ctypes.c_char_p
+    L.pm_abi_version.restype = ctypes.c_int
+    if path is None:
+        _LIB = L
+    return L
+
+
+def _check(rc: int) -> int:
+    if rc < 0:
+        raise PmError(rc, load_library().pm_last_error().decode())
+    return rc
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+@dataclass
+class LineData:
+    """Zeeman pattern + centre of one spectral line (what create_cuantic provides)."""
+
+    lambda0: float
+    quantum: tuple  # (SLOI, LLOI, JLOI, SUPI, LUPI, JUPI) as readFileCuanticLines decodes them
+    _c: _Line = field(default=None, repr=False)
+
+    def __post_init__(self):
+        if self._c is None:
+            self._c = _Line()
+            _check(load_library().pm_line_from_quantum(self.lambda0, *[float(q) for q in self.quantum],
+                                                       ctypes.byref(self._c)))
+
+    @classmethod
+    def from_lines_entry(cls, text: str, lambda0: float | None = None) -> "LineData":
+        idx, lam, q = parse_lines_entry(text)
+        return cls(lam if lambda0 is None else lambda0, q)
+
+    @property
+    def geff(self) -> float:
+        return self._c.geff
+
+    def cuantic_dat(self) -> np.ndarray:
+        """The 7-double array readFileCuanticLines produces ({1, quantum numbers})."""
+        return np.array([1.0, *self.quantum], dtype=np.float64)
+
+
+def line_from_quantum(lambda0: float, sl, ll, jl, su, lu, ju) -> LineData:
+    return LineData(lambda0, (sl, ll, jl, su, lu, ju))
+
+
+def psf_gaussian(fwhm_ma: float, lam: np.ndarray) -> np.ndarray:
+    lam = np.ascontiguousarray(lam, dtype=np.float64)
+    out = np.zeros_like(lam)
+    _check(load_library().pm_psf_gaussian(float(fwhm_ma), lam.size, _dptr(lam), _dptr(out)))
+    return out
+
+
+def psf_from_table(offsets_ma: np.ndarray, values: np.ndarray, grid_offsets_ma: np.ndarray) -> np.ndarray:
+    dl = np.ascontiguousarray(offsets_ma, dtype=np.float64)
+    ps = np.ascontiguousarray(values, dtype=np.float64)
+    go = np.ascontiguousarray(grid_offsets_ma, dtype=np.float64)
+    out = np.zeros_like(go)
+    _check(load_library().pm_psf_interpolate(dl.size, _dptr(dl), _dptr(ps), go.size, _dptr(go), _dptr(out)))
+    return out
+
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+def _model_struct(m) -> _Model:
+    v = [float(x) for x in np.asarray(m, dtype=np.float64).ravel()]
+    if len(v) != 11:
+        raise ValueError("a model has 11 parameters (eta0, B, vlos, dopp, aa, gm, az, S0, S1, mac, alfa)")
+    return _Model(*v)
+
+
+class Inverter:
+    """One pm_ctx: a wavelength grid, a line, a PSF and the control settings.
+
+    Mirrors the inputs lm_mils takes from the control file (.mtrol): weights,
+    noise (sigma^2 = 1/SN^2), initial diagonal element, toplim, number of cycles,
+    the fix[] switches (reference order eta0, B, vlos, dopp, aa, gm, az, S0, S1,
+    mac, alfa), NTERMS, the diagonal-acceleration switch and mu.
+    """
+
+    def __init__(self, line: LineData, lam, psf=None, *, weights=(1.0, 1.0, 1.0, 1.0), noise=1e-6, ilambda=0.1,
+                 toplim=1e-12, miter=50, fix=None, nterms=None, logclambda=0, mu=1.0, classical=True,
+                 precision=PREC_FP32, solver=SOLVE_DEFAULT, stream=None):
+        self.L = load_library()
+        self.line = line
+        self.lam = np.ascontiguousarray(lam, dtype=np.float64)
+        self.nl = int(self.lam.size)
+        self.psf = None if psf is None else np.ascontiguousarray(psf, dtype=np.float64)
+        fix = list(fix) if fix is not None else [1] * 9 + [0, 0]
+        if nterms is None:
+            nterms = 11 - (0 if fix[10] else 1) - (0 if fix[9] else 1)
+        self.nterms = nterms
+        self.precision = precision
+        c = _Config()
+        c.nlambda = self.nl
+        c.lambda_ = _dptr(self.lam)
+        c.psf = _dptr(self.psf) if self.psf is not None else ctypes.POINTER(ctypes.c_double)()
+        c.weight[:] = [float(w) for w in weights]
+        c.noise, c.ilambda, c.toplim, c.miter = float(noise), float(ilambda), float(toplim), int(miter)
+        c.fix[:] = [int(bool(f)) for f in fix]
+        c.nterms, c.logclambda, c.mu = int(nterms), int(logclambda), float(mu)
+        c.classical_estimates, c.precision, c.solver = int(bool(classical)), int(precision), int(solver)
+        self._cfg = c
+        ctx = ctypes.c_void_p()
+        st = ctypes.c_void_p(int(stream)) if stream is not None else None
+        _check(self.L.pm_ctx_create(ctypes.byref(line._c), ctypes.byref(c), st, ctypes.byref(ctx)))
+        self.ctx = ctx
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.L.pm_ctx_destroy(self.ctx)
+            self.ctx = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- batched inversion ----
+    def invert(self, spectro, guess, *, slight=None, slight_mode=None, want_spectra=True, want_status=True):
+        """Invert [npix][4][nl] float32 profiles.  numpy in -> numpy out (host staging);
+        torch CUDA in -> torch CUDA out (no copies)."""
+        if _is_torch(spectro):
+            return self._invert_device(spectro, guess, slight, slight_mode, want_spectra, want_status)
+        obs = np.ascontiguousarray(spectro, dtype=np.float32).reshape(-1, 4, self.nl)
+        npix = obs.shape[0]
+        sl, mode = self._slight_host(slight, slight_mode, npix)
+        models = np.zeros((npix, 11), dtype=np.float64)
+        chi = np.zeros(npix, dtype=np.float32)
+        its = np.zeros(npix, dtype=np.int32)
+        sp = np.zeros((npix, 4, self.nl), dtype=np.float32) if want_spectra else None
+        stt = np.zeros(npix, dtype=np.int32) if want_status else None
+        g = _model_struct(guess)
+        _check(self.L.pm_invert_batch(self.ctx, npix, obs.ctypes.data, None if sl is None else sl.ctypes.data, mode,
+                                      ctypes.byref(g), models.ctypes.data, chi.ctypes.data, its.ctypes.data,
+                                      None if sp is None else sp.ctypes.data,
+                                      None if stt is None else stt.ctypes.data, MEM_HOST))
+        out = {"models": models, "chisq": chi, "iters": its}
+        if sp is not None:
+            out["spectra"] = sp
+        if stt is not None:
+            out["status"] = stt
+        return out
+
+    def _slight_host(self, slight, mode, npix):
+        if slight is None:
+            return None, SLIGHT_NONE
+        sl = np.ascontiguousarray(slight, dtype=np.float32)
+        if mode is None:
+            mode = SLIGHT_SHARED if sl.size == 4 * self.nl else SLIGHT_PER_PIXEL
+        if mode == SLIGHT_PER_PIXEL and sl.size != npix * 4 * self.nl:
+            raise ValueError("per-pixel stray light must be [npix][4][nl]")
+        return sl, mode
+
+    def _invert_device(self, spectro, guess, slight, slight_mode, want_spectra, want_status):
+        import torch
+
+        obs = spectro.contiguous().view(-1, 4, self.nl)
+        if obs.dtype != torch.float32 or not obs.is_cuda:
+            raise TypeError("device inversion wants a float32 CUDA tensor")
+        npix = obs.shape[0]
+        dev = obs.device
+        models = torch.empty((npix, 11), dtype=torch.float64, device=dev)
+        chi = torch.empty(npix, dtype=torch.float32, device=dev)
+        its = torch.empty(npix, dtype=torch.int32, device=dev)
+        sp = torch.empty((npix, 4, self.nl), dtype=torch.float32, device=dev) if want_spectra else None
+        stt = torch.empty(npix, dtype=torch.int32, device=dev) if want_status else None
+        mode = SLIGHT_NONE
+        slp = None
+        if slight is not None:
+            sl = slight.contiguous()
+            mode = slight_mode if slight_mode is not None else (
+                SLIGHT_SHARED if sl.numel() == 4 * self.nl else SLIGHT_PER_PIXEL)
+            slp = sl.data_ptr()
+        g = _model_struct(guess)
+        _check(self.L.pm_invert_batch(self.ctx, npix, obs.data_ptr(), slp, mode, ctypes.byref(g), models.data_ptr(),
+                                      chi.data_ptr(), its.data_ptr(), None if sp is None else sp.data_ptr(),
+                                      None if stt is None else stt.data_ptr(), MEM_DEVICE))
+        out = {"models": models, "chisq": chi, "iters": its}
+        if sp is not None:
+            out["spectra"] = sp
+        if stt is not None:
+            out["status"] = stt
+        return out
+
+    # ---- forward synthesis ----
+    def synth(self, models, *, slight=None, slight_mode=None, rf=False):
+        """Synthesize [npix][11] models -> [npix][4][nl] (+ RFs [npix][4][nterms][nl])."""
+        if _is_torch(models):
+            import torch
+
+            m = models.contiguous().to(torch.float64).view(-1, 11)
+            npix = m.shape[0]
+            sp = torch.empty((npix, 4, self.nl), dtype=torch.float32, device=m.device)
+            rfo = torch.empty((npix, 4, self.nterms, self.nl), dtype=torch.float32, device=m.device) if rf else None
+            mode, slp = SLIGHT_NONE, None
+            if slight is not None:
+                sl = slight.contiguous()
+                mode = slight_mode if slight_mode is not None else (
+                    SLIGHT_SHARED if sl.numel() == 4 * self.nl else SLIGHT_PER_PIXEL)
+                slp = sl.data_ptr()
+            _check(self.L.pm_synth_batch(self.ctx, npix, m.data_ptr(), slp, mode, sp.data_ptr(),
+                                         None if rfo is None else rfo.data_ptr(), MEM_DEVICE))
+            return (sp, rfo) if rf else sp
+        m = np.ascontiguousarray(models, dtype=np.float64).reshape(-1, 11)
+        npix = m.shape[0]
+        sl, mode = self._slight_host(slight, slight_mode, npix)
+        sp = np.zeros((npix, 4, self.nl), dtype=np.float32)
+        rfo = np.zeros((npix, 4, self.nterms, self.nl), dtype=np.float32) if rf else None
+        _check(self.L.pm_synth_batch(self.ctx, npix, m.ctypes.data, None if sl is None else sl.ctypes.data, mode,
+                                     sp.ctypes.data, None if rfo is None else rfo.ctypes.data, MEM_HOST))
+        return (sp, rfo) if rf else sp
+
+    # ---- lm_mils, batch of one ----
+    def lm_mils(self, spectro, init_model, slight=None):
+        """Returns (rc, model, spectra, chisq, iter) like lm_mils' outputs."""
+        obs = np.ascontiguousarray(spectro, dtype=np.float32).reshape(4 * self.nl)
+        m = _model_struct(init_model)
+        sp = np.zeros(4 * self.nl, dtype=np.float32)
+        chi = ctypes.c_float()
+        it = ctypes.c_int()
+        sl = None if slight is None else np.ascontiguousarray(slight, dtype=np.float32).reshape(4 * self.nl)
+        rc = _check(self.L.pm_lm_mils(self.ctx, obs.ctypes.data, ctypes.byref(m), sp.ctypes.data, ctypes.byref(chi),
+                                      None if sl is None else sl.ctypes.data, ctypes.byref(it)))
+        model = np.array([getattr(m, n) for n in MODEL_FIELDS])
+        return rc, model, sp.reshape(4, self.nl), chi.value, it.value
+
+    def stats(self) -> dict:
+        s = _Stats()
+        _check(self.L.pm_get_stats(self.ctx, ctypes.byref(s)))
+        return {k: getattr(s, k) for k, _ in _Stats._fields_}

@@ -1,0 +1,177 @@
+"""Generate the golden fixtures of tests/golden/ from the REFERENCE itself.
+
+Run in a container where the reference tree exists (its sources are compiled by
+oracle/Makefile into oracle/_ref/):
+
+    python tests/golden/make_golden.py [--reference /root/reference]
+
+Writes
+  kat_synthesis.npz   the reference's own known-answer test (test/synthesis.mtrol:
+                      obs.mod + malla.grid + LINES entry 1 + straylight.fits ->
+                      synthesis_results.per), inputs and expected profiles
+  ref_cases.npz       per configuration (0, 1, 2; 48 pixels each): grid, PSF taps,
+                      truth models, observed profiles, and the reference's
+                      inversion results in both builds (REAL = float / double),
+                      plus mil_sinrf + me_der outputs at 12 models
+  ref_psf.npz         the reference's fgauss_WL and interpolationLinearPSF on the
+                      configuration grids (host precompute pinning)
+The fixtures are what the CPU test-suite compares the oracle restatement and the
+host precompute with, so those tests need neither the reference nor a GPU.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+import pyoracle as po  # noqa: E402
+from fitsmini import read_fits_f32  # noqa: E402
+
+TRIPLET = np.array([1.0, 2.0, 1.0, 1.0, 2.0, 2.0, 0.0])
+GUESS = np.array([8.0, 400.0, 0.0, 0.03, 0.1, 30.0, 30.0, 0.25, 0.75, 0.0, 1.0])
+
+
+def grid(ini, step, fin, l0):
+    nl = int((fin - ini) / step) + 1
+    offs = np.zeros(nl)
+    offs[0] = ini
+    for i in range(1, nl):
+        offs[i] = offs[i - 1] + step
+    lam = np.zeros(nl)
+    lam[0] = l0 + ini / 1000.0
+    for i in range(1, nl):
+        lam[i] = lam[i - 1] + step / 1000.0
+    return offs, lam
+
+
+def gauss_table(fwhm, half=1500.0, step=1.0):
+    x = np.arange(-half, half + step / 2, step)
+    sig = fwhm / (2.0 * np.sqrt(2.0 * np.log(2.0)))
+    y = np.exp(-0.5 * (x / sig) ** 2)
+    y /= y.sum() * step
+    return x, y
+
+
+def kat(refdir):
+    t = os.path.join(refdir, "test")
+    gold = np.loadtxt(os.path.join(t, "synthesis_results.per"))
+    _, dims, sl = read_fits_f32(os.path.join(t, "straylight.fits"))
+    offs, lam = grid(-600.0, 25.0, 600.0, 6173.3356)
+    model = np.array([14.0, 1200.0, 0.5, 0.07, 0.05, 130.0, 25.0, 0.2, 0.75, 0.0, 0.85])
+    return dict(lam=lam, offs=offs, lambda0=6173.3356, cuantic=TRIPLET, model=model, slight=sl.reshape(4, -1),
+                expected=gold[:, 2:].T.copy(), expected_offsets=gold[:, 1].copy(), nterms=10)
+
+
+def case(cfg, seed, npix=48):
+    rng = np.random.default_rng(1000 + cfg)
+    offs, lam = grid(-350.0, 25.0, 375.0, 6173.3354)
+    psf = None
+    setup0 = po.LineSetup(lam, 6173.3354, TRIPLET, None, 9)
+    if cfg in (1, 2):
+        x, y = gauss_table(60.0)
+        psf = po.Reference(setup0, "f64").interp_psf(x, y, offs, 0.0)
+    K = 10 if cfg == 2 else 9
+    fix = [1] * 9 + [0, 1 if K == 10 else 0]
+    guess = GUESS.copy()
+    if K == 10:
+        guess[10] = 0.9
+    truth = np.zeros((npix, 11))
+    truth[:, 0] = rng.uniform(1, 20, npix)
+    truth[:, 1] = rng.uniform(0, 3000, npix)
+    truth[:, 2] = rng.uniform(-3, 3, npix)
+    truth[:, 3] = rng.uniform(0.02, 0.05, npix)
+    truth[:, 4] = rng.uniform(0.01, 0.5, npix)
+    truth[:, 5] = rng.uniform(0, 180, npix)
+    truth[:, 6] = rng.uniform(0, 180, npix)
+    truth[:, 7] = rng.uniform(0.1, 0.4, npix)
+    truth[:, 8] = rng.uniform(0.4, 0.9, npix)
+    truth[:, 10] = 1.0
+    slight = None
+    if cfg == 2:
+        weak = np.arange(npix) % 10 < 7
+        truth[weak, 1] = rng.uniform(0, 200, weak.sum())
+        truth[weak, 0] = rng.uniform(1, 5, weak.sum())
+        truth[~weak, 1] = rng.uniform(1500, 3500, (~weak).sum())
+        truth[:, 10] = 1.0 - rng.uniform(0, 0.3, npix)
+        r9 = po.Reference(po.LineSetup(lam, 6173.3354, TRIPLET, psf, 9), "f64")
+        slight, _ = r9.synth(np.array([13.0, 0.0, 0.2, 0.035, 0.19, 30.0, 30.0, 0.26, 0.74, 0.0, 1.0]), rf=False)
+        slight = slight.astype(np.float32).astype(np.float64)
+    setup = po.LineSetup(lam, 6173.3354, TRIPLET, psf, K)
+    out = dict(lam=lam, offs=offs, psf=np.zeros(0) if psf is None else psf, truth=truth, guess=guess,
+               fix=np.array(fix, dtype=np.int32), nterms=K, slight=np.zeros(0) if slight is None else slight)
+    ref64 = po.Reference(setup, "f64")
+    obs = np.array([ref64.synth(m, slight, fix=fix, rf=False)[0] for m in truth], dtype=np.float32)
+    obs += rng.normal(0, 1e-3, obs.shape).astype(np.float32)
+    if cfg == 0:  # ghost points: two masked wavelengths in two pixels
+        obs[3, :, 0] = -2.0
+        obs[5, 3, 7] = -1.5
+    out["obs"] = obs
+    for flav in ("f32", "f64"):
+        ref = po.Reference(setup, flav)
+        noise = float(np.float32(np.float32(1.0 / 1000) ** 2)) if flav == "f32" else (1.0 / 1000) ** 2
+        r = ref.invert(obs, guess, slight=slight, fix=fix, noise=noise)
+        for k in ("models", "chisq", "iters", "spectra"):
+            out[f"{flav}_{k}"] = r[k]
+        models = truth[:12].copy()
+        sp, rf = zip(*[ref.synth(m, slight, fix=fix) for m in models])
+        out[f"{flav}_synth_models"] = models
+        out[f"{flav}_synth"] = np.array(sp)
+        out[f"{flav}_rf"] = np.array(rf)
+    return out
+
+
+def psf_pins():
+    ref = po.Reference(po.LineSetup(*grid(-350.0, 25.0, 375.0, 6173.3354)[1:], 6173.3354, TRIPLET, None, 9), "f64")
+    out = {}
+    for name, (ini, step, fin, l0), fw in (("c1", (-350.0, 25.0, 375.0, 6173.3354), 60.0),
+                                          ("c3a", (-172.5, 69.0, 172.5, 6173.3354), 60.0),
+                                          ("c3b", (-350.0, 50.0, 350.0, 6173.3354), 60.0),
+                                          ("c4", (-1204.0, 21.5, 1182.5, 6302.4936), 25.0),
+                                          ("kat", (-600.0, 25.0, 600.0, 6173.3356), 60.0)):
+        offs, lam = grid(ini, step, fin, l0)
+        n = lam.size
+        out[f"{name}_lam"] = lam
+        out[f"{name}_offs"] = offs
+        out[f"{name}_fgauss"] = ref.fgauss_wl(fw, lam[1] - lam[0], lam[0], lam[n // 2], n)
+        x, y = gauss_table(fw)
+        # the milos.c:332-340 re-centring: offset when the zero sample is not nl/2
+        posWL = 0
+        for i in range(n):
+            if posWL:
+                break
+            if abs(np.trunc(offs[i])) == 0:
+                posWL = i
+        offset = 0.0 if posWL == n // 2 else ((n // 2 - posWL) * (step / 1000.0)) * 1000
+        out[f"{name}_table_x"] = x
+        out[f"{name}_table_y"] = y
+        out[f"{name}_interp"] = ref.interp_psf(x, y, offs, offset)
+        out[f"{name}_fwhm"] = fw
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default="/root/reference")
+    a = ap.parse_args()
+    os.environ["PM_REFERENCE_SRC"] = os.path.join(a.reference, "src")
+    po.build()
+    np.savez_compressed(os.path.join(HERE, "kat_synthesis.npz"), **kat(a.reference))
+    cases = {}
+    for cfg in (0, 1, 2):
+        for k, v in case(cfg, cfg).items():
+            cases[f"c{cfg}_{k}"] = v
+    np.savez_compressed(os.path.join(HERE, "ref_cases.npz"), **cases)
+    np.savez_compressed(os.path.join(HERE, "ref_psf.npz"), **psf_pins())
+    for f in ("kat_synthesis.npz", "ref_cases.npz", "ref_psf.npz"):
+        print(f, os.path.getsize(os.path.join(HERE, f)), "bytes")
+
+
+if __name__ == "__main__":
+    main()
