@@ -66,6 +66,7 @@ struct DevBuf {
 struct pm_ctx {
   PmParams P;
   int precision = PM_PREC_FP32;
+  int variant = 0;  // kernel variant (occupancy target), see pmk_invert
   int device = 0;
   int num_sms = 148;
   cudaStream_t stream = nullptr;
@@ -333,6 +334,7 @@ extern "C" int pm_ctx_create(const pm_line* line, const pm_config* cfg, void* st
                 prop.minor);
   }
   c->num_sms = prop.multiProcessorCount;
+  if (const char* v = std::getenv("PMILOS_VARIANT")) c->variant = std::atoi(v);
   rc = c->ctr.ensure(sizeof(unsigned long long) * PMC_COUNT);
   if (rc != PM_OK) {
     delete c;
@@ -358,7 +360,7 @@ namespace {
 // One launch over n pixels whose buffers are all device pointers.
 int run_invert(pm_ctx* c, PmIO io, float* kernel_ms) {
   PM_CUDA(cudaMemsetAsync(io.ctr, 0, sizeof(unsigned long long) * PMC_COUNT, c->stream), "counter reset");
-  int rc = pmk_invert(c->P, io, c->precision, c->stream, c->num_sms, kernel_ms);
+  int rc = pmk_invert(c->P, io, c->precision, c->variant, c->stream, c->num_sms, kernel_ms);
   if (rc != PM_OK) return fail(rc, "%s", pmk_last_cuda_error());
   unsigned long long h[PMC_COUNT];
   PM_CUDA(cudaMemcpyAsync(h, io.ctr, sizeof h, cudaMemcpyDeviceToHost, c->stream), "counter D2H");

@@ -30,6 +30,8 @@
 //   invert_kernel    lm_mils milosUtils.c:466-635 over the pixel loop of milos.c:958-1009
 #include <cuda_runtime.h>
 #include <math.h>
+#include <stddef.h>
+#include <utility>
 #include <stdio.h>
 
 #include "pm_params.h"
@@ -105,8 +107,14 @@ __device__ __forceinline__ void voigt(R a, R v, R& h, R& f) {
   const bool c = fabs(dr) >= fabs(di);
   const R big = c ? dr : di, small = c ? di : dr;
   const R x1 = c ? nr : ni, x2 = c ? ni : nr;
-  const R r = small / big;
-  const R inv = R(1) / (big + small * r);
+  R r, inv;
+  if constexpr (sizeof(R) == 4) {
+    r = __fdividef(small, big);
+    inv = __frcp_rn(big + small * r);
+  } else {
+    r = small / big;
+    inv = R(1) / (big + small * r);
+  }
   const R wr = (x1 + x2 * r) * inv;
   const R wi = (c ? R(1) : R(-1)) * (x2 - x1 * r) * inv;
   h = wr;
@@ -166,16 +174,21 @@ __device__ __forceinline__ void model_terms(const PmParams& P, const double* m, 
   const R LD = R(m[3]), E0 = R(T.E0), l0 = R(P.lambda0);
   T.E0_2 = E0 / R(2);
   T.cosi_E0_2 = T.E0_2 * T.cosi;
-  T.invLD = R(1) / LD;
-  T.ulos = (R(m[2]) * l0) / (R(kVLight) * LD);
-  const R parcial = ((l0 * l0) / LD) * R(kZeeman);
+  if constexpr (f32) {
+    T.invLD = __frcp_rn(LD);
+    T.invE0 = __frcp_rn(E0);
+  } else {
+    T.invLD = R(1) / LD;
+    T.invE0 = R(1) / E0;
+  }
+  T.ulos = (R(m[2]) * l0) * T.invLD * R(1.0 / kVLight);
+  const R parcial = (l0 * l0) * T.invLD * R(kZeeman);
 #pragma unroll
   for (int g = 0; g < 3; ++g) {
     T.zs[g] = parcial * R(P.nu[g][0]);
     T.zsB[g] = T.zs[g] * R(m[1]);
   }
-  T.auxCte = (-l0) / (R(kVLight) * LD);
-  T.invE0 = R(1) / E0;
+  T.auxCte = (-l0) * T.invLD * R(1.0 / kVLight);
   T.sc = E0 * T.sinis_cosa / R(2);
   T.ss = E0 * T.sinis_sina / R(2);
   T.cosi_2_E0 = E0 * T.cosi / R(2);
@@ -240,37 +253,95 @@ __device__ __forceinline__ void synth_lane(const PmParams& P, const ModelTerms<R
   S[3] = dtiaux * s.g6;
 }
 
-// Per-warp shared memory.
+// Shared memory.  Per block: the PSF taps, centred and reversed, in VEC shifted
+// copies so that any 32-tap window can be read with aligned 16-byte broadcast
+// loads.  Per warp: the RF transpose buffer (also scratch for the synthesis
+// correlation, the reduction and the eigen solver), the padded Stokes rows of
+// the synthesis correlation, alpha/beta, the eigen-solver state and the model.
+constexpr int XSR = 100;  // synthesis row length: 3 float4-aligned windows of 36
+
 template <typename R>
-struct WarpSmem {
-  R tr[NL * TRS];      // response functions: [profile][lambda] (transpose buffer)
-  R xs[4][3 * NL];     // padded Stokes rows for the synthesis PSF correlation
+struct alignas(16) BlockSmem {
+  static constexpr int VEC = 16 / sizeof(R);
+  // rv[c][u] = G[31 - (u + c) + half] (0 outside [0, nl)): for input m the
+  // taps of outputs k = 0..31 are rv[c][b + k] with b + c = 31 - m, b % VEC == 0
+  R rv[VEC][64 + VEC];
+};
+
+template <typename R>
+struct alignas(16) WarpSmem {
+  R tr[NL * TRS];       // response functions: [profile][lambda] (transpose buffer)
+  R xs[4][XSR];         // padded Stokes rows for the synthesis PSF correlation
   double ab[PM_NTERMS_MAX * PM_NTERMS_MAX + PM_NTERMS_MAX];  // alpha (K*K) then beta (K)
-  double ev[2][12 * 12];  // eigen solver: A (double-buffered rows reuse ev[1]) and V
+  double ev[2][12 * 12];  // eigen solver: A and V
   double rot[12][3];      // per index: partner, c, signed s
   int pq[6][2];           // the rotated pairs of the current round
   double delta[PM_NTERMS_MAX];
+  double model[11], trial[11];
 };
 
-// PSF correlation of the four synthesized profiles in the lane = wavelength
-// layout: out[k] = sum_j G[j] x[k + j - nl/2] with zero padding; Stokes I
-// correlates Ic - I and returns Ic - result, Ic = max(I[0], I[nl-1])
-// (mil_sinrf.c:387-402, convolution.c:54-121).
+// The 16-byte vector loads of psf_rows and rf_correlate need every per-warp
+// region, every xs row and every rv row to start on a 16-byte boundary.
+template <typename R>
+constexpr bool smem_layout_ok() {
+  return sizeof(BlockSmem<R>) % 16 == 0 && sizeof(WarpSmem<R>) % 16 == 0 &&
+         offsetof(WarpSmem<R>, xs) % 16 == 0 && (XSR * sizeof(R)) % 16 == 0 &&
+         ((64 + BlockSmem<R>::VEC) * sizeof(R)) % 16 == 0;
+}
+static_assert(smem_layout_ok<float>(), "shared-memory layout breaks 16-byte vector loads (float)");
+static_assert(smem_layout_ok<double>(), "shared-memory layout breaks 16-byte vector loads (double)");
+
+template <typename R>
+__device__ __forceinline__ void load_taps(const PmParams& P, BlockSmem<R>& bs) {
+  constexpr int VEC = BlockSmem<R>::VEC;
+  for (int e = threadIdx.x; e < VEC * (64 + VEC); e += blockDim.x) {
+    const int c = e / (64 + VEC), u = e % (64 + VEC);
+    const int t = 62 - (u + c);  // index into the centred table gc[t] = G[t - 31 + half]
+    bs.rv[c][u] = (t >= 0 && t < PMK_GC) ? gcen<R>(P, t) : R(0);
+  }
+}
+
+// PSF correlation of the four synthesized profiles (mil_sinrf.c:387-402,
+// convolution.c:54-121): out[k] = sum_j G[j] x[k + j - nl/2], zero padding;
+// Stokes I correlates Ic - I and returns Ic - result, Ic = max(I[0], I[nl-1]).
+// Lane l computes outputs 4c..4c+3 (c = l & 7) of Stokes l >> 3 from one aligned
+// 36-sample window: 9 vector loads and 128 FMAs whose taps are compile-time
+// indexed constant operands.
 template <typename R>
 __device__ __forceinline__ void psf_rows(const PmParams& P, WarpSmem<R>& sm, int lane, bool valid, R S[4]) {
   const R i0 = __shfl_sync(kFull, S[0], 0), in = __shfl_sync(kFull, S[0], P.nl - 1);
   const R ic = (i0 > in) ? i0 : in;
+  const int off = NL + (P.half & 3);  // data at xs[s][off + i]; off - half is a multiple of 4
 #pragma unroll
-  for (int s = 0; s < 4; ++s) sm.xs[s][NL + lane] = valid ? (s == 0 ? ic - S[0] : S[s]) : R(0);
+  for (int s = 0; s < 4; ++s) sm.xs[s][off + lane] = valid ? (s == 0 ? ic - S[0] : S[s]) : R(0);
   __syncwarp();
-  const int base = NL + lane - P.half;
+  const int st = lane >> 3, c = lane & 7;
+  constexpr int VEC = 16 / sizeof(R);
+  const R* w0 = &sm.xs[st][off + 4 * c - P.half];
+  R w[NL + 4];
 #pragma unroll
-  for (int s = 0; s < 4; ++s) {
-    R acc = 0;
-#pragma unroll
-    for (int j = 0; j < NL; ++j) acc = fma(taps<R>(P, j), sm.xs[s][base + j], acc);
-    S[s] = (s == 0) ? ic - acc : acc;
+  for (int t = 0; t < NL + 4; t += VEC) {
+    if constexpr (VEC == 4) {
+      const float4 q = *reinterpret_cast<const float4*>(w0 + t);
+      w[t] = q.x; w[t + 1] = q.y; w[t + 2] = q.z; w[t + 3] = q.w;
+    } else {
+      const double2 q = *reinterpret_cast<const double2*>(w0 + t);
+      w[t] = q.x; w[t + 1] = q.y;
+    }
   }
+  R acc[4] = {R(0), R(0), R(0), R(0)};
+#pragma unroll
+  for (int j = 0; j < NL; ++j) {
+    const R g = taps<R>(P, j);
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) acc[kk] = fma(g, w[kk + j], acc[kk]);
+  }
+  R* o = sm.tr;  // scratch [4][NL]
+#pragma unroll
+  for (int kk = 0; kk < 4; ++kk) o[st * NL + 4 * c + kk] = (st == 0) ? ic - acc[kk] : acc[kk];
+  __syncwarp();
+#pragma unroll
+  for (int s = 0; s < 4; ++s) S[s] = valid ? o[s * NL + lane] : R(0);
   __syncwarp();
 }
 
@@ -397,29 +468,41 @@ __device__ __forceinline__ void rf_lane(const PmParams& P, const ModelTerms<R>& 
 }
 
 // PSF correlation of the 32 response-function profiles, one profile per lane
-// (me_der.c:471-496).  Lane p loads its whole profile into registers and forms
-// out[k] = sum_m x[m] G[m - k + nl/2]; the tap is a compile-time-indexed read of
-// the centred table in the parameter block, i.e. a constant operand of the FMA.
-// Stokes-I rows correlate Ic - x with Ic = max of the row's end points.
+// (me_der.c:471-496): out[k] = sum_m x[m] G[m - k + nl/2].  A runtime loop over
+// the inputs m keeps the code small: per m one load of x[m] from the lane's own
+// row and the 32 taps of all outputs as aligned broadcast vector loads.  Stokes-I
+// rows correlate Ic - x with Ic = max of the row's end points.
 template <typename R>
-__device__ __forceinline__ void rf_correlate(const PmParams& P, WarpSmem<R>& sm, int lane) {
+__device__ __forceinline__ void rf_correlate(const PmParams& P, const BlockSmem<R>& bs, WarpSmem<R>& sm,
+                                             int lane) {
+  constexpr int VEC = BlockSmem<R>::VEC;
   __syncwarp();
   R* row = sm.tr + lane * TRS;
-  R x[NL];
-#pragma unroll
-  for (int m = 0; m < NL; ++m) x[m] = row[m];
   const bool isI = (lane & 3) == 0;
-  const R e0 = x[0], en = row[P.nl - 1];
+  const R e0 = row[0], en = row[P.nl - 1];
   const R ic = isI ? ((e0 > en) ? e0 : en) : R(0);
-#pragma unroll
-  for (int m = 0; m < NL; ++m) x[m] = (m < P.nl) ? (isI ? ic - x[m] : x[m]) : R(0);
   R acc[NL];
 #pragma unroll
   for (int k = 0; k < NL; ++k) acc[k] = 0;
+#pragma unroll 1
+  for (int m = 0; m < P.nl; ++m) {
+    const R xm = isI ? ic - row[m] : row[m];
+    const int c = (31 - m) & (VEC - 1), b = (31 - m) - c;
+    const R* g = bs.rv[c] + b;
 #pragma unroll
-  for (int m = 0; m < NL; ++m) {
-#pragma unroll
-    for (int k = 0; k < NL; ++k) acc[k] = fma(x[m], gcen<R>(P, m - k + (NL - 1)), acc[k]);
+    for (int k = 0; k < NL; k += VEC) {
+      if constexpr (VEC == 4) {
+        const float4 q = *reinterpret_cast<const float4*>(g + k);
+        acc[k] = fma(xm, q.x, acc[k]);
+        acc[k + 1] = fma(xm, q.y, acc[k + 1]);
+        acc[k + 2] = fma(xm, q.z, acc[k + 2]);
+        acc[k + 3] = fma(xm, q.w, acc[k + 3]);
+      } else {
+        const double2 q = *reinterpret_cast<const double2*>(g + k);
+        acc[k] = fma(xm, q.x, acc[k]);
+        acc[k + 1] = fma(xm, q.y, acc[k + 1]);
+      }
+    }
   }
 #pragma unroll
   for (int k = 0; k < NL; ++k) row[k] = isI ? ic - acc[k] : acc[k];
@@ -427,22 +510,26 @@ __device__ __forceinline__ void rf_correlate(const PmParams& P, WarpSmem<R>& sm,
 }
 
 // Reduce N values held by every lane across the warp; afterwards lane l holds
-// the totals of entries [l*N/32, (l+1)*N/32) in v[0 .. N/32).  Recursive halving:
-// 31*N/32 shuffles in total.
+// the totals of entries [l*N/32, (l+1)*N/32) in v[0 .. N/32).  Recursive halving
+// (31*N/32 shuffles); one template instance per stage keeps every index into v
+// a compile-time constant, so v stays in registers.
+template <typename T, int N, int O>
+__device__ __forceinline__ void treduce_stage(T (&v)[N], int lane) {
+  constexpr int half = (N * O) / 32;
+  const bool up = (lane & O) != 0;
+#pragma unroll
+  for (int i = 0; i < half; ++i) {
+    const T send = up ? v[i] : v[i + half];
+    const T keep = up ? v[i + half] : v[i];
+    v[i] = keep + __shfl_xor_sync(kFull, send, O);
+  }
+  if constexpr (O > 1) treduce_stage<T, N, O / 2>(v, lane);
+}
+
 template <typename T, int N>
 __device__ __forceinline__ void transpose_reduce(T (&v)[N], int lane) {
   static_assert(N % 32 == 0, "N must be a multiple of 32");
-#pragma unroll
-  for (int o = 16, len = N; o > 0; o >>= 1, len >>= 1) {
-    const bool up = (lane & o) != 0;
-    const int half = len / 2;
-#pragma unroll
-    for (int i = 0; i < half; ++i) {
-      const T send = up ? v[i] : v[i + half];
-      const T keep = up ? v[i + half] : v[i];
-      v[i] = keep + __shfl_xor_sync(kFull, send, o);
-    }
-  }
+  treduce_stage<T, N, 16>(v, lane);
 }
 
 // Response functions at this lane's wavelength after correlation, filling factor
@@ -482,46 +569,75 @@ __device__ __forceinline__ void gather_rf(const PmParams& P, const WarpSmem<R>& 
   }
 }
 
+// Entry e of the packed normal-equation vector: the upper triangle of alpha row
+// by row (a <= b), then beta.  Constant-folded inside unrolled loops.
+__host__ __device__ constexpr int ne_row(int e, int K) {
+  int a = 0;
+  while (a < K && e >= K - a) { e -= K - a; ++a; }
+  return a;  // == K for the beta part
+}
+__host__ __device__ constexpr int ne_col(int e, int K) {
+  int a = 0;
+  while (a < K && e >= K - a) { e -= K - a; ++a; }
+  return a < K ? a + e : e;
+}
+
+// One packed entry with compile-time (a, b): an alpha product or a beta term.
+template <typename R, int KT, int E>
+__device__ __forceinline__ R ne_entry(const R (&d)[KT][4], const R (&cw)[4], const R (&rw)[4]) {
+  constexpr int NT = KT * (KT + 1) / 2 + KT;
+  if constexpr (E >= NT) {
+    return R(0);
+  } else {
+    constexpr int a = ne_row(E, KT), b = ne_col(E, KT);
+    R acc = 0;
+    if constexpr (a < KT) {
+#pragma unroll
+      for (int s = 0; s < 4; ++s) acc = fma(d[a][s] * d[b][s], cw[s], acc);
+    } else {
+#pragma unroll
+      for (int s = 0; s < 4; ++s) acc = fma(rw[s], d[b][s], acc);
+    }
+    return acc;
+  }
+}
+
+template <typename R, int KT, int CH, int... I>
+__device__ __forceinline__ void ne_chunk(R (&v)[32], const R (&d)[KT][4], const R (&cw)[4], const R (&rw)[4],
+                                         std::integer_sequence<int, I...>) {
+  ((v[I] = ne_entry<R, KT, CH * 32 + I>(d, cw, rw)), ...);
+}
+
+template <typename R, int KT, int CH>
+__device__ __forceinline__ void ne_reduce_chunk(double* red, int lane, const R (&d)[KT][4], const R (&cw)[4],
+                                                const R (&rw)[4]) {
+  R v[32];
+  ne_chunk<R, KT, CH>(v, d, cw, rw, std::make_integer_sequence<int, 32>{});
+  transpose_reduce<R, 32>(v, lane);
+  red[CH * 32 + lane] = double(v[0]);
+}
+
 // Normal equations (covarm2): alpha = sum w_s/sigma^2 d_a d_b (upper triangle),
-// beta = sum w_s (S - O)/sigma^2 d_b, reduced over the warp and stored in FP64.
+// beta = sum w_s (S - O)/sigma^2 d_b, reduced over the warp in chunks of 32
+// entries (31 shuffles each) and stored in FP64.
 template <typename R, int KT>
 __device__ __forceinline__ void normal_eq(const PmParams& P, WarpSmem<R>& sm, int lane, const R (&d)[KT][4],
                                           const R S[4], const float O[4], const R isig[4]) {
   constexpr int NA = KT * (KT + 1) / 2;
-  constexpr int NV = ((NA + KT + 31) / 32) * 32;
-  R v[NV];
-#pragma unroll
-  for (int i = 0; i < NV; ++i) v[i] = 0;
+  constexpr int NT = NA + KT;
+  constexpr int NCH = (NT + 31) / 32;
+  static_assert(NCH <= 3, "at most 96 packed entries");
   R cw[4], rw[4];
 #pragma unroll
   for (int s = 0; s < 4; ++s) {
     cw[s] = R(P.w[s]) * isig[s];
     rw[s] = R(P.w[s]) * (S[s] - R(O[s])) * isig[s];
   }
-  int idx = 0;
-#pragma unroll
-  for (int a = 0; a < KT; ++a) {
-#pragma unroll
-    for (int b = a; b < KT; ++b) {
-      R acc = 0;
-#pragma unroll
-      for (int s = 0; s < 4; ++s) acc = fma(d[a][s] * d[b][s], cw[s], acc);
-      v[idx++] = acc;
-    }
-  }
-#pragma unroll
-  for (int b = 0; b < KT; ++b) {
-    R acc = 0;
-#pragma unroll
-    for (int s = 0; s < 4; ++s) acc = fma(rw[s], d[b][s], acc);
-    v[NA + b] = acc;
-  }
-  transpose_reduce<R, NV>(v, lane);
-  constexpr int M = NV / 32;
-  double* red = reinterpret_cast<double*>(sm.tr);  // scratch: the RFs are consumed
+  double* red = reinterpret_cast<double*>(sm.tr);  // scratch: the RFs are in registers now
   __syncwarp();
-#pragma unroll
-  for (int i = 0; i < M; ++i) red[lane * M + i] = double(v[i]);
+  ne_reduce_chunk<R, KT, 0>(red, lane, d, cw, rw);
+  if constexpr (NCH > 1) ne_reduce_chunk<R, KT, 1>(red, lane, d, cw, rw);
+  if constexpr (NCH > 2) ne_reduce_chunk<R, KT, 2>(red, lane, d, cw, rw);
   __syncwarp();
   // unpack: full symmetric alpha (K x K) and beta
   for (int e = lane; e < KT * KT + KT; e += 32) {
@@ -529,8 +645,7 @@ __device__ __forceinline__ void normal_eq(const PmParams& P, WarpSmem<R>& sm, in
     if (e < KT * KT) {
       int a = e / KT, b = e % KT;
       if (a > b) { int t = a; a = b; b = t; }
-      const int u = a * KT - (a * (a - 1)) / 2 + (b - a);
-      val = red[u];
+      val = red[a * KT - (a * (a - 1)) / 2 + (b - a)];
     } else {
       val = red[NA + (e - KT * KT)];
     }
@@ -561,7 +676,7 @@ __device__ __forceinline__ double chisq(const PmParams& P, const R S[4], const f
 // the absolute 1e-12 eigenvalue cut of mil_svd.  Warp-cooperative; every lane
 // returns delta.
 template <typename R, int KT>
-__device__ void solve_eigen(const PmParams& P, WarpSmem<R>& sm, int lane, double flambda, double (&delta)[KT]) {
+__device__ __noinline__ void solve_eigen(const PmParams& P, WarpSmem<R>& sm, int lane, double flambda) {
   constexpr int M = (KT + 1) & ~1;  // padded to even; index KT (if any) is a dummy
   double* A = sm.ev[0];
   double* V = sm.ev[1];
@@ -654,58 +769,59 @@ __device__ void solve_eigen(const PmParams& P, WarpSmem<R>& sm, int lane, double
     sm.delta[lane] = sum;
   }
   __syncwarp();
-#pragma unroll
-  for (int i = 0; i < KT; ++i) delta[i] = sm.delta[i];
-  __syncwarp();
 }
 
 // FP64 Cholesky, computed redundantly by every lane in registers (the matrix is
-// uniform across the warp).  Exactly-zero rows (fixed parameters) get a zero step
-// like the pseudo-inverse would give them.  Returns false on a pivot <= 1e-12.
+// uniform across the warp).  Division-free: one reciprocal square root per pivot,
+// reused by both triangular solves.  Exactly-zero rows (fixed parameters) get a
+// zero step, as the pseudo-inverse gives them.  Returns false on a pivot <= 1e-12
+// (the caller then uses the eigen solver for this step).
 template <typename R, int KT>
-__device__ bool solve_cholesky(WarpSmem<R>& sm, double flambda, double (&delta)[KT]) {
-  double L[KT][KT];
-  bool zr[KT];
+__device__ __forceinline__ bool solve_cholesky(WarpSmem<R>& sm, double flambda, double (&delta)[KT]) {
+  constexpr int NL_ = KT * (KT + 1) / 2;
+  double L[NL_];
+  double rinv[KT];
+  unsigned zr = 0;
 #pragma unroll
   for (int i = 0; i < KT; ++i) {
-    zr[i] = sm.ab[i * KT + i] == 0.0;
 #pragma unroll
-    for (int j = 0; j <= i; ++j) L[i][j] = sm.ab[i * KT + j];
-    L[i][i] *= (1.0 + flambda);
+    for (int j = 0; j <= i; ++j) L[i * (i + 1) / 2 + j] = sm.ab[i * KT + j];
+    if (L[i * (i + 1) / 2 + i] == 0.0) zr |= 1u << i;
+    L[i * (i + 1) / 2 + i] *= (1.0 + flambda);
   }
   bool ok = true;
 #pragma unroll
   for (int j = 0; j < KT; ++j) {
-    double d = L[j][j];
+    double dj = L[j * (j + 1) / 2 + j];
 #pragma unroll
-    for (int k = 0; k < j; ++k) d -= L[j][k] * L[j][k];
-    const bool skip = zr[j];
-    ok = ok && (skip || (d > 1e-12 && isfinite(d)));
-    const double rinv = skip ? 0.0 : rsqrt(d);
-    L[j][j] = skip ? 1.0 : d * rinv;
+    for (int k = 0; k < j; ++k) dj -= L[j * (j + 1) / 2 + k] * L[j * (j + 1) / 2 + k];
+    const bool skip = (zr >> j) & 1u;
+    ok = ok && (skip || (dj > 1e-12 && dj < 1e300));
+    const double r = skip ? 0.0 : rsqrt(dj);
+    rinv[j] = r;
 #pragma unroll
     for (int i = j + 1; i < KT; ++i) {
-      double a = L[i][j];
+      double a = L[i * (i + 1) / 2 + j];
 #pragma unroll
-      for (int k = 0; k < j; ++k) a -= L[i][k] * L[j][k];
-      L[i][j] = a * rinv;
+      for (int k = 0; k < j; ++k) a -= L[i * (i + 1) / 2 + k] * L[j * (j + 1) / 2 + k];
+      L[i * (i + 1) / 2 + j] = a * r;
     }
   }
   const double* beta = sm.ab + KT * KT;
   double y[KT];
 #pragma unroll
   for (int j = 0; j < KT; ++j) {
-    double a = zr[j] ? 0.0 : beta[j];
+    double a = beta[j];
 #pragma unroll
-    for (int k = 0; k < j; ++k) a -= L[j][k] * y[k];
-    y[j] = a / L[j][j];
+    for (int k = 0; k < j; ++k) a -= L[j * (j + 1) / 2 + k] * y[k];
+    y[j] = a * rinv[j];
   }
 #pragma unroll
   for (int j = KT - 1; j >= 0; --j) {
     double a = y[j];
 #pragma unroll
-    for (int k = j + 1; k < KT; ++k) a -= L[k][j] * delta[k];
-    delta[j] = zr[j] ? 0.0 : a / L[j][j];
+    for (int k = j + 1; k < KT; ++k) a -= L[k * (k + 1) / 2 + j] * delta[k];
+    delta[j] = a * rinv[j];
   }
   return ok;
 }
@@ -822,12 +938,12 @@ __device__ void classical(const PmParams& P, const float O[4], int lane, bool va
 
 // Response functions at the current synthesis -> alpha, beta in shared memory.
 template <typename R, int KT>
-__device__ __forceinline__ void rf_and_normal_eq(const PmParams& P, WarpSmem<R>& sm, int lane, bool valid,
-                                                 const ModelTerms<R>& T, const LaneState<R>& st, const R S[4],
-                                                 const R Sff[4], const float O[4], const R isig[4],
-                                                 const float* sl_pix) {
+__device__ __forceinline__ void rf_and_normal_eq(const PmParams& P, const BlockSmem<R>& bs, WarpSmem<R>& sm,
+                                                 int lane, bool valid, const ModelTerms<R>& T,
+                                                 const LaneState<R>& st, const R S[4], const R Sff[4],
+                                                 const float O[4], const R isig[4], const float* sl_pix) {
   rf_lane<R>(P, T, st, sm, lane, valid);
-  if (P.has_psf) rf_correlate<R>(P, sm, lane);
+  if (P.has_psf) rf_correlate<R>(P, bs, sm, lane);
   __syncwarp();
   R d[KT][4];
   gather_rf<R, KT>(P, sm, lane, valid, T, Sff, sl_pix, d);
@@ -844,15 +960,23 @@ __device__ __forceinline__ void rf_and_normal_eq(const PmParams& P, WarpSmem<R>&
 // Inversion kernel: persistent warps over an atomic pixel queue; lm_mils per
 // pixel (milosUtils.c:466-635).
 // ---------------------------------------------------------------------------
-template <typename R, int KT>
-__global__ void __launch_bounds__(128) invert_kernel(const __grid_constant__ PmParams P, const PmIO io) {
+template <typename R>
+__device__ __forceinline__ WarpSmem<R>& warp_smem(unsigned char* raw, int warp) {
+  return reinterpret_cast<WarpSmem<R>*>(raw + sizeof(BlockSmem<R>))[warp];
+}
+
+template <typename R, int KT, int MINB>
+__global__ void __launch_bounds__(128, MINB) invert_kernel(const __grid_constant__ PmParams P, const PmIO io) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  WarpSmem<R>& sm = reinterpret_cast<WarpSmem<R>*>(smem_raw)[warp];
-  for (int e = lane; e < 4 * 3 * NL; e += 32) (&sm.xs[0][0])[e] = R(0);
-  __syncwarp();
+  BlockSmem<R>& bs = *reinterpret_cast<BlockSmem<R>*>(smem_raw);
+  WarpSmem<R>& sm = warp_smem<R>(smem_raw, warp);
+  load_taps<R>(P, bs);
+  for (int e = lane; e < 4 * XSR; e += 32) (&sm.xs[0][0])[e] = R(0);
+  __syncthreads();
   const bool valid = lane < P.nl;
-  const int li = valid ? lane : 0;
+  double* m = sm.model;
+  double* trial = sm.trial;
 
   while (true) {
     unsigned long long pix = 0;
@@ -872,42 +996,65 @@ __global__ void __launch_bounds__(128) invert_kernel(const __grid_constant__ PmP
       ghosts += __popc(__ballot_sync(kFull, g));
       isig[s] = R(1.0 / (g ? kGhostSigma : P.noise));
     }
-    double m[11];
+    {
+      double g[11];
 #pragma unroll
-    for (int i = 0; i < 11; ++i) m[i] = P.guess[i];
-    if (P.classical) classical(P, O, lane, valid, m);
+      for (int i = 0; i < 11; ++i) g[i] = P.guess[i];
+      if (P.classical) classical(P, O, lane, valid, g);
+      __syncwarp();
+      if (lane < 11) m[lane] = g[lane];
+      __syncwarp();
+    }
 
     const int nfree = P.nfree_base - ghosts;
     int status = PM_PIX_MAXITER, iter = 0, accepted = 0, fallbacks = 0;
     double ochi = 0;
-    ModelTerms<R> T;
-    LaneState<R> st;
-    R S[4], Su[4];
+    R S[4];
     if (nfree == 0) {
       status = PM_PIX_NFREE;
       iter = -1;
 #pragma unroll
       for (int s = 0; s < 4; ++s) S[s] = 0;
     } else {
-      synthesize<R>(P, sm, m, sl_pix, lane, valid, T, st, S, Su);
-      rf_and_normal_eq<R, KT>(P, sm, lane, valid, T, st, S, Su, O, isig, sl_pix);
+      {
+        ModelTerms<R> T;
+        LaneState<R> st;
+        R Su[4];
+        synthesize<R>(P, sm, m, sl_pix, lane, valid, T, st, S, Su);
+        rf_and_normal_eq<R, KT>(P, bs, sm, lane, valid, T, st, S, Su, O, isig, sl_pix);
+      }
       ochi = chisq<R>(P, S, O, isig, valid, double(nfree));
       const double chi0 = ochi;
       double flambda = P.ilambda, factor = 1.0;
-      double trial[11];
-#pragma unroll
-      for (int i = 0; i < 11; ++i) trial[i] = m[i];
+      if (lane < 11) trial[lane] = m[lane];
+      __syncwarp();
       bool stop = false;
       do {
-        double dlt[KT];
-        bool ok = true;
-        if (P.solver == PM_SOLVE_CHOLESKY) ok = solve_cholesky<R, KT>(sm, flambda, dlt);
-        if (P.solver != PM_SOLVE_CHOLESKY || !ok) {
-          if (P.solver == PM_SOLVE_CHOLESKY) ++fallbacks;
-          solve_eigen<R, KT>(P, sm, lane, flambda, dlt);
+        {
+          double dlt[KT];
+          bool ok = true;
+          if (P.solver == PM_SOLVE_CHOLESKY) ok = solve_cholesky<R, KT>(sm, flambda, dlt);
+          if (P.solver != PM_SOLVE_CHOLESKY || !ok) {
+            if (P.solver == PM_SOLVE_CHOLESKY) ++fallbacks;
+            solve_eigen<R, KT>(P, sm, lane, flambda);  // step in sm.delta
+#pragma unroll
+            for (int i = 0; i < KT; ++i) dlt[i] = sm.delta[i];
+            __syncwarp();
+          }
+          if (lane == 0) {
+            double t[11];
+#pragma unroll
+            for (int i = 0; i < 11; ++i) t[i] = trial[i];
+            apply_delta<KT>(P, m, dlt, t);
+            check_model(t);
+#pragma unroll
+            for (int i = 0; i < 11; ++i) trial[i] = t[i];
+          }
+          __syncwarp();
         }
-        apply_delta<KT>(P, m, dlt, trial);
-        check_model(trial);
+        ModelTerms<R> T;
+        LaneState<R> st;
+        R Su[4];
         synthesize<R>(P, sm, trial, sl_pix, lane, valid, T, st, S, Su);
         const double chi = chisq<R>(P, S, O, isig, valid, double(nfree));
         if ((fabs((ochi - chi) * 100 / chi) < P.toplim) || (chi < 0.0001)) {
@@ -916,9 +1063,9 @@ __global__ void __launch_bounds__(128) invert_kernel(const __grid_constant__ PmP
         }
         if (chi - ochi < 0.) {
           flambda = flambda / (5.0 * factor);
-#pragma unroll
-          for (int i = 0; i < 11; ++i) m[i] = trial[i];
-          rf_and_normal_eq<R, KT>(P, sm, lane, valid, T, st, S, S, O, isig, sl_pix);
+          if (lane < 11) m[lane] = trial[lane];
+          __syncwarp();
+          rf_and_normal_eq<R, KT>(P, bs, sm, lane, valid, T, st, S, S, O, isig, sl_pix);
           ochi = chi;
           ++accepted;
         } else {
@@ -950,7 +1097,7 @@ __global__ void __launch_bounds__(128) invert_kernel(const __grid_constant__ PmP
 #pragma unroll
       for (int s = 0; s < 4; ++s) io.spectra_out[base + s * P.nl + lane] = float(S[s]);
     }
-    (void)li;
+    __syncwarp();
   }
 }
 
@@ -960,28 +1107,29 @@ template <typename R, int KT>
 __global__ void __launch_bounds__(128) synth_kernel(const __grid_constant__ PmParams P, const PmIO io) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  WarpSmem<R>& sm = reinterpret_cast<WarpSmem<R>*>(smem_raw)[warp];
-  for (int e = lane; e < 4 * 3 * NL; e += 32) (&sm.xs[0][0])[e] = R(0);
-  __syncwarp();
+  BlockSmem<R>& bs = *reinterpret_cast<BlockSmem<R>*>(smem_raw);
+  WarpSmem<R>& sm = warp_smem<R>(smem_raw, warp);
+  load_taps<R>(P, bs);
+  for (int e = lane; e < 4 * XSR; e += 32) (&sm.xs[0][0])[e] = R(0);
+  __syncthreads();
   const bool valid = lane < P.nl;
   const int64_t nwarps = int64_t(gridDim.x) * (blockDim.x >> 5);
   for (int64_t pix = int64_t(blockIdx.x) * (blockDim.x >> 5) + warp; pix < io.npix; pix += nwarps) {
     const size_t base = size_t(pix) * 4 * P.nl;
     const float* sl_pix = (P.slight_mode == PM_SLIGHT_PER_PIXEL) ? io.slight + base : nullptr;
-    double m[11];
-#pragma unroll
-    for (int i = 0; i < 11; ++i) m[i] = io.models_in[size_t(pix) * 11 + i];
+    if (lane < 11) sm.model[lane] = io.models_in[size_t(pix) * 11 + lane];
+    __syncwarp();
     ModelTerms<R> T;
     LaneState<R> st;
     R S[4], Su[4];
-    synthesize<R>(P, sm, m, sl_pix, lane, valid, T, st, S, Su);
+    synthesize<R>(P, sm, sm.model, sl_pix, lane, valid, T, st, S, Su);
     if (valid) {
 #pragma unroll
       for (int s = 0; s < 4; ++s) io.spectra_out[base + s * P.nl + lane] = float(S[s]);
     }
     if (io.rf_out) {
       rf_lane<R>(P, T, st, sm, lane, valid);
-      if (P.has_psf) rf_correlate<R>(P, sm, lane);
+      if (P.has_psf) rf_correlate<R>(P, bs, sm, lane);
       __syncwarp();
       R d[KT][4];
       gather_rf<R, KT>(P, sm, lane, valid, T, Su, sl_pix, d);
@@ -994,16 +1142,17 @@ __global__ void __launch_bounds__(128) synth_kernel(const __grid_constant__ PmPa
           for (int r = 0; r < KT; ++r) io.rf_out[rb + (size_t(s) * KT + r) * P.nl + lane] = float(d[r][s]);
       }
     }
+    __syncwarp();
   }
 }
 
 char g_err[256];
 
-template <typename R, int KT>
+template <typename R, int KT, int MINB>
 int launch_invert(const PmParams& P, const PmIO& io, cudaStream_t st, int num_sms, float* kernel_ms) {
   const int threads = 128;
-  const size_t smem = sizeof(WarpSmem<R>) * (threads / 32);
-  auto kern = invert_kernel<R, KT>;
+  const size_t smem = sizeof(BlockSmem<R>) + sizeof(WarpSmem<R>) * (threads / 32);
+  auto kern = invert_kernel<R, KT, MINB>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return snprintf(g_err, sizeof g_err, "%s", cudaGetErrorString(e)), PM_EIO;
   int per_sm = 0;
@@ -1034,7 +1183,7 @@ int launch_invert(const PmParams& P, const PmIO& io, cudaStream_t st, int num_sm
 template <typename R, int KT>
 int launch_synth(const PmParams& P, const PmIO& io, cudaStream_t st) {
   const int threads = 128;
-  const size_t smem = sizeof(WarpSmem<R>) * (threads / 32);
+  const size_t smem = sizeof(BlockSmem<R>) + sizeof(WarpSmem<R>) * (threads / 32);
   auto kern = synth_kernel<R, KT>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return snprintf(g_err, sizeof g_err, "%s", cudaGetErrorString(e)), PM_EIO;
@@ -1049,14 +1198,21 @@ int launch_synth(const PmParams& P, const PmIO& io, cudaStream_t st) {
 
 }  // namespace
 
-int pmk_invert(const PmParams& P, const PmIO& io, int precision, void* stream, int num_sms, float* kernel_ms) {
+// variant: occupancy target of the FP32 kernel (register cap): 0 = 3 blocks
+// (168 registers, no spills), 1 = 4 blocks (128 registers, small spills).
+int pmk_invert(const PmParams& P, const PmIO& io, int precision, int variant, void* stream, int num_sms,
+               float* kernel_ms) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (precision == PM_PREC_FP32) {
-    if (P.K == 9) return launch_invert<float, 9>(P, io, st, num_sms, kernel_ms);
-    if (P.K == 10) return launch_invert<float, 10>(P, io, st, num_sms, kernel_ms);
+    if (P.K == 9)
+      return variant == 1 ? launch_invert<float, 9, 4>(P, io, st, num_sms, kernel_ms)
+                          : launch_invert<float, 9, 3>(P, io, st, num_sms, kernel_ms);
+    if (P.K == 10)
+      return variant == 1 ? launch_invert<float, 10, 4>(P, io, st, num_sms, kernel_ms)
+                          : launch_invert<float, 10, 3>(P, io, st, num_sms, kernel_ms);
   } else {
-    if (P.K == 9) return launch_invert<double, 9>(P, io, st, num_sms, kernel_ms);
-    if (P.K == 10) return launch_invert<double, 10>(P, io, st, num_sms, kernel_ms);
+    if (P.K == 9) return launch_invert<double, 9, 1>(P, io, st, num_sms, kernel_ms);
+    if (P.K == 10) return launch_invert<double, 10, 1>(P, io, st, num_sms, kernel_ms);
   }
   snprintf(g_err, sizeof g_err, "nterms=%d has no compiled kernel", P.K);
   return PM_ENOTSUP;

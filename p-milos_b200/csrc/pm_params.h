@@ -68,6 +68,7 @@ struct PmIO {
 enum PmVariant { PMV_FP64 = 0, PMV_FP32 = 1 };
 
 // Host-side launchers (pm_kernels.cu).
-int pmk_invert(const PmParams& P, const PmIO& io, int precision, void* stream, int num_sms, float* kernel_ms);
+int pmk_invert(const PmParams& P, const PmIO& io, int precision, int variant, void* stream, int num_sms,
+               float* kernel_ms);
 int pmk_synth(const PmParams& P, const PmIO& io, int precision, void* stream);
 const char* pmk_last_cuda_error();

