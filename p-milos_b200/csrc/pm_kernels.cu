@@ -46,6 +46,7 @@ constexpr double kZeeman = 4.6686411e-13;
 constexpr double kRsqrtPi = 0.5641895836;
 constexpr double kGhostSigma = 1e21;
 constexpr unsigned kFull = 0xffffffffu;
+constexpr int kLaneStateWords = 35;  // words of LaneState (synthesis state kept for the RFs)
 
 // Hui, Armstrong & Wray (1978) rational approximation of w(z), z = a - i v:
 // numerator degree 6, monic denominator degree 7 (published coefficients).
@@ -204,6 +205,9 @@ struct LaneState {
   R etai, etai_2, gp1, gp2, gp3, dt, dti, g4, g5, g6;
 };
 
+static_assert(sizeof(LaneState<float>) == kLaneStateWords * sizeof(float), "LaneState layout");
+static_assert(sizeof(LaneState<double>) == kLaneStateWords * sizeof(double), "LaneState layout");
+
 // ME synthesis at wavelength offset dl (mil_sinrf.c:117-285): the three Zeeman
 // groups, the propagation matrix, and the Unno-Rachkovsky solution.
 template <typename R>
@@ -273,7 +277,8 @@ struct alignas(16) WarpSmem {
   R tr[NL * TRS];       // response functions: [profile][lambda] (transpose buffer)
   R xs[4][XSR];         // padded Stokes rows for the synthesis PSF correlation
   double ab[PM_NTERMS_MAX * PM_NTERMS_MAX + PM_NTERMS_MAX];  // alpha (K*K) then beta (K)
-  double ev[2][12 * 12];  // eigen solver: A and V
+  R ls[kLaneStateWords][NL];  // synthesis state the response functions need, per lane
+  ModelTerms<R> mt;           // per-model terms of the last synthesis (uniform)
   double rot[12][3];      // per index: partner, c, signed s
   int pq[6][2];           // the rotated pairs of the current round
   double delta[PM_NTERMS_MAX];
@@ -347,12 +352,21 @@ __device__ __forceinline__ void psf_rows(const PmParams& P, WarpSmem<R>& sm, int
 
 // Synthesis of the model at this lane's wavelength, PSF and stray light included.
 // S gets the final (mixed) profile, Su the profile before the stray-light mix.
+// The per-model terms and this lane's synthesis state are left in shared memory
+// for the response functions, as the reference leaves them in globals.
 template <typename R>
 __device__ __forceinline__ void synthesize(const PmParams& P, WarpSmem<R>& sm, const double* m,
-                                           const float* sl_pix, int lane, bool valid, ModelTerms<R>& T,
-                                           LaneState<R>& st, R S[4], R Su[4]) {
+                                           const float* sl_pix, int lane, bool valid, R S[4], R Su[4]) {
+  ModelTerms<R> T;
+  LaneState<R> st;
   model_terms<R>(P, m, T);
   synth_lane<R>(P, T, P.dl[valid ? lane : 0], st, S);
+  {
+    const R* w = reinterpret_cast<const R*>(&st);
+#pragma unroll
+    for (int k = 0; k < kLaneStateWords; ++k) sm.ls[k][lane] = w[k];
+  }
+  if (lane == 0) sm.mt = T;
   if (P.has_psf) psf_rows<R>(P, sm, lane, valid, S);
 #pragma unroll
   for (int s = 0; s < 4; ++s) Su[s] = S[s];
@@ -364,6 +378,14 @@ __device__ __forceinline__ void synthesize(const PmParams& P, WarpSmem<R>& sm, c
       S[s] = S[s] * T.alf + slv * T.oma;
     }
   }
+  __syncwarp();
+}
+
+template <typename R>
+__device__ __forceinline__ void load_lane_state(const WarpSmem<R>& sm, int lane, LaneState<R>& st) {
+  R* w = reinterpret_cast<R*>(&st);
+#pragma unroll
+  for (int k = 0; k < kLaneStateWords; ++k) w[k] = sm.ls[k][lane];
 }
 
 // Response functions at this lane's wavelength (me_der.c:85-312) written into the
@@ -536,8 +558,7 @@ __device__ __forceinline__ void transpose_reduce(T (&v)[N], int lane) {
 // and FijaACeroDerivadasNoNecesarias: d[row][stokes] for rows 0..K-1.
 template <typename R, int KT>
 __device__ __forceinline__ void gather_rf(const PmParams& P, const WarpSmem<R>& sm, int lane, bool valid,
-                                          const ModelTerms<R>& T, const R Sff[4], const float* sl_pix,
-                                          R (&d)[KT][4]) {
+                                          R alf, const R Sff[4], const float* sl_pix, R (&d)[KT][4]) {
   const R* col = sm.tr + lane;
 #pragma unroll
   for (int r = 0; r < KT; ++r) {
@@ -558,7 +579,7 @@ __device__ __forceinline__ void gather_rf(const PmParams& P, const WarpSmem<R>& 
     for (int r = 0; r < KT; ++r) {
 #pragma unroll
       for (int s = 0; s < 4; ++s) {
-        d[r][s] = d[r][s] * T.alf;
+        d[r][s] = d[r][s] * alf;
         if (r == P.ff_row) {
           const int idx = s * P.nl + (valid ? lane : 0);
           const R slv = P.slight_mode == PM_SLIGHT_SHARED ? slshared<R>(P, idx) : R(sl_pix[idx]);
@@ -678,9 +699,10 @@ __device__ __forceinline__ double chisq(const PmParams& P, const R S[4], const f
 template <typename R, int KT>
 __device__ __noinline__ void solve_eigen(const PmParams& P, WarpSmem<R>& sm, int lane, double flambda) {
   constexpr int M = (KT + 1) & ~1;  // padded to even; index KT (if any) is a dummy
-  double* A = sm.ev[0];
-  double* V = sm.ev[1];
-  double* A2 = reinterpret_cast<double*>(sm.tr);  // second A buffer
+  static_assert(3 * M * M * sizeof(double) <= sizeof(WarpSmem<R>::tr), "eigen scratch exceeds tr");
+  double* A = reinterpret_cast<double*>(sm.tr);  // the transpose buffer is idle during the solve
+  double* V = A + M * M;
+  double* A2 = V + M * M;
   for (int e = lane; e < M * M; e += 32) {
     const int i = e / M, j = e % M;
     double a = 0;
@@ -771,58 +793,72 @@ __device__ __noinline__ void solve_eigen(const PmParams& P, WarpSmem<R>& sm, int
   __syncwarp();
 }
 
-// FP64 Cholesky, computed redundantly by every lane in registers (the matrix is
-// uniform across the warp).  Division-free: one reciprocal square root per pivot,
-// reused by both triangular solves.  Exactly-zero rows (fixed parameters) get a
-// zero step, as the pseudo-inverse gives them.  Returns false on a pivot <= 1e-12
-// (the caller then uses the eigen solver for this step).
+// FP64 Cholesky solve of the damped normal equations, warp-cooperative: lane i
+// owns row i.  Right-looking factorisation: the pivot and the new column of L
+// travel by shuffle, one reciprocal square root per pivot (no divisions); the
+// forward solve is column-oriented (lane i updates its own right-hand side);
+// the back solve reads the factor from shared memory.  Every lane returns the
+// step.  Exactly-zero rows (fixed parameters) get a zero step, as the
+// pseudo-inverse gives them.  Returns false on a pivot <= 1e-12 (the caller
+// then uses the eigen solver for this step).
 template <typename R, int KT>
-__device__ __forceinline__ bool solve_cholesky(WarpSmem<R>& sm, double flambda, double (&delta)[KT]) {
-  constexpr int NL_ = KT * (KT + 1) / 2;
-  double L[NL_];
-  double rinv[KT];
-  unsigned zr = 0;
+__device__ __forceinline__ bool solve_cholesky(WarpSmem<R>& sm, int lane, double flambda, double (&delta)[KT]) {
+  const int i = lane < KT ? lane : KT - 1;
+  const double damp = 1.0 + flambda;
+  double a[KT];
+  bool zdiag = false;
 #pragma unroll
-  for (int i = 0; i < KT; ++i) {
-#pragma unroll
-    for (int j = 0; j <= i; ++j) L[i * (i + 1) / 2 + j] = sm.ab[i * KT + j];
-    if (L[i * (i + 1) / 2 + i] == 0.0) zr |= 1u << i;
-    L[i * (i + 1) / 2 + i] *= (1.0 + flambda);
+  for (int k = 0; k < KT; ++k) {
+    a[k] = sm.ab[i * KT + k];
+    if (k == i) {
+      zdiag = a[k] == 0.0;
+      a[k] *= damp;
+    }
   }
+  const unsigned zr = __ballot_sync(kFull, lane < KT && zdiag);
+  double rinv[KT];
   bool ok = true;
 #pragma unroll
   for (int j = 0; j < KT; ++j) {
-    double dj = L[j * (j + 1) / 2 + j];
-#pragma unroll
-    for (int k = 0; k < j; ++k) dj -= L[j * (j + 1) / 2 + k] * L[j * (j + 1) / 2 + k];
+    const double piv = __shfl_sync(kFull, a[j], j);
     const bool skip = (zr >> j) & 1u;
-    ok = ok && (skip || (dj > 1e-12 && dj < 1e300));
-    const double r = skip ? 0.0 : rsqrt(dj);
+    ok = ok && (skip || (piv > 1e-12 && piv < 1e300));
+    const double r = skip ? 0.0 : rsqrt(piv);
     rinv[j] = r;
+    const double l = a[j] * r;  // L[i][j] for i > j
 #pragma unroll
-    for (int i = j + 1; i < KT; ++i) {
-      double a = L[i * (i + 1) / 2 + j];
-#pragma unroll
-      for (int k = 0; k < j; ++k) a -= L[i * (i + 1) / 2 + k] * L[j * (j + 1) / 2 + k];
-      L[i * (i + 1) / 2 + j] = a * r;
+    for (int k = j + 1; k < KT; ++k) {
+      const double lk = __shfl_sync(kFull, l, k);  // L[k][j]
+      a[k] = fma(-l, lk, a[k]);
     }
+    a[j] = l;
   }
+  // forward: L y = beta (lane i keeps b_i; y is uniform)
   const double* beta = sm.ab + KT * KT;
+  double b = (zr >> i) & 1u ? 0.0 : beta[i];
   double y[KT];
 #pragma unroll
   for (int j = 0; j < KT; ++j) {
-    double a = beta[j];
-#pragma unroll
-    for (int k = 0; k < j; ++k) a -= L[j * (j + 1) / 2 + k] * y[k];
-    y[j] = a * rinv[j];
+    y[j] = __shfl_sync(kFull, b, j) * rinv[j];
+    if (i > j) b = fma(-a[j], y[j], b);
   }
+  // back: L^T x = y, with L^T read from shared memory (L[k][j] at lt[j*KT + k])
+  double* lt = reinterpret_cast<double*>(sm.tr);
+  __syncwarp();
+  if (lane < KT) {
+#pragma unroll
+    for (int j = 0; j < KT; ++j)
+      if (j < i) lt[j * KT + i] = a[j];
+  }
+  __syncwarp();
 #pragma unroll
   for (int j = KT - 1; j >= 0; --j) {
-    double a = y[j];
+    double s = y[j];
 #pragma unroll
-    for (int k = j + 1; k < KT; ++k) a -= L[k * (k + 1) / 2 + j] * delta[k];
-    delta[j] = a * rinv[j];
+    for (int k = j + 1; k < KT; ++k) s = fma(-lt[j * KT + k], delta[k], s);
+    delta[j] = s * rinv[j];
   }
+  __syncwarp();
   return ok;
 }
 
@@ -939,14 +975,20 @@ __device__ void classical(const PmParams& P, const float O[4], int lane, bool va
 // Response functions at the current synthesis -> alpha, beta in shared memory.
 template <typename R, int KT>
 __device__ __forceinline__ void rf_and_normal_eq(const PmParams& P, const BlockSmem<R>& bs, WarpSmem<R>& sm,
-                                                 int lane, bool valid, const ModelTerms<R>& T,
-                                                 const LaneState<R>& st, const R S[4], const R Sff[4],
+                                                 int lane, bool valid, const R S[4], const R Sff[4],
                                                  const float O[4], const R isig[4], const float* sl_pix) {
-  rf_lane<R>(P, T, st, sm, lane, valid);
+  R alf;
+  {
+    const ModelTerms<R> T = sm.mt;
+    LaneState<R> st;
+    load_lane_state<R>(sm, lane, st);
+    rf_lane<R>(P, T, st, sm, lane, valid);
+    alf = T.alf;
+  }
   if (P.has_psf) rf_correlate<R>(P, bs, sm, lane);
   __syncwarp();
   R d[KT][4];
-  gather_rf<R, KT>(P, sm, lane, valid, T, Sff, sl_pix, d);
+  gather_rf<R, KT>(P, sm, lane, valid, alf, Sff, sl_pix, d);
 #pragma unroll
   for (int r = 0; r < KT; ++r)
     if (P.zero_row[r]) {
@@ -956,10 +998,6 @@ __device__ __forceinline__ void rf_and_normal_eq(const PmParams& P, const BlockS
   normal_eq<R, KT>(P, sm, lane, d, S, O, isig);
 }
 
-// ---------------------------------------------------------------------------
-// Inversion kernel: persistent warps over an atomic pixel queue; lm_mils per
-// pixel (milosUtils.c:466-635).
-// ---------------------------------------------------------------------------
 template <typename R>
 __device__ __forceinline__ WarpSmem<R>& warp_smem(unsigned char* raw, int warp) {
   return reinterpret_cast<WarpSmem<R>*>(raw + sizeof(BlockSmem<R>))[warp];
@@ -996,15 +1034,10 @@ __global__ void __launch_bounds__(128, MINB) invert_kernel(const __grid_constant
       ghosts += __popc(__ballot_sync(kFull, g));
       isig[s] = R(1.0 / (g ? kGhostSigma : P.noise));
     }
-    {
-      double g[11];
-#pragma unroll
-      for (int i = 0; i < 11; ++i) g[i] = P.guess[i];
-      if (P.classical) classical(P, O, lane, valid, g);
-      __syncwarp();
-      if (lane < 11) m[lane] = g[lane];
-      __syncwarp();
-    }
+    // initial model: the guess, or the classical estimates the pre-pass kernel
+    // (classical_kernel) left in models_out
+    if (lane < 11) m[lane] = P.classical ? io.models_out[size_t(pix) * 11 + lane] : P.guess[lane];
+    __syncwarp();
 
     const int nfree = P.nfree_base - ghosts;
     int status = PM_PIX_MAXITER, iter = 0, accepted = 0, fallbacks = 0;
@@ -1017,11 +1050,9 @@ __global__ void __launch_bounds__(128, MINB) invert_kernel(const __grid_constant
       for (int s = 0; s < 4; ++s) S[s] = 0;
     } else {
       {
-        ModelTerms<R> T;
-        LaneState<R> st;
         R Su[4];
-        synthesize<R>(P, sm, m, sl_pix, lane, valid, T, st, S, Su);
-        rf_and_normal_eq<R, KT>(P, bs, sm, lane, valid, T, st, S, Su, O, isig, sl_pix);
+        synthesize<R>(P, sm, m, sl_pix, lane, valid, S, Su);
+        rf_and_normal_eq<R, KT>(P, bs, sm, lane, valid, S, Su, O, isig, sl_pix);
       }
       ochi = chisq<R>(P, S, O, isig, valid, double(nfree));
       const double chi0 = ochi;
@@ -1033,7 +1064,7 @@ __global__ void __launch_bounds__(128, MINB) invert_kernel(const __grid_constant
         {
           double dlt[KT];
           bool ok = true;
-          if (P.solver == PM_SOLVE_CHOLESKY) ok = solve_cholesky<R, KT>(sm, flambda, dlt);
+          if (P.solver == PM_SOLVE_CHOLESKY) ok = solve_cholesky<R, KT>(sm, lane, flambda, dlt);
           if (P.solver != PM_SOLVE_CHOLESKY || !ok) {
             if (P.solver == PM_SOLVE_CHOLESKY) ++fallbacks;
             solve_eigen<R, KT>(P, sm, lane, flambda);  // step in sm.delta
@@ -1052,10 +1083,8 @@ __global__ void __launch_bounds__(128, MINB) invert_kernel(const __grid_constant
           }
           __syncwarp();
         }
-        ModelTerms<R> T;
-        LaneState<R> st;
         R Su[4];
-        synthesize<R>(P, sm, trial, sl_pix, lane, valid, T, st, S, Su);
+        synthesize<R>(P, sm, trial, sl_pix, lane, valid, S, Su);
         const double chi = chisq<R>(P, S, O, isig, valid, double(nfree));
         if ((fabs((ochi - chi) * 100 / chi) < P.toplim) || (chi < 0.0001)) {
           stop = true;
@@ -1065,7 +1094,7 @@ __global__ void __launch_bounds__(128, MINB) invert_kernel(const __grid_constant
           flambda = flambda / (5.0 * factor);
           if (lane < 11) m[lane] = trial[lane];
           __syncwarp();
-          rf_and_normal_eq<R, KT>(P, bs, sm, lane, valid, T, st, S, S, O, isig, sl_pix);
+          rf_and_normal_eq<R, KT>(P, bs, sm, lane, valid, S, S, O, isig, sl_pix);
           ochi = chi;
           ++accepted;
         } else {
@@ -1101,6 +1130,27 @@ __global__ void __launch_bounds__(128, MINB) invert_kernel(const __grid_constant
   }
 }
 
+// Classical estimates of every pixel (estimacionesClasicas + the NaN fixes of
+// milos.c:975-983), one warp per pixel, written to models_out as the starting
+// model of invert_kernel.  A separate pass keeps this FP64 transcendental code
+// out of the LM kernel's instruction working set.
+__global__ void __launch_bounds__(256) classical_kernel(const __grid_constant__ PmParams P, const PmIO io) {
+  const int lane = threadIdx.x & 31;
+  const bool valid = lane < P.nl;
+  const int64_t nwarps = int64_t(gridDim.x) * (blockDim.x >> 5);
+  for (int64_t pix = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); pix < io.npix; pix += nwarps) {
+    const size_t base = size_t(pix) * 4 * P.nl;
+    float O[4];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) O[s] = valid ? io.spectro[base + s * P.nl + lane] : 0.0f;
+    double g[11];
+#pragma unroll
+    for (int i = 0; i < 11; ++i) g[i] = P.guess[i];
+    classical(P, O, lane, valid, g);
+    if (lane < 11) io.models_out[size_t(pix) * 11 + lane] = g[lane];
+  }
+}
+
 // Synthesis (and response functions) of given models, one warp per model, as the
 // reference's synthesis mode runs mil_sinrf + me_der (milos.c:601-602).
 template <typename R, int KT>
@@ -1119,20 +1169,25 @@ __global__ void __launch_bounds__(128) synth_kernel(const __grid_constant__ PmPa
     const float* sl_pix = (P.slight_mode == PM_SLIGHT_PER_PIXEL) ? io.slight + base : nullptr;
     if (lane < 11) sm.model[lane] = io.models_in[size_t(pix) * 11 + lane];
     __syncwarp();
-    ModelTerms<R> T;
-    LaneState<R> st;
     R S[4], Su[4];
-    synthesize<R>(P, sm, sm.model, sl_pix, lane, valid, T, st, S, Su);
+    synthesize<R>(P, sm, sm.model, sl_pix, lane, valid, S, Su);
     if (valid) {
 #pragma unroll
       for (int s = 0; s < 4; ++s) io.spectra_out[base + s * P.nl + lane] = float(S[s]);
     }
     if (io.rf_out) {
-      rf_lane<R>(P, T, st, sm, lane, valid);
+      R alf;
+      {
+        const ModelTerms<R> T = sm.mt;
+        LaneState<R> st;
+        load_lane_state<R>(sm, lane, st);
+        rf_lane<R>(P, T, st, sm, lane, valid);
+        alf = T.alf;
+      }
       if (P.has_psf) rf_correlate<R>(P, bs, sm, lane);
       __syncwarp();
       R d[KT][4];
-      gather_rf<R, KT>(P, sm, lane, valid, T, Su, sl_pix, d);
+      gather_rf<R, KT>(P, sm, lane, valid, alf, Su, sl_pix, d);
       __syncwarp();
       if (valid) {
         const size_t rb = size_t(pix) * 4 * KT * P.nl;
@@ -1166,6 +1221,11 @@ int launch_invert(const PmParams& P, const PmIO& io, cudaStream_t st, int num_sm
     cudaEventCreate(&a);
     cudaEventCreate(&b);
     cudaEventRecord(a, st);
+  }
+  if (P.classical) {
+    int64_t cb = (io.npix + 7) / 8;
+    if (cb > int64_t(num_sms) * 16) cb = int64_t(num_sms) * 16;
+    classical_kernel<<<unsigned(cb), 256, 0, st>>>(P, io);
   }
   kern<<<unsigned(blocks), threads, smem, st>>>(P, io);
   e = cudaGetLastError();
