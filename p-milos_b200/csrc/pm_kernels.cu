@@ -47,6 +47,7 @@ constexpr double kRsqrtPi = 0.5641895836;
 constexpr double kGhostSigma = 1e21;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kLaneStateWords = 35;  // words of LaneState (synthesis state kept for the RFs)
+constexpr int kLaneStatePad = 36;    // row stride: 16-byte rows, conflict-free 128-bit access
 
 // Hui, Armstrong & Wray (1978) rational approximation of w(z), z = a - i v:
 // numerator degree 6, monic denominator degree 7 (published coefficients).
@@ -127,7 +128,7 @@ __device__ __forceinline__ void voigt(R a, R v, R& h, R& f) {
 // N_SIG = 1, e.g. Fe I 6173 and 6302, 5P1.0-5D0.0); the host rejects multiplets.
 // The FP32 form evaluates these terms in FP32 as well.
 template <typename R>
-struct ModelTerms {
+struct alignas(16) ModelTerms {
   R sin_gm, cosi, sinis, cosis, cosis_2, sina, cosa, sinda, cosda, sindi, cosdi, sinis_cosa, sinis_sina;
   R E0_2, cosi_E0_2, ulos, invLD, A, alf, oma;
   R zs[3];   // Zeeman splitting per gauss of each group, in Doppler units (nupB/nubB/nurB)
@@ -195,18 +196,29 @@ __device__ __forceinline__ void model_terms(const PmParams& P, const double* m, 
   T.cosi_2_E0 = E0 * T.cosi / R(2);
 }
 
+// Copy a 16-byte-aligned POD in 16-byte units (128-bit shared-memory accesses).
+template <typename T>
+__device__ __forceinline__ void copy16(T& dst, const T& src) {
+  static_assert(sizeof(T) % 16 == 0 && alignof(T) >= 16, "copy16 needs 16-byte units");
+  float4* d = reinterpret_cast<float4*>(&dst);
+  const float4* s = reinterpret_cast<const float4*>(&src);
+#pragma unroll
+  for (int k = 0; k < int(sizeof(T) / 16); ++k) d[k] = s[k];
+}
+
 // Everything the response functions need from the synthesis at one wavelength
 // (the reference keeps it in process globals between mil_sinrf and me_der).
 template <typename R>
-struct LaneState {
+struct alignas(16) LaneState {
   R fi[3], shi[3], uu[3], H[3], F[3];
   R parcial1, parcial2, parcial3;
   R etain, etaq, etau, etav, rhoq, rhou, rhov;
   R etai, etai_2, gp1, gp2, gp3, dt, dti, g4, g5, g6;
+  R pad_;
 };
 
-static_assert(sizeof(LaneState<float>) == kLaneStateWords * sizeof(float), "LaneState layout");
-static_assert(sizeof(LaneState<double>) == kLaneStateWords * sizeof(double), "LaneState layout");
+static_assert(sizeof(LaneState<float>) == kLaneStatePad * sizeof(float), "LaneState layout");
+static_assert(sizeof(LaneState<double>) == kLaneStatePad * sizeof(double), "LaneState layout");
 
 // ME synthesis at wavelength offset dl (mil_sinrf.c:117-285): the three Zeeman
 // groups, the propagation matrix, and the Unno-Rachkovsky solution.
@@ -277,7 +289,7 @@ struct alignas(16) WarpSmem {
   R tr[NL * TRS];       // response functions: [profile][lambda] (transpose buffer)
   R xs[4][XSR];         // padded Stokes rows for the synthesis PSF correlation
   double ab[PM_NTERMS_MAX * PM_NTERMS_MAX + PM_NTERMS_MAX];  // alpha (K*K) then beta (K)
-  R ls[kLaneStateWords][NL];  // synthesis state the response functions need, per lane
+  R ls[NL][kLaneStatePad];    // synthesis state the response functions need, per lane
   ModelTerms<R> mt;           // per-model terms of the last synthesis (uniform)
   double rot[12][3];      // per index: partner, c, signed s
   int pq[6][2];           // the rotated pairs of the current round
@@ -361,12 +373,8 @@ __device__ __forceinline__ void synthesize(const PmParams& P, WarpSmem<R>& sm, c
   LaneState<R> st;
   model_terms<R>(P, m, T);
   synth_lane<R>(P, T, P.dl[valid ? lane : 0], st, S);
-  {
-    const R* w = reinterpret_cast<const R*>(&st);
-#pragma unroll
-    for (int k = 0; k < kLaneStateWords; ++k) sm.ls[k][lane] = w[k];
-  }
-  if (lane == 0) sm.mt = T;
+  copy16(*reinterpret_cast<LaneState<R>*>(sm.ls[lane]), st);
+  if (lane == 0) copy16(sm.mt, T);
   if (P.has_psf) psf_rows<R>(P, sm, lane, valid, S);
 #pragma unroll
   for (int s = 0; s < 4; ++s) Su[s] = S[s];
@@ -383,9 +391,7 @@ __device__ __forceinline__ void synthesize(const PmParams& P, WarpSmem<R>& sm, c
 
 template <typename R>
 __device__ __forceinline__ void load_lane_state(const WarpSmem<R>& sm, int lane, LaneState<R>& st) {
-  R* w = reinterpret_cast<R*>(&st);
-#pragma unroll
-  for (int k = 0; k < kLaneStateWords; ++k) w[k] = sm.ls[k][lane];
+  copy16(st, *reinterpret_cast<const LaneState<R>*>(sm.ls[lane]));
 }
 
 // Response functions at this lane's wavelength (me_der.c:85-312) written into the
@@ -979,7 +985,8 @@ __device__ __forceinline__ void rf_and_normal_eq(const PmParams& P, const BlockS
                                                  const float O[4], const R isig[4], const float* sl_pix) {
   R alf;
   {
-    const ModelTerms<R> T = sm.mt;
+    ModelTerms<R> T;
+    copy16(T, sm.mt);
     LaneState<R> st;
     load_lane_state<R>(sm, lane, st);
     rf_lane<R>(P, T, st, sm, lane, valid);
@@ -1072,15 +1079,16 @@ __global__ void __launch_bounds__(128, MINB) invert_kernel(const __grid_constant
             for (int i = 0; i < KT; ++i) dlt[i] = sm.delta[i];
             __syncwarp();
           }
-          if (lane == 0) {
-            double t[11];
+          // every lane forms the (uniform) trial model; lane i stores parameter i
+          double t[11];
 #pragma unroll
-            for (int i = 0; i < 11; ++i) t[i] = trial[i];
-            apply_delta<KT>(P, m, dlt, t);
-            check_model(t);
+          for (int i = 0; i < 11; ++i) t[i] = trial[i];
+          apply_delta<KT>(P, m, dlt, t);
+          check_model(t);
+          __syncwarp();
 #pragma unroll
-            for (int i = 0; i < 11; ++i) trial[i] = t[i];
-          }
+          for (int i = 0; i < 11; ++i)
+            if (lane == i) trial[i] = t[i];
           __syncwarp();
         }
         R Su[4];
@@ -1178,7 +1186,8 @@ __global__ void __launch_bounds__(128) synth_kernel(const __grid_constant__ PmPa
     if (io.rf_out) {
       R alf;
       {
-        const ModelTerms<R> T = sm.mt;
+        ModelTerms<R> T;
+        copy16(T, sm.mt);
         LaneState<R> st;
         load_lane_state<R>(sm, lane, st);
         rf_lane<R>(P, T, st, sm, lane, valid);
