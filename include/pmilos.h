@@ -193,6 +193,26 @@ int pm_synth_batch(pm_ctx *ctx, int64_t npix, const pm_model *models, const floa
 int pm_lm_mils(pm_ctx *ctx, const float *spectro, pm_model *init_model, float *spectra, float *chisqrf,
                const float *slight, int *iter);
 
+/* Allocation-free form of pm_invert_batch.  It has no counterpart in the
+ * reference.  It is for hosts that keep their cubes in host memory but must not
+ * create GPU allocations themselves or through this library (device memory
+ * reserved up front by another component, allocation-free real-time loops,
+ * memory-accounted services): no context is needed, and the call makes no
+ * cudaMalloc/cudaFree or other allocation.  Inputs and outputs are the caller's
+ * HOST arrays (same meaning as pm_invert_batch with PM_MEM_HOST); all device-side
+ * staging and the work-queue counters live in one static device array built into
+ * the library (about 6.5 MB, held on every GPU that loads the library until the
+ * process exits), sized for at most PM_NOALLOC_MAX_PIXELS pixels of up to 32
+ * wavelengths per call: larger calls fail with PM_ERANGE.  The first call on a
+ * device looks up that array's device address (cudaGetSymbolAddress) and caches
+ * it; make that first call before any stream capture.  All calls share the one
+ * array: calls whose GPU work overlaps (other host threads, other streams) race
+ * and must be serialised by the caller.  stream: a cudaStream_t or NULL. */
+#define PM_NOALLOC_MAX_PIXELS 4096
+int pm_invert_batch_noalloc(const pm_line *line, const pm_config *cfg, int64_t npix, const float *spectro,
+                            const float *slight, int slight_mode, const pm_model *guess, pm_model *models_out,
+                            float *chisq_out, int *iters_out, float *best_fit_out, int *status_out, void *stream);
+
 int pm_get_stats(const pm_ctx *ctx, pm_stats *out);
 const char *pm_last_error(void);
 int pm_abi_version(void);

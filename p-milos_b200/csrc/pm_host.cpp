@@ -309,6 +309,11 @@ int set_slight(PmParams& P, const float* slight, int mode, int mem) {
 
 }  // namespace
 
+// Helpers shared with the other translation units of the library.
+int pmh_fill_params(const pm_line* L, const pm_config* c, PmParams& P) { return fill_params(L, c, P); }
+void pmh_set_guess(PmParams& P, const pm_model* g) { set_guess(P, g); }
+int pmh_fail(int code, const char* msg) { return fail(code, "%s", msg); }
+
 extern "C" int pm_ctx_create(const pm_line* line, const pm_config* cfg, void* stream, pm_ctx** out) {
   if (!line || !cfg || !out) return fail(PM_EINVAL, "pm_ctx_create: NULL argument");
   *out = nullptr;

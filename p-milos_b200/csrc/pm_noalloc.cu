@@ -1,0 +1,170 @@
+// pm_noalloc.cu -- pm_invert_batch_noalloc: the batched inversion for callers that
+// must not allocate GPU memory.
+//
+// Who needs it.  A host program that keeps its cubes in host memory (like the
+// reference's own drivers, which hold every pixel in malloc'd arrays) but runs
+// where it may not create device allocations of its own: a process whose device
+// memory is reserved up front by another component, a memory-accounted service
+// that forbids allocations after start-up, or a real-time acquisition loop that
+// cannot afford the latency and possible failure of cudaMalloc/cudaFree on the
+// critical path.  pm_invert_batch cannot serve them: its context allocates the
+// work-queue counters and, for host buffers, device staging copies.
+//
+// How.  Everything the call needs on the device beyond the caller's own arrays
+// lives in one file-scope static device array, g_noalloc_scratch (about 6.5 MB,
+// fixed at build time): the work-queue/statistics counters and staging room for
+// at most PM_NOALLOC_MAX_PIXELS pixels of up to 32 wavelengths (observed
+// profiles, a per-pixel stray-light cube, models, chi^2, iterations, status,
+// best-fit profiles).  Every GPU that loads the library holds this memory until
+// the process exits.  The run constants go in the kernel's by-value parameter
+// block, so no context is needed either.  The call makes no cudaMalloc/cudaFree
+// (nor any other allocating call) and creates no CUDA events or streams.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+#include "pm_params.h"
+
+namespace {
+
+constexpr int64_t kMaxPix = PM_NOALLOC_MAX_PIXELS;
+constexpr size_t kProf = sizeof(float) * 4 * PMK_NL;  // one pixel's profiles at the largest grid
+constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+constexpr size_t kOffCtr = 0;
+constexpr size_t kOffSpectro = align256(kOffCtr + sizeof(unsigned long long) * PMC_COUNT);
+constexpr size_t kOffSlight = align256(kOffSpectro + kMaxPix * kProf);
+constexpr size_t kOffModels = align256(kOffSlight + kMaxPix * kProf);
+constexpr size_t kOffChisq = align256(kOffModels + kMaxPix * sizeof(pm_model));
+constexpr size_t kOffIters = align256(kOffChisq + kMaxPix * sizeof(float));
+constexpr size_t kOffStatus = align256(kOffIters + kMaxPix * sizeof(int));
+constexpr size_t kOffBest = align256(kOffStatus + kMaxPix * sizeof(int));
+constexpr size_t kScratchBytes = align256(kOffBest + kMaxPix * kProf);
+
+}  // namespace
+
+// The scratch.  Host code must not use this name as an address: on the host it
+// is a stand-in object, not device memory (a kernel given it would fault, or on
+// systems where the GPU can reach host memory, silently use the wrong memory).
+// The device address comes from cudaGetSymbolAddress, once per device.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+std::mutex g_mu;
+unsigned char* g_scratch[kMaxDevices] = {};
+int g_sms[kMaxDevices] = {};
+
+// Device address of the scratch on the current device, looked up on the first
+// call made on that device (with the device current) and cached.
+int scratch_for_current_device(unsigned char** out, int* sms) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return pmh_fail(PM_ENODEV, cudaGetErrorString(e));
+  if (dev < 0 || dev >= kMaxDevices) return pmh_fail(PM_ERANGE, "device index beyond 63");
+  std::lock_guard<std::mutex> lock(g_mu);
+  if (!g_scratch[dev]) {
+    int major = 0, nsm = 0;
+    e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return pmh_fail(PM_ENODEV, cudaGetErrorString(e));
+    if (major != 10) return pmh_fail(PM_ENODEV, "pm_invert_batch_noalloc: this library is built for sm_100a");
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) return pmh_fail(PM_EIO, e != cudaSuccess ? cudaGetErrorString(e) : "null symbol");
+    g_scratch[dev] = static_cast<unsigned char*>(p);
+    g_sms[dev] = nsm;
+  }
+  *out = g_scratch[dev];
+  *sms = g_sms[dev];
+  return PM_OK;
+}
+
+int cuda_err(cudaError_t e, const char* what) {
+  char msg[256];
+  std::snprintf(msg, sizeof msg, "%s: %s", what, cudaGetErrorString(e));
+  return pmh_fail(PM_EIO, msg);
+}
+
+}  // namespace
+
+extern "C" int pm_invert_batch_noalloc(const pm_line* line, const pm_config* cfg, int64_t npix, const float* spectro,
+                                       const float* slight, int slight_mode, const pm_model* guess,
+                                       pm_model* models_out, float* chisq_out, int* iters_out, float* best_fit_out,
+                                       int* status_out, void* stream) {
+  if (!line || !cfg || !spectro || !guess || !models_out || !chisq_out || !iters_out)
+    return pmh_fail(PM_EINVAL, "pm_invert_batch_noalloc: NULL argument");
+  if (npix < 0) return pmh_fail(PM_EINVAL, "pm_invert_batch_noalloc: npix < 0");
+  if (npix > kMaxPix) {
+    char msg[160];
+    std::snprintf(msg, sizeof msg,
+                  "pm_invert_batch_noalloc: %lld pixels exceed the static scratch (at most %d pixels per call)",
+                  (long long)npix, PM_NOALLOC_MAX_PIXELS);
+    return pmh_fail(PM_ERANGE, msg);
+  }
+  if (guess->mac != 0.0) return pmh_fail(PM_ENOTSUP, "macroturbulence (guess.mac > 0) is outside this implementation");
+  PmParams P;
+  int rc = pmh_fill_params(line, cfg, P);
+  if (rc != PM_OK) return rc;
+  pmh_set_guess(P, guess);
+  P.slight_mode = slight_mode;
+  if (slight_mode != PM_SLIGHT_NONE) {
+    if (!slight) return pmh_fail(PM_EINVAL, "pm_invert_batch_noalloc: slight_mode set but slight is NULL");
+    if (P.K != 10) return pmh_fail(PM_EINVAL, "stray light requires nterms == 10 (filling factor inverted)");
+    if (slight_mode == PM_SLIGHT_SHARED) {
+      for (int i = 0; i < 4 * P.nl; ++i) {
+        P.sl_d[i] = slight[i];
+        P.sl_f[i] = slight[i];
+      }
+    } else if (slight_mode != PM_SLIGHT_PER_PIXEL) {
+      return pmh_fail(PM_EINVAL, "pm_invert_batch_noalloc: bad slight_mode");
+    }
+  }
+  if (npix == 0) return PM_OK;
+  unsigned char* base = nullptr;
+  int sms = 0;
+  rc = scratch_for_current_device(&base, &sms);
+  if (rc != PM_OK) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t prof = sizeof(float) * 4 * P.nl;
+  unsigned long long* ctr = reinterpret_cast<unsigned long long*>(base + kOffCtr);
+  cudaError_t e;
+  // the scratch keeps the previous call's contents: the work-queue counters must
+  // start at zero
+  if ((e = cudaMemsetAsync(ctr, 0, sizeof(unsigned long long) * PMC_COUNT, st)) != cudaSuccess)
+    return cuda_err(e, "counter reset");
+  if ((e = cudaMemcpyAsync(base + kOffSpectro, spectro, prof * npix, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+    return cuda_err(e, "spectro H2D");
+  if (slight_mode == PM_SLIGHT_PER_PIXEL &&
+      (e = cudaMemcpyAsync(base + kOffSlight, slight, prof * npix, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+    return cuda_err(e, "slight H2D");
+  PmIO io{};
+  io.npix = npix;
+  io.spectro = reinterpret_cast<const float*>(base + kOffSpectro);
+  io.slight = slight_mode == PM_SLIGHT_PER_PIXEL ? reinterpret_cast<const float*>(base + kOffSlight) : nullptr;
+  io.models_out = reinterpret_cast<double*>(base + kOffModels);
+  io.chisq_out = reinterpret_cast<float*>(base + kOffChisq);
+  io.iters_out = reinterpret_cast<int*>(base + kOffIters);
+  io.status_out = status_out ? reinterpret_cast<int*>(base + kOffStatus) : nullptr;
+  io.spectra_out = best_fit_out ? reinterpret_cast<float*>(base + kOffBest) : nullptr;
+  io.ctr = ctr;
+  rc = pmk_invert(P, io, cfg->precision, 0, st, sms, nullptr);
+  if (rc != PM_OK) return pmh_fail(rc, pmk_last_cuda_error());
+  if ((e = cudaMemcpyAsync(models_out, io.models_out, sizeof(pm_model) * npix, cudaMemcpyDeviceToHost, st)) !=
+      cudaSuccess)
+    return cuda_err(e, "models D2H");
+  if ((e = cudaMemcpyAsync(chisq_out, io.chisq_out, sizeof(float) * npix, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+    return cuda_err(e, "chisq D2H");
+  if ((e = cudaMemcpyAsync(iters_out, io.iters_out, sizeof(int) * npix, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+    return cuda_err(e, "iters D2H");
+  if (status_out &&
+      (e = cudaMemcpyAsync(status_out, io.status_out, sizeof(int) * npix, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+    return cuda_err(e, "status D2H");
+  if (best_fit_out &&
+      (e = cudaMemcpyAsync(best_fit_out, io.spectra_out, prof * npix, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+    return cuda_err(e, "best fit D2H");
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_err(e, "pm_invert_batch_noalloc");
+  return PM_OK;
+}

@@ -72,3 +72,8 @@ int pmk_invert(const PmParams& P, const PmIO& io, int precision, int variant, vo
                float* kernel_ms);
 int pmk_synth(const PmParams& P, const PmIO& io, int precision, void* stream);
 const char* pmk_last_cuda_error();
+
+// Host helpers (pm_host.cpp) shared with pm_noalloc.cu.
+int pmh_fill_params(const pm_line* L, const pm_config* c, PmParams& P);
+void pmh_set_guess(PmParams& P, const pm_model* g);
+int pmh_fail(int code, const char* msg);

@@ -51,8 +51,10 @@ NL_MAX = 128
 # Every symbol include/pmilos.h declares (checked by the CPU test suite).
 EXPORTED_SYMBOLS = (
     "pm_line_from_quantum", "pm_psf_gaussian", "pm_psf_interpolate", "pm_ctx_create", "pm_ctx_destroy",
-    "pm_invert_batch", "pm_synth_batch", "pm_lm_mils", "pm_get_stats", "pm_last_error", "pm_abi_version",
+    "pm_invert_batch", "pm_synth_batch", "pm_lm_mils", "pm_invert_batch_noalloc", "pm_get_stats", "pm_last_error",
+    "pm_abi_version",
 )
+NOALLOC_MAX_PIXELS = 4096
 
 
 class PmError(RuntimeError):
@@ -115,6 +117,8 @@ def load_library(path: str | None = None):
     L.pm_synth_batch.argtypes = [vp, i64, vp, F, ctypes.c_int, vp, vp, ctypes.c_int]
     L.pm_lm_mils.argtypes = [vp, F, ctypes.POINTER(_Model), vp, ctypes.POINTER(ctypes.c_float), F,
                              ctypes.POINTER(ctypes.c_int)]
+    L.pm_invert_batch_noalloc.argtypes = [ctypes.POINTER(_Line), ctypes.POINTER(_Config), i64, F, F, ctypes.c_int,
+                                          ctypes.POINTER(_Model), vp, vp, vp, vp, vp, vp]
     L.pm_get_stats.argtypes = [vp, ctypes.POINTER(_Stats)]
     L.pm_last_error.restype = ctypes.c_char_p
     L.pm_abi_version.restype = ctypes.c_int
@@ -350,6 +354,32 @@ class Inverter:
                                       None if sl is None else sl.ctypes.data, ctypes.byref(it)))
         model = np.array([getattr(m, n) for n in MODEL_FIELDS])
         return rc, model, sp.reshape(4, self.nl), chi.value, it.value
+
+    def invert_noalloc(self, spectro, guess, *, slight=None, slight_mode=None, want_spectra=True, want_status=True):
+        """The same inversion as ``invert`` on host arrays, through
+        pm_invert_batch_noalloc: no GPU memory is allocated (the library stages
+        through its built-in static device array), so at most
+        NOALLOC_MAX_PIXELS pixels per call."""
+        obs = np.ascontiguousarray(spectro, dtype=np.float32).reshape(-1, 4, self.nl)
+        npix = obs.shape[0]
+        sl, mode = self._slight_host(slight, slight_mode, npix)
+        models = np.zeros((npix, 11), dtype=np.float64)
+        chi = np.zeros(npix, dtype=np.float32)
+        its = np.zeros(npix, dtype=np.int32)
+        sp = np.zeros((npix, 4, self.nl), dtype=np.float32) if want_spectra else None
+        stt = np.zeros(npix, dtype=np.int32) if want_status else None
+        g = _model_struct(guess)
+        _check(self.L.pm_invert_batch_noalloc(ctypes.byref(self.line._c), ctypes.byref(self._cfg), npix,
+                                              obs.ctypes.data, None if sl is None else sl.ctypes.data, mode,
+                                              ctypes.byref(g), models.ctypes.data, chi.ctypes.data, its.ctypes.data,
+                                              None if sp is None else sp.ctypes.data,
+                                              None if stt is None else stt.ctypes.data, None))
+        out = {"models": models, "chisq": chi, "iters": its}
+        if sp is not None:
+            out["spectra"] = sp
+        if stt is not None:
+            out["status"] = stt
+        return out
 
     def stats(self) -> dict:
         s = _Stats()

@@ -9,7 +9,7 @@ PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG_DIR)                  # p-milos_b200/
 CSRC = os.path.join(ROOT, "csrc")
 OUT = os.path.join(ROOT, "libpmilos_b200.so")
-SOURCES = ("pm_kernels.cu", "pm_host.cpp")
+SOURCES = ("pm_kernels.cu", "pm_host.cpp", "pm_noalloc.cu")
 ARCH = "-gencode=arch=compute_100a,code=sm_100a"
 
 
