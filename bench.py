@@ -166,7 +166,7 @@ def host_cores() -> int:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", type=int, default=1)
@@ -188,9 +188,11 @@ def main():
 
     metric = "pixels/s inverted on 1 B200"
     w = workloads.config(args.config, npix=args.npix)
+    psf_desc = "no PSF" if w.psf is None else "Gaussian PSF"
+    stray_desc = ", stray light mixed at alpha~U(0.7,1)" if w.cfg == 2 else ""
     cfg_desc = {"workload": f"ME inversion, benchmark configuration {args.config}: {w.npix} pixels "
                             f"({int(np.sqrt(w.npix))}^2) x 4 Stokes x {w.nl} wavelengths, Fe I {w.line.lambda0} A, "
-                            f"PSF FWHM 60 mA, {w.nterms} free parameters, <= {w.miter} LM iterations",
+                            f"{psf_desc}{stray_desc}, {w.nterms} free parameters, <= {w.miter} LM iterations",
                 "pixels_per_step": w.npix, "nlambda": w.nl, "nterms": w.nterms,
                 "parallelism": f"replicas x{args.gpus}", "l2": "flushed between timed steps (256 MiB write)"}
 
@@ -237,6 +239,8 @@ def main():
     rng = np.random.default_rng(w.seed + 1000 * rank)
     obs = workloads.synthesize(w, inv_fp64=inv64, rng=rng)
     obs_d = torch.as_tensor(obs, device="cuda")
+    sl_h = None if w.slight is None else np.ascontiguousarray(w.slight, dtype=np.float32)
+    sl_d = None if sl_h is None else torch.as_tensor(sl_h, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     def barrier():
@@ -246,7 +250,7 @@ def main():
 
     def step_device(inv):
         flush.fill_(1)  # L2 flush outside the timed kernel
-        r = inv.invert(obs_d, w.guess, want_spectra=False, want_status=False)
+        r = inv.invert(obs_d, w.guess, slight=sl_d, want_spectra=False, want_status=False)
         s = inv.stats()
         return r, s
 
@@ -274,12 +278,12 @@ def main():
     if not args.no_e2e:
         obs_pinned = torch.from_numpy(obs).pin_memory().numpy()
         for _ in range(max(1, args.warmup)):
-            inv32.invert(obs_pinned, w.guess, want_spectra=False, want_status=False)
+            inv32.invert(obs_pinned, w.guess, slight=sl_h, want_spectra=False, want_status=False)
         e2e_ms = []
         for _ in range(args.steps):
             flush.fill_(1)
             torch.cuda.synchronize()
-            inv32.invert(obs_pinned, w.guess, want_spectra=False, want_status=False)
+            inv32.invert(obs_pinned, w.guess, slight=sl_h, want_spectra=False, want_status=False)
             e2e_ms.append(inv32.stats()["total_ms"])
         e2e_v = world * w.npix / (float(np.mean(e2e_ms)) / 1000.0)
     h2d = obs.nbytes
@@ -308,8 +312,13 @@ def main():
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     hbm_peak = json.load(open(peaks_path))["hbm_gbs"] if os.path.exists(peaks_path) else 6650.0
     hbm_bytes = w.npix * args.steps * (16 * w.nl + 11 * 8 + 8)
+    # DRAM bytes per pixel of the FP32 inversion kernel from one ncu capture
+    # (profiles/invert_kernel_fp32_config1.md: 80.2 MB for 131,072 pixels of the
+    # configuration-1 workload), scaled to this launch by its pixel count
+    traffic = 612.0 * w.npix if (args.config == 1 and w.nl == 30) else None
     roofline = {"bound": "fp32", "achieved": round(achieved, 3), "peak": round(peak_fp32, 2), "unit": "TFLOP/s",
-                "frac": round(achieved / peak_fp32, 4), "traffic": None,
+                "frac": round(achieved / peak_fp32, 4), "traffic": traffic,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per pixel, scaled",
                 "peak_source": f"148 SMs x 128 FP32 lanes x 2 x sampled SM clock {sm_mhz:.0f} MHz (nominal; no "
                                "measured FP32-pipe peak in MEASURED_PEAKS.json)",
                 "flops_per_pixel_fp32": round(f32 / (w.npix * args.steps)),
