@@ -209,6 +209,7 @@ int pm_lm_mils(pm_ctx *ctx, const float *spectro, pm_model *init_model, float *s
  * array: calls whose GPU work overlaps (other host threads, other streams) race
  * and must be serialised by the caller.  stream: a cudaStream_t or NULL. */
 #define PM_NOALLOC_MAX_PIXELS 4096
+#define PM_NOALLOC_MAX_WAVELENGTHS 32
 int pm_invert_batch_noalloc(const pm_line *line, const pm_config *cfg, int64_t npix, const float *spectro,
                             const float *slight, int slight_mode, const pm_model *guess, pm_model *models_out,
                             float *chisq_out, int *iters_out, float *best_fit_out, int *status_out, void *stream);

@@ -264,16 +264,30 @@ int fill_params(const pm_line* L, const pm_config* c, PmParams& P) {
   P.ilambda = c->ilambda;
   P.toplim = c->toplim;
   P.mu = c->mu;
+  P.G = P.nl <= 32 ? 1 : (P.nl <= 64 ? 2 : 4);
   if (c->psf) {
+    double peak = 0;
     for (int j = 0; j < P.nl; ++j) {
       P.taps_d[j] = c->psf[j];
       P.taps_f[j] = float(c->psf[j]);
+      peak = std::max(peak, std::fabs(c->psf[j]));
     }
-    for (int t = 0; t < PMK_GC; ++t) {
-      const int j = t - (PMK_NL - 1) + P.half;
-      const double g = (j >= 0 && j < P.nl) ? c->psf[j] : 0.0;
-      P.gc_d[t] = g;
-      P.gc_f[t] = float(g);
+    // Support of the kernel for the multi-warp correlations: taps below 1e-18 of
+    // the peak change no output by more than 1e-18 of the largest input.
+    P.tap_lo = 0;
+    P.tap_hi = P.nl - 1;
+    while (P.tap_lo < P.tap_hi && !(std::fabs(c->psf[P.tap_lo]) > 1e-18 * peak)) ++P.tap_lo;
+    while (P.tap_hi > P.tap_lo && !(std::fabs(c->psf[P.tap_hi]) > 1e-18 * peak)) --P.tap_hi;
+    // Stokes I is correlated as Ic - x (direct_convolution_ic): with zero padding
+    // that is Ic (1 - W_k) + sum_j G_j x_{k+j-half}, W_k the in-grid tap sum.
+    for (int k = 0; k < P.nl; ++k) {
+      double w = 0;
+      for (int j = P.tap_lo; j <= P.tap_hi; ++j) {
+        const int m = k + j - P.half;
+        if (m >= 0 && m < P.nl) w += c->psf[j];
+      }
+      P.omw_d[k] = 1.0 - w;
+      P.omw_f[k] = float(1.0 - w);
     }
   }
   return PM_OK;

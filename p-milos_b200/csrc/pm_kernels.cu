@@ -38,7 +38,7 @@
 
 namespace {
 
-constexpr int NL = PMK_NL;
+constexpr int NL = 32;      // lanes: wavelengths of a one-warp pixel
 constexpr int TRS = NL + 1;  // transpose row stride (odd: conflict-free column reads)
 constexpr double kPi = 3.14159265358979323846264338327950288419716939937510;
 constexpr double kVLight = 2.99792458e+5;
@@ -63,11 +63,11 @@ __device__ __forceinline__ float taps<float>(const PmParams& P, int j) { return 
 template <>
 __device__ __forceinline__ double taps<double>(const PmParams& P, int j) { return P.taps_d[j]; }
 template <typename R>
-__device__ __forceinline__ R gcen(const PmParams& P, int t);
+__device__ __forceinline__ R omw(const PmParams& P, int k);
 template <>
-__device__ __forceinline__ float gcen<float>(const PmParams& P, int t) { return P.gc_f[t]; }
+__device__ __forceinline__ float omw<float>(const PmParams& P, int k) { return P.omw_f[k]; }
 template <>
-__device__ __forceinline__ double gcen<double>(const PmParams& P, int t) { return P.gc_d[t]; }
+__device__ __forceinline__ double omw<double>(const PmParams& P, int k) { return P.omw_d[k]; }
 template <typename R>
 __device__ __forceinline__ R slshared(const PmParams& P, int i);
 template <>
@@ -284,16 +284,21 @@ struct alignas(16) BlockSmem {
   R rv[VEC][64 + VEC];
 };
 
+// State of the damped solve: the normal equations and the Jacobi rotation tables.
+struct alignas(16) SolveSmem {
+  double ab[PM_NTERMS_MAX * PM_NTERMS_MAX + PM_NTERMS_MAX];  // alpha (K*K) then beta (K)
+  double rot[12][3];      // per index: partner, c, signed s
+  int pq[6][2];           // the rotated pairs of the current round
+  double delta[PM_NTERMS_MAX];
+};
+
 template <typename R>
 struct alignas(16) WarpSmem {
   R tr[NL * TRS];       // response functions: [profile][lambda] (transpose buffer)
   R xs[4][XSR];         // padded Stokes rows for the synthesis PSF correlation
-  double ab[PM_NTERMS_MAX * PM_NTERMS_MAX + PM_NTERMS_MAX];  // alpha (K*K) then beta (K)
+  SolveSmem sv;
   R ls[NL][kLaneStatePad];    // synthesis state the response functions need, per lane
   ModelTerms<R> mt;           // per-model terms of the last synthesis (uniform)
-  double rot[12][3];      // per index: partner, c, signed s
-  int pq[6][2];           // the rotated pairs of the current round
-  double delta[PM_NTERMS_MAX];
   double model[11], trial[11];
 };
 
@@ -303,18 +308,20 @@ template <typename R>
 constexpr bool smem_layout_ok() {
   return sizeof(BlockSmem<R>) % 16 == 0 && sizeof(WarpSmem<R>) % 16 == 0 &&
          offsetof(WarpSmem<R>, xs) % 16 == 0 && (XSR * sizeof(R)) % 16 == 0 &&
+         offsetof(WarpSmem<R>, ls) % 16 == 0 && offsetof(WarpSmem<R>, mt) % 16 == 0 &&
          ((64 + BlockSmem<R>::VEC) * sizeof(R)) % 16 == 0;
 }
 static_assert(smem_layout_ok<float>(), "shared-memory layout breaks 16-byte vector loads (float)");
 static_assert(smem_layout_ok<double>(), "shared-memory layout breaks 16-byte vector loads (double)");
+static_assert(3 * 10 * 10 * sizeof(double) <= sizeof(float) * NL * TRS, "eigen scratch exceeds the transpose buffer");
 
 template <typename R>
 __device__ __forceinline__ void load_taps(const PmParams& P, BlockSmem<R>& bs) {
   constexpr int VEC = BlockSmem<R>::VEC;
   for (int e = threadIdx.x; e < VEC * (64 + VEC); e += blockDim.x) {
     const int c = e / (64 + VEC), u = e % (64 + VEC);
-    const int t = 62 - (u + c);  // index into the centred table gc[t] = G[t - 31 + half]
-    bs.rv[c][u] = (t >= 0 && t < PMK_GC) ? gcen<R>(P, t) : R(0);
+    const int j = 31 - (u + c) + P.half;
+    bs.rv[c][u] = (j >= 0 && j < P.nl) ? taps<R>(P, j) : R(0);
   }
 }
 
@@ -394,13 +401,13 @@ __device__ __forceinline__ void load_lane_state(const WarpSmem<R>& sm, int lane,
   copy16(st, *reinterpret_cast<const LaneState<R>*>(sm.ls[lane]));
 }
 
-// Response functions at this lane's wavelength (me_der.c:85-312) written into the
-// transpose buffer: profile p = r*4 + s for rows r = 0..6 (eta0, B, vlos, dopp,
+// Response functions at this thread's wavelength (me_der.c:85-312), profile p
+// stored at col[p * STRIDE]: p = r*4 + s for rows r = 0..6 (eta0, B, vlos, dopp,
 // a, gamma, azimuth) and r = 7 holding RF row 8 (S1).  Row 7 of the reference
 // (S0: I = 1, Q = U = V = 0) is not convolved and is added in registers later.
-template <typename R>
-__device__ __forceinline__ void rf_lane(const PmParams& P, const ModelTerms<R>& T, const LaneState<R>& st,
-                                        WarpSmem<R>& sm, int lane, bool valid) {
+template <typename R, int STRIDE>
+__device__ __forceinline__ void rf_lane(const PmParams& P, const ModelTerms<R>& T, const LaneState<R>& st, R* col,
+                                        bool valid) {
   R dfi[3][4], dshi[3][4];
 #pragma unroll
   for (int g = 0; g < 3; ++g) {
@@ -436,7 +443,6 @@ __device__ __forceinline__ void rf_lane(const PmParams& P, const ModelTerms<R>& 
   const R ext2 = a2 * etau + etaq * rhov - etav * rhoq;
   const R ext3 = a2 * etav + etau * rhoq - etaq * rhou;
   const R ext4 = a2 * st.gp1;
-  R* col = sm.tr + lane;
 #pragma unroll
   for (int il = 0; il < 7; ++il) {
     R de, dq, du, dv, rq, ru, rv;
@@ -482,17 +488,17 @@ __device__ __forceinline__ void rf_lane(const PmParams& P, const ModelTerms<R>& 
     const R dgp6 = de * ext3 + etai_2 * dv + etai * (rhoq * du + etau * rq - rhou * dq - etaq * ru);
     R dV = ((dgp6 + rv * st.gp2 + rhov * dgp2) * st.dt - d_dt * st.g6) * dtaux;
     if (il == 6) { dI = 0; dV = 0; }  // me_der.c:309-312
-    col[(il * 4 + 0) * TRS] = valid ? dI : R(0);
-    col[(il * 4 + 1) * TRS] = valid ? dQ : R(0);
-    col[(il * 4 + 2) * TRS] = valid ? dU : R(0);
-    col[(il * 4 + 3) * TRS] = valid ? dV : R(0);
+    col[(il * 4 + 0) * STRIDE] = valid ? dI : R(0);
+    col[(il * 4 + 1) * STRIDE] = valid ? dQ : R(0);
+    col[(il * 4 + 2) * STRIDE] = valid ? dU : R(0);
+    col[(il * 4 + 3) * STRIDE] = valid ? dV : R(0);
   }
   // S1 (me_der.c:281-298)
   const R dti_s1 = -(st.dti * R(P.mu));
-  col[(7 * 4 + 0) * TRS] = valid ? -dti_s1 * etai_gp3 : R(0);
-  col[(7 * 4 + 1) * TRS] = valid ? dti_s1 * st.g4 : R(0);
-  col[(7 * 4 + 2) * TRS] = valid ? dti_s1 * st.g5 : R(0);
-  col[(7 * 4 + 3) * TRS] = valid ? dti_s1 * st.g6 : R(0);
+  col[(7 * 4 + 0) * STRIDE] = valid ? -dti_s1 * etai_gp3 : R(0);
+  col[(7 * 4 + 1) * STRIDE] = valid ? dti_s1 * st.g4 : R(0);
+  col[(7 * 4 + 2) * STRIDE] = valid ? dti_s1 * st.g5 : R(0);
+  col[(7 * 4 + 3) * STRIDE] = valid ? dti_s1 * st.g6 : R(0);
 }
 
 // PSF correlation of the 32 response-function profiles, one profile per lane
@@ -676,7 +682,7 @@ __device__ __forceinline__ void normal_eq(const PmParams& P, WarpSmem<R>& sm, in
     } else {
       val = red[NA + (e - KT * KT)];
     }
-    sm.ab[e] = val;
+    sm.sv.ab[e] = val;
   }
   __syncwarp();
 }
@@ -702,11 +708,15 @@ __device__ __forceinline__ double chisq(const PmParams& P, const R S[4], const f
 // all K/2 rotations of a round applied at once), then the pseudo-inverse with
 // the absolute 1e-12 eigenvalue cut of mil_svd.  Warp-cooperative; every lane
 // returns delta.
-template <typename R, int KT>
-__device__ __noinline__ void solve_eigen(const PmParams& P, WarpSmem<R>& sm, int lane, double flambda) {
+template <int KT>
+constexpr int eigen_scratch_doubles() {
+  return 3 * ((KT + 1) & ~1) * ((KT + 1) & ~1);
+}
+
+template <int KT>
+__device__ __noinline__ void solve_eigen(SolveSmem& sm, double* scratch, int lane, double flambda) {
   constexpr int M = (KT + 1) & ~1;  // padded to even; index KT (if any) is a dummy
-  static_assert(3 * M * M * sizeof(double) <= sizeof(WarpSmem<R>::tr), "eigen scratch exceeds tr");
-  double* A = reinterpret_cast<double*>(sm.tr);  // the transpose buffer is idle during the solve
+  double* A = scratch;  // eigen_scratch_doubles<KT>() doubles, idle otherwise during the solve
   double* V = A + M * M;
   double* A2 = V + M * M;
   for (int e = lane; e < M * M; e += 32) {
@@ -807,8 +817,9 @@ __device__ __noinline__ void solve_eigen(const PmParams& P, WarpSmem<R>& sm, int
 // step.  Exactly-zero rows (fixed parameters) get a zero step, as the
 // pseudo-inverse gives them.  Returns false on a pivot <= 1e-12 (the caller
 // then uses the eigen solver for this step).
-template <typename R, int KT>
-__device__ __forceinline__ bool solve_cholesky(WarpSmem<R>& sm, int lane, double flambda, double (&delta)[KT]) {
+template <int KT>
+__device__ __forceinline__ bool solve_cholesky(SolveSmem& sm, double* scratch, int lane, double flambda,
+                                               double (&delta)[KT]) {
   const int i = lane < KT ? lane : KT - 1;
   const double damp = 1.0 + flambda;
   double a[KT];
@@ -849,7 +860,7 @@ __device__ __forceinline__ bool solve_cholesky(WarpSmem<R>& sm, int lane, double
     if (i > j) b = fma(-a[j], y[j], b);
   }
   // back: L^T x = y, with L^T read from shared memory (L[k][j] at lt[j*KT + k])
-  double* lt = reinterpret_cast<double*>(sm.tr);
+  double* lt = scratch;
   __syncwarp();
   if (lane < KT) {
 #pragma unroll
@@ -917,31 +928,23 @@ __device__ __forceinline__ void check_model(double* m) {
 }
 
 // estimacionesClasicas (milosUtils.c:287-452, forInitialUse = 1) followed by the
-// NaN fixes of the drivers (milos.c:976-983).  Sums in FP64 across the warp.
-__device__ void classical(const PmParams& P, const float O[4], int lane, bool valid, double* m) {
-  const int nl = P.nl;
-  const unsigned neg = __ballot_sync(kFull, valid && O[0] < 0.0f);
-  const unsigned validm = (nl >= 32) ? kFull : ((1u << nl) - 1u);
-  // leading and trailing ghost wavelengths (I < 0)
-  const unsigned nonneg = validm & ~neg;
-  if (nonneg == 0) return;  // every intensity negative: no estimate possible
-  const int begin = __ffs(nonneg) - 1;
-  const int end = 32 - __clz(nonneg);  // one past the last non-negative
-  const double Ic = __shfl_sync(kFull, double(O[0]), end - 1);
-  const double dl = valid ? P.dl[lane] : 0.0;
-  const bool in = valid && lane >= begin && lane < end - 1;
+// NaN fixes of the drivers (milos.c:976-983), in two halves around the sums over
+// wavelengths (accumulated in FP64): the terms at one wavelength w, between the
+// leading and trailing ghost wavelengths [begin, end), with Ic = I[end - 1] ...
+__device__ __forceinline__ void classical_terms(const PmParams& P, const float O[4], int w, bool valid, int begin,
+                                                int end, double Ic, double (&v)[10]) {
+  const double dl = valid ? P.dl[w] : 0.0;
+  const bool in = valid && w >= begin && w < end - 1;
   const bool iv = in && O[0] > -1.0f && O[3] > -1.0f;
   const double a = iv ? Ic - double(O[0] + O[3]) : 0.0;
   const double av = iv ? Ic - double(O[0]) : 0.0;
   const double am = iv ? Ic - double(O[0] - O[3]) : 0.0;
-  const double x = warp_sum(a * dl), y = warp_sum(a);
-  const double xv = warp_sum(av * dl), yv = warp_sum(av);
-  const double xm = warp_sum(am * dl), ym = warp_sum(am);
-  const double lp = fabs(y) > 1e-15 ? x / y : 0.0;
-  const double lmn = fabs(ym) > 1e-15 ? xm / ym : 0.0;
-  const double C = kZeeman * (P.lambda0 * P.lambda0) * P.geff;
-  const double Blos = (1 / C) * ((lp - lmn) / 2);
-  double Vlos = (kVLight / P.lambda0) * ((xv / yv) / 2);
+  v[0] = a * dl;
+  v[1] = a;
+  v[2] = av * dl;
+  v[3] = av;
+  v[4] = am * dl;
+  v[5] = am;
   const bool iq = in && O[1] > -1.0f && O[2] > -1.0f && O[3] > -1.0f;
   double gx = 0, gy = 0;
   if (iq) {
@@ -950,16 +953,30 @@ __device__ void classical(const PmParams& P, const float O[4], int lane, bool va
     gx = fabs(double(O[3])) * mm;
     gy = fabs(double(O[3])) * fabs(double(O[3]));
   }
-  const double sx = warp_sum(gx);
-  const double sy = warp_sum(gy) * fabs(3 * C * Blos);
+  v[6] = gx;
+  v[7] = gy;
+  const bool iu = valid && O[2] > -1.0f && O[1] > -1.0f && (fabs(O[2]) > 0.0001f || fabs(O[1]) > 0.0001f);
+  v[8] = iu ? double(O[2]) : 0.0;
+  v[9] = iu ? double(O[1]) : 0.0;
+}
+
+// ... and the estimates from the ten sums.
+__device__ __forceinline__ void classical_finish(const PmParams& P, const double (&v)[10], double* m) {
+  const double x = v[0], y = v[1], xv = v[2], yv = v[3], xm = v[4], ym = v[5];
+  const double lp = fabs(y) > 1e-15 ? x / y : 0.0;
+  const double lmn = fabs(ym) > 1e-15 ? xm / ym : 0.0;
+  const double C = kZeeman * (P.lambda0 * P.lambda0) * P.geff;
+  const double Blos = (1 / C) * ((lp - lmn) / 2);
+  double Vlos = (kVLight / P.lambda0) * ((xv / yv) / 2);
+  const double sx = v[6];
+  const double sy = v[7] * fabs(3 * C * Blos);
   const double tan_gamma = fabs(sqrt(sx / sy));
   double gamma_rad = atan(tan_gamma);
   double gamma = gamma_rad * (180 / kPi);
   if (gamma >= 85 && gamma <= 90) gamma_rad = 85 * (kPi / 180);
   if (gamma > 90 && gamma <= 95) gamma_rad = 95 * (kPi / 180);
   if (Blos < 0) gamma = 180 - gamma;
-  const bool iu = valid && O[2] > -1.0f && O[1] > -1.0f && (fabs(O[2]) > 0.0001f || fabs(O[1]) > 0.0001f);
-  const double su = warp_sum(iu ? double(O[2]) : 0.0), sq = warp_sum(iu ? double(O[1]) : 0.0);
+  const double su = v[8], sq = v[9];
   double phi = (atan(su / sq) * 180 / kPi) / 2;
   if (su > 0 && sq > 0) phi = phi;
   else if (su < 0 && sq > 0) phi = phi + 180;
@@ -978,6 +995,24 @@ __device__ void classical(const PmParams& P, const float O[4], int lane, bool va
   if (isnan(m[6])) m[6] = 1;
 }
 
+// Classical estimates of a one-warp pixel (lane = wavelength).
+__device__ void classical(const PmParams& P, const float O[4], int lane, bool valid, double* m) {
+  const int nl = P.nl;
+  const unsigned neg = __ballot_sync(kFull, valid && O[0] < 0.0f);
+  const unsigned validm = (nl >= 32) ? kFull : ((1u << nl) - 1u);
+  // leading and trailing ghost wavelengths (I < 0)
+  const unsigned nonneg = validm & ~neg;
+  if (nonneg == 0) return;  // every intensity negative: no estimate possible
+  const int begin = __ffs(nonneg) - 1;
+  const int end = 32 - __clz(nonneg);  // one past the last non-negative
+  const double Ic = __shfl_sync(kFull, double(O[0]), end - 1);
+  double v[10];
+  classical_terms(P, O, lane, valid, begin, end, Ic, v);
+#pragma unroll
+  for (int i = 0; i < 10; ++i) v[i] = warp_sum(v[i]);
+  classical_finish(P, v, m);
+}
+
 // Response functions at the current synthesis -> alpha, beta in shared memory.
 template <typename R, int KT>
 __device__ __forceinline__ void rf_and_normal_eq(const PmParams& P, const BlockSmem<R>& bs, WarpSmem<R>& sm,
@@ -989,7 +1024,7 @@ __device__ __forceinline__ void rf_and_normal_eq(const PmParams& P, const BlockS
     copy16(T, sm.mt);
     LaneState<R> st;
     load_lane_state<R>(sm, lane, st);
-    rf_lane<R>(P, T, st, sm, lane, valid);
+    rf_lane<R, TRS>(P, T, st, sm.tr + lane, valid);
     alf = T.alf;
   }
   if (P.has_psf) rf_correlate<R>(P, bs, sm, lane);
@@ -1071,12 +1106,13 @@ __global__ void __launch_bounds__(128, MINB) invert_kernel(const __grid_constant
         {
           double dlt[KT];
           bool ok = true;
-          if (P.solver == PM_SOLVE_CHOLESKY) ok = solve_cholesky<R, KT>(sm, lane, flambda, dlt);
+          double* scratch = reinterpret_cast<double*>(sm.tr);  // the transpose buffer is idle here
+          if (P.solver == PM_SOLVE_CHOLESKY) ok = solve_cholesky<KT>(sm.sv, scratch, lane, flambda, dlt);
           if (P.solver != PM_SOLVE_CHOLESKY || !ok) {
             if (P.solver == PM_SOLVE_CHOLESKY) ++fallbacks;
-            solve_eigen<R, KT>(P, sm, lane, flambda);  // step in sm.delta
+            solve_eigen<KT>(sm.sv, scratch, lane, flambda);  // step in sm.sv.delta
 #pragma unroll
-            for (int i = 0; i < KT; ++i) dlt[i] = sm.delta[i];
+            for (int i = 0; i < KT; ++i) dlt[i] = sm.sv.delta[i];
             __syncwarp();
           }
           // every lane forms the (uniform) trial model; lane i stores parameter i
@@ -1190,7 +1226,7 @@ __global__ void __launch_bounds__(128) synth_kernel(const __grid_constant__ PmPa
         copy16(T, sm.mt);
         LaneState<R> st;
         load_lane_state<R>(sm, lane, st);
-        rf_lane<R>(P, T, st, sm, lane, valid);
+        rf_lane<R, TRS>(P, T, st, sm.tr + lane, valid);
         alf = T.alf;
       }
       if (P.has_psf) rf_correlate<R>(P, bs, sm, lane);
@@ -1207,6 +1243,517 @@ __global__ void __launch_bounds__(128) synth_kernel(const __grid_constant__ PmPa
       }
     }
     __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Wide grids: 32 < nl <= 128.  G = 2 or 4 warps invert one pixel; the block is
+// one pixel group and thread t owns wavelength t.  The per-wavelength work
+// (synthesis, response functions, their terms of chi^2 and of the normal
+// equations) is the one-warp code; what crosses warps goes through shared
+// memory: the PSF correlations read neighbouring wavelengths' rows, sums are
+// reduced per warp by shuffles and then across the G warps in a fixed order (so
+// every thread holds the same total), and warp 0 alone runs the damped solve.
+// ---------------------------------------------------------------------------
+template <typename R, int G>
+struct alignas(16) WideSmem {
+  static constexpr int NT = 32 * G;                 // threads = wavelength slots
+  static constexpr int VEC = 16 / sizeof(R);
+  static constexpr int RS = 32 + VEC;               // RF row stride: conflict-free 16-byte row reads
+  static constexpr int RED = 96;                    // reduction slots per warp
+  R xs[NT][4];                 // synthesized (I, Q, U, V) per wavelength: the PSF input
+  R rf[NT][RS];                // response functions [lambda][profile]; solver scratch
+  R ls[NT][kLaneStatePad];     // synthesis state per wavelength
+  ModelTerms<R> mt;
+  SolveSmem sv;
+  double red[2][G][RED];       // per-warp partial sums, double-buffered
+  double model[11], trial[11];
+  unsigned long long pix;
+};
+
+template <typename R, int G>
+constexpr bool wide_layout_ok() {
+  using W = WideSmem<R, G>;
+  return offsetof(W, xs) % 16 == 0 && offsetof(W, rf) % 16 == 0 && offsetof(W, ls) % 16 == 0 &&
+         offsetof(W, mt) % 16 == 0 && (W::RS * sizeof(R)) % 16 == 0 && (4 * sizeof(R)) % 16 == 0 &&
+         sizeof(W::rf) >= eigen_scratch_doubles<10>() * sizeof(double);
+}
+static_assert(wide_layout_ok<float, 2>() && wide_layout_ok<float, 4>(), "wide shared-memory layout (float)");
+static_assert(wide_layout_ok<double, 2>() && wide_layout_ok<double, 4>(), "wide shared-memory layout (double)");
+
+// Sum N values over the block: per warp by shuffles, then the G warp totals in
+// warp order from red[slot] ([2][G][STRIDE]).  Every thread returns the same
+// totals.  The slot alternates between calls, so one barrier per call suffices:
+// a slot is rewritten only after the next call's barrier, which every thread
+// reaches after reading this call's totals.
+template <int G, int STRIDE, int N>
+__device__ __forceinline__ void block_sum(double* red, int& slot, double (&v)[N]) {
+  static_assert(N <= STRIDE, "too many sums for the reduction slots");
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < N; ++i) v[i] = warp_sum(v[i]);
+  double* r = red + slot * G * STRIDE;
+  if (lane == 0) {
+#pragma unroll
+    for (int i = 0; i < N; ++i) r[warp * STRIDE + i] = v[i];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    double t = r[i];
+#pragma unroll
+    for (int g = 1; g < G; ++g) t += r[g * STRIDE + i];
+    v[i] = t;
+  }
+  slot ^= 1;
+}
+
+template <typename R>
+__device__ __forceinline__ void store4(R* dst, const R S[4]) {
+  if constexpr (sizeof(R) == 4) {
+    *reinterpret_cast<float4*>(dst) = make_float4(S[0], S[1], S[2], S[3]);
+  } else {
+    reinterpret_cast<double2*>(dst)[0] = make_double2(S[0], S[1]);
+    reinterpret_cast<double2*>(dst)[1] = make_double2(S[2], S[3]);
+  }
+}
+
+template <typename R>
+__device__ __forceinline__ void load4(const R* src, R x[4]) {
+  if constexpr (sizeof(R) == 4) {
+    const float4 q = *reinterpret_cast<const float4*>(src);
+    x[0] = q.x; x[1] = q.y; x[2] = q.z; x[3] = q.w;
+  } else {
+    const double2 a = reinterpret_cast<const double2*>(src)[0], b = reinterpret_cast<const double2*>(src)[1];
+    x[0] = a.x; x[1] = a.y; x[2] = b.x; x[3] = b.y;
+  }
+}
+
+// PSF correlation of the four synthesized profiles across the block (the
+// convolution psf_rows does within a warp): thread t forms output t from the
+// rows t + j - nl/2 of the in-grid taps j in [tap_lo, tap_hi].  Stokes I is
+// Ic (1 - W_t) + sum_j G_j I_{t+j-nl/2}, which equals Ic - sum_j G_j (Ic - I).
+// The caller separates the reads here from the next call's writes by a barrier.
+template <typename R, int G>
+__device__ __forceinline__ void psf_wide(const PmParams& P, WideSmem<R, G>& sm, int t, bool valid, R omw_t,
+                                         R S[4]) {
+  if (valid) store4<R>(sm.xs[t], S);
+  __syncthreads();
+  const int nl = P.nl;
+  const R i0 = sm.xs[0][0], in = sm.xs[nl - 1][0];
+  const R ic = (i0 > in) ? i0 : in;
+  R acc[4] = {R(0), R(0), R(0), R(0)};
+  const int b = t - P.half;
+#pragma unroll 2
+  for (int j = P.tap_lo; j <= P.tap_hi; ++j) {
+    const int mm = b + j;
+    if (mm >= 0 && mm < nl) {
+      const R g = taps<R>(P, j);
+      R x[4];
+      load4<R>(sm.xs[mm], x);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[q] = fma(g, x[q], acc[q]);
+    }
+  }
+  S[0] = valid ? fma(ic, omw_t, acc[0]) : R(0);
+#pragma unroll
+  for (int q = 1; q < 4; ++q) S[q] = valid ? acc[q] : R(0);
+}
+
+template <typename R, int G>
+__device__ __forceinline__ void synthesize_wide(const PmParams& P, WideSmem<R, G>& sm, const double* m,
+                                                const float* sl_pix, int t, bool valid, double dl_t, R omw_t,
+                                                R S[4], R Su[4]) {
+  ModelTerms<R> T;
+  LaneState<R> st;
+  model_terms<R>(P, m, T);
+  synth_lane<R>(P, T, dl_t, st, S);
+  copy16(*reinterpret_cast<LaneState<R>*>(sm.ls[t]), st);
+  if (t == 0) copy16(sm.mt, T);
+  if (P.has_psf) psf_wide<R, G>(P, sm, t, valid, omw_t, S);
+#pragma unroll
+  for (int s = 0; s < 4; ++s) Su[s] = S[s];
+  if (P.slight_mode != PM_SLIGHT_NONE) {
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      const int idx = s * P.nl + (valid ? t : 0);
+      const R slv = P.slight_mode == PM_SLIGHT_SHARED ? slshared<R>(P, idx) : R(sl_pix[idx]);
+      S[s] = S[s] * T.alf + slv * T.oma;
+    }
+  }
+}
+
+// PSF correlation of the 32 response-function profiles across the block: thread
+// t forms output t of every profile from rows t + j - nl/2 (eight 16-byte loads
+// and 32 FMAs per tap).  Stokes-I profiles add Ic (1 - W_t), Ic = max of the
+// profile's end points (me_der.c:471-496).
+template <typename R, int G>
+__device__ __forceinline__ void rf_correlate_wide(const PmParams& P, const WideSmem<R, G>& sm, int t, R omw_t,
+                                                  R (&v)[32]) {
+  constexpr int VEC = WideSmem<R, G>::VEC;
+  const int nl = P.nl;
+#pragma unroll
+  for (int p = 0; p < 32; ++p) v[p] = 0;
+  const int b = t - P.half;
+#pragma unroll 1
+  for (int j = P.tap_lo; j <= P.tap_hi; ++j) {
+    const int mm = b + j;
+    if (mm >= 0 && mm < nl) {
+      const R g = taps<R>(P, j);
+      const R* row = sm.rf[mm];
+#pragma unroll
+      for (int p = 0; p < 32; p += VEC) {
+        if constexpr (VEC == 4) {
+          const float4 q = *reinterpret_cast<const float4*>(row + p);
+          v[p] = fma(g, q.x, v[p]);
+          v[p + 1] = fma(g, q.y, v[p + 1]);
+          v[p + 2] = fma(g, q.z, v[p + 2]);
+          v[p + 3] = fma(g, q.w, v[p + 3]);
+        } else {
+          const double2 q = *reinterpret_cast<const double2*>(row + p);
+          v[p] = fma(g, q.x, v[p]);
+          v[p + 1] = fma(g, q.y, v[p + 1]);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    const R e0 = sm.rf[0][4 * r], en = sm.rf[nl - 1][4 * r];
+    v[4 * r] = fma((e0 > en) ? e0 : en, omw_t, v[4 * r]);
+  }
+}
+
+// Response functions of the last synthesis at this thread's wavelength, after
+// correlation, stray light and filling factor (as gather_rf): d[row][stokes].
+// Sff is the spectrum the filling-factor row is built from.
+template <typename R, int KT, int G>
+__device__ __forceinline__ void rf_wide(const PmParams& P, WideSmem<R, G>& sm, int t, bool valid, R omw_t,
+                                        const R Sff[4], const float* sl_pix, R (&d)[KT][4]) {
+  R alf;
+  {
+    ModelTerms<R> T;
+    copy16(T, sm.mt);
+    LaneState<R> st;
+    copy16(st, *reinterpret_cast<const LaneState<R>*>(sm.ls[t]));
+    rf_lane<R, 1>(P, T, st, sm.rf[t], valid);
+    alf = T.alf;
+  }
+  __syncthreads();
+  R v[32];
+  if (P.has_psf) {
+    rf_correlate_wide<R, G>(P, sm, t, omw_t, v);
+  } else {
+#pragma unroll
+    for (int p = 0; p < 32; ++p) v[p] = sm.rf[t][p];
+  }
+#pragma unroll
+  for (int r = 0; r < KT; ++r) {
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      R x;
+      if (r < 7) x = v[r * 4 + s];
+      else if (r == 7) x = (s == 0) ? R(1) : R(0);  // S0 (me_der.c:301-306)
+      else if (r == 8) x = v[7 * 4 + s];
+      else x = R(0);
+      d[r][s] = valid ? x : R(0);
+    }
+  }
+  if (P.slight_mode != PM_SLIGHT_NONE) {
+#pragma unroll
+    for (int r = 0; r < KT; ++r) {
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+        d[r][s] = d[r][s] * alf;
+        if (r == P.ff_row) {
+          const int idx = s * P.nl + (valid ? t : 0);
+          const R slv = P.slight_mode == PM_SLIGHT_SHARED ? slshared<R>(P, idx) : R(sl_pix[idx]);
+          d[r][s] = valid ? Sff[s] - slv : R(0);
+        }
+      }
+    }
+  }
+}
+
+// Normal equations over the block: packed entries reduced per warp (as
+// normal_eq), then the G warp totals summed in warp order into sv.ab.
+template <typename R, int KT, int G>
+__device__ __forceinline__ void normal_eq_wide(const PmParams& P, WideSmem<R, G>& sm, int& slot,
+                                               const R (&d)[KT][4], const R S[4], const float O[4],
+                                               const R isig[4]) {
+  constexpr int NA = KT * (KT + 1) / 2;
+  constexpr int NT = NA + KT;
+  constexpr int NCH = (NT + 31) / 32;
+  constexpr int RED = WideSmem<R, G>::RED;
+  static_assert(NCH * 32 <= RED, "reduction slots too small");
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  R cw[4], rw[4];
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    cw[s] = R(P.w[s]) * isig[s];
+    rw[s] = R(P.w[s]) * (S[s] - R(O[s])) * isig[s];
+  }
+  double* red = &sm.red[slot][0][0];
+  double* mine = red + warp * RED;
+  ne_reduce_chunk<R, KT, 0>(mine, lane, d, cw, rw);
+  if constexpr (NCH > 1) ne_reduce_chunk<R, KT, 1>(mine, lane, d, cw, rw);
+  if constexpr (NCH > 2) ne_reduce_chunk<R, KT, 2>(mine, lane, d, cw, rw);
+  __syncthreads();
+  for (int e = threadIdx.x; e < KT * KT + KT; e += 32 * G) {
+    int idx;
+    if (e < KT * KT) {
+      int a = e / KT, b = e % KT;
+      if (a > b) { int tt = a; a = b; b = tt; }
+      idx = a * KT - (a * (a - 1)) / 2 + (b - a);
+    } else {
+      idx = NA + (e - KT * KT);
+    }
+    double val = red[idx];
+#pragma unroll
+    for (int g = 1; g < G; ++g) val += red[g * RED + idx];
+    sm.sv.ab[e] = val;
+  }
+  slot ^= 1;
+  __syncthreads();
+}
+
+template <typename R, int G>
+__device__ __forceinline__ double chisq_wide(const PmParams& P, WideSmem<R, G>& sm, int& slot, const R S[4],
+                                             const float O[4], const R isig[4], bool valid, double nfree) {
+  double acc[1] = {0.0};
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    const R dif = S[s] - R(O[s]);
+    acc[0] += valid ? double(dif * dif) * P.w[s] * double(isig[s]) : 0.0;
+  }
+  block_sum<G, WideSmem<R, G>::RED>(&sm.red[0][0][0], slot, acc);
+  return acc[0] / nfree;
+}
+
+template <typename R, int KT, int G>
+__device__ __forceinline__ void rf_and_normal_eq_wide(const PmParams& P, WideSmem<R, G>& sm, int& slot, int t,
+                                                      bool valid, R omw_t, const R S[4], const R Sff[4],
+                                                      const float O[4], const R isig[4], const float* sl_pix) {
+  R d[KT][4];
+  rf_wide<R, KT, G>(P, sm, t, valid, omw_t, Sff, sl_pix, d);
+#pragma unroll
+  for (int r = 0; r < KT; ++r)
+    if (P.zero_row[r]) {
+#pragma unroll
+      for (int s = 0; s < 4; ++s) d[r][s] = 0;
+    }
+  normal_eq_wide<R, KT, G>(P, sm, slot, d, S, O, isig);
+}
+
+// lm_mils over pixels of a wide grid: the control flow of invert_kernel with
+// block-wide reductions; the solve and the trial model come from warp 0.
+template <typename R, int KT, int G, int MINB>
+__global__ void __launch_bounds__(32 * G, MINB) invert_wide_kernel(const __grid_constant__ PmParams P,
+                                                                     const PmIO io) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  WideSmem<R, G>& sm = *reinterpret_cast<WideSmem<R, G>*>(smem_raw);
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const bool valid = t < P.nl;
+  const double dl_t = P.dl[valid ? t : 0];
+  const R omw_t = valid ? omw<R>(P, t) : R(0);
+  double* m = sm.model;
+  double* trial = sm.trial;
+  int slot = 0;
+
+  while (true) {
+    if (t == 0) sm.pix = atomicAdd(&io.ctr[PMC_NEXT], 1ull);
+    __syncthreads();
+    const unsigned long long pix = sm.pix;
+    if (pix >= (unsigned long long)io.npix) break;
+    const size_t base = size_t(pix) * 4 * P.nl;
+    const float* sl_pix = (P.slight_mode == PM_SLIGHT_PER_PIXEL) ? io.slight + base : nullptr;
+
+    float O[4];
+    R isig[4];
+    double gh[1] = {0.0};
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      O[s] = valid ? io.spectro[base + s * P.nl + t] : 0.0f;
+      const bool g = valid && O[s] <= -1.0f;
+      gh[0] += g ? 1.0 : 0.0;
+      isig[s] = R(1.0 / (g ? kGhostSigma : P.noise));
+    }
+    if (t < 11) m[t] = P.classical ? io.models_out[size_t(pix) * 11 + t] : P.guess[t];
+    block_sum<G, WideSmem<R, G>::RED>(&sm.red[0][0][0], slot, gh);  // also publishes m
+
+    const int nfree = P.nfree_base - int(gh[0]);
+    int status = PM_PIX_MAXITER, iter = 0, accepted = 0, fallbacks = 0;
+    double ochi = 0;
+    R S[4];
+    if (nfree == 0) {
+      status = PM_PIX_NFREE;
+      iter = -1;
+#pragma unroll
+      for (int s = 0; s < 4; ++s) S[s] = 0;
+    } else {
+      {
+        R Su[4];
+        synthesize_wide<R, G>(P, sm, m, sl_pix, t, valid, dl_t, omw_t, S, Su);
+        ochi = chisq_wide<R, G>(P, sm, slot, S, O, isig, valid, double(nfree));
+        rf_and_normal_eq_wide<R, KT, G>(P, sm, slot, t, valid, omw_t, S, Su, O, isig, sl_pix);
+      }
+      const double chi0 = ochi;
+      double flambda = P.ilambda, factor = 1.0;
+      if (t < 11) trial[t] = m[t];
+      __syncthreads();
+      bool stop = false;
+      do {
+        if (warp == 0) {
+          double dlt[KT];
+          bool ok = true;
+          double* scratch = reinterpret_cast<double*>(&sm.rf[0][0]);  // idle during the solve
+          if (P.solver == PM_SOLVE_CHOLESKY) ok = solve_cholesky<KT>(sm.sv, scratch, lane, flambda, dlt);
+          if (P.solver != PM_SOLVE_CHOLESKY || !ok) {
+            if (P.solver == PM_SOLVE_CHOLESKY) ++fallbacks;
+            solve_eigen<KT>(sm.sv, scratch, lane, flambda);
+#pragma unroll
+            for (int i = 0; i < KT; ++i) dlt[i] = sm.sv.delta[i];
+            __syncwarp();
+          }
+          double tt[11];
+#pragma unroll
+          for (int i = 0; i < 11; ++i) tt[i] = trial[i];
+          apply_delta<KT>(P, m, dlt, tt);
+          check_model(tt);
+          __syncwarp();
+#pragma unroll
+          for (int i = 0; i < 11; ++i)
+            if (lane == i) trial[i] = tt[i];
+        }
+        __syncthreads();
+        R Su[4];
+        synthesize_wide<R, G>(P, sm, trial, sl_pix, t, valid, dl_t, omw_t, S, Su);
+        const double chi = chisq_wide<R, G>(P, sm, slot, S, O, isig, valid, double(nfree));
+        if ((fabs((ochi - chi) * 100 / chi) < P.toplim) || (chi < 0.0001)) {
+          stop = true;
+          status = PM_PIX_CONVERGED;
+        }
+        if (chi - ochi < 0.) {
+          flambda = flambda / (5.0 * factor);
+          if (t < 11) m[t] = trial[t];
+          rf_and_normal_eq_wide<R, KT, G>(P, sm, slot, t, valid, omw_t, S, S, O, isig, sl_pix);
+          ochi = chi;
+          ++accepted;
+        } else {
+          flambda = flambda * 10.0 * factor;
+        }
+        if ((flambda > 1e+7) || (flambda < 1e-25)) {
+          if (!stop) status = PM_PIX_LAMBDA;
+          stop = true;
+        }
+        ++iter;
+        if (P.logclambda) factor = double(log10f(float(chi)) / log10f(float(chi0)));
+      } while (iter < P.miter && !stop);
+      __syncthreads();  // the last accepted model in m is visible to every thread
+      bool finite = isfinite(ochi);
+#pragma unroll
+      for (int i = 0; i < 11; ++i) finite = finite && isfinite(m[i]);
+      if (!finite) status = PM_PIX_NONFINITE;
+    }
+    if (t < 11) io.models_out[size_t(pix) * 11 + t] = m[t];
+    if (t == 0) {
+      io.chisq_out[pix] = float(ochi);
+      io.iters_out[pix] = iter;
+      if (io.status_out) io.status_out[pix] = status;
+      atomicAdd(&io.ctr[PMC_ITERS], (unsigned long long)(iter > 0 ? iter : 0));
+      atomicAdd(&io.ctr[PMC_ACCEPTED], (unsigned long long)accepted);
+      if (fallbacks) atomicAdd(&io.ctr[PMC_FALLBACK], (unsigned long long)fallbacks);
+    }
+    if (io.spectra_out && valid) {
+#pragma unroll
+      for (int s = 0; s < 4; ++s) io.spectra_out[base + s * P.nl + t] = float(S[s]);
+    }
+    __syncthreads();
+  }
+}
+
+// Classical estimates for wide grids, one block of G warps per pixel.
+template <int G>
+__global__ void __launch_bounds__(32 * G) classical_wide_kernel(const __grid_constant__ PmParams P, const PmIO io) {
+  constexpr int STR = 16;
+  __shared__ double red[2 * G * STR];
+  __shared__ unsigned mask[2][G];
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const bool valid = t < P.nl;
+  int slot = 0, ms = 0;
+  for (int64_t pix = blockIdx.x; pix < io.npix; pix += gridDim.x) {
+    const size_t base = size_t(pix) * 4 * P.nl;
+    float O[4];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) O[s] = valid ? io.spectro[base + s * P.nl + t] : 0.0f;
+    const unsigned nn = __ballot_sync(kFull, valid && !(O[0] < 0.0f));
+    if (lane == 0) mask[ms][warp] = nn;
+    __syncthreads();
+    // leading and trailing ghost wavelengths (I < 0)
+    int begin = -1, end = -1;
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      const unsigned k = mask[ms][g];
+      if (k) {
+        if (begin < 0) begin = 32 * g + __ffs(k) - 1;
+        end = 32 * g + 32 - __clz(k);
+      }
+    }
+    ms ^= 1;
+    // every intensity negative (begin < 0, uniform over the block): no estimate, the guess stays
+    double v[10];
+    if (begin >= 0) {
+      const double Ic = double(io.spectro[base + end - 1]);
+      classical_terms(P, O, t, valid, begin, end, Ic, v);
+      block_sum<G, STR>(red, slot, v);
+    }
+    if (t < 11) {
+      double g[11];
+#pragma unroll
+      for (int i = 0; i < 11; ++i) g[i] = P.guess[i];
+      if (begin >= 0) classical_finish(P, v, g);
+      double out = g[0];
+#pragma unroll
+      for (int i = 1; i < 11; ++i)
+        if (t == i) out = g[i];
+      io.models_out[size_t(pix) * 11 + t] = out;
+    }
+  }
+}
+
+// Synthesis (and response functions) of given models on a wide grid.
+template <typename R, int KT, int G>
+__global__ void __launch_bounds__(32 * G) synth_wide_kernel(const __grid_constant__ PmParams P, const PmIO io) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  WideSmem<R, G>& sm = *reinterpret_cast<WideSmem<R, G>*>(smem_raw);
+  const int t = threadIdx.x;
+  const bool valid = t < P.nl;
+  const double dl_t = P.dl[valid ? t : 0];
+  const R omw_t = valid ? omw<R>(P, t) : R(0);
+  for (int64_t pix = blockIdx.x; pix < io.npix; pix += gridDim.x) {
+    const size_t base = size_t(pix) * 4 * P.nl;
+    const float* sl_pix = (P.slight_mode == PM_SLIGHT_PER_PIXEL) ? io.slight + base : nullptr;
+    if (t < 11) sm.model[t] = io.models_in[size_t(pix) * 11 + t];
+    __syncthreads();
+    R S[4], Su[4];
+    synthesize_wide<R, G>(P, sm, sm.model, sl_pix, t, valid, dl_t, omw_t, S, Su);
+    if (valid) {
+#pragma unroll
+      for (int s = 0; s < 4; ++s) io.spectra_out[base + s * P.nl + t] = float(S[s]);
+    }
+    if (io.rf_out) {
+      __syncthreads();  // the model terms from thread 0
+      R d[KT][4];
+      rf_wide<R, KT, G>(P, sm, t, valid, omw_t, Su, sl_pix, d);
+      if (valid) {
+        const size_t rb = size_t(pix) * 4 * KT * P.nl;
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+#pragma unroll
+          for (int r = 0; r < KT; ++r) io.rf_out[rb + (size_t(s) * KT + r) * P.nl + t] = float(d[r][s]);
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -1265,6 +1812,80 @@ int launch_synth(const PmParams& P, const PmIO& io, cudaStream_t st) {
   return PM_OK;
 }
 
+template <typename R, int KT, int G, int MINB>
+int launch_invert_wide(const PmParams& P, const PmIO& io, cudaStream_t st, int num_sms, float* kernel_ms) {
+  const int threads = 32 * G;
+  const size_t smem = sizeof(WideSmem<R, G>);
+  auto kern = invert_wide_kernel<R, KT, G, MINB>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return snprintf(g_err, sizeof g_err, "%s", cudaGetErrorString(e)), PM_EIO;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+  if (e != cudaSuccess || per_sm < 1) return snprintf(g_err, sizeof g_err, "occupancy: %s", cudaGetErrorString(e)), PM_EIO;
+  int64_t blocks = int64_t(per_sm) * num_sms;
+  if (blocks > io.npix) blocks = io.npix > 0 ? io.npix : 1;
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (kernel_ms) {
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, st);
+  }
+  if (P.classical) {
+    int64_t cb = io.npix;
+    if (cb > int64_t(num_sms) * (64 / G)) cb = int64_t(num_sms) * (64 / G);
+    if (cb < 1) cb = 1;
+    classical_wide_kernel<G><<<unsigned(cb), threads, 0, st>>>(P, io);
+  }
+  kern<<<unsigned(blocks), threads, smem, st>>>(P, io);
+  e = cudaGetLastError();
+  if (kernel_ms) {
+    cudaEventRecord(b, st);
+    cudaEventSynchronize(b);
+    cudaEventElapsedTime(kernel_ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  }
+  if (e != cudaSuccess) return snprintf(g_err, sizeof g_err, "invert launch: %s", cudaGetErrorString(e)), PM_EIO;
+  return PM_OK;
+}
+
+template <typename R, int KT, int G>
+int launch_synth_wide(const PmParams& P, const PmIO& io, cudaStream_t st) {
+  const int threads = 32 * G;
+  const size_t smem = sizeof(WideSmem<R, G>);
+  auto kern = synth_wide_kernel<R, KT, G>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return snprintf(g_err, sizeof g_err, "%s", cudaGetErrorString(e)), PM_EIO;
+  int64_t blocks = io.npix;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  if (blocks < 1) blocks = 1;
+  kern<<<unsigned(blocks), threads, smem, st>>>(P, io);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return snprintf(g_err, sizeof g_err, "synth launch: %s", cudaGetErrorString(e)), PM_EIO;
+  return PM_OK;
+}
+
+template <typename R, int KT>
+int launch_invert_any(const PmParams& P, const PmIO& io, cudaStream_t st, int num_sms, float* kernel_ms,
+                      int variant) {
+  constexpr bool f32 = sizeof(R) == 4;
+  if (P.G == 2) return launch_invert_wide<R, KT, 2, f32 ? 8 : 1>(P, io, st, num_sms, kernel_ms);
+  if (P.G == 4) return launch_invert_wide<R, KT, 4, f32 ? 4 : 1>(P, io, st, num_sms, kernel_ms);
+  if constexpr (f32) {
+    return variant == 1 ? launch_invert<float, KT, 4>(P, io, st, num_sms, kernel_ms)
+                        : launch_invert<float, KT, 3>(P, io, st, num_sms, kernel_ms);
+  } else {
+    return launch_invert<double, KT, 1>(P, io, st, num_sms, kernel_ms);
+  }
+}
+
+template <typename R, int KT>
+int launch_synth_any(const PmParams& P, const PmIO& io, cudaStream_t st) {
+  if (P.G == 2) return launch_synth_wide<R, KT, 2>(P, io, st);
+  if (P.G == 4) return launch_synth_wide<R, KT, 4>(P, io, st);
+  return launch_synth<R, KT>(P, io, st);
+}
+
 }  // namespace
 
 // variant: occupancy target of the FP32 kernel (register cap): 0 = 3 blocks
@@ -1272,16 +1893,16 @@ int launch_synth(const PmParams& P, const PmIO& io, cudaStream_t st) {
 int pmk_invert(const PmParams& P, const PmIO& io, int precision, int variant, void* stream, int num_sms,
                float* kernel_ms) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (P.G != 1 && P.G != 2 && P.G != 4) {
+    snprintf(g_err, sizeof g_err, "nl=%d: no kernel for %d warps per pixel", P.nl, P.G);
+    return PM_ERANGE;
+  }
   if (precision == PM_PREC_FP32) {
-    if (P.K == 9)
-      return variant == 1 ? launch_invert<float, 9, 4>(P, io, st, num_sms, kernel_ms)
-                          : launch_invert<float, 9, 3>(P, io, st, num_sms, kernel_ms);
-    if (P.K == 10)
-      return variant == 1 ? launch_invert<float, 10, 4>(P, io, st, num_sms, kernel_ms)
-                          : launch_invert<float, 10, 3>(P, io, st, num_sms, kernel_ms);
+    if (P.K == 9) return launch_invert_any<float, 9>(P, io, st, num_sms, kernel_ms, variant);
+    if (P.K == 10) return launch_invert_any<float, 10>(P, io, st, num_sms, kernel_ms, variant);
   } else {
-    if (P.K == 9) return launch_invert<double, 9, 1>(P, io, st, num_sms, kernel_ms);
-    if (P.K == 10) return launch_invert<double, 10, 1>(P, io, st, num_sms, kernel_ms);
+    if (P.K == 9) return launch_invert_any<double, 9>(P, io, st, num_sms, kernel_ms, variant);
+    if (P.K == 10) return launch_invert_any<double, 10>(P, io, st, num_sms, kernel_ms, variant);
   }
   snprintf(g_err, sizeof g_err, "nterms=%d has no compiled kernel", P.K);
   return PM_ENOTSUP;
@@ -1289,12 +1910,16 @@ int pmk_invert(const PmParams& P, const PmIO& io, int precision, int variant, vo
 
 int pmk_synth(const PmParams& P, const PmIO& io, int precision, void* stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (P.G != 1 && P.G != 2 && P.G != 4) {
+    snprintf(g_err, sizeof g_err, "nl=%d: no kernel for %d warps per pixel", P.nl, P.G);
+    return PM_ERANGE;
+  }
   if (precision == PM_PREC_FP32) {
-    if (P.K == 9) return launch_synth<float, 9>(P, io, st);
-    if (P.K == 10) return launch_synth<float, 10>(P, io, st);
+    if (P.K == 9) return launch_synth_any<float, 9>(P, io, st);
+    if (P.K == 10) return launch_synth_any<float, 10>(P, io, st);
   } else {
-    if (P.K == 9) return launch_synth<double, 9>(P, io, st);
-    if (P.K == 10) return launch_synth<double, 10>(P, io, st);
+    if (P.K == 9) return launch_synth_any<double, 9>(P, io, st);
+    if (P.K == 10) return launch_synth_any<double, 10>(P, io, st);
   }
   snprintf(g_err, sizeof g_err, "nterms=%d has no compiled kernel", P.K);
   return PM_ENOTSUP;

@@ -30,7 +30,8 @@
 namespace {
 
 constexpr int64_t kMaxPix = PM_NOALLOC_MAX_PIXELS;
-constexpr size_t kProf = sizeof(float) * 4 * PMK_NL;  // one pixel's profiles at the largest grid
+constexpr int kMaxNl = PM_NOALLOC_MAX_WAVELENGTHS;
+constexpr size_t kProf = sizeof(float) * 4 * kMaxNl;  // one pixel's profiles at the largest grid
 constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 constexpr size_t kOffCtr = 0;
 constexpr size_t kOffSpectro = align256(kOffCtr + sizeof(unsigned long long) * PMC_COUNT);
@@ -105,6 +106,12 @@ extern "C" int pm_invert_batch_noalloc(const pm_line* line, const pm_config* cfg
     return pmh_fail(PM_ERANGE, msg);
   }
   if (guess->mac != 0.0) return pmh_fail(PM_ENOTSUP, "macroturbulence (guess.mac > 0) is outside this implementation");
+  if (cfg->nlambda > kMaxNl) {
+    char msg[160];
+    std::snprintf(msg, sizeof msg, "pm_invert_batch_noalloc: %d wavelengths exceed the static scratch (at most %d)",
+                  cfg->nlambda, kMaxNl);
+    return pmh_fail(PM_ERANGE, msg);
+  }
   PmParams P;
   int rc = pmh_fill_params(line, cfg, P);
   if (rc != PM_OK) return rc;

@@ -10,10 +10,8 @@
 
 #include "../../include/pmilos.h"
 
-// Wavelengths handled by one warp in this build: one per lane.
-#define PMK_NL 32
-// Centred-tap table length for the profile-per-lane correlation.
-#define PMK_GC (2 * PMK_NL - 1)
+// Largest wavelength grid: one thread per wavelength, up to four warps per pixel.
+#define PMK_NL 128
 
 struct PmParams {
   int nl;          // wavelengths
@@ -28,6 +26,8 @@ struct PmParams {
   int slight_mode; // PM_SLIGHT_*
   int want_rf;     // synth kernel: also write response functions
   int n_pi, n_sig;
+  int G;           // warps per pixel: 1 (nl <= 32), 2 (nl <= 64) or 4 (nl <= 128)
+  int tap_lo, tap_hi;  // PSF support: taps outside [tap_lo, tap_hi] are below 1e-18 of the peak
   int fix[11];
   int zero_row[PM_NTERMS_MAX];  // FijaACeroDerivadasNoNecesarias (milosUtils.c:199-227)
   int ff_row;      // RF row that holds d/d(filling factor), or -1
@@ -41,8 +41,8 @@ struct PmParams {
   double guess[11];
   double taps_d[PMK_NL];                   // G[j], zero for j >= nl
   float taps_f[PMK_NL];
-  double gc_d[PMK_GC];                     // gc[t] = G[t - (PMK_NL-1) + half] inside [0,nl), else 0
-  float gc_f[PMK_GC];
+  double omw_d[PMK_NL];                    // 1 - sum of the taps [tap_lo, tap_hi] that land inside the grid at output k
+  float omw_f[PMK_NL];
   double sl_d[4 * PMK_NL];                 // shared stray-light profile [4][nl]
   float sl_f[4 * PMK_NL];
 };

@@ -15,6 +15,11 @@ Writes
                       plus mil_sinrf + me_der outputs at 12 models
   ref_psf.npz         the reference's fgauss_WL and interpolationLinearPSF on the
                       configuration grids (host precompute pinning)
+  ref_cases_wide.npz  the same per-case content on grids wider than one warp:
+                      w112 (112 points of Fe I 6302 at 21.5 mA, 25 mA PSF, the
+                      large-cube configuration) and w49 (the known-answer test's
+                      49-point grid with a 60 mA PSF, stray light and the filling
+                      factor inverted); 16 pixels each
 The fixtures are what the CPU test-suite compares the oracle restatement and the
 host precompute with, so those tests need neither the reference nor a GPU.
 """
@@ -69,15 +74,26 @@ def kat(refdir):
                 expected=gold[:, 2:].T.copy(), expected_offsets=gold[:, 1].copy(), nterms=10)
 
 
-def case(cfg, seed, npix=48):
+# grid (ini, step, fin, lambda0), PSF FWHM [mA] (None = no PSF), stray light + filling factor
+CASE_SPECS = {
+    0: ((-350.0, 25.0, 375.0, 6173.3354), None, False),
+    1: ((-350.0, 25.0, 375.0, 6173.3354), 60.0, False),
+    2: ((-350.0, 25.0, 375.0, 6173.3354), 60.0, True),
+    112: ((-1204.0, 21.5, 1182.5, 6302.4936), 25.0, False),
+    49: ((-600.0, 25.0, 600.0, 6173.3356), 60.0, True),
+}
+
+
+def case(cfg, seed, npix=48, nsynth=12):
     rng = np.random.default_rng(1000 + cfg)
-    offs, lam = grid(-350.0, 25.0, 375.0, 6173.3354)
+    (ini, step, fin, l0), fwhm, stray = CASE_SPECS[cfg]
+    offs, lam = grid(ini, step, fin, l0)
     psf = None
-    setup0 = po.LineSetup(lam, 6173.3354, TRIPLET, None, 9)
-    if cfg in (1, 2):
-        x, y = gauss_table(60.0)
+    setup0 = po.LineSetup(lam, l0, TRIPLET, None, 9)
+    if fwhm is not None:
+        x, y = gauss_table(fwhm)
         psf = po.Reference(setup0, "f64").interp_psf(x, y, offs, 0.0)
-    K = 10 if cfg == 2 else 9
+    K = 10 if stray else 9
     fix = [1] * 9 + [0, 1 if K == 10 else 0]
     guess = GUESS.copy()
     if K == 10:
@@ -94,17 +110,17 @@ def case(cfg, seed, npix=48):
     truth[:, 8] = rng.uniform(0.4, 0.9, npix)
     truth[:, 10] = 1.0
     slight = None
-    if cfg == 2:
+    if stray:
         weak = np.arange(npix) % 10 < 7
         truth[weak, 1] = rng.uniform(0, 200, weak.sum())
         truth[weak, 0] = rng.uniform(1, 5, weak.sum())
         truth[~weak, 1] = rng.uniform(1500, 3500, (~weak).sum())
         truth[:, 10] = 1.0 - rng.uniform(0, 0.3, npix)
-        r9 = po.Reference(po.LineSetup(lam, 6173.3354, TRIPLET, psf, 9), "f64")
+        r9 = po.Reference(po.LineSetup(lam, l0, TRIPLET, psf, 9), "f64")
         slight, _ = r9.synth(np.array([13.0, 0.0, 0.2, 0.035, 0.19, 30.0, 30.0, 0.26, 0.74, 0.0, 1.0]), rf=False)
         slight = slight.astype(np.float32).astype(np.float64)
-    setup = po.LineSetup(lam, 6173.3354, TRIPLET, psf, K)
-    out = dict(lam=lam, offs=offs, psf=np.zeros(0) if psf is None else psf, truth=truth, guess=guess,
+    setup = po.LineSetup(lam, l0, TRIPLET, psf, K)
+    out = dict(lam=lam, offs=offs, lambda0=l0, psf=np.zeros(0) if psf is None else psf, truth=truth, guess=guess,
                fix=np.array(fix, dtype=np.int32), nterms=K, slight=np.zeros(0) if slight is None else slight)
     ref64 = po.Reference(setup, "f64")
     obs = np.array([ref64.synth(m, slight, fix=fix, rf=False)[0] for m in truth], dtype=np.float32)
@@ -119,7 +135,7 @@ def case(cfg, seed, npix=48):
         r = ref.invert(obs, guess, slight=slight, fix=fix, noise=noise)
         for k in ("models", "chisq", "iters", "spectra"):
             out[f"{flav}_{k}"] = r[k]
-        models = truth[:12].copy()
+        models = truth[:nsynth].copy()
         sp, rf = zip(*[ref.synth(m, slight, fix=fix) for m in models])
         out[f"{flav}_synth_models"] = models
         out[f"{flav}_synth"] = np.array(sp)
@@ -159,17 +175,26 @@ def psf_pins():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--only", choices=("all", "wide"), default="all")
     a = ap.parse_args()
     os.environ["PM_REFERENCE_SRC"] = os.path.join(a.reference, "src")
     po.build()
-    np.savez_compressed(os.path.join(HERE, "kat_synthesis.npz"), **kat(a.reference))
-    cases = {}
-    for cfg in (0, 1, 2):
-        for k, v in case(cfg, cfg).items():
-            cases[f"c{cfg}_{k}"] = v
-    np.savez_compressed(os.path.join(HERE, "ref_cases.npz"), **cases)
-    np.savez_compressed(os.path.join(HERE, "ref_psf.npz"), **psf_pins())
-    for f in ("kat_synthesis.npz", "ref_cases.npz", "ref_psf.npz"):
+    files = ["ref_cases_wide.npz"]
+    if a.only == "all":
+        np.savez_compressed(os.path.join(HERE, "kat_synthesis.npz"), **kat(a.reference))
+        cases = {}
+        for cfg in (0, 1, 2):
+            for k, v in case(cfg, cfg).items():
+                cases[f"c{cfg}_{k}"] = v
+        np.savez_compressed(os.path.join(HERE, "ref_cases.npz"), **cases)
+        np.savez_compressed(os.path.join(HERE, "ref_psf.npz"), **psf_pins())
+        files += ["kat_synthesis.npz", "ref_cases.npz", "ref_psf.npz"]
+    wide = {}
+    for cfg in (112, 49):
+        for k, v in case(cfg, cfg, npix=16, nsynth=4).items():
+            wide[f"w{cfg}_{k}"] = v
+    np.savez_compressed(os.path.join(HERE, "ref_cases_wide.npz"), **wide)
+    for f in files:
         print(f, os.path.getsize(os.path.join(HERE, f)), "bytes")
 
 

@@ -92,3 +92,30 @@ def test_restatement_matches_reference_on_fresh_models():
             a, da = ref.synth(m)
             b, db = own.synth(m)
             assert np.array_equal(a, b) and np.array_equal(da, db)
+
+
+WIDE = np.load(os.path.join(GOLDEN, "ref_cases_wide.npz"))
+
+
+def _wide_setup(name):
+    g = lambda k: WIDE[f"{name}_{k}"]
+    psf = g("psf") if g("psf").size else None
+    return po.LineSetup(g("lam"), float(g("lambda0")), np.array([1.0, 2, 1, 1, 2, 2, 0]), psf, int(g("nterms")))
+
+
+@pytest.mark.parametrize("flav", ["f32", "f64"])
+@pytest.mark.parametrize("name", ["w112", "w49"])
+def test_wide_grids_bit_exact(name, flav):
+    """Grids wider than one warp (112 and 49 wavelengths): synthesis, response
+    functions and full inversions of the restatement equal the reference's."""
+    g = lambda k: WIDE[f"{name}_{k}"]
+    ora = po.Restatement(_wide_setup(name), flav)
+    sl = g("slight") if g("slight").size else None
+    fix = list(g("fix"))
+    for m, sp_ref, rf_ref in zip(g(f"{flav}_synth_models"), g(f"{flav}_synth"), g(f"{flav}_rf")):
+        sp, rf = ora.synth(m, sl, fix=fix)
+        assert np.array_equal(sp, sp_ref)
+        assert np.array_equal(rf, rf_ref)
+    r = ora.invert(g("obs"), g("guess"), slight=sl, fix=fix, noise=_noise(flav))
+    for k in ("iters", "chisq", "models", "spectra"):
+        assert np.array_equal(r[k], g(f"{flav}_{k}")), k
