@@ -155,11 +155,113 @@ def cpu_baseline(w, obs, sample_pixels: int, cores: int):
     return n / wall, info
 
 
+def _mem_available() -> int:
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return 0
+
+
 def host_cores() -> int:
     try:
         return len(os.sched_getaffinity(0))
     except AttributeError:
         return os.cpu_count() or 1
+
+
+# ---- served stream (configuration 3) ----
+SIZES = (256 * 256, 512 * 512, 1024 * 1024, 2048 * 2048)
+
+
+def bench_served(args, rank: int, world: int, metric: str):
+    """Poisson stream of scans (mean 20/s) through pm_server: each scan a cube of
+    256^2..2048^2 pixels on one of the 6/15/30-point grids, FP32; then the first
+    --plain-requests scans of the same schedule on a plain FP64 server."""
+    import torch
+
+    import pmilos_b200 as pm
+    from pmilos_b200 import workloads
+
+    # N > 1: replicas, every rank serves its own stream (no collective)
+    line = pm.LineData(workloads.FE6173, workloads.TRIPLET)
+    specs = [workloads.config(3, npix=1, grid=g) for g in range(3)]
+
+    def grids(precision):
+        return [pm.Grid(lam=w.lam, psf=w.psf, guess=w.guess, noise=w.noise, fix=w.fix, nterms=9,
+                        precision=precision) for w in specs]
+
+    rng = np.random.default_rng(3 + 1000 * rank)
+    n = args.requests + args.warmup
+    arrivals = np.cumsum(rng.exponential(1.0 / 20.0, n))
+    sizes = rng.choice(len(SIZES), n)
+    which = rng.choice(3, n)
+    # one pinned cube per (size, grid): synthesized on the device, FP64, seeded
+    pool = {}
+    for si, g in sorted(set(zip(sizes.tolist(), which.tolist()))):
+        w = workloads.config(3, npix=SIZES[si], grid=g)
+        with pm.Inverter(w.line, w.lam, w.psf, noise=w.noise, fix=w.fix, nterms=9, precision=pm.PREC_FP64) as inv64:
+            d = workloads.synthesize_device(w, inv64, seed=100 * si + g + 1000 * rank)
+        h = torch.empty(tuple(d.shape), dtype=torch.float32, pin_memory=True)
+        h.copy_(d)
+        del d
+        pool[(si, g)] = h.numpy()
+    torch.cuda.empty_cache()
+
+    def run(precision, count):
+        lat, pix, infos = [], 0, []
+        with pm.Server(line, grids(precision), hbm_budget_bytes=int(args.budget_gb * (1 << 30)), max_inflight=64,
+                       linger_ms=5.0) as srv:
+            for i in range(min(args.warmup, count)):  # warm-up scans (untimed): smallest cube of each grid
+                srv.wait(srv.submit(int(which[i]), pool[(0, int(which[i]))] if (0, int(which[i])) in pool else
+                                    pool[(int(sizes[i]), int(which[i]))]))
+            t0 = time.perf_counter()
+            ids = []
+            for i in range(args.warmup, args.warmup + count):
+                dt = t0 + (arrivals[i] - arrivals[args.warmup]) - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                ids.append(srv.submit(int(which[i]), pool[(int(sizes[i]), int(which[i]))], want_status=False))
+            for sid in ids:
+                r = srv.wait(sid)
+                infos.append(r["info"])
+            st = srv.stats()
+        first = min(x["submit_ms"] for x in infos)
+        last = max(x["done_ms"] for x in infos)
+        lat = np.array([x["done_ms"] - x["submit_ms"] for x in infos])
+        pix = sum(x["npix"] for x in infos)
+        its = sum(x["iterations"] for x in infos)
+        return {"pixels_per_s": pix / ((last - first) / 1000.0), "pixels": int(pix), "scans": len(infos),
+                "wall_ms": last - first, "latency_p50_ms": float(np.percentile(lat, 50)),
+                "latency_p99_ms": float(np.percentile(lat, 99)), "latency_max_ms": float(lat.max()),
+                "kernel_launches": st["kernel_launches"], "arena_peak_gib": st["arena_peak_bytes"] / 2**30,
+                "iterations_per_pixel": its / pix}
+
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        fp32 = run(pm.PREC_FP32, args.requests)
+    plain = run(pm.PREC_FP64, min(args.plain_requests, args.requests)) if args.plain_requests > 0 else None
+    h2d = sum(pool[(int(sizes[i]), int(which[i]))].nbytes for i in range(args.warmup, n)) / args.requests
+    d2h = sum(SIZES[int(sizes[i])] for i in range(args.warmup, n)) * (11 * 8 + 4 + 4) / args.requests
+    cfg_desc = {"workload": "served stream: Poisson scans (mean 20/s), cubes of 256^2..2048^2 pixels on 6/15/30-point "
+                            "grids around Fe I 6173.3354 A, 60 mA PSF, 9 free parameters, config-2 atmosphere mix",
+                "scans": args.requests, "hbm_budget_gib": args.budget_gb, "parallelism": f"replicas x{world}",
+                "l2": "scan cubes (up to 2 GB) exceed L2; no flush"}
+    if rank == 0:
+        print(json.dumps({
+            "metric": metric + " (served stream)", "value": fp32["pixels_per_s"], "unit": "pixels/s",
+            "n_gpus": world, "steps": args.requests, "warmup": args.warmup,
+            "ms_per_step": fp32["wall_ms"] / args.requests, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg_desc,
+            "e2e": {"value": fp32["pixels_per_s"], "unit": "pixels/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h,
+                    "note": "host clock from each scan's submit (host buffers) to its results in host memory"},
+            "latency_ms": {"p50": fp32["latency_p50_ms"], "p99": fp32["latency_p99_ms"],
+                           "max": fp32["latency_max_ms"]},
+            "served_fp32": fp32, "plain_fp64": plain, "clocks": clk.summary(),
+            "gpu_launches": fp32["kernel_launches"]}), flush=True)
 
 
 # ---- main ----
@@ -175,6 +277,12 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--plain-npix", type=int, default=None,
+                    help="pixels of the cube the plain FP64 forms invert (default: all, or 2^18 above 2^20)")
+    ap.add_argument("--requests", type=int, default=48, help="served stream (configuration 3): scans timed")
+    ap.add_argument("--plain-requests", type=int, default=12,
+                    help="served stream: scans of the same schedule timed on the plain FP64 server")
+    ap.add_argument("--budget-gb", type=float, default=24.0, help="served stream: device arena of the server")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -206,7 +314,7 @@ def main():
         rng = np.random.default_rng(w.seed)
         truth = workloads.truth_models(w, rng)
         cores = host_cores()
-        n = args.cpu_sample or min(w.npix, 1500 * cores)
+        n = args.cpu_sample or min(w.npix, (1500 if w.nl <= 32 else 200) * cores)
         ora = po.Restatement(po.LineSetup(w.lam, w.line.lambda0, w.line.cuantic_dat(), w.psf, w.nterms), "f64")
         obs = np.array([ora.synth(m, None, fix=w.fix, rf=False)[0] for m in truth[:n]], dtype=np.float32)
         obs += rng.normal(0, 1e-3, obs.shape).astype(np.float32)
@@ -226,6 +334,8 @@ def main():
         return
 
     torch.cuda.set_device(local)
+    if args.config == 3:
+        return bench_served(args, rank, world, metric)
     dist = None
     if world > 1:
         import datetime
@@ -237,8 +347,13 @@ def main():
     inv32 = pm.Inverter(w.line, w.lam, w.psf, noise=w.noise, fix=w.fix, nterms=w.nterms, precision=pm.PREC_FP32)
     inv64 = pm.Inverter(w.line, w.lam, w.psf, noise=w.noise, fix=w.fix, nterms=w.nterms, precision=pm.PREC_FP64)
     rng = np.random.default_rng(w.seed + 1000 * rank)
-    obs = workloads.synthesize(w, inv_fp64=inv64, rng=rng)
-    obs_d = torch.as_tensor(obs, device="cuda")
+    if w.npix * w.nl * 16 > (4 << 30):
+        # cubes above 4 GB are drawn and synthesized on the device, in chunks
+        obs = None
+        obs_d = workloads.synthesize_device(w, inv64, seed=w.seed + 1000 * rank)
+    else:
+        obs = workloads.synthesize(w, inv_fp64=inv64, rng=rng)
+        obs_d = torch.as_tensor(obs, device="cuda")
     sl_h = None if w.slight is None else np.ascontiguousarray(w.slight, dtype=np.float32)
     sl_d = None if sl_h is None else torch.as_tensor(sl_h, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
@@ -248,9 +363,10 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    def step_device(inv):
+    def step_device(inv, cube=None):
         flush.fill_(1)  # L2 flush outside the timed kernel
-        r = inv.invert(obs_d, w.guess, slight=sl_d, want_spectra=False, want_status=False)
+        r = inv.invert(obs_d if cube is None else cube, w.guess, slight=sl_d, want_spectra=False,
+                       want_status=False)
         s = inv.stats()
         return r, s
 
@@ -264,7 +380,7 @@ def main():
             kms.append(s["kernel_ms"])
             iters += s["iterations"]
             acc += s["accepted"]
-            launches += 1
+            launches += 2  # classical-estimates pre-pass + inversion kernel
         barrier()
     ms = float(np.mean(kms))
     if dist is not None:
@@ -274,9 +390,17 @@ def main():
     value = world * w.npix / (ms / 1000.0)
 
     # e2e: host buffers (pinned) through the C ABI; copies inside the timed region
-    e2e_v = None
-    if not args.no_e2e:
-        obs_pinned = torch.from_numpy(obs).pin_memory().numpy()
+    e2e_v, e2e_note = None, None
+    cube_bytes = obs_d.numel() * 4
+    if not args.no_e2e and obs is None and _mem_available() < 3 * cube_bytes:
+        e2e_note = f"not measured: {cube_bytes / 2**30:.1f} GiB cube, host memory available {_mem_available() / 2**30:.1f} GiB"
+    elif not args.no_e2e:
+        if obs is None:
+            pinned = torch.empty(tuple(obs_d.shape), dtype=torch.float32, pin_memory=True)
+            pinned.copy_(obs_d)
+        else:
+            pinned = torch.from_numpy(obs).pin_memory()
+        obs_pinned = pinned.numpy()
         for _ in range(max(1, args.warmup)):
             inv32.invert(obs_pinned, w.guess, slight=sl_h, want_spectra=False, want_status=False)
         e2e_ms = []
@@ -286,23 +410,29 @@ def main():
             inv32.invert(obs_pinned, w.guess, slight=sl_h, want_spectra=False, want_status=False)
             e2e_ms.append(inv32.stats()["total_ms"])
         e2e_v = world * w.npix / (float(np.mean(e2e_ms)) / 1000.0)
-    h2d = obs.nbytes
+        del obs_pinned, pinned
+    h2d = cube_bytes
     d2h = w.npix * (11 * 8 + 4 + 4)
 
     # plain FP64 forms on the same cube (fewer steps: slower)
     plain = {}
     if not args.no_plain:
+        pn = args.plain_npix or (w.npix if w.npix <= (1 << 20) else (1 << 18))
+        sub = obs_d[:pn]
         for name, solver in (("fp64_eigen", pm.SOLVE_EIGEN), ("fp64_cholesky", pm.SOLVE_CHOLESKY)):
             with pm.Inverter(w.line, w.lam, w.psf, noise=w.noise, fix=w.fix, nterms=w.nterms,
                              precision=pm.PREC_FP64, solver=solver) as inv:
-                step_device(inv)
+                step_device(inv, sub)
                 t = []
                 for _ in range(max(1, min(2, args.steps))):
-                    t.append(step_device(inv)[1]["kernel_ms"])
-                plain[name] = {"value": w.npix / (float(np.mean(t)) / 1000.0), "unit": "pixels/s",
-                               "ms_per_step": float(np.mean(t))}
+                    t.append(step_device(inv, sub)[1]["kernel_ms"])
+                plain[name] = {"value": pn / (float(np.mean(t)) / 1000.0), "unit": "pixels/s",
+                               "ms_per_step": float(np.mean(t)), "pixels": pn}
 
-    fm = flop_model(w.nl, w.nl, w.nterms, w.psf is not None, w.slight is not None)
+    # taps per output: every tap for one-warp grids (the reference's direct
+    # convolution), the support above 1e-18 of the peak on multi-warp grids
+    taps = w.nl if w.nl <= 32 else workloads.psf_support(w.psf)
+    fm = flop_model(w.nl, taps, w.nterms, w.psf is not None, w.slight is not None)
     f32, f64 = flops(fm, w.npix * args.steps, iters, acc)
     kernel_s = sum(kms) / 1000.0
     clocks = clk.summary()
@@ -331,8 +461,9 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cores = host_cores()
-        n = args.cpu_sample or min(w.npix, 1500 * cores)
-        v, info = cpu_baseline(w, obs, n, cores)
+        n = args.cpu_sample or min(w.npix, (1500 if w.nl <= 32 else 200) * cores)
+        sample = obs if obs is not None else obs_d[:n].cpu().numpy()
+        v, info = cpu_baseline(w, sample, n, cores)
         cpu = {"value": v, "unit": "pixels/s", "cores": info["cores"], "kind": info["kind"],
                "sample": info["sample"]}
 
@@ -341,7 +472,8 @@ def main():
             "metric": metric, "value": value, "unit": "pixels/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg_desc,
-            "e2e": {"value": e2e_v, "unit": "pixels/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "e2e": {"value": e2e_v, "unit": "pixels/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    **({"note": e2e_note} if e2e_note else {})},
             "plain": plain, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
             "gpu_launches": launches}), flush=True)
     inv32.close()

@@ -140,9 +140,26 @@ typedef struct pm_stats {
   int64_t eigen_fallbacks;/* CHOLESKY solves that fell back to EIGEN */
   double kernel_ms;       /* device time of the inversion kernel (CUDA events) */
   double total_ms;        /* device time of the whole call incl. copies */
+  int64_t graph_replays;  /* calls served by replaying a captured CUDA graph (pm_tuning.graphs) */
 } pm_stats;
 
 typedef struct pm_ctx pm_ctx;
+
+/* Launch choices of a context (what pm_autotune picks).  No counterpart in the
+ * reference, which has no device launches to tune. */
+#define PM_STAGING_MAX 64
+typedef struct pm_tuning {
+  int variant;          /* FP32 register budget per thread: 0 = 168 (3 blocks of 4 warps per SM),
+                           1 = 128 (4 blocks per SM, a few spills) */
+  int staging_depth;    /* host-buffer calls on grids of <= 32 wavelengths: the cube is copied in this
+                           many pieces while the inversion kernel already runs (1..PM_STAGING_MAX);
+                           0 = copy everything, then launch */
+  int warps_per_block;  /* pixels (one warp each) per block of the one-warp kernels: 1, 2 or 4 */
+  int graphs;           /* 1: host-buffer calls of at most PM_GRAPH_MAX_PIXELS pixels on grids of <= 32
+                           wavelengths (pm_lm_mils among them) stage through pinned memory and replay a
+                           CUDA graph of the whole call, captured once per size; 0: no graphs */
+} pm_tuning;
+#define PM_GRAPH_MAX_PIXELS 1024
 
 /* ---- host-side precompute (no GPU needed) ---- */
 
@@ -213,6 +230,75 @@ int pm_lm_mils(pm_ctx *ctx, const float *spectro, pm_model *init_model, float *s
 int pm_invert_batch_noalloc(const pm_line *line, const pm_config *cfg, int64_t npix, const float *spectro,
                             const float *slight, int slight_mode, const pm_model *guess, pm_model *models_out,
                             float *chisq_out, int *iters_out, float *best_fit_out, int *status_out, void *stream);
+
+/* ---- serving: continuous batching of spectral scans ----
+ *
+ * No counterpart in the reference, whose drivers invert one cube per process
+ * run.  A server holds up to PM_SERVER_MAX_GRIDS wavelength grids (line, grid,
+ * PSF and settings resident on the device; every grid has <= 32 wavelengths and
+ * all share nterms and precision) and a device arena of hbm_budget_bytes.  A
+ * scheduler thread admits submitted scans in arrival order as arena space and
+ * in-flight slots free up: it copies each admitted scan to the device and
+ * publishes its pixels to one persistent inversion kernel that is already
+ * running, so scans that arrive while others are on the GPU join them; the
+ * results of each scan are copied back as soon as its last pixel is done.
+ * Scans on different grids share the launch.  Each pixel's arithmetic is the
+ * same whatever else is in flight. */
+#define PM_SERVER_MAX_GRIDS 4
+#define PM_SERVER_MAX_INFLIGHT 256
+#define PM_ETIMEDOUT (-110)   /* pm_server_wait: the scan did not finish in time */
+
+typedef struct pm_server pm_server;
+
+typedef struct pm_server_config {
+  size_t hbm_budget_bytes;  /* device arena for admitted scans (inputs + results) */
+  int max_inflight;         /* scans admitted at once: 1 .. PM_SERVER_MAX_INFLIGHT */
+  double linger_ms;         /* an idle persistent kernel exits after this long (relaunched on demand) */
+} pm_server_config;
+
+typedef struct pm_scan_info {
+  int64_t npix;
+  int grid;
+  int rc;                   /* PM_OK, or the error that ended the scan */
+  double submit_ms, admit_ms, done_ms;  /* host monotonic clock, from server creation */
+  int64_t iterations;       /* summed over the scan's pixels */
+} pm_scan_info;
+
+typedef struct pm_server_stats {
+  int64_t scans_done, pixels_done, kernel_launches;
+  double latency_p50_ms, latency_p99_ms, latency_max_ms;  /* submit -> results in host memory */
+  double busy_ms;           /* first submit -> last completion */
+  size_t arena_peak_bytes;
+} pm_server_stats;
+
+/* grids[g], guesses[g]: the settings and initial model of grid g (g < ngrids). */
+int pm_server_create(const pm_line *line, const pm_config *const *grids, const pm_model *guesses, int ngrids,
+                     const pm_server_config *sc, pm_server **out);
+/* Queue a scan of npix pixels on grid `grid`: spectro [npix][4][nl] in host
+ * memory (pinned memory lets its copy overlap the kernel); results into the
+ * host arrays models_out, chisq_out, iters_out, status_out (nullable).  The
+ * arrays must stay valid until the scan is done.  Returns at once with the
+ * scan's id; PM_ERANGE if the scan alone exceeds the arena. */
+int pm_server_submit(pm_server *srv, int grid, int64_t npix, const float *spectro, pm_model *models_out,
+                     float *chisq_out, int *iters_out, int *status_out, uint64_t *id_out);
+/* Block until scan `id` is done (its results are in the host arrays) or
+ * timeout_s passes (PM_ETIMEDOUT).  info (nullable) gets its timings. */
+int pm_server_wait(pm_server *srv, uint64_t id, double timeout_s, pm_scan_info *info);
+int pm_server_get_stats(pm_server *srv, pm_server_stats *out);
+/* Finishes every queued scan, then stops the scheduler and frees the device state. */
+int pm_server_destroy(pm_server *srv);
+
+int pm_get_tuning(const pm_ctx *ctx, pm_tuning *out);
+int pm_set_tuning(pm_ctx *ctx, const pm_tuning *in);
+
+/* Autotuner: inverts npix sample pixels (host buffers, the same call path as
+ * pm_invert_batch with PM_MEM_HOST, so copies and kernel are both timed) once per
+ * candidate tuning and repetition, and keeps the fastest tuning in the context.
+ * Candidates: variant {0, 1} x warps_per_block {1, 2, 4} x staging_depth
+ * {0, 4, 16}.  *out (nullable) receives the choice.  No counterpart in the
+ * reference. */
+int pm_autotune(pm_ctx *ctx, int64_t npix, const float *spectro, const float *slight, int slight_mode,
+                const pm_model *guess, int reps, pm_tuning *out);
 
 int pm_get_stats(const pm_ctx *ctx, pm_stats *out);
 const char *pm_last_error(void);

@@ -63,15 +63,60 @@ struct DevBuf {
 
 }  // namespace
 
+// Pinned host words the streamed calls copy from and read back into.
+struct HostCtl {
+  unsigned long long avail[PM_STAGING_MAX];  // published ticket counts, one per piece
+  unsigned long long one;                    // 1: the value of PmStreamQ::closed
+  PmJob job;
+  PmStreamQ qinit;                           // queue state before a fully published launch
+  PmStreamQ qread;                           // queue state after the kernel (counters, err)
+};
+
+// A captured CUDA graph of a whole small host-buffer call (uploads from pinned
+// staging, job and queue, kernel, downloads into pinned staging) and what it
+// was captured for: a replay is valid while all of these are unchanged.
+struct SmallGraph {
+  cudaGraphExec_t exec = nullptr;
+  int64_t npix = -1;
+  int slight_mode = -1;
+  bool spectra = false, status = false;
+  pm_tuning tuning{};
+  void* dev[8] = {};
+  std::vector<unsigned char> params;
+};
+constexpr int kGraphCache = 4;
+constexpr size_t kProfMax = sizeof(float) * 4 * 32;  // one pixel's profiles, one-warp grids
+
+// Pinned staging of the graph path, PM_GRAPH_MAX_PIXELS pixels of each array.
+struct SmallStage {
+  float spectro[PM_GRAPH_MAX_PIXELS * 4 * 32];
+  float slight[PM_GRAPH_MAX_PIXELS * 4 * 32];
+  float spectra[PM_GRAPH_MAX_PIXELS * 4 * 32];
+  pm_model models[PM_GRAPH_MAX_PIXELS];
+  float chisq[PM_GRAPH_MAX_PIXELS];
+  int iters[PM_GRAPH_MAX_PIXELS];
+  int status[PM_GRAPH_MAX_PIXELS];
+};
+
 struct pm_ctx {
   PmParams P;
   int precision = PM_PREC_FP32;
-  int variant = 0;  // kernel variant (occupancy target), see pmk_invert
+  pm_tuning tuning{0, 8, 4, 1};
   int device = 0;
   int num_sms = 148;
   cudaStream_t stream = nullptr;
-  int64_t chunk = 1 << 20;  // pixels per staging chunk in host mode
+  size_t resident_bytes = size_t(8) << 30;  // device staging of one host-mode chunk
   DevBuf spectro, slight, models, chisq, iters, spectra, status, rf, ctr;
+  // streamed host-buffer calls: kernel and copy streams, the ticket queue, one job
+  cudaStream_t s_kern = nullptr, s_copy = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_q = nullptr, ev_done = nullptr, t0 = nullptr, t1 = nullptr, k0 = nullptr,
+              k1 = nullptr;
+  DevBuf q, jobs;
+  HostCtl* hc = nullptr;
+  PmGridSet* gs = nullptr;  // kernel parameters of the streamed kernel (the context's one grid)
+  SmallGraph graphs[kGraphCache];
+  int graph_next = 0;
+  SmallStage* stage = nullptr;  // pinned
   pm_stats stats{};
 };
 
@@ -312,7 +357,6 @@ int set_slight(PmParams& P, const float* slight, int mode, int mem) {
       std::memcpy(h.data(), slight, sizeof(float) * 4 * P.nl);
     }
     for (int i = 0; i < 4 * P.nl; ++i) {
-      P.sl_d[i] = h[i];
       P.sl_f[i] = h[i];
     }
     return PM_OK;
@@ -353,7 +397,8 @@ extern "C" int pm_ctx_create(const pm_line* line, const pm_config* cfg, void* st
                 prop.minor);
   }
   c->num_sms = prop.multiProcessorCount;
-  if (const char* v = std::getenv("PMILOS_VARIANT")) c->variant = std::atoi(v);
+  if (const char* v = std::getenv("PMILOS_VARIANT")) c->tuning.variant = std::atoi(v);
+  if (const char* v = std::getenv("PMILOS_STAGING")) c->tuning.staging_depth = std::atoi(v);
   rc = c->ctr.ensure(sizeof(unsigned long long) * PMC_COUNT);
   if (rc != PM_OK) {
     delete c;
@@ -367,27 +412,357 @@ extern "C" int pm_ctx_destroy(pm_ctx* c) {
   if (!c) return PM_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
   else cudaDeviceSynchronize();
+  if (c->s_kern) cudaStreamSynchronize(c->s_kern);
+  if (c->s_copy) cudaStreamSynchronize(c->s_copy);
   for (DevBuf* b : {&c->spectro, &c->slight, &c->models, &c->chisq, &c->iters, &c->spectra, &c->status, &c->rf,
-                    &c->ctr})
+                    &c->ctr, &c->q, &c->jobs})
     b->release();
+  for (cudaEvent_t ev : {c->ev_start, c->ev_q, c->ev_done, c->t0, c->t1, c->k0, c->k1})
+    if (ev) cudaEventDestroy(ev);
+  if (c->s_kern) cudaStreamDestroy(c->s_kern);
+  if (c->s_copy) cudaStreamDestroy(c->s_copy);
+  if (c->hc) cudaFreeHost(c->hc);
+  if (c->stage) cudaFreeHost(c->stage);
+  for (SmallGraph& g : c->graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  delete c->gs;
   delete c;
   return PM_OK;
 }
 
 namespace {
 
-// One launch over n pixels whose buffers are all device pointers.
+// Resources of the streamed launches, created on first use.
+int stream_resources(pm_ctx* c) {
+  if (c->hc) return PM_OK;
+  PM_CUDA(cudaStreamCreateWithFlags(&c->s_kern, cudaStreamNonBlocking), "stream create");
+  PM_CUDA(cudaStreamCreateWithFlags(&c->s_copy, cudaStreamNonBlocking), "stream create");
+  for (cudaEvent_t* ev : {&c->ev_start, &c->ev_q, &c->ev_done})
+    PM_CUDA(cudaEventCreateWithFlags(ev, cudaEventDisableTiming), "event create");
+  for (cudaEvent_t* ev : {&c->t0, &c->t1, &c->k0, &c->k1}) PM_CUDA(cudaEventCreate(ev), "event create");
+  int rc = c->q.ensure(sizeof(PmStreamQ));
+  if (rc == PM_OK) rc = c->jobs.ensure(sizeof(PmJob));
+  if (rc != PM_OK) return rc;
+  c->gs = new (std::nothrow) PmGridSet();
+  if (!c->gs) return fail(PM_ENOMEM, "out of host memory");
+  void* h = nullptr;
+  PM_CUDA(cudaHostAlloc(&h, sizeof(HostCtl), cudaHostAllocDefault), "cudaHostAlloc");
+  std::memset(h, 0, sizeof(HostCtl));
+  c->hc = static_cast<HostCtl*>(h);
+  c->hc->one = 1;
+  return PM_OK;
+}
+
+// One resident chunk of a host-buffer inversion, streamed: the persistent
+// kernel starts at once and inverts the pixels of each piece as soon as the
+// copy engine has brought it in (pieces are published through the ticket
+// queue); the results come back after the kernel.  Pieces hold a multiple of
+// 32 pixels, so no 128-byte line of the cube spans two pieces.
+int run_streamed(pm_ctx* c, int64_t n, const float* spectro, const float* slight, int slight_mode,
+                 pm_model* models_out, float* chisq_out, int* iters_out, float* best_fit_out, int* status_out,
+                 float* kernel_ms, float* total_ms) {
+  int rc = stream_resources(c);
+  if (rc != PM_OK) return rc;
+  const int nl = c->P.nl;
+  const size_t prof = sizeof(float) * 4 * nl;
+  HostCtl* hc = c->hc;
+  PmJob& job = hc->job;
+  std::memset(&job, 0, sizeof job);
+  job.t0 = 0;
+  job.npix = n;
+  job.grid = 0;
+  job.spectro = static_cast<const float*>(c->spectro.p);
+  job.slight = slight_mode == PM_SLIGHT_PER_PIXEL ? static_cast<const float*>(c->slight.p) : nullptr;
+  job.models = static_cast<double*>(c->models.p);
+  job.chisq = static_cast<float*>(c->chisq.p);
+  job.iters = static_cast<int*>(c->iters.p);
+  job.status = status_out ? static_cast<int*>(c->status.p) : nullptr;
+  job.spectra = best_fit_out ? static_cast<float*>(c->spectra.p) : nullptr;
+  PmStreamQ* q = static_cast<PmStreamQ*>(c->q.p);
+
+  // order after the caller's earlier work on its stream
+  PM_CUDA(cudaEventRecord(c->ev_start, c->stream), "event");
+  PM_CUDA(cudaStreamWaitEvent(c->s_copy, c->ev_start, 0), "wait");
+  PM_CUDA(cudaStreamWaitEvent(c->s_kern, c->ev_start, 0), "wait");
+  PM_CUDA(cudaEventRecord(c->t0, c->s_copy), "event");
+  PM_CUDA(cudaMemsetAsync(q, 0, sizeof(PmStreamQ), c->s_copy), "queue reset");
+  PM_CUDA(cudaMemcpyAsync(c->jobs.p, &job, sizeof(PmJob), cudaMemcpyHostToDevice, c->s_copy), "job H2D");
+  PM_CUDA(cudaEventRecord(c->ev_q, c->s_copy), "event");
+  PM_CUDA(cudaStreamWaitEvent(c->s_kern, c->ev_q, 0), "wait");
+
+  c->gs->ngrids = 1;
+  c->gs->g[0] = c->P;
+  PmStreamIO sio{};
+  sio.q = q;
+  sio.jobs = static_cast<const PmJob*>(c->jobs.p);
+  sio.jobs_cap = 1;
+  sio.first_job = 0;
+  sio.linger_ns = -1;
+  sio.wait_limit_ns = 20000000000LL;  // 20 s without a published piece: give up (PMQ_ERR_WAIT)
+  PM_CUDA(cudaEventRecord(c->k0, c->s_kern), "event");
+  rc = pmk_invert_stream(*c->gs, sio, c->precision, c->tuning.variant, c->tuning.warps_per_block, false, c->s_kern,
+                         c->num_sms, nullptr);
+  if (rc != PM_OK) {
+    cudaStreamSynchronize(c->s_copy);
+    return fail(rc, "%s", pmk_last_cuda_error());
+  }
+  PM_CUDA(cudaEventRecord(c->k1, c->s_kern), "event");
+
+  const int pieces = std::max(1, std::min(c->tuning.staging_depth, PM_STAGING_MAX));
+  int64_t per = (n + pieces - 1) / pieces;
+  per = std::max<int64_t>(32, (per + 31) / 32 * 32);
+  int i = 0;
+  cudaError_t ce = cudaSuccess;
+  for (int64_t p0 = 0; p0 < n && ce == cudaSuccess; p0 += per, ++i) {
+    const int64_t m = std::min(per, n - p0);
+    ce = cudaMemcpyAsync(static_cast<char*>(c->spectro.p) + prof * p0, spectro + p0 * 4 * nl, prof * m,
+                         cudaMemcpyHostToDevice, c->s_copy);
+    if (ce == cudaSuccess && slight_mode == PM_SLIGHT_PER_PIXEL)
+      ce = cudaMemcpyAsync(static_cast<char*>(c->slight.p) + prof * p0, slight + p0 * 4 * nl, prof * m,
+                           cudaMemcpyHostToDevice, c->s_copy);
+    hc->avail[i] = (unsigned long long)(p0 + m);
+    if (ce == cudaSuccess)
+      ce = cudaMemcpyAsync(&q->avail, &hc->avail[i], sizeof(unsigned long long), cudaMemcpyHostToDevice,
+                           c->s_copy);
+  }
+  // closed after the last piece (and after a failed copy, so that the kernel ends)
+  const cudaError_t ce2 = cudaMemcpyAsync(&q->closed, &hc->one, sizeof(unsigned long long), cudaMemcpyHostToDevice,
+                                          c->s_copy);
+  if (ce != cudaSuccess || ce2 != cudaSuccess) {
+    cudaStreamSynchronize(c->s_kern);
+    return cuda_fail(ce != cudaSuccess ? ce : ce2, "streamed H2D");
+  }
+  PM_CUDA(cudaMemcpyAsync(models_out, c->models.p, sizeof(pm_model) * n, cudaMemcpyDeviceToHost, c->s_kern),
+          "models D2H");
+  PM_CUDA(cudaMemcpyAsync(chisq_out, c->chisq.p, sizeof(float) * n, cudaMemcpyDeviceToHost, c->s_kern), "chisq D2H");
+  PM_CUDA(cudaMemcpyAsync(iters_out, c->iters.p, sizeof(int) * n, cudaMemcpyDeviceToHost, c->s_kern), "iters D2H");
+  if (best_fit_out)
+    PM_CUDA(cudaMemcpyAsync(best_fit_out, c->spectra.p, prof * n, cudaMemcpyDeviceToHost, c->s_kern),
+            "best fit D2H");
+  if (status_out)
+    PM_CUDA(cudaMemcpyAsync(status_out, c->status.p, sizeof(int) * n, cudaMemcpyDeviceToHost, c->s_kern),
+            "status D2H");
+  PM_CUDA(cudaMemcpyAsync(&hc->qread, q, sizeof(PmStreamQ), cudaMemcpyDeviceToHost, c->s_kern), "queue D2H");
+  PM_CUDA(cudaEventRecord(c->t1, c->s_kern), "event");
+  PM_CUDA(cudaEventRecord(c->ev_done, c->s_kern), "event");
+  PM_CUDA(cudaStreamWaitEvent(c->stream, c->ev_done, 0), "wait");
+  PM_CUDA(cudaEventSynchronize(c->t1), "streamed inversion");
+  PM_CUDA(cudaStreamSynchronize(c->s_copy), "streamed H2D");
+  if (hc->qread.err)
+    return fail(PM_EIO, "streamed inversion: %s", hc->qread.err == PMQ_ERR_WAIT ? "a piece never arrived (wait limit)"
+                                                                                : "ticket without a job");
+  if (hc->qread.next != (unsigned long long)n)
+    return fail(PM_EIO, "streamed inversion: %llu of %lld pixels handed out", hc->qread.next, (long long)n);
+  cudaEventElapsedTime(kernel_ms, c->k0, c->k1);
+  cudaEventElapsedTime(total_ms, c->t0, c->t1);
+  c->stats.pixels += n;
+  c->stats.iterations += int64_t(hc->qread.ctr[PMC_ITERS]);
+  c->stats.accepted += int64_t(hc->qread.ctr[PMC_ACCEPTED]);
+  c->stats.eigen_fallbacks += int64_t(hc->qread.ctr[PMC_FALLBACK]);
+  return PM_OK;
+}
+
+// A small host-buffer call (npix <= PM_GRAPH_MAX_PIXELS, one-warp grid) as one
+// CUDA graph: the caller's arrays are staged through pinned memory, so that
+// the graph's copies always use the same addresses and one capture per size
+// (and parameter block, tuning and device buffers) serves every later call.
+int run_graph_small(pm_ctx* c, int64_t n, const float* spectro, const float* slight, int slight_mode,
+                    pm_model* models_out, float* chisq_out, int* iters_out, float* best_fit_out, int* status_out) {
+  int rc = stream_resources(c);
+  if (rc != PM_OK) return rc;
+  if (!c->stage) {
+    void* h = nullptr;
+    PM_CUDA(cudaHostAlloc(&h, sizeof(SmallStage), cudaHostAllocDefault), "cudaHostAlloc");
+    c->stage = static_cast<SmallStage*>(h);
+  }
+  const size_t kg = PM_GRAPH_MAX_PIXELS;
+  for (DevBuf* b : {&c->spectro, &c->slight, &c->spectra})
+    if ((rc = b->ensure(kProfMax * kg)) != PM_OK) return rc;
+  if ((rc = c->models.ensure(sizeof(pm_model) * kg)) != PM_OK) return rc;
+  for (DevBuf* b : {&c->chisq, &c->iters, &c->status})
+    if ((rc = b->ensure(sizeof(float) * kg)) != PM_OK) return rc;
+  const int nl = c->P.nl;
+  const size_t prof = sizeof(float) * 4 * nl;
+  SmallStage* st = c->stage;
+  HostCtl* hc = c->hc;
+  PmStreamQ* q = static_cast<PmStreamQ*>(c->q.p);
+  const bool want_spectra = best_fit_out != nullptr, want_status = status_out != nullptr;
+  PmJob& job = hc->job;
+  std::memset(&job, 0, sizeof job);
+  job.npix = n;
+  job.spectro = static_cast<const float*>(c->spectro.p);
+  job.slight = slight_mode == PM_SLIGHT_PER_PIXEL ? static_cast<const float*>(c->slight.p) : nullptr;
+  job.models = static_cast<double*>(c->models.p);
+  job.chisq = static_cast<float*>(c->chisq.p);
+  job.iters = static_cast<int*>(c->iters.p);
+  job.status = want_status ? static_cast<int*>(c->status.p) : nullptr;
+  job.spectra = want_spectra ? static_cast<float*>(c->spectra.p) : nullptr;
+  std::memset(&hc->qinit, 0, sizeof hc->qinit);
+  hc->qinit.avail = (unsigned long long)n;
+  hc->qinit.closed = 1;
+  c->gs->ngrids = 1;
+  c->gs->g[0] = c->P;
+  void* dev[8] = {c->spectro.p, c->slight.p, c->spectra.p, c->models.p, c->chisq.p, c->iters.p, c->status.p, c->q.p};
+  const unsigned char* pb = reinterpret_cast<const unsigned char*>(&c->P);
+
+  SmallGraph* G = nullptr;
+  for (SmallGraph& g : c->graphs) {
+    if (g.exec && g.npix == n && g.slight_mode == slight_mode && g.spectra == want_spectra &&
+        g.status == want_status && std::memcmp(&g.tuning, &c->tuning, sizeof g.tuning) == 0 &&
+        std::memcmp(g.dev, dev, sizeof dev) == 0 && g.params.size() == sizeof(PmParams) &&
+        std::memcmp(g.params.data(), pb, sizeof(PmParams)) == 0) {
+      G = &g;
+      break;
+    }
+  }
+  if (!G) {
+    G = &c->graphs[c->graph_next];
+    c->graph_next = (c->graph_next + 1) % kGraphCache;
+    if (G->exec) cudaGraphExecDestroy(G->exec);
+    G->exec = nullptr;
+    cudaStream_t s = c->s_kern;
+    PM_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed), "graph capture");
+    cudaError_t e = cudaMemcpyAsync(c->spectro.p, st->spectro, prof * n, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && slight_mode == PM_SLIGHT_PER_PIXEL)
+      e = cudaMemcpyAsync(c->slight.p, st->slight, prof * n, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c->jobs.p, &hc->job, sizeof(PmJob), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(q, &hc->qinit, sizeof(PmStreamQ), cudaMemcpyHostToDevice, s);
+    int krc = PM_OK;
+    if (e == cudaSuccess) {
+      PmStreamIO sio{};
+      sio.q = q;
+      sio.jobs = static_cast<const PmJob*>(c->jobs.p);
+      sio.jobs_cap = 1;
+      sio.linger_ns = -1;
+      sio.wait_limit_ns = 20000000000LL;
+      krc = pmk_invert_stream(*c->gs, sio, c->precision, c->tuning.variant, c->tuning.warps_per_block, false, s,
+                              c->num_sms, nullptr);
+    }
+    if (e == cudaSuccess && krc == PM_OK)
+      e = cudaMemcpyAsync(st->models, c->models.p, sizeof(pm_model) * n, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && krc == PM_OK)
+      e = cudaMemcpyAsync(st->chisq, c->chisq.p, sizeof(float) * n, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && krc == PM_OK)
+      e = cudaMemcpyAsync(st->iters, c->iters.p, sizeof(int) * n, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && krc == PM_OK && want_status)
+      e = cudaMemcpyAsync(st->status, c->status.p, sizeof(int) * n, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && krc == PM_OK && want_spectra)
+      e = cudaMemcpyAsync(st->spectra, c->spectra.p, prof * n, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && krc == PM_OK)
+      e = cudaMemcpyAsync(&hc->qread, q, sizeof(PmStreamQ), cudaMemcpyDeviceToHost, s);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(s, &graph);
+    if (krc != PM_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return fail(krc, "%s", pmk_last_cuda_error());
+    }
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      return cuda_fail(e != cudaSuccess ? e : e2, "graph capture");
+    }
+    e = cudaGraphInstantiate(&G->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      G->exec = nullptr;
+      return cuda_fail(e, "graph instantiate");
+    }
+    G->npix = n;
+    G->slight_mode = slight_mode;
+    G->spectra = want_spectra;
+    G->status = want_status;
+    G->tuning = c->tuning;
+    std::memcpy(G->dev, dev, sizeof dev);
+    G->params.assign(pb, pb + sizeof(PmParams));
+  }
+  std::memcpy(st->spectro, spectro, prof * n);
+  if (slight_mode == PM_SLIGHT_PER_PIXEL) std::memcpy(st->slight, slight, prof * n);
+  PM_CUDA(cudaEventRecord(c->ev_start, c->stream), "event");
+  PM_CUDA(cudaStreamWaitEvent(c->s_kern, c->ev_start, 0), "wait");
+  PM_CUDA(cudaEventRecord(c->t0, c->s_kern), "event");
+  PM_CUDA(cudaGraphLaunch(G->exec, c->s_kern), "graph launch");
+  PM_CUDA(cudaEventRecord(c->t1, c->s_kern), "event");
+  PM_CUDA(cudaEventRecord(c->ev_done, c->s_kern), "event");
+  PM_CUDA(cudaStreamWaitEvent(c->stream, c->ev_done, 0), "wait");
+  PM_CUDA(cudaEventSynchronize(c->t1), "graph replay");
+  if (hc->qread.err || hc->qread.next != (unsigned long long)n)
+    return fail(PM_EIO, "inversion kernel: queue error %llu, %llu of %lld pixels handed out", hc->qread.err,
+                hc->qread.next, (long long)n);
+  std::memcpy(models_out, st->models, sizeof(pm_model) * n);
+  std::memcpy(chisq_out, st->chisq, sizeof(float) * n);
+  std::memcpy(iters_out, st->iters, sizeof(int) * n);
+  if (want_status) std::memcpy(status_out, st->status, sizeof(int) * n);
+  if (want_spectra) std::memcpy(best_fit_out, st->spectra, prof * n);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->t0, c->t1);
+  c->stats.kernel_ms = ms;
+  c->stats.pixels += n;
+  c->stats.iterations += int64_t(hc->qread.ctr[PMC_ITERS]);
+  c->stats.accepted += int64_t(hc->qread.ctr[PMC_ACCEPTED]);
+  c->stats.eigen_fallbacks += int64_t(hc->qread.ctr[PMC_FALLBACK]);
+  c->stats.graph_replays += 1;
+  return PM_OK;
+}
+
+// One launch over n pixels whose buffers are all device pointers.  One-warp
+// grids: the streamed kernel with every pixel published before the launch (the
+// same compiled code as the pipelined host-buffer path and the server).
 int run_invert(pm_ctx* c, PmIO io, float* kernel_ms) {
-  PM_CUDA(cudaMemsetAsync(io.ctr, 0, sizeof(unsigned long long) * PMC_COUNT, c->stream), "counter reset");
-  int rc = pmk_invert(c->P, io, c->precision, c->variant, c->stream, c->num_sms, kernel_ms);
+  if (c->P.G != 1) {
+    PM_CUDA(cudaMemsetAsync(io.ctr, 0, sizeof(unsigned long long) * PMC_COUNT, c->stream), "counter reset");
+    int rc = pmk_invert(c->P, io, c->precision, c->stream, c->num_sms, kernel_ms);
+    if (rc != PM_OK) return fail(rc, "%s", pmk_last_cuda_error());
+    unsigned long long h[PMC_COUNT];
+    PM_CUDA(cudaMemcpyAsync(h, io.ctr, sizeof h, cudaMemcpyDeviceToHost, c->stream), "counter D2H");
+    PM_CUDA(cudaStreamSynchronize(c->stream), "invert kernel");
+    c->stats.pixels += io.npix;
+    c->stats.iterations += int64_t(h[PMC_ITERS]);
+    c->stats.accepted += int64_t(h[PMC_ACCEPTED]);
+    c->stats.eigen_fallbacks += int64_t(h[PMC_FALLBACK]);
+    return PM_OK;
+  }
+  int rc = stream_resources(c);
+  if (rc != PM_OK) return rc;
+  HostCtl* hc = c->hc;
+  PmJob& job = hc->job;
+  std::memset(&job, 0, sizeof job);
+  job.npix = io.npix;
+  job.spectro = io.spectro;
+  job.slight = io.slight;
+  job.models = io.models_out;
+  job.chisq = io.chisq_out;
+  job.iters = io.iters_out;
+  job.status = io.status_out;
+  job.spectra = io.spectra_out;
+  std::memset(&hc->qinit, 0, sizeof hc->qinit);
+  hc->qinit.avail = (unsigned long long)io.npix;
+  hc->qinit.closed = 1;
+  PmStreamQ* q = static_cast<PmStreamQ*>(c->q.p);
+  PM_CUDA(cudaMemcpyAsync(c->jobs.p, &job, sizeof job, cudaMemcpyHostToDevice, c->stream), "job H2D");
+  PM_CUDA(cudaMemcpyAsync(q, &hc->qinit, sizeof hc->qinit, cudaMemcpyHostToDevice, c->stream), "queue H2D");
+  c->gs->ngrids = 1;
+  c->gs->g[0] = c->P;
+  PmStreamIO sio{};
+  sio.q = q;
+  sio.jobs = static_cast<const PmJob*>(c->jobs.p);
+  sio.jobs_cap = 1;
+  sio.first_job = 0;
+  sio.linger_ns = -1;
+  sio.wait_limit_ns = 20000000000LL;
+  PM_CUDA(cudaEventRecord(c->k0, c->stream), "event");
+  rc = pmk_invert_stream(*c->gs, sio, c->precision, c->tuning.variant, c->tuning.warps_per_block, false, c->stream,
+                         c->num_sms, nullptr);
   if (rc != PM_OK) return fail(rc, "%s", pmk_last_cuda_error());
-  unsigned long long h[PMC_COUNT];
-  PM_CUDA(cudaMemcpyAsync(h, io.ctr, sizeof h, cudaMemcpyDeviceToHost, c->stream), "counter D2H");
+  PM_CUDA(cudaEventRecord(c->k1, c->stream), "event");
+  PM_CUDA(cudaMemcpyAsync(&hc->qread, q, sizeof(PmStreamQ), cudaMemcpyDeviceToHost, c->stream), "queue D2H");
   PM_CUDA(cudaStreamSynchronize(c->stream), "invert kernel");
+  if (hc->qread.err || hc->qread.next != (unsigned long long)io.npix)
+    return fail(PM_EIO, "inversion kernel: queue error %llu, %llu of %lld pixels handed out", hc->qread.err,
+                hc->qread.next, (long long)io.npix);
+  if (kernel_ms) cudaEventElapsedTime(kernel_ms, c->k0, c->k1);
   c->stats.pixels += io.npix;
-  c->stats.iterations += int64_t(h[PMC_ITERS]);
-  c->stats.accepted += int64_t(h[PMC_ACCEPTED]);
-  c->stats.eigen_fallbacks += int64_t(h[PMC_FALLBACK]);
+  c->stats.iterations += int64_t(hc->qread.ctr[PMC_ITERS]);
+  c->stats.accepted += int64_t(hc->qread.ctr[PMC_ACCEPTED]);
+  c->stats.eigen_fallbacks += int64_t(hc->qread.ctr[PMC_FALLBACK]);
   return PM_OK;
 }
 
@@ -425,8 +800,15 @@ extern "C" int pm_invert_batch(pm_ctx* c, int64_t npix, const float* spectro, co
     io.status_out = status_out;
     io.ctr = static_cast<unsigned long long*>(c->ctr.p);
     rc = run_invert(c, io, &kms_total);
+  } else if (c->P.G == 1 && c->tuning.graphs && npix <= PM_GRAPH_MAX_PIXELS) {
+    rc = run_graph_small(c, npix, spectro, slight, slight_mode, models_out, chisq_out, iters_out, best_fit_out,
+                         status_out);
+    kms_total = float(c->stats.kernel_ms);
   } else {
-    const int64_t chunk = std::min<int64_t>(npix, c->chunk);
+    // pixels per resident chunk: the device copies of one chunk's inputs and outputs fit resident_bytes
+    const size_t per_pixel = prof * (1 + (slight_mode == PM_SLIGHT_PER_PIXEL) + (best_fit_out != nullptr)) +
+                             sizeof(pm_model) + sizeof(float) + 2 * sizeof(int);
+    const int64_t chunk = std::min<int64_t>(npix, std::max<int64_t>(32, int64_t(c->resident_bytes / per_pixel)));
     if ((rc = c->spectro.ensure(prof * chunk)) != PM_OK) return rc;
     if (slight_mode == PM_SLIGHT_PER_PIXEL && (rc = c->slight.ensure(prof * chunk)) != PM_OK) return rc;
     if ((rc = c->models.ensure(sizeof(pm_model) * chunk)) != PM_OK) return rc;
@@ -435,7 +817,17 @@ extern "C" int pm_invert_batch(pm_ctx* c, int64_t npix, const float* spectro, co
     if (best_fit_out && (rc = c->spectra.ensure(prof * chunk)) != PM_OK) return rc;
     if (status_out && (rc = c->status.ensure(sizeof(int) * chunk)) != PM_OK) return rc;
     pm_stats acc{};
-    for (int64_t p0 = 0; p0 < npix && rc == PM_OK; p0 += chunk) {
+    const bool streamed = c->P.G == 1 && c->tuning.staging_depth > 0;
+    for (int64_t p0 = 0; p0 < npix && rc == PM_OK && streamed; p0 += chunk) {
+      const int64_t n = std::min(chunk, npix - p0);
+      float kms = 0, tms = 0;
+      rc = run_streamed(c, n, spectro + p0 * 4 * nl, slight_mode == PM_SLIGHT_PER_PIXEL ? slight + p0 * 4 * nl : slight,
+                        slight_mode, models_out + p0, chisq_out + p0, iters_out + p0,
+                        best_fit_out ? best_fit_out + p0 * 4 * nl : nullptr, status_out ? status_out + p0 : nullptr,
+                        &kms, &tms);
+      kms_total += kms;
+    }
+    for (int64_t p0 = 0; p0 < npix && rc == PM_OK && !streamed; p0 += chunk) {
       const int64_t n = std::min(chunk, npix - p0);
       PM_CUDA(cudaMemcpyAsync(c->spectro.p, spectro + p0 * 4 * nl, prof * n, cudaMemcpyHostToDevice, c->stream),
               "spectro H2D");
@@ -475,7 +867,7 @@ extern "C" int pm_invert_batch(pm_ctx* c, int64_t npix, const float* spectro, co
         PM_CUDA(cudaMemcpyAsync(status_out + p0, c->status.p, sizeof(int) * n, cudaMemcpyDeviceToHost, c->stream),
                 "status D2H");
     }
-    c->stats = acc;
+    if (!streamed) c->stats = acc;
   }
   cudaEventRecord(t1, c->stream);
   cudaEventSynchronize(t1);
@@ -548,6 +940,72 @@ extern "C" int pm_lm_mils(pm_ctx* c, const float* spectro, pm_model* init_model,
   *chisqrf = chi;
   *iter = it;
   return status == PM_PIX_NFREE ? -1 : 1;
+}
+
+extern "C" int pm_get_tuning(const pm_ctx* c, pm_tuning* out) {
+  if (!c || !out) return fail(PM_EINVAL, "pm_get_tuning: NULL argument");
+  *out = c->tuning;
+  return PM_OK;
+}
+
+extern "C" int pm_set_tuning(pm_ctx* c, const pm_tuning* in) {
+  if (!c || !in) return fail(PM_EINVAL, "pm_set_tuning: NULL argument");
+  if (in->variant != 0 && in->variant != 1) return fail(PM_EINVAL, "pm_set_tuning: variant=%d", in->variant);
+  if (in->staging_depth < 0 || in->staging_depth > PM_STAGING_MAX)
+    return fail(PM_EINVAL, "pm_set_tuning: staging_depth=%d (0..%d)", in->staging_depth, PM_STAGING_MAX);
+  if (in->warps_per_block != 1 && in->warps_per_block != 2 && in->warps_per_block != 4)
+    return fail(PM_EINVAL, "pm_set_tuning: warps_per_block=%d (1, 2 or 4)", in->warps_per_block);
+  if (in->graphs != 0 && in->graphs != 1) return fail(PM_EINVAL, "pm_set_tuning: graphs=%d (0 or 1)", in->graphs);
+  c->tuning = *in;
+  return PM_OK;
+}
+
+// The autotuner: every candidate inverts the caller's sample through the
+// host-buffer entry point (copies + kernel), the fastest median total time wins.
+extern "C" int pm_autotune(pm_ctx* c, int64_t npix, const float* spectro, const float* slight, int slight_mode,
+                           const pm_model* guess, int reps, pm_tuning* out) {
+  if (!c || !spectro || !guess) return fail(PM_EINVAL, "pm_autotune: NULL argument");
+  if (npix < 1) return fail(PM_EINVAL, "pm_autotune: npix=%lld", (long long)npix);
+  reps = std::max(1, std::min(reps, 16));
+  std::vector<pm_model> models(static_cast<size_t>(npix));
+  std::vector<float> chi(static_cast<size_t>(npix));
+  std::vector<int> its(static_cast<size_t>(npix));
+  std::vector<pm_tuning> cands;
+  const bool fp32 = c->precision == PM_PREC_FP32;
+  for (int variant : {0, 1}) {
+    if (!fp32 && variant != c->tuning.variant) continue;  // the FP64 kernel has one register budget
+    for (int wpb : {1, 2, 4})
+      for (int depth : {0, 4, 16}) {
+        if (c->P.G != 1 && depth != 0) continue;  // multi-warp grids are not streamed
+        cands.push_back(pm_tuning{variant, depth, wpb, c->tuning.graphs});
+      }
+  }
+  const pm_tuning saved = c->tuning;
+  pm_tuning best = saved;
+  double best_ms = 1e300;
+  for (const pm_tuning& t : cands) {
+    c->tuning = t;
+    std::vector<double> ms;
+    for (int r = 0; r <= reps; ++r) {
+      const int rc = pm_invert_batch(c, npix, spectro, slight, slight_mode, guess, models.data(), chi.data(),
+                                     its.data(), nullptr, nullptr, PM_MEM_HOST);
+      if (rc != PM_OK) {
+        c->tuning = saved;
+        return rc;
+      }
+      if (r > 0) ms.push_back(c->stats.total_ms);  // the first run is a warm-up
+    }
+    std::sort(ms.begin(), ms.end());
+    const double med = ms[ms.size() / 2];
+    if (med < best_ms) {
+      best_ms = med;
+      best = t;
+    }
+  }
+  c->tuning = best;
+  c->stats = pm_stats{};
+  if (out) *out = best;
+  return PM_OK;
 }
 
 extern "C" int pm_get_stats(const pm_ctx* c, pm_stats* out) {

@@ -12,13 +12,15 @@
 //
 // How.  Everything the call needs on the device beyond the caller's own arrays
 // lives in one file-scope static device array, g_noalloc_scratch (about 6.5 MB,
-// fixed at build time): the work-queue/statistics counters and staging room for
-// at most PM_NOALLOC_MAX_PIXELS pixels of up to 32 wavelengths (observed
-// profiles, a per-pixel stray-light cube, models, chi^2, iterations, status,
-// best-fit profiles).  Every GPU that loads the library holds this memory until
-// the process exits.  The run constants go in the kernel's by-value parameter
-// block, so no context is needed either.  The call makes no cudaMalloc/cudaFree
-// (nor any other allocating call) and creates no CUDA events or streams.
+// fixed at build time): the ticket queue with its statistics counters, the job
+// descriptor, and staging room for at most PM_NOALLOC_MAX_PIXELS pixels of up to
+// 32 wavelengths (observed profiles, a per-pixel stray-light cube, models,
+// chi^2, iterations, status, best-fit profiles).  Every GPU that loads the
+// library holds this memory until the process exits.  The run constants go in
+// the kernel's by-value parameter block, so no context is needed either.  The
+// inversion is the streamed kernel of every one-warp call path, with all pixels
+// published before the launch.  The call makes no cudaMalloc/cudaFree (nor any
+// other allocating call) and creates no CUDA events or streams.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -33,8 +35,9 @@ constexpr int64_t kMaxPix = PM_NOALLOC_MAX_PIXELS;
 constexpr int kMaxNl = PM_NOALLOC_MAX_WAVELENGTHS;
 constexpr size_t kProf = sizeof(float) * 4 * kMaxNl;  // one pixel's profiles at the largest grid
 constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
-constexpr size_t kOffCtr = 0;
-constexpr size_t kOffSpectro = align256(kOffCtr + sizeof(unsigned long long) * PMC_COUNT);
+constexpr size_t kOffQueue = 0;
+constexpr size_t kOffJob = align256(kOffQueue + sizeof(PmStreamQ));
+constexpr size_t kOffSpectro = align256(kOffJob + sizeof(PmJob));
 constexpr size_t kOffSlight = align256(kOffSpectro + kMaxPix * kProf);
 constexpr size_t kOffModels = align256(kOffSlight + kMaxPix * kProf);
 constexpr size_t kOffChisq = align256(kOffModels + kMaxPix * sizeof(pm_model));
@@ -122,7 +125,6 @@ extern "C" int pm_invert_batch_noalloc(const pm_line* line, const pm_config* cfg
     if (P.K != 10) return pmh_fail(PM_EINVAL, "stray light requires nterms == 10 (filling factor inverted)");
     if (slight_mode == PM_SLIGHT_SHARED) {
       for (int i = 0; i < 4 * P.nl; ++i) {
-        P.sl_d[i] = slight[i];
         P.sl_f[i] = slight[i];
       }
     } else if (slight_mode != PM_SLIGHT_PER_PIXEL) {
@@ -136,12 +138,9 @@ extern "C" int pm_invert_batch_noalloc(const pm_line* line, const pm_config* cfg
   if (rc != PM_OK) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const size_t prof = sizeof(float) * 4 * P.nl;
-  unsigned long long* ctr = reinterpret_cast<unsigned long long*>(base + kOffCtr);
+  PmStreamQ* q = reinterpret_cast<PmStreamQ*>(base + kOffQueue);
+  PmJob* job_dev = reinterpret_cast<PmJob*>(base + kOffJob);
   cudaError_t e;
-  // the scratch keeps the previous call's contents: the work-queue counters must
-  // start at zero
-  if ((e = cudaMemsetAsync(ctr, 0, sizeof(unsigned long long) * PMC_COUNT, st)) != cudaSuccess)
-    return cuda_err(e, "counter reset");
   if ((e = cudaMemcpyAsync(base + kOffSpectro, spectro, prof * npix, cudaMemcpyHostToDevice, st)) != cudaSuccess)
     return cuda_err(e, "spectro H2D");
   if (slight_mode == PM_SLIGHT_PER_PIXEL &&
@@ -149,15 +148,41 @@ extern "C" int pm_invert_batch_noalloc(const pm_line* line, const pm_config* cfg
     return cuda_err(e, "slight H2D");
   PmIO io{};
   io.npix = npix;
-  io.spectro = reinterpret_cast<const float*>(base + kOffSpectro);
-  io.slight = slight_mode == PM_SLIGHT_PER_PIXEL ? reinterpret_cast<const float*>(base + kOffSlight) : nullptr;
   io.models_out = reinterpret_cast<double*>(base + kOffModels);
   io.chisq_out = reinterpret_cast<float*>(base + kOffChisq);
   io.iters_out = reinterpret_cast<int*>(base + kOffIters);
   io.status_out = status_out ? reinterpret_cast<int*>(base + kOffStatus) : nullptr;
   io.spectra_out = best_fit_out ? reinterpret_cast<float*>(base + kOffBest) : nullptr;
-  io.ctr = ctr;
-  rc = pmk_invert(P, io, cfg->precision, 0, st, sms, nullptr);
+  // the job and the queue (every ticket published, closed) from this stack
+  // frame: a copy from pageable memory has read its source when it returns
+  PmJob job{};
+  job.npix = npix;
+  job.spectro = reinterpret_cast<const float*>(base + kOffSpectro);
+  job.slight = slight_mode == PM_SLIGHT_PER_PIXEL ? reinterpret_cast<const float*>(base + kOffSlight) : nullptr;
+  job.models = io.models_out;
+  job.chisq = io.chisq_out;
+  job.iters = io.iters_out;
+  job.status = io.status_out;
+  job.spectra = io.spectra_out;
+  PmStreamQ qinit{};
+  qinit.avail = (unsigned long long)npix;
+  qinit.closed = 1;
+  if ((e = cudaMemcpyAsync(job_dev, &job, sizeof job, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+    return cuda_err(e, "job H2D");
+  if ((e = cudaMemcpyAsync(q, &qinit, sizeof qinit, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+    return cuda_err(e, "queue H2D");
+  PmGridSet gs;
+  std::memset(&gs, 0, sizeof gs);
+  gs.ngrids = 1;
+  gs.g[0] = P;
+  PmStreamIO sio{};
+  sio.q = q;
+  sio.jobs = job_dev;
+  sio.jobs_cap = 1;
+  sio.first_job = 0;
+  sio.linger_ns = -1;
+  sio.wait_limit_ns = 20000000000LL;
+  rc = pmk_invert_stream(gs, sio, cfg->precision, 0, 4, false, st, sms, nullptr);
   if (rc != PM_OK) return pmh_fail(rc, pmk_last_cuda_error());
   if ((e = cudaMemcpyAsync(models_out, io.models_out, sizeof(pm_model) * npix, cudaMemcpyDeviceToHost, st)) !=
       cudaSuccess)
@@ -172,6 +197,11 @@ extern "C" int pm_invert_batch_noalloc(const pm_line* line, const pm_config* cfg
   if (best_fit_out &&
       (e = cudaMemcpyAsync(best_fit_out, io.spectra_out, prof * npix, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
     return cuda_err(e, "best fit D2H");
+  PmStreamQ qread{};
+  if ((e = cudaMemcpyAsync(&qread, q, sizeof qread, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+    return cuda_err(e, "queue D2H");
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_err(e, "pm_invert_batch_noalloc");
+  if (qread.err || qread.next != (unsigned long long)npix)
+    return pmh_fail(PM_EIO, "pm_invert_batch_noalloc: the inversion kernel stopped early");
   return PM_OK;
 }

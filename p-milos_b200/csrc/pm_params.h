@@ -43,12 +43,59 @@ struct PmParams {
   float taps_f[PMK_NL];
   double omw_d[PMK_NL];                    // 1 - sum of the taps [tap_lo, tap_hi] that land inside the grid at output k
   float omw_f[PMK_NL];
-  double sl_d[4 * PMK_NL];                 // shared stray-light profile [4][nl]
-  float sl_f[4 * PMK_NL];
+  float sl_f[4 * PMK_NL];                  // shared stray-light profile [4][nl] (float, as read from the cube)
 };
 
 // Work-queue / statistics counters (device memory, zeroed before each launch).
 enum { PMC_NEXT = 0, PMC_ITERS = 1, PMC_ACCEPTED = 2, PMC_FALLBACK = 3, PMC_COUNT = 4 };
+
+// ---- streamed inversion (a persistent kernel fed while it runs) ----
+// Grids (wavelength grid + line + PSF + settings) one streamed launch serves.
+#define PMK_MAX_GRIDS 4
+struct PmGridSet {
+  int ngrids;
+  int pad_;
+  PmParams g[PMK_MAX_GRIDS];
+};
+
+// Ticket queue in device memory.  next: the next ticket to hand out; avail:
+// tickets published (written by the host through the copy engine, after the
+// data they cover); closed: nonzero once no more tickets will be published.
+enum { PMQ_ERR_WAIT = 1, PMQ_ERR_JOB = 2 };
+struct PmStreamQ {
+  unsigned long long next, avail, closed, err;
+  unsigned long long ctr[PMC_COUNT];  // statistics, as PmIO::ctr
+};
+
+// One scan (job) of the stream: tickets [t0, t0 + npix) with its own buffers
+// (device pointers, layouts as PmIO) and grid.
+struct PmJob {
+  unsigned long long t0;
+  long long npix;
+  int grid;
+  int pad_;
+  const float* spectro;
+  const float* slight;      // PM_SLIGHT_PER_PIXEL grids: [npix][4][nl]
+  double* models;
+  float* chisq;
+  int* iters;
+  int* status;              // nullable
+  float* spectra;           // nullable
+  unsigned long long* done; // device counter of finished pixels (zeroed before publication), nullable
+  int* host_flag;           // mapped host word set to 1 when the last pixel is done, nullable
+};
+
+static_assert(sizeof(PmGridSet) + 64 <= 32764, "kernel parameter block of the streamed kernel exceeds 32 KB");
+
+struct PmStreamIO {
+  PmStreamQ* q;
+  const PmJob* jobs;        // ring of jobs_cap descriptors; job k lives in slot k % jobs_cap
+  int jobs_cap;
+  int pad_;
+  long long first_job;      // no ticket left belongs to a job before this one
+  long long linger_ns;      // exit after this long without work (-1: only when closed and drained)
+  long long wait_limit_ns;  // longest wait for a ticket before giving up with PMQ_ERR_WAIT
+};
 
 struct PmIO {
   int64_t npix;
@@ -68,9 +115,15 @@ struct PmIO {
 enum PmVariant { PMV_FP64 = 0, PMV_FP32 = 1 };
 
 // Host-side launchers (pm_kernels.cu).
-int pmk_invert(const PmParams& P, const PmIO& io, int precision, int variant, void* stream, int num_sms,
-               float* kernel_ms);
+int pmk_invert(const PmParams& P, const PmIO& io, int precision, void* stream, int num_sms, float* kernel_ms);
 int pmk_synth(const PmParams& P, const PmIO& io, int precision, void* stream);
+// Grids of more than 32 wavelengths (pm_wide.cu), called by pmk_invert / pmk_synth.
+int pmk_invert_wide(const PmParams& P, const PmIO& io, int precision, void* stream, int num_sms, float* kernel_ms);
+int pmk_synth_wide(const PmParams& P, const PmIO& io, int precision, void* stream);
+// Streamed inversion: every grid of GS has the same nterms and nl <= 32.
+// multi: grids differ between jobs (dynamic grid index) rather than one grid.
+int pmk_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, int precision, int variant, int warps_per_block,
+                      bool multi, void* stream, int num_sms, size_t* smem_out);
 const char* pmk_last_cuda_error();
 
 // Host helpers (pm_host.cpp) shared with pm_noalloc.cu.

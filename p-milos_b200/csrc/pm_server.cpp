@@ -1,0 +1,590 @@
+// pm_server.cpp -- the serving loop of include/pmilos.h (pm_server_*): continuous
+// batching of spectral scans on one persistent streamed inversion kernel
+// (pm_stream.cu), with admission by device-memory budget.
+//
+// Device state: an arena of hbm_budget_bytes for admitted scans (each scan's
+// cube and results), the ticket queue, a ring of job descriptors, per-job done
+// counters, and the grids' parameter blocks (kernel parameters).  Host state
+// (pinned): the ring's source copies of descriptors and published counts, and
+// mapped completion flags the kernel sets when a scan's last pixel is done.
+//
+// One scheduler thread owns every CUDA call after creation.  Per round it
+//  1. admits queued scans in arrival order while a slot and arena space are
+//     free: copy the cube (copy stream), write the job descriptor, then
+//     publish the scan's tickets (PmStreamQ::avail) -- in that stream order;
+//  2. relaunches the persistent kernel if it has exited (it lingers
+//     linger_ms without work) while admitted pixels remain;
+//  3. for every scan whose completion flag is set, copies its results back
+//     (output stream) and, once that copy is done, frees its arena space and
+//     wakes its waiters.
+// Scans thus join a kernel that is already running, and results leave while
+// other scans are still on the GPU.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <new>
+#include <thread>
+#include <vector>
+
+#include "pm_params.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+constexpr int kRing = 4096;  // job descriptor ring: job k lives in slot k % kRing
+constexpr size_t kAlign = 256;
+
+size_t round_up(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
+
+// First-fit allocator over the arena [0, size), 256-byte granules; neighbours
+// merge on release.
+class Arena {
+ public:
+  explicit Arena(size_t size) {
+    if (size) free_[0] = size;
+  }
+  bool alloc(size_t bytes, size_t* off) {
+    bytes = round_up(bytes);
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second < bytes) continue;
+      *off = it->first;
+      const size_t rest = it->second - bytes, start = it->first + bytes;
+      free_.erase(it);
+      if (rest) free_[start] = rest;
+      used_ += bytes;
+      peak_ = std::max(peak_, used_);
+      return true;
+    }
+    return false;
+  }
+  void release(size_t off, size_t bytes) {
+    bytes = round_up(bytes);
+    used_ -= bytes;
+    auto it = free_.emplace(off, bytes).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_.erase(nx);
+    }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+  size_t peak() const { return peak_; }
+
+ private:
+  std::map<size_t, size_t> free_;
+  size_t used_ = 0, peak_ = 0;
+};
+
+struct Scan {
+  uint64_t id = 0;
+  int grid = 0;
+  int64_t npix = 0;
+  const float* spectro = nullptr;
+  pm_model* models_out = nullptr;
+  float* chisq_out = nullptr;
+  int* iters_out = nullptr;
+  int* status_out = nullptr;
+  size_t off = 0, bytes = 0;                       // arena placement
+  size_t o_models = 0, o_chisq = 0, o_iters = 0, o_status = 0;
+  long long job = -1;
+  enum State { QUEUED, ADMITTED, COPYING_OUT, DONE } state = QUEUED;
+  cudaEvent_t ev_out = nullptr;
+  pm_scan_info info{};
+};
+
+thread_local char g_err[256];
+
+}  // namespace
+
+struct pm_server {
+  int device = 0, num_sms = 148, precision = PM_PREC_FP32, variant = 0, ngrids = 0;
+  PmGridSet* gs = nullptr;
+  pm_server_config sc{};
+  size_t prof[PM_SERVER_MAX_GRIDS] = {};
+  cudaStream_t s_kern = nullptr, s_copy = nullptr, s_out = nullptr;
+  cudaEvent_t ev_kernel = nullptr;
+  bool kernel_running = false;
+  unsigned char* arena_dev = nullptr;
+  Arena* arena = nullptr;
+  PmStreamQ* q = nullptr;
+  PmJob* jobs_dev = nullptr;
+  unsigned long long* done_dev = nullptr;
+  PmJob* jobs_host = nullptr;               // pinned
+  unsigned long long* avail_host = nullptr; // pinned
+  unsigned long long* one_host = nullptr;   // pinned word holding 1
+  int* flags_host = nullptr;                // mapped pinned
+  int* flags_dev = nullptr;
+  unsigned long long t_next = 0;
+  long long next_job = 0;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<Scan*> queued;
+  std::vector<Scan*> active;
+  std::map<uint64_t, Scan*> scans;
+  uint64_t next_id = 1;
+  bool stop = false;
+  int error = PM_OK;
+  char error_msg[256] = "";
+  std::thread worker;
+  Clock::time_point t0;
+  // statistics
+  int64_t launches = 0, scans_done = 0, pixels_done = 0;
+  std::vector<double> latencies;
+  double first_submit = -1, last_done = 0;
+
+  double now_ms() const { return std::chrono::duration<double, std::milli>(Clock::now() - t0).count(); }
+  long long oldest_job() const {
+    long long k = next_job;
+    for (const Scan* s : active) k = std::min(k, s->job);
+    return k;
+  }
+};
+
+namespace {
+
+int sfail(int code, const char* fmt, const char* a = "", const char* b = "") {
+  std::snprintf(g_err, sizeof g_err, fmt, a, b);
+  return pmh_fail(code, g_err);
+}
+
+// Device error inside the scheduler: every queued and active scan ends with it.
+void fail_all(pm_server* s, const char* what, cudaError_t e) {
+  s->error = PM_EIO;
+  std::snprintf(s->error_msg, sizeof s->error_msg, "%s: %s", what, cudaGetErrorString(e));
+  for (Scan* sc : s->active) {
+    sc->info.rc = PM_EIO;
+    sc->state = Scan::DONE;
+  }
+  for (Scan* sc : s->queued) {
+    sc->info.rc = PM_EIO;
+    sc->state = Scan::DONE;
+  }
+  s->active.clear();
+  s->queued.clear();
+  s->cv_done.notify_all();
+}
+
+bool admit(pm_server* s, Scan* sc) {
+  const size_t prof = s->prof[sc->grid];
+  const long long k = s->next_job;
+  const int slot = int(k % kRing);
+  unsigned char* base = s->arena_dev + sc->off;
+  PmJob& J = s->jobs_host[slot];
+  std::memset(&J, 0, sizeof J);
+  J.t0 = s->t_next;
+  J.npix = sc->npix;
+  J.grid = sc->grid;
+  J.spectro = reinterpret_cast<const float*>(base);
+  J.models = reinterpret_cast<double*>(base + sc->o_models);
+  J.chisq = reinterpret_cast<float*>(base + sc->o_chisq);
+  J.iters = reinterpret_cast<int*>(base + sc->o_iters);
+  J.status = reinterpret_cast<int*>(base + sc->o_status);
+  J.done = s->done_dev + slot;
+  J.host_flag = s->flags_dev + slot;
+  reinterpret_cast<volatile int*>(s->flags_host)[slot] = 0;
+  cudaError_t e = cudaMemsetAsync(s->done_dev + slot, 0, sizeof(unsigned long long), s->s_copy);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(base, sc->spectro, prof * size_t(sc->npix), cudaMemcpyHostToDevice, s->s_copy);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(s->jobs_dev + slot, &J, sizeof J, cudaMemcpyHostToDevice, s->s_copy);
+  s->avail_host[slot] = s->t_next + (unsigned long long)sc->npix;
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&s->q->avail, &s->avail_host[slot], sizeof(unsigned long long), cudaMemcpyHostToDevice,
+                        s->s_copy);
+  if (e != cudaSuccess) {
+    sc->info.rc = PM_EIO;
+    sc->state = Scan::DONE;
+    fail_all(s, "scan admission", e);
+    return false;
+  }
+  s->t_next += (unsigned long long)sc->npix;
+  s->next_job = k + 1;
+  sc->job = k;
+  sc->state = Scan::ADMITTED;
+  sc->info.admit_ms = s->now_ms();
+  s->active.push_back(sc);
+  return true;
+}
+
+bool launch(pm_server* s) {
+  PmStreamIO sio{};
+  sio.q = s->q;
+  sio.jobs = s->jobs_dev;
+  sio.jobs_cap = kRing;
+  sio.first_job = s->oldest_job();
+  sio.linger_ns = (long long)(s->sc.linger_ms * 1e6);
+  sio.wait_limit_ns = sio.linger_ns + 30000000000LL;
+  const int rc = pmk_invert_stream(*s->gs, sio, s->precision, s->variant, 4, s->ngrids > 1, s->s_kern, s->num_sms,
+                                   nullptr);
+  if (rc != PM_OK) {
+    s->error = rc;
+    std::snprintf(s->error_msg, sizeof s->error_msg, "%s", pmk_last_cuda_error());
+    for (Scan* sc : s->active) {
+      sc->info.rc = rc;
+      sc->state = Scan::DONE;
+    }
+    s->active.clear();
+    s->cv_done.notify_all();
+    return false;
+  }
+  cudaEventRecord(s->ev_kernel, s->s_kern);
+  s->kernel_running = true;
+  ++s->launches;
+  return true;
+}
+
+void copy_out(pm_server* s, Scan* sc) {
+  unsigned char* base = s->arena_dev + sc->off;
+  const size_t n = size_t(sc->npix);
+  cudaError_t e = cudaMemcpyAsync(sc->models_out, base + sc->o_models, sizeof(pm_model) * n, cudaMemcpyDeviceToHost,
+                                  s->s_out);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(sc->chisq_out, base + sc->o_chisq, sizeof(float) * n, cudaMemcpyDeviceToHost, s->s_out);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(sc->iters_out, base + sc->o_iters, sizeof(int) * n, cudaMemcpyDeviceToHost, s->s_out);
+  if (e == cudaSuccess && sc->status_out)
+    e = cudaMemcpyAsync(sc->status_out, base + sc->o_status, sizeof(int) * n, cudaMemcpyDeviceToHost, s->s_out);
+  if (e == cudaSuccess && !sc->ev_out) e = cudaEventCreateWithFlags(&sc->ev_out, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventRecord(sc->ev_out, s->s_out);
+  if (e != cudaSuccess) return fail_all(s, "scan results", e);
+  sc->state = Scan::COPYING_OUT;
+}
+
+void finish(pm_server* s, Scan* sc) {
+  sc->info.done_ms = s->now_ms();
+  sc->info.rc = PM_OK;
+  int64_t it = 0;
+  for (int64_t i = 0; i < sc->npix; ++i) it += sc->iters_out[i] > 0 ? sc->iters_out[i] : 0;
+  sc->info.iterations = it;
+  s->arena->release(sc->off, sc->bytes);
+  sc->state = Scan::DONE;
+  ++s->scans_done;
+  s->pixels_done += sc->npix;
+  s->latencies.push_back(sc->info.done_ms - sc->info.submit_ms);
+  s->last_done = sc->info.done_ms;
+}
+
+void serve(pm_server* s) {
+  std::unique_lock<std::mutex> lk(s->mu);
+  while (true) {
+    bool progress = false;
+    if (s->error == PM_OK) {
+      // 1. admission, in arrival order
+      while (!s->queued.empty() && int(s->active.size()) < s->sc.max_inflight &&
+             s->next_job - s->oldest_job() < kRing) {
+        Scan* sc = s->queued.front();
+        size_t off = 0;
+        if (!s->arena->alloc(sc->bytes, &off)) break;
+        s->queued.pop_front();
+        sc->off = off;
+        if (!admit(s, sc)) break;
+        progress = true;
+      }
+      // 2. completions
+      for (size_t i = 0; i < s->active.size() && s->error == PM_OK;) {
+        Scan* sc = s->active[i];
+        const int slot = int(sc->job % kRing);
+        if (sc->state == Scan::ADMITTED && reinterpret_cast<volatile int*>(s->flags_host)[slot] == 1) {
+          copy_out(s, sc);
+          progress = true;
+        }
+        if (sc->state == Scan::COPYING_OUT) {
+          const cudaError_t e = cudaEventQuery(sc->ev_out);
+          if (e == cudaSuccess) {
+            finish(s, sc);
+            s->active.erase(s->active.begin() + i);
+            s->cv_done.notify_all();
+            progress = true;
+            continue;
+          }
+          if (e != cudaErrorNotReady) fail_all(s, "scan results", e);
+        }
+        ++i;
+      }
+      // 3. the persistent kernel: relaunched while admitted pixels remain
+      if (s->error == PM_OK && s->kernel_running) {
+        const cudaError_t e = cudaEventQuery(s->ev_kernel);
+        if (e == cudaSuccess) {
+          s->kernel_running = false;
+        } else if (e != cudaErrorNotReady) {
+          fail_all(s, "inversion kernel", e);
+        }
+      }
+      if (s->error == PM_OK && !s->kernel_running) {
+        bool pending = false;
+        for (const Scan* sc : s->active) pending = pending || sc->state == Scan::ADMITTED;
+        // (a scan still ADMITTED here has pixels no kernel has handed out)
+        if (pending) {
+          // read the queue's error word after a finished launch
+          PmStreamQ qh{};
+          if (s->launches > 0 &&
+              cudaMemcpyAsync(&qh, s->q, sizeof qh, cudaMemcpyDeviceToHost, s->s_kern) == cudaSuccess &&
+              cudaStreamSynchronize(s->s_kern) == cudaSuccess && qh.err) {
+            s->error = PM_EIO;
+            std::snprintf(s->error_msg, sizeof s->error_msg, "streamed kernel stopped (error %llu)", qh.err);
+            for (Scan* sc : s->active) {
+              sc->info.rc = PM_EIO;
+              sc->state = Scan::DONE;
+            }
+            s->active.clear();
+            s->cv_done.notify_all();
+          } else if (launch(s)) {
+            progress = true;
+          }
+        }
+      }
+    }
+    if (s->stop && s->queued.empty() && s->active.empty()) break;
+    if (!progress) {
+      if (s->active.empty() && (s->queued.empty() || s->error != PM_OK)) {
+        if (s->stop) break;
+        s->cv_work.wait(lk);
+      } else {
+        lk.unlock();
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
+        lk.lock();
+      }
+    }
+  }
+}
+
+void release(pm_server* s) {
+  if (s->s_copy && s->q && s->one_host) {
+    // an idle kernel may still linger: close the queue so that it exits now
+    cudaMemcpyAsync(&s->q->closed, s->one_host, sizeof(unsigned long long), cudaMemcpyHostToDevice, s->s_copy);
+  }
+  for (cudaStream_t st : {s->s_copy, s->s_kern, s->s_out})
+    if (st) cudaStreamSynchronize(st);
+  for (auto& kv : s->scans) {
+    if (kv.second->ev_out) cudaEventDestroy(kv.second->ev_out);
+    delete kv.second;
+  }
+  s->scans.clear();
+  if (s->ev_kernel) cudaEventDestroy(s->ev_kernel);
+  for (cudaStream_t st : {s->s_copy, s->s_kern, s->s_out})
+    if (st) cudaStreamDestroy(st);
+  for (void* p : {(void*)s->arena_dev, (void*)s->q, (void*)s->jobs_dev, (void*)s->done_dev})
+    if (p) cudaFree(p);
+  for (void* p : {(void*)s->jobs_host, (void*)s->avail_host, (void*)s->one_host, (void*)s->flags_host})
+    if (p) cudaFreeHost(p);
+  delete s->arena;
+  delete s->gs;
+  delete s;
+}
+
+}  // namespace
+
+extern "C" int pm_server_create(const pm_line* line, const pm_config* const* grids, const pm_model* guesses,
+                                int ngrids, const pm_server_config* sc, pm_server** out) {
+  if (!line || !grids || !guesses || !sc || !out) return sfail(PM_EINVAL, "pm_server_create: NULL argument");
+  *out = nullptr;
+  if (ngrids < 1 || ngrids > PM_SERVER_MAX_GRIDS) return sfail(PM_EINVAL, "pm_server_create: ngrids out of 1..4");
+  if (sc->max_inflight < 1 || sc->max_inflight > PM_SERVER_MAX_INFLIGHT)
+    return sfail(PM_EINVAL, "pm_server_create: max_inflight out of 1..256");
+  if (sc->hbm_budget_bytes < (size_t(1) << 20)) return sfail(PM_EINVAL, "pm_server_create: budget below 1 MiB");
+  if (!(sc->linger_ms >= 0)) return sfail(PM_EINVAL, "pm_server_create: linger_ms < 0");
+  pm_server* s = new (std::nothrow) pm_server();
+  if (!s) return sfail(PM_ENOMEM, "pm_server_create: out of host memory");
+  s->gs = new (std::nothrow) PmGridSet();
+  if (!s->gs) {
+    delete s;
+    return sfail(PM_ENOMEM, "pm_server_create: out of host memory");
+  }
+  s->sc = *sc;
+  s->ngrids = ngrids;
+  s->gs->ngrids = ngrids;
+  for (int g = 0; g < ngrids; ++g) {
+    if (!grids[g]) {
+      release(s);
+      return sfail(PM_EINVAL, "pm_server_create: grid is NULL");
+    }
+    int rc = pmh_fill_params(line, grids[g], s->gs->g[g]);
+    if (rc != PM_OK) {
+      release(s);
+      return rc;
+    }
+    if (guesses[g].mac != 0.0) {
+      release(s);
+      return sfail(PM_ENOTSUP, "macroturbulence (guess.mac > 0) is outside this implementation");
+    }
+    pmh_set_guess(s->gs->g[g], &guesses[g]);
+    const PmParams& P = s->gs->g[g];
+    if (P.G != 1) {
+      release(s);
+      return sfail(PM_ENOTSUP, "pm_server_create: served grids have at most 32 wavelengths");
+    }
+    if (grids[g]->precision != grids[0]->precision || P.K != s->gs->g[0].K) {
+      release(s);
+      return sfail(PM_EINVAL, "pm_server_create: grids differ in precision or nterms");
+    }
+    s->prof[g] = sizeof(float) * 4 * size_t(P.nl);
+  }
+  s->precision = grids[0]->precision;
+  if (const char* v = std::getenv("PMILOS_VARIANT")) s->variant = std::atoi(v) == 1 ? 1 : 0;
+  cudaDeviceProp prop;
+  cudaError_t e = cudaGetDevice(&s->device);
+  if (e == cudaSuccess) e = cudaGetDeviceProperties(&prop, s->device);
+  if (e != cudaSuccess || prop.major != 10) {
+    release(s);
+    return sfail(PM_ENODEV, "pm_server_create: no sm_100 device");
+  }
+  s->num_sms = prop.multiProcessorCount;
+  void* p = nullptr;
+#define SRV_CUDA(call, what)                                                   \
+  do {                                                                         \
+    cudaError_t e_ = (call);                                                   \
+    if (e_ != cudaSuccess) {                                                   \
+      release(s);                                                              \
+      return sfail(e_ == cudaErrorMemoryAllocation ? PM_ENOMEM : PM_EIO, "%s: %s", what, cudaGetErrorString(e_)); \
+    }                                                                          \
+  } while (0)
+  SRV_CUDA(cudaStreamCreateWithFlags(&s->s_kern, cudaStreamNonBlocking), "stream");
+  SRV_CUDA(cudaStreamCreateWithFlags(&s->s_copy, cudaStreamNonBlocking), "stream");
+  SRV_CUDA(cudaStreamCreateWithFlags(&s->s_out, cudaStreamNonBlocking), "stream");
+  SRV_CUDA(cudaEventCreateWithFlags(&s->ev_kernel, cudaEventDisableTiming), "event");
+  SRV_CUDA(cudaMalloc(&p, sc->hbm_budget_bytes), "arena (hbm_budget_bytes)");
+  s->arena_dev = static_cast<unsigned char*>(p);
+  s->arena = new (std::nothrow) Arena(sc->hbm_budget_bytes);
+  SRV_CUDA(cudaMalloc(&p, sizeof(PmStreamQ)), "queue");
+  s->q = static_cast<PmStreamQ*>(p);
+  SRV_CUDA(cudaMemset(s->q, 0, sizeof(PmStreamQ)), "queue");
+  SRV_CUDA(cudaMalloc(&p, sizeof(PmJob) * kRing), "job ring");
+  s->jobs_dev = static_cast<PmJob*>(p);
+  SRV_CUDA(cudaMemset(s->jobs_dev, 0, sizeof(PmJob) * kRing), "job ring");
+  SRV_CUDA(cudaMalloc(&p, sizeof(unsigned long long) * kRing), "done counters");
+  s->done_dev = static_cast<unsigned long long*>(p);
+  SRV_CUDA(cudaHostAlloc(&p, sizeof(PmJob) * kRing, cudaHostAllocDefault), "pinned jobs");
+  s->jobs_host = static_cast<PmJob*>(p);
+  SRV_CUDA(cudaHostAlloc(&p, sizeof(unsigned long long) * kRing, cudaHostAllocDefault), "pinned counts");
+  s->avail_host = static_cast<unsigned long long*>(p);
+  SRV_CUDA(cudaHostAlloc(&p, sizeof(unsigned long long), cudaHostAllocDefault), "pinned word");
+  s->one_host = static_cast<unsigned long long*>(p);
+  *s->one_host = 1;
+  SRV_CUDA(cudaHostAlloc(&p, sizeof(int) * kRing, cudaHostAllocMapped), "mapped flags");
+  s->flags_host = static_cast<int*>(p);
+  std::memset(s->flags_host, 0, sizeof(int) * kRing);
+  SRV_CUDA(cudaHostGetDevicePointer(&p, s->flags_host, 0), "mapped flags");
+  s->flags_dev = static_cast<int*>(p);
+#undef SRV_CUDA
+  if (!s->arena) {
+    release(s);
+    return sfail(PM_ENOMEM, "pm_server_create: out of host memory");
+  }
+  s->t0 = Clock::now();
+  s->worker = std::thread(serve, s);
+  *out = s;
+  return PM_OK;
+}
+
+extern "C" int pm_server_submit(pm_server* s, int grid, int64_t npix, const float* spectro, pm_model* models_out,
+                                float* chisq_out, int* iters_out, int* status_out, uint64_t* id_out) {
+  if (!s || !spectro || !models_out || !chisq_out || !iters_out || !id_out)
+    return sfail(PM_EINVAL, "pm_server_submit: NULL argument");
+  if (grid < 0 || grid >= s->ngrids) return sfail(PM_EINVAL, "pm_server_submit: no such grid");
+  if (npix < 1) return sfail(PM_EINVAL, "pm_server_submit: npix < 1");
+  Scan* sc = new (std::nothrow) Scan();
+  if (!sc) return sfail(PM_ENOMEM, "pm_server_submit: out of host memory");
+  const size_t n = size_t(npix);
+  sc->grid = grid;
+  sc->npix = npix;
+  sc->spectro = spectro;
+  sc->models_out = models_out;
+  sc->chisq_out = chisq_out;
+  sc->iters_out = iters_out;
+  sc->status_out = status_out;
+  sc->o_models = round_up(s->prof[grid] * n);
+  sc->o_chisq = sc->o_models + round_up(sizeof(pm_model) * n);
+  sc->o_iters = sc->o_chisq + round_up(sizeof(float) * n);
+  sc->o_status = sc->o_iters + round_up(sizeof(int) * n);
+  sc->bytes = sc->o_status + round_up(sizeof(int) * n);
+  sc->info.npix = npix;
+  sc->info.grid = grid;
+  if (sc->bytes > s->sc.hbm_budget_bytes) {
+    delete sc;
+    return sfail(PM_ERANGE, "pm_server_submit: the scan needs more device memory than the whole budget");
+  }
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->error != PM_OK) {
+      delete sc;
+      return pmh_fail(s->error, s->error_msg);
+    }
+    sc->id = s->next_id++;
+    sc->info.submit_ms = s->now_ms();
+    if (s->first_submit < 0) s->first_submit = sc->info.submit_ms;
+    s->scans[sc->id] = sc;
+    s->queued.push_back(sc);
+    *id_out = sc->id;
+  }
+  s->cv_work.notify_one();
+  return PM_OK;
+}
+
+extern "C" int pm_server_wait(pm_server* s, uint64_t id, double timeout_s, pm_scan_info* info) {
+  if (!s) return sfail(PM_EINVAL, "pm_server_wait: NULL server");
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->scans.find(id);
+  if (it == s->scans.end()) return sfail(PM_EINVAL, "pm_server_wait: unknown scan id (already waited for?)");
+  Scan* sc = it->second;
+  const auto deadline = Clock::now() + std::chrono::duration_cast<Clock::duration>(
+                                           std::chrono::duration<double>(std::max(0.0, timeout_s)));
+  if (!s->cv_done.wait_until(lk, deadline, [&] { return sc->state == Scan::DONE; }))
+    return sfail(PM_ETIMEDOUT, "pm_server_wait: scan not done in time");
+  if (info) *info = sc->info;
+  const int rc = sc->info.rc;
+  s->scans.erase(it);
+  if (sc->ev_out) cudaEventDestroy(sc->ev_out);
+  delete sc;
+  if (rc != PM_OK) return pmh_fail(rc, s->error_msg);
+  return PM_OK;
+}
+
+extern "C" int pm_server_get_stats(pm_server* s, pm_server_stats* out) {
+  if (!s || !out) return sfail(PM_EINVAL, "pm_server_get_stats: NULL argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  std::memset(out, 0, sizeof *out);
+  out->scans_done = s->scans_done;
+  out->pixels_done = s->pixels_done;
+  out->kernel_launches = s->launches;
+  out->arena_peak_bytes = s->arena->peak();
+  if (!s->latencies.empty()) {
+    std::vector<double> v = s->latencies;
+    std::sort(v.begin(), v.end());
+    auto pct = [&](double p) {
+      const double r = p * double(v.size() - 1);
+      const size_t lo = size_t(r), hi = std::min(v.size() - 1, lo + 1);
+      return v[lo] + (r - double(lo)) * (v[hi] - v[lo]);
+    };
+    out->latency_p50_ms = pct(0.50);
+    out->latency_p99_ms = pct(0.99);
+    out->latency_max_ms = v.back();
+  }
+  out->busy_ms = s->first_submit >= 0 ? s->last_done - s->first_submit : 0;
+  return PM_OK;
+}
+
+extern "C" int pm_server_destroy(pm_server* s) {
+  if (!s) return PM_OK;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+  }
+  s->cv_work.notify_all();
+  if (s->worker.joinable()) s->worker.join();
+  release(s);
+  return PM_OK;
+}

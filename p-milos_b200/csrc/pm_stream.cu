@@ -1,0 +1,201 @@
+// pm_stream.cu -- the streamed inversion kernel (a persistent kernel fed while it
+// runs: pipelined host-buffer calls and the serving loop) and its launcher.
+#include "pm_device.cuh"
+
+namespace {
+// ---------------------------------------------------------------------------
+// Streamed inversion: a persistent kernel fed while it runs.  Pixels are
+// tickets; the host publishes tickets in stream order after the data they cover
+// has been copied (a copy engine writes PmStreamQ::avail), and appends scans
+// ("jobs": a run of tickets with its own buffers and wavelength grid) to a ring
+// of descriptors.  A warp takes the next ticket with a compare-and-swap below
+// avail, so a ticket is never handed out before it is published and none is
+// lost when the kernel exits.  Waits are bounded: a batch kernel exits once the
+// host has closed the queue and it is drained (or sets err after
+// wait_limit_ns); a serving kernel also exits after linger_ns without work and
+// the host relaunches it when new work arrives.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ long long global_ns() {
+  long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Next ticket, or -1 when the kernel should exit.
+__device__ long long next_ticket(PmStreamQ* q, long long linger_ns, long long limit_ns) {
+  unsigned long long n = ld_acquire(&q->next);
+  long long idle_since = -1;
+  unsigned sleep = 32;
+  while (true) {
+    const unsigned long long avail = ld_acquire(&q->avail);
+    if (n < avail) {
+      const unsigned long long old = atomicCAS(&q->next, n, n + 1);
+      if (old == n) return (long long)n;
+      n = old;
+      continue;
+    }
+    if (ld_acquire(&q->closed)) {
+      // closed is written after the last avail: re-read it once
+      if (n >= ld_acquire(&q->avail)) return -1;
+      continue;
+    }
+    const long long now = global_ns();
+    if (idle_since < 0) idle_since = now;
+    if (linger_ns >= 0 && now - idle_since > linger_ns) return -1;
+    if (now - idle_since > limit_ns) {
+      atomicExch(&q->err, (unsigned long long)PMQ_ERR_WAIT);
+      return -1;
+    }
+    __nanosleep(sleep);
+    sleep = sleep < 2048 ? 2 * sleep : 2048;
+    n = ld_acquire(&q->next);
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ T* ld_ptr(T* const* p) {
+  return reinterpret_cast<T*>(__ldcg(reinterpret_cast<const unsigned long long*>(p)));
+}
+
+template <typename R, int KT, int MINB, bool MULTI>
+__global__ void __launch_bounds__(128, MINB) invert_stream_kernel(const __grid_constant__ PmGridSet GS,
+                                                                    const PmStreamIO sio) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int NG = MULTI ? PMK_MAX_GRIDS : 1;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  BlockSmem<R>* bs = reinterpret_cast<BlockSmem<R>*>(smem_raw);
+  WarpSmem<R>& sm = reinterpret_cast<WarpSmem<R>*>(smem_raw + NG * sizeof(BlockSmem<R>))[warp];
+#pragma unroll 1
+  for (int g = 0; g < NG && g < GS.ngrids; ++g) load_taps<R>(GS.g[g], bs[g]);
+  __syncthreads();
+  int cur = -1;             // grid of the previous pixel: the padded rows are re-zeroed on a change
+  long long k = sio.first_job;
+  while (true) {
+    long long t = 0;
+    if (lane == 0) t = next_ticket(sio.q, sio.linger_ns, sio.wait_limit_ns);
+    t = __shfl_sync(kFull, t, 0);
+    if (t < 0) break;
+    // the job of ticket t: jobs are appended in ticket order, so it is at or
+    // after this warp's previous one
+    const PmJob* jp = nullptr;
+    unsigned long long t0 = 0;
+    for (int guard = 0; guard <= sio.jobs_cap; ++guard, ++k) {
+      const PmJob* c = sio.jobs + (k % sio.jobs_cap);
+      const unsigned long long c0 = __ldcg(&c->t0);
+      const unsigned long long cn = __ldcg(reinterpret_cast<const unsigned long long*>(&c->npix));
+      if ((unsigned long long)t >= c0 && (unsigned long long)t < c0 + cn) {
+        jp = c;
+        t0 = c0;
+        break;
+      }
+    }
+    if (!jp) {
+      if (lane == 0) atomicExch(&sio.q->err, (unsigned long long)PMQ_ERR_JOB);
+      break;
+    }
+    const int gi = MULTI ? __ldcg(&jp->grid) : 0;
+    const PmParams& P = GS.g[gi];
+    if (gi != cur) {
+      for (int e = lane; e < 4 * XSR; e += 32) (&sm.xs[0][0])[e] = R(0);
+      cur = gi;
+      __syncwarp();
+    }
+    const unsigned long long p = (unsigned long long)t - t0;
+    const size_t base = size_t(p) * 4 * P.nl;
+    const float* slight = ld_ptr(&jp->slight);
+    float* spectra = ld_ptr(&jp->spectra);
+    int* status = ld_ptr(&jp->status);
+    PixIO px;
+    px.obs = ld_ptr(&jp->spectro) + base;
+    px.sl_pix = (P.slight_mode == PM_SLIGHT_PER_PIXEL && slight) ? slight + base : nullptr;
+    px.model_out = ld_ptr(&jp->models) + size_t(p) * 11;
+    px.chisq_out = ld_ptr(&jp->chisq) + p;
+    px.iters_out = ld_ptr(&jp->iters) + p;
+    px.status_out = status ? status + p : nullptr;
+    px.spectra_out = spectra ? spectra + base : nullptr;
+    px.ctr = sio.q->ctr;
+    invert_pixel<R, KT>(P, bs[gi], sm, lane, px);
+    if (lane == 0) {
+      unsigned long long* done = ld_ptr(&jp->done);
+      int* flag = ld_ptr(&jp->host_flag);
+      __threadfence();  // this pixel's results before its count
+      if (done) {
+        const unsigned long long np = __ldcg(reinterpret_cast<const unsigned long long*>(&jp->npix));
+        if (atomicAdd(done, 1ull) + 1 == np && flag) {
+          __threadfence_system();
+          *reinterpret_cast<volatile int*>(flag) = 1;
+        }
+      }
+    }
+    __syncwarp();
+  }
+}
+
+
+template <typename R, int KT, int MINB, bool MULTI>
+int launch_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, cudaStream_t st, int num_sms,
+                         size_t* smem_out, int wpb) {
+  const int threads = 32 * wpb;
+  const size_t smem = (MULTI ? PMK_MAX_GRIDS : 1) * sizeof(BlockSmem<R>) + sizeof(WarpSmem<R>) * (threads / 32);
+  if (smem_out) *smem_out = smem;
+  auto kern = invert_stream_kernel<R, KT, MINB, MULTI>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return snprintf(pmk_g_err, sizeof pmk_g_err, "%s", cudaGetErrorString(e)), PM_EIO;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+  if (e != cudaSuccess || per_sm < 1) return snprintf(pmk_g_err, sizeof pmk_g_err, "occupancy: %s", cudaGetErrorString(e)), PM_EIO;
+  kern<<<unsigned(per_sm * num_sms), threads, smem, st>>>(GS, sio);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return snprintf(pmk_g_err, sizeof pmk_g_err, "stream launch: %s", cudaGetErrorString(e)), PM_EIO;
+  return PM_OK;
+}
+
+template <typename R, int KT>
+int launch_stream_any(const PmGridSet& GS, const PmStreamIO& sio, cudaStream_t st, int num_sms, int variant,
+                      int wpb, bool multi, size_t* smem_out) {
+  if constexpr (sizeof(R) == 4) {
+    if (multi) return launch_invert_stream<float, KT, 4, true>(GS, sio, st, num_sms, smem_out, wpb);
+    return variant == 1 ? launch_invert_stream<float, KT, 4, false>(GS, sio, st, num_sms, smem_out, wpb)
+                        : launch_invert_stream<float, KT, 3, false>(GS, sio, st, num_sms, smem_out, wpb);
+  } else {
+    return multi ? launch_invert_stream<double, KT, 1, true>(GS, sio, st, num_sms, smem_out, wpb)
+                 : launch_invert_stream<double, KT, 1, false>(GS, sio, st, num_sms, smem_out, wpb);
+  }
+}
+
+
+}  // namespace
+
+int pmk_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, int precision, int variant, int warps_per_block,
+                      bool multi, void* stream, int num_sms, size_t* smem_out) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int wpb = (warps_per_block == 1 || warps_per_block == 2) ? warps_per_block : 4;
+  if (GS.ngrids < 1 || GS.ngrids > PMK_MAX_GRIDS || (!multi && GS.ngrids != 1)) {
+    snprintf(pmk_g_err, sizeof pmk_g_err, "stream: %d grids", GS.ngrids);
+    return PM_EINVAL;
+  }
+  const int K = GS.g[0].K;
+  for (int g = 0; g < GS.ngrids; ++g) {
+    if (GS.g[g].G != 1 || GS.g[g].K != K) {
+      snprintf(pmk_g_err, sizeof pmk_g_err, "stream: grid %d has nl=%d, nterms=%d (streams take nl <= 32, one nterms)", g,
+               GS.g[g].nl, GS.g[g].K);
+      return PM_ENOTSUP;
+    }
+  }
+  if (precision == PM_PREC_FP32) {
+    if (K == 9) return launch_stream_any<float, 9>(GS, sio, st, num_sms, variant, wpb, multi, smem_out);
+    if (K == 10) return launch_stream_any<float, 10>(GS, sio, st, num_sms, variant, wpb, multi, smem_out);
+  } else {
+    if (K == 9) return launch_stream_any<double, 9>(GS, sio, st, num_sms, variant, wpb, multi, smem_out);
+    if (K == 10) return launch_stream_any<double, 10>(GS, sio, st, num_sms, variant, wpb, multi, smem_out);
+  }
+  snprintf(pmk_g_err, sizeof pmk_g_err, "nterms=%d has no compiled kernel", K);
+  return PM_ENOTSUP;
+}
+

@@ -32,7 +32,7 @@ __all__ = [
     "MODEL_FIELDS", "PmError", "LineData", "Inverter", "load_library", "line_from_quantum", "psf_gaussian",
     "psf_from_table", "grid_from_malla", "parse_lines_entry", "read_grid_file", "read_lines_file",
     "read_model_file", "read_psf_file", "read_trol_file", "PREC_FP64", "PREC_FP32", "SOLVE_DEFAULT",
-    "SOLVE_EIGEN", "SOLVE_CHOLESKY", "SLIGHT_NONE", "SLIGHT_SHARED", "SLIGHT_PER_PIXEL",
+    "SOLVE_EIGEN", "SOLVE_CHOLESKY", "SLIGHT_NONE", "SLIGHT_SHARED", "SLIGHT_PER_PIXEL", "Server", "Grid",
 ]
 
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
@@ -52,8 +52,12 @@ NL_MAX = 128
 EXPORTED_SYMBOLS = (
     "pm_line_from_quantum", "pm_psf_gaussian", "pm_psf_interpolate", "pm_ctx_create", "pm_ctx_destroy",
     "pm_invert_batch", "pm_synth_batch", "pm_lm_mils", "pm_invert_batch_noalloc", "pm_get_stats", "pm_last_error",
-    "pm_abi_version",
+    "pm_abi_version", "pm_get_tuning", "pm_set_tuning", "pm_autotune", "pm_server_create", "pm_server_submit",
+    "pm_server_wait", "pm_server_get_stats", "pm_server_destroy",
 )
+SERVER_MAX_GRIDS = 4
+SERVER_MAX_INFLIGHT = 256
+ETIMEDOUT = -110
 NOALLOC_MAX_PIXELS = 4096
 
 
@@ -89,9 +93,31 @@ class _Config(ctypes.Structure):
     ]
 
 
+class _Tuning(ctypes.Structure):
+    _fields_ = [("variant", ctypes.c_int), ("staging_depth", ctypes.c_int), ("warps_per_block", ctypes.c_int),
+                ("graphs", ctypes.c_int)]
+
+
+class _ServerConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_size_t), ("max_inflight", ctypes.c_int), ("linger_ms", ctypes.c_double)]
+
+
+class _ScanInfo(ctypes.Structure):
+    _fields_ = [("npix", ctypes.c_int64), ("grid", ctypes.c_int), ("rc", ctypes.c_int), ("submit_ms", ctypes.c_double),
+                ("admit_ms", ctypes.c_double), ("done_ms", ctypes.c_double), ("iterations", ctypes.c_int64)]
+
+
+class _ServerStats(ctypes.Structure):
+    _fields_ = [("scans_done", ctypes.c_int64), ("pixels_done", ctypes.c_int64), ("kernel_launches", ctypes.c_int64),
+                ("latency_p50_ms", ctypes.c_double), ("latency_p99_ms", ctypes.c_double),
+                ("latency_max_ms", ctypes.c_double), ("busy_ms", ctypes.c_double),
+                ("arena_peak_bytes", ctypes.c_size_t)]
+
+
 class _Stats(ctypes.Structure):
     _fields_ = [("pixels", ctypes.c_int64), ("iterations", ctypes.c_int64), ("accepted", ctypes.c_int64),
-                ("eigen_fallbacks", ctypes.c_int64), ("kernel_ms", ctypes.c_double), ("total_ms", ctypes.c_double)]
+                ("eigen_fallbacks", ctypes.c_int64), ("kernel_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
+                ("graph_replays", ctypes.c_int64)]
 
 
 _LIB = None
@@ -120,6 +146,17 @@ def load_library(path: str | None = None):
     L.pm_invert_batch_noalloc.argtypes = [ctypes.POINTER(_Line), ctypes.POINTER(_Config), i64, F, F, ctypes.c_int,
                                           ctypes.POINTER(_Model), vp, vp, vp, vp, vp, vp]
     L.pm_get_stats.argtypes = [vp, ctypes.POINTER(_Stats)]
+    L.pm_get_tuning.argtypes = [vp, ctypes.POINTER(_Tuning)]
+    L.pm_set_tuning.argtypes = [vp, ctypes.POINTER(_Tuning)]
+    L.pm_autotune.argtypes = [vp, i64, F, F, ctypes.c_int, ctypes.POINTER(_Model), ctypes.c_int,
+                              ctypes.POINTER(_Tuning)]
+    L.pm_server_create.argtypes = [ctypes.POINTER(_Line), ctypes.POINTER(ctypes.POINTER(_Config)),
+                                   ctypes.POINTER(_Model), ctypes.c_int, ctypes.POINTER(_ServerConfig),
+                                   ctypes.POINTER(vp)]
+    L.pm_server_submit.argtypes = [vp, ctypes.c_int, i64, F, vp, vp, vp, vp, ctypes.POINTER(ctypes.c_uint64)]
+    L.pm_server_wait.argtypes = [vp, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(_ScanInfo)]
+    L.pm_server_get_stats.argtypes = [vp, ctypes.POINTER(_ServerStats)]
+    L.pm_server_destroy.argtypes = [vp]
     L.pm_last_error.restype = ctypes.c_char_p
     L.pm_abi_version.restype = ctypes.c_int
     if path is None:
@@ -381,7 +418,150 @@ class Inverter:
             out["status"] = stt
         return out
 
+    @property
+    def tuning(self) -> dict:
+        t = _Tuning()
+        _check(self.L.pm_get_tuning(self.ctx, ctypes.byref(t)))
+        return {k: getattr(t, k) for k, _ in _Tuning._fields_}
+
+    @tuning.setter
+    def tuning(self, value: dict):
+        t = _Tuning()
+        _check(self.L.pm_get_tuning(self.ctx, ctypes.byref(t)))
+        for k, v in value.items():
+            setattr(t, k, int(v))
+        _check(self.L.pm_set_tuning(self.ctx, ctypes.byref(t)))
+
+    def autotune(self, spectro, guess, *, slight=None, slight_mode=None, reps: int = 2) -> dict:
+        """Time every candidate tuning on this host-memory sample and keep the fastest."""
+        obs = np.ascontiguousarray(spectro, dtype=np.float32).reshape(-1, 4, self.nl)
+        sl, mode = self._slight_host(slight, slight_mode, obs.shape[0])
+        g = _model_struct(guess)
+        t = _Tuning()
+        _check(self.L.pm_autotune(self.ctx, obs.shape[0], obs.ctypes.data, None if sl is None else sl.ctypes.data,
+                                  mode, ctypes.byref(g), int(reps), ctypes.byref(t)))
+        return {k: getattr(t, k) for k, _ in _Tuning._fields_}
+
     def stats(self) -> dict:
         s = _Stats()
         _check(self.L.pm_get_stats(self.ctx, ctypes.byref(s)))
         return {k: getattr(s, k) for k, _ in _Stats._fields_}
+
+
+# ---- serving ----
+@dataclass
+class Grid:
+    """One wavelength grid a Server holds resident: the pm_config fields of an
+    Inverter plus the initial model of the grid's scans."""
+    lam: np.ndarray
+    psf: np.ndarray | None = None
+    guess: np.ndarray | None = None
+    weights: tuple = (1.0, 1.0, 1.0, 1.0)
+    noise: float = 1e-6
+    ilambda: float = 0.1
+    toplim: float = 1e-12
+    miter: int = 50
+    fix: list | None = None
+    nterms: int | None = None
+    mu: float = 1.0
+    classical: bool = True
+    precision: int = PREC_FP32
+    solver: int = SOLVE_DEFAULT
+
+
+class Server:
+    """pm_server: continuous batching of spectral scans on resident grids.
+
+    submit() queues a scan (a [npix][4][nl] float32 host array; pinned memory
+    lets its copy overlap the kernel) and returns its id at once; wait() blocks
+    until its models, chi^2, iterations and status are in host memory.  Scans
+    that arrive while others are on the GPU join the running kernel as device
+    memory (hbm_budget_bytes) and in-flight slots free up."""
+
+    def __init__(self, line: LineData, grids, *, hbm_budget_bytes: int = 8 << 30, max_inflight: int = 64,
+                 linger_ms: float = 2.0):
+        self.L = load_library()
+        self.line = line
+        self.grids = list(grids)
+        self._keep = []
+        cfgs = (ctypes.POINTER(_Config) * len(self.grids))()
+        guesses = (_Model * len(self.grids))()
+        self.nl = []
+        for i, g in enumerate(self.grids):
+            lam = np.ascontiguousarray(g.lam, dtype=np.float64)
+            psf = None if g.psf is None else np.ascontiguousarray(g.psf, dtype=np.float64)
+            fix = list(g.fix) if g.fix is not None else [1] * 9 + [0, 0]
+            nterms = g.nterms if g.nterms is not None else 11 - (0 if fix[10] else 1) - (0 if fix[9] else 1)
+            c = _Config()
+            c.nlambda = lam.size
+            c.lambda_ = _dptr(lam)
+            c.psf = _dptr(psf) if psf is not None else ctypes.POINTER(ctypes.c_double)()
+            c.weight[:] = [float(w) for w in g.weights]
+            c.noise, c.ilambda, c.toplim, c.miter = float(g.noise), float(g.ilambda), float(g.toplim), int(g.miter)
+            c.fix[:] = [int(bool(f)) for f in fix]
+            c.nterms, c.logclambda, c.mu = int(nterms), 0, float(g.mu)
+            c.classical_estimates, c.precision, c.solver = int(bool(g.classical)), int(g.precision), int(g.solver)
+            self._keep += [lam, psf, c]
+            cfgs[i] = ctypes.pointer(c)
+            guesses[i] = _model_struct(g.guess if g.guess is not None else np.array(
+                [8.0, 400.0, 0.0, 0.03, 0.1, 30.0, 30.0, 0.25, 0.75, 0.0, 1.0]))
+            self.nl.append(int(lam.size))
+        sc = _ServerConfig(int(hbm_budget_bytes), int(max_inflight), float(linger_ms))
+        srv = ctypes.c_void_p()
+        _check(self.L.pm_server_create(ctypes.byref(line._c), cfgs, guesses, len(self.grids), ctypes.byref(sc),
+                                       ctypes.byref(srv)))
+        self.srv = srv
+        self._pending = {}
+
+    def submit(self, grid: int, spectro, want_status: bool = True) -> int:
+        obs = spectro if (isinstance(spectro, np.ndarray) and spectro.dtype == np.float32 and
+                          spectro.flags.c_contiguous) else np.ascontiguousarray(spectro, dtype=np.float32)
+        if not 0 <= grid < len(self.nl):
+            raise PmError(-22, f"no grid {grid} (the server holds {len(self.nl)})")
+        nl = self.nl[grid]
+        if obs.size % (4 * nl):
+            raise ValueError(f"grid {grid} has {nl} wavelengths: spectro must be [npix][4][{nl}]")
+        npix = obs.size // (4 * nl)
+        models = np.zeros((npix, 11))
+        chi = np.zeros(npix, dtype=np.float32)
+        its = np.zeros(npix, dtype=np.int32)
+        stt = np.zeros(npix, dtype=np.int32) if want_status else None
+        sid = ctypes.c_uint64()
+        _check(self.L.pm_server_submit(self.srv, int(grid), npix, obs.ctypes.data, models.ctypes.data,
+                                       chi.ctypes.data, its.ctypes.data, None if stt is None else stt.ctypes.data,
+                                       ctypes.byref(sid)))
+        self._pending[sid.value] = (obs, models, chi, its, stt)
+        return sid.value
+
+    def wait(self, sid: int, timeout: float = 600.0) -> dict:
+        info = _ScanInfo()
+        rc = self.L.pm_server_wait(self.srv, ctypes.c_uint64(sid), float(timeout), ctypes.byref(info))
+        if rc == ETIMEDOUT:
+            raise TimeoutError(f"scan {sid} not done after {timeout} s")
+        bufs = self._pending.pop(sid, None)
+        _check(rc)
+        _, models, chi, its, stt = bufs
+        out = {"models": models, "chisq": chi, "iters": its,
+               "info": {k: getattr(info, k) for k, _ in _ScanInfo._fields_}}
+        if stt is not None:
+            out["status"] = stt
+        return out
+
+    def stats(self) -> dict:
+        st = _ServerStats()
+        _check(self.L.pm_server_get_stats(self.srv, ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in _ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "srv", None):
+            self.L.pm_server_destroy(self.srv)
+            self.srv = None
+            self._pending.clear()
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

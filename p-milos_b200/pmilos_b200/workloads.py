@@ -137,3 +137,57 @@ def synthesize(w: Workload, inv_fp64=None, rng: np.random.Generator | None = Non
     obs = obs + rng.normal(0.0, NOISE_SIGMA, obs.shape).astype(np.float32)
     obs = np.ascontiguousarray(obs, dtype=np.float32)
     return (obs, truth) if return_truth else obs
+
+
+def truth_models_device(w: Workload, seed: int, device="cuda"):
+    """The truth_models distributions drawn on the device (torch generator
+    seeded with ``seed``): for cubes too large to build in host memory."""
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    n = w.npix
+
+    def U(lo, hi, k=n):
+        return lo + (hi - lo) * torch.rand(k, generator=g, device=device, dtype=torch.float64)
+
+    m = torch.zeros((n, 11), dtype=torch.float64, device=device)
+    for col, (lo, hi) in enumerate([(1, 20), (0, 3000), (-3, 3), (0.02, 0.05), (0.01, 0.5), (0, 180), (0, 180),
+                                    (0.1, 0.4), (0.4, 0.9)]):
+        m[:, col] = U(lo, hi)
+    m[:, 10] = 1.0
+    if w.cfg in (2, 3):
+        weak = torch.rand(n, generator=g, device=device) < 0.7
+        m[:, 1] = torch.where(weak, U(0, 200), U(1500, 3500))
+        m[:, 0] = torch.where(weak, U(1, 5), m[:, 0])
+    if w.cfg == 2:
+        m[:, 10] = 1.0 - U(0, 0.3)
+    return m
+
+
+def synthesize_device(w: Workload, inv_fp64, seed: int, chunk: int = 1 << 21):
+    """Observed profiles as a CUDA float32 tensor [npix][4][nl]: FP64 synthesis
+    of device-drawn truth models plus N(0, 1e-3) noise, generated in chunks so
+    that only the cube itself (and one chunk of temporaries) is resident."""
+    import torch
+
+    truth = truth_models_device(w, seed)
+    obs = torch.empty((w.npix, 4, w.nl), dtype=torch.float32, device="cuda")
+    g = torch.Generator(device="cuda")
+    g.manual_seed(int(seed) + 1)
+    for p0 in range(0, w.npix, chunk):
+        p1 = min(w.npix, p0 + chunk)
+        obs[p0:p1] = inv_fp64.synth(truth[p0:p1], slight=None if w.slight is None else
+                                    torch.as_tensor(np.asarray(w.slight, dtype=np.float32), device="cuda"))
+        obs[p0:p1] += NOISE_SIGMA * torch.randn((p1 - p0, 4, w.nl), generator=g, device="cuda")
+    del truth
+    return obs
+
+
+def psf_support(psf) -> int:
+    """Taps the multi-warp correlations use: those above 1e-18 of the peak."""
+    if psf is None:
+        return 0
+    a = np.abs(np.asarray(psf))
+    idx = np.nonzero(a > 1e-18 * a.max())[0]
+    return int(idx[-1] - idx[0] + 1) if idx.size else 0

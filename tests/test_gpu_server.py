@@ -1,0 +1,131 @@
+"""The serving loop (pm_server): continuous batching of scans on resident grids.
+
+Grids: the served-stream configuration's three scans around Fe I 6173.3354 A --
+6 points at +-172.5/+-103.5/+-34.5 mA, 15 points at 50 mA, 30 points at 25 mA --
+with a 60 mA Gaussian PSF, nine free parameters, FP32.  Observed profiles are
+synthesized by this library's FP64 path with seeded atmospheres (70% weak-field,
+30% strong-field) and N(0, 1e-3) noise.
+"""
+import numpy as np
+import pytest
+
+import pmilos_b200 as pm
+from gpu_common import NOISE64, within_tolerance
+from pmilos_b200 import workloads
+
+pytestmark = pytest.mark.gpu
+
+LINE = pm.LineData(workloads.FE6173, workloads.TRIPLET)
+
+
+def grids():
+    out = []
+    for which in range(3):
+        w = workloads.config(3, npix=1, grid=which)
+        out.append(pm.Grid(lam=w.lam, psf=w.psf, guess=w.guess, noise=NOISE64, fix=w.fix, nterms=9))
+    return out
+
+
+def cube(which: int, npix: int, seed: int):
+    w = workloads.config(3, npix=npix, grid=which)
+    w.seed = seed
+    return workloads.synthesize(w, rng=np.random.default_rng(seed))
+
+
+@pytest.fixture(scope="module")
+def cubes():
+    return {(g, n, s): cube(g, n, s) for g, n, s in [(2, 3000, 1), (0, 20000, 2), (1, 9000, 3), (2, 5000, 4),
+                                                      (0, 700, 5), (1, 64, 6)]}
+
+
+def _eq(a, b):
+    for k in ("models", "chisq", "iters", "status"):
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_scan_same_alone_and_in_the_mix(cubes):
+    """A scan's results do not depend on what else is in flight: alone, and
+    submitted among scans of all three grids, bit for bit (and so within the
+    stated tolerance)."""
+    A = cubes[(2, 3000, 1)]
+    with pm.Server(LINE, grids(), hbm_budget_bytes=1 << 30, max_inflight=16) as srv:
+        alone = srv.wait(srv.submit(2, A))
+        ids = [srv.submit(0, cubes[(0, 20000, 2)]), srv.submit(1, cubes[(1, 9000, 3)]), srv.submit(2, A),
+               srv.submit(2, cubes[(2, 5000, 4)]), srv.submit(0, cubes[(0, 700, 5)]), srv.submit(1, cubes[(1, 64, 6)])]
+        res = [srv.wait(i) for i in ids]
+        st = srv.stats()
+    mixed = res[2]
+    _eq(alone, mixed)
+    assert np.all(within_tolerance(mixed["models"], alone["models"]))
+    # the mix overlapped: the repeated scan was admitted before the first scan of the mix finished
+    assert res[2]["info"]["admit_ms"] < res[0]["info"]["done_ms"]
+    assert st["scans_done"] == 7 and st["pixels_done"] == 3000 * 2 + 20000 + 9000 + 5000 + 700 + 64
+
+
+def test_served_scans_match_the_batch_entry_point(cubes):
+    """Every grid: the server's FP32 results against pm_invert_batch's FP32
+    results on the same cube (the one-grid streamed kernel), within the stated
+    FP32 tolerance; iteration statistics alike."""
+    G = grids()
+    with pm.Server(LINE, G, hbm_budget_bytes=1 << 30) as srv:
+        for (g, n, s) in [(0, 700, 5), (1, 9000, 3), (2, 3000, 1)]:
+            obs = cubes[(g, n, s)]
+            r = srv.wait(srv.submit(g, obs))
+            with pm.Inverter(LINE, G[g].lam, G[g].psf, noise=NOISE64, fix=G[g].fix, nterms=9,
+                             precision=pm.PREC_FP32) as inv:
+                b = inv.invert(obs, G[g].guess)
+            dB = np.abs(r["models"][:, 1] - b["models"][:, 1])
+            assert np.median(dB) < 1.0 and (dB < 5.0).mean() >= 0.9, g
+            assert abs(np.median(r["iters"]) - np.median(b["iters"])) <= 2
+            assert r["info"]["iterations"] == int(np.maximum(r["iters"], 0).sum())
+
+
+def test_admission_respects_the_budget(cubes):
+    """A budget that holds one scan at a time: every scan still completes, the
+    arena never exceeds the budget, and a scan larger than the budget is refused."""
+    A = cubes[(2, 3000, 1)]
+    one_scan = 3000 * (4 * 30 * 4 + 88 + 12) + 4096
+    with pm.Server(LINE, grids(), hbm_budget_bytes=max(one_scan, 1 << 20) + 1024, max_inflight=8) as srv:
+        ids = [srv.submit(2, A) for _ in range(4)]
+        res = [srv.wait(i) for i in ids]
+        st = srv.stats()
+        with pytest.raises(pm.PmError) as e:
+            srv.submit(0, np.zeros((100000, 4, 6), dtype=np.float32))
+        assert e.value.code == -34
+    for r in res[1:]:
+        _eq(r, res[0])
+        assert r["info"]["admit_ms"] >= res[0]["info"]["admit_ms"]
+    assert st["arena_peak_bytes"] <= max(one_scan, 1 << 20) + 1024
+    # one scan at a time: each admission waited for the previous scan's results
+    for a, b in zip(res, res[1:]):
+        assert b["info"]["admit_ms"] >= a["info"]["done_ms"] - 1.0
+
+
+def test_many_small_scans_share_a_kernel(cubes):
+    """Continuous batching: scans submitted while the kernel runs join it, so
+    there are far fewer kernel launches than scans."""
+    small = cubes[(1, 64, 6)]
+    big = cubes[(0, 20000, 2)]
+    with pm.Server(LINE, grids(), hbm_budget_bytes=1 << 30, max_inflight=64, linger_ms=50.0) as srv:
+        first = srv.submit(0, big)
+        ids = [srv.submit(1, small) for _ in range(40)]
+        res = [srv.wait(i) for i in ids]
+        srv.wait(first)
+        st = srv.stats()
+    for r in res[1:]:
+        _eq(r, res[0])
+    assert st["kernel_launches"] <= 5, st
+    assert st["latency_p99_ms"] >= st["latency_p50_ms"] > 0
+
+
+def test_wait_timeout_and_unknown_id(cubes):
+    with pm.Server(LINE, grids(), hbm_budget_bytes=1 << 30) as srv:
+        sid = srv.submit(0, cubes[(0, 20000, 2)])
+        with pytest.raises(TimeoutError):
+            srv.wait(sid, timeout=0.0)
+        r = srv.wait(sid)
+        assert r["models"].shape == (20000, 11)
+        with pytest.raises(pm.PmError):
+            srv.wait(sid)
+        with pytest.raises(pm.PmError):
+            srv.submit(7, cubes[(0, 700, 5)])

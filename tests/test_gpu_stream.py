@@ -1,0 +1,115 @@
+"""Streamed host-buffer inversion and the launch tunings.
+
+Every one-warp inversion runs the streamed kernel: device-buffer calls publish
+all pixels before the launch; host-buffer calls launch first and publish the
+cube piece by piece as the copy engine brings it in (pm_tuning.staging_depth
+pieces).  Staging depth and pixels per block do not change the compiled code,
+so results are bit-identical across them and equal to the device-buffer call.
+The two register budgets (pm_tuning.variant) are separately compiled kernels
+whose floating-point contractions may differ in the last bits: between them the
+stated FP32 tolerance applies.
+"""
+import numpy as np
+import pytest
+import torch
+
+import pmilos_b200 as pm
+from gpu_common import case, inverter
+
+pytestmark = pytest.mark.gpu
+
+
+def _device_reference(inv, c):
+    obs_d = torch.as_tensor(c["obs"], device="cuda")
+    sl = None if c["slight"] is None else torch.as_tensor(np.asarray(c["slight"], dtype=np.float32), device="cuda")
+    r = inv.invert(obs_d, c["guess"], slight=sl)
+    return {k: (v.cpu().numpy() if hasattr(v, "cpu") else v) for k, v in r.items()}
+
+
+def _same(a, b):
+    for k in ("models", "chisq", "iters", "spectra", "status"):
+        assert np.array_equal(a[k], b[k]), k
+
+
+@pytest.mark.parametrize("cfg", [0, 1, 2])
+@pytest.mark.parametrize("precision", [pm.PREC_FP32, pm.PREC_FP64])
+def test_every_tuning_gives_the_device_call_result(cfg, precision):
+    c = case(cfg)
+    with inverter(c, precision) as inv:
+        refs = []
+        for variant in ((0, 1) if precision == pm.PREC_FP32 else (0,)):
+            inv.tuning = {"variant": variant, "staging_depth": 8, "warps_per_block": 4}
+            ref = _device_reference(inv, c)
+            refs.append(ref)
+            for depth in (0, 1, 3, 64):
+                for wpb in (1, 2, 4):
+                    inv.tuning = {"variant": variant, "staging_depth": depth, "warps_per_block": wpb}
+                    r = inv.invert(c["obs"], c["guess"], slight=c["slight"])
+                    _same(r, ref)
+    for other in refs[1:]:
+        # the stated FP32 tolerance: |dB| < 5 G for 90% of pixels, median below 1 G
+        dB = np.abs(other["models"][:, 1] - refs[0]["models"][:, 1])
+        assert np.median(dB) < 1.0 and (dB < 5.0).mean() >= 0.9
+
+
+def test_streamed_many_pieces_large_cube():
+    """More pixels than pieces x 32, ragged last piece, per-pixel stray light."""
+    c = case(2)
+    reps = 70
+    obs = np.ascontiguousarray(np.tile(c["obs"], (reps, 1, 1))[:3333])
+    sl = np.ascontiguousarray(np.broadcast_to(np.asarray(c["slight"], dtype=np.float32), obs.shape))
+    with inverter(c, pm.PREC_FP32) as inv:
+        inv.tuning = {"staging_depth": 0}
+        a = inv.invert(obs, c["guess"], slight=sl, slight_mode=pm.SLIGHT_PER_PIXEL)
+        inv.tuning = {"staging_depth": 37}
+        b = inv.invert(obs, c["guess"], slight=sl, slight_mode=pm.SLIGHT_PER_PIXEL)
+        s = inv.stats()
+    _same(a, b)
+    assert s["pixels"] == obs.shape[0] and s["iterations"] == int(np.maximum(b["iters"], 0).sum())
+
+
+def test_autotune_picks_a_valid_tuning_and_keeps_results():
+    c = case(1)
+    with inverter(c, pm.PREC_FP32) as inv:
+        ref = inv.invert(c["obs"], c["guess"])
+        t = inv.autotune(np.tile(c["obs"], (64, 1, 1)), c["guess"], reps=1)
+        assert t == inv.tuning
+        assert t["variant"] in (0, 1) and t["warps_per_block"] in (1, 2, 4) and t["staging_depth"] in (0, 4, 16)
+        _same(inv.invert(c["obs"], c["guess"]), ref)
+
+
+def test_bad_tuning_is_rejected():
+    c = case(1)
+    with inverter(c, pm.PREC_FP32) as inv:
+        for bad in ({"warps_per_block": 3}, {"staging_depth": 65}, {"variant": 2}):
+            with pytest.raises(pm.PmError) as e:
+                inv.tuning = bad
+            assert e.value.code == -22
+
+
+def test_small_calls_replay_a_captured_graph():
+    """Host-buffer calls of <= PM_GRAPH_MAX_PIXELS pixels replay one CUDA graph per
+    size: the first call captures, later ones replay; results equal the
+    graph-free streamed call bit for bit, also after the parameters change."""
+    c = case(2)
+    with inverter(c, pm.PREC_FP32) as inv:
+        inv.tuning = {"graphs": 0}
+        ref = inv.invert(c["obs"], c["guess"], slight=c["slight"])
+        assert inv.stats()["graph_replays"] == 0
+        inv.tuning = {"graphs": 1}
+        for _ in range(3):
+            r = inv.invert(c["obs"], c["guess"], slight=c["slight"])
+            assert inv.stats()["graph_replays"] == 1
+            _same(r, ref)
+        # another size, then a changed guess (a new parameter block) recapture
+        r5 = inv.invert(c["obs"][:5], c["guess"], slight=c["slight"])
+        _same({k: v for k, v in r5.items()}, {k: v[:5] for k, v in ref.items()})
+        g2 = np.array(c["guess"], dtype=float)
+        g2[1] = 900.0
+        inv.tuning = {"graphs": 0}
+        ref2 = inv.invert(c["obs"], g2, slight=c["slight"])
+        inv.tuning = {"graphs": 1}
+        _same(inv.invert(c["obs"], g2, slight=c["slight"]), ref2)
+        # lm_mils, the batch of one, takes the graph path too
+        rc, model, spectra, chi, it = inv.lm_mils(c["obs"][7], c["guess"], slight=c["slight"])
+        assert np.array_equal(model, ref["models"][7]) and it == ref["iters"][7]
