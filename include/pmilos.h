@@ -231,6 +231,35 @@ int pm_invert_batch_noalloc(const pm_line *line, const pm_config *cfg, int64_t n
                             const float *slight, int slight_mode, const pm_model *guess, pm_model *models_out,
                             float *chisq_out, int *iters_out, float *best_fit_out, int *status_out, void *stream);
 
+/* ---- cube ingest: FITS spectro cubes into the inversion layout ----
+ *
+ * The reference reads cubes with CFITSIO and reorders them on the host
+ * (readFitsSpectroImage, utilsFits.c:25-368).  Here the host parses the header
+ * and the data block goes to the device as stored in the file (big-endian
+ * float32); one kernel byte-swaps and permutes it into [pixel][I,Q,U,V][lambda]
+ * with pixel = column * rows + row, the reference's generic mapping
+ * (utilsFits.c:242-336) for every axis order. */
+typedef struct pm_fits_cube {
+  int naxis;             /* 4 */
+  int64_t naxes[4];      /* NAXIS1..4 */
+  int axis_row, axis_col, axis_lambda, axis_stokes;  /* 0-based axis of each role */
+  int from_ctype;        /* 1: roles from CTYPE1..4 (HPLN-TAN, HPLT-TAN, WAVE-GRI, STOKES); 0: inferred
+                            like the reference (smallest axis Stokes, next smallest wavelength, then
+                            rows and columns in axis order) */
+  int64_t nrows, ncols, npix;
+  int nlambda;
+  int64_t data_offset;   /* bytes from the start of the file to the data block */
+  int64_t data_bytes;    /* size of the data block */
+} pm_fits_cube;
+
+/* Parse the primary header (bytes: the file's first nbytes, at least up to END).
+ * PM_ENOTSUP unless BITPIX = -32; PM_EINVAL unless 4 axes with a 4-plane Stokes axis. */
+int pm_fits_parse_header(const void *bytes, size_t nbytes, pm_fits_cube *out);
+/* Reorder the data block on the device: data_dev holds info->data_bytes bytes as
+ * stored in the file, cube_dev receives npix * 4 * nlambda floats.  Device
+ * pointers; stream: a cudaStream_t or NULL (asynchronous on it). */
+int pm_fits_reorder(const pm_fits_cube *info, const void *data_dev, float *cube_dev, void *stream);
+
 /* ---- serving: continuous batching of spectral scans ----
  *
  * No counterpart in the reference, whose drivers invert one cube per process
@@ -299,6 +328,13 @@ int pm_set_tuning(pm_ctx *ctx, const pm_tuning *in);
  * reference. */
 int pm_autotune(pm_ctx *ctx, int64_t npix, const float *spectro, const float *slight, int slight_mode,
                 const pm_model *guess, int reps, pm_tuning *out);
+
+/* Self-test of the streamed kernel's bounded wait (no counterpart in the
+ * reference): launches it on ctx's grid with a queue that nothing ever
+ * publishes to, and a wait limit of limit_ms.  The kernel must give up by itself
+ * and report it: *queue_error receives the queue's error word (1 = wait limit
+ * reached) and *elapsed_ms the kernel's run time; the context stays usable. */
+int pm_selftest_stalled_queue(pm_ctx *ctx, double limit_ms, int *queue_error, double *elapsed_ms);
 
 int pm_get_stats(const pm_ctx *ctx, pm_stats *out);
 const char *pm_last_error(void);

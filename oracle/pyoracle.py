@@ -271,3 +271,59 @@ class Reference(_Lib):
         out = np.zeros(offs.size)
         self.L.pmref_interp_psf(_d(dl), _d(psf), dl.size, _d(offs), offs.size, offset, _d(out))
         return out
+
+
+# ---- cube ingest ----
+def fits_bytes(data: np.ndarray, ctypes_: list | None) -> bytes:
+    """A FITS file (primary HDU, BITPIX = -32) holding ``data``, a float32 array
+    whose numpy shape is (NAXIS4, NAXIS3, NAXIS2, NAXIS1); ``ctypes_``: CTYPE1..4
+    strings, or None for a header without them."""
+    dims = list(data.shape[::-1])
+    cards = ["SIMPLE  =                    T", "BITPIX  =                  -32", "NAXIS   =                    4"]
+    cards += [f"NAXIS{i + 1}  = {d:20d}" for i, d in enumerate(dims)]
+    if ctypes_:
+        cards += [f"CTYPE{i + 1}  = '{c:<8s}'" for i, c in enumerate(ctypes_)]
+    cards.append("END")
+    hdr = "".join(c.ljust(80) for c in cards).encode("ascii")
+    hdr += b" " * (-len(hdr) % 2880)
+    body = np.ascontiguousarray(data, dtype=">f4").tobytes()
+    body += b"\0" * (-len(body) % 2880)
+    return hdr + body
+
+
+def fits_roles(dims: list, ctypes_: list | None) -> tuple:
+    """(row, col, lambda, stokes) axis indices as readFitsSpectroImage assigns
+    them (utilsFits.c:69-150): from CTYPE1..4, else smallest axis = Stokes, the
+    smallest other = wavelength, the remaining two rows then columns."""
+    if ctypes_:
+        idx = {c.strip(): i for i, c in enumerate(ctypes_)}
+        return idx["HPLN-TAN"], idx["HPLT-TAN"], idx["WAVE-GRI"], idx["STOKES"]
+    s = min(range(4), key=lambda a: (dims[a], a))
+    lam = min((a for a in range(4) if a != s), key=lambda a: (dims[a], a))
+    rest = [a for a in range(4) if a not in (s, lam)]
+    return rest[0], rest[1], lam, s
+
+
+def fits_ingest(data: np.ndarray, ctypes_: list | None) -> np.ndarray:
+    """Restatement of the generic reorder (utilsFits.c:242-336): out[pixel][s][l]
+    with pixel = col * rows + row, for an array of numpy shape
+    (NAXIS4, NAXIS3, NAXIS2, NAXIS1)."""
+    dims = list(data.shape[::-1])
+    row, col, lam, s = fits_roles(dims, ctypes_)
+    f = np.asarray(data, dtype=np.float32)
+    # numpy axis of FITS axis a is 3 - a; target order (col, row, stokes, lambda)
+    t = np.transpose(f, (3 - col, 3 - row, 3 - s, 3 - lam))
+    return np.ascontiguousarray(t).reshape(dims[col] * dims[row], dims[s], dims[lam])
+
+
+def reference_fits_read(path: str, nlambda: int, npix_cap: int):
+    """The reference's own reader (oracle/_ref/libpmref_fits.so): (cube, rows, cols)."""
+    lib = ctypes.CDLL(os.path.join(REF, "libpmref_fits.so"))
+    lib.pmref_fits_read.argtypes = [ctypes.c_char_p, ctypes.c_int, _F, ctypes.c_longlong, _I, _I]
+    out = np.zeros(npix_cap * 4 * nlambda, dtype=np.float32)
+    rows, cols = ctypes.c_int(), ctypes.c_int()
+    rc = lib.pmref_fits_read(path.encode(), nlambda, _f(out), out.size, ctypes.byref(rows), ctypes.byref(cols))
+    if rc != 0:
+        raise RuntimeError(f"reference reader failed ({rc})")
+    n = rows.value * cols.value
+    return out[: n * 4 * nlambda].reshape(n, 4, nlambda), rows.value, cols.value

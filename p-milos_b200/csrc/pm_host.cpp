@@ -497,7 +497,6 @@ int run_streamed(pm_ctx* c, int64_t n, const float* spectro, const float* slight
   sio.jobs = static_cast<const PmJob*>(c->jobs.p);
   sio.jobs_cap = 1;
   sio.first_job = 0;
-  sio.linger_ns = -1;
   sio.wait_limit_ns = 20000000000LL;  // 20 s without a published piece: give up (PMQ_ERR_WAIT)
   PM_CUDA(cudaEventRecord(c->k0, c->s_kern), "event");
   rc = pmk_invert_stream(*c->gs, sio, c->precision, c->tuning.variant, c->tuning.warps_per_block, false, c->s_kern,
@@ -551,7 +550,7 @@ int run_streamed(pm_ctx* c, int64_t n, const float* spectro, const float* slight
   if (hc->qread.err)
     return fail(PM_EIO, "streamed inversion: %s", hc->qread.err == PMQ_ERR_WAIT ? "a piece never arrived (wait limit)"
                                                                                 : "ticket without a job");
-  if (hc->qread.next != (unsigned long long)n)
+  if (hc->qread.next < (unsigned long long)n)
     return fail(PM_EIO, "streamed inversion: %llu of %lld pixels handed out", hc->qread.next, (long long)n);
   cudaEventElapsedTime(kernel_ms, c->k0, c->k1);
   cudaEventElapsedTime(total_ms, c->t0, c->t1);
@@ -633,7 +632,6 @@ int run_graph_small(pm_ctx* c, int64_t n, const float* spectro, const float* sli
       sio.q = q;
       sio.jobs = static_cast<const PmJob*>(c->jobs.p);
       sio.jobs_cap = 1;
-      sio.linger_ns = -1;
       sio.wait_limit_ns = 20000000000LL;
       krc = pmk_invert_stream(*c->gs, sio, c->precision, c->tuning.variant, c->tuning.warps_per_block, false, s,
                               c->num_sms, nullptr);
@@ -684,7 +682,7 @@ int run_graph_small(pm_ctx* c, int64_t n, const float* spectro, const float* sli
   PM_CUDA(cudaEventRecord(c->ev_done, c->s_kern), "event");
   PM_CUDA(cudaStreamWaitEvent(c->stream, c->ev_done, 0), "wait");
   PM_CUDA(cudaEventSynchronize(c->t1), "graph replay");
-  if (hc->qread.err || hc->qread.next != (unsigned long long)n)
+  if (hc->qread.err || hc->qread.next < (unsigned long long)n)
     return fail(PM_EIO, "inversion kernel: queue error %llu, %llu of %lld pixels handed out", hc->qread.err,
                 hc->qread.next, (long long)n);
   std::memcpy(models_out, st->models, sizeof(pm_model) * n);
@@ -746,7 +744,6 @@ int run_invert(pm_ctx* c, PmIO io, float* kernel_ms) {
   sio.jobs = static_cast<const PmJob*>(c->jobs.p);
   sio.jobs_cap = 1;
   sio.first_job = 0;
-  sio.linger_ns = -1;
   sio.wait_limit_ns = 20000000000LL;
   PM_CUDA(cudaEventRecord(c->k0, c->stream), "event");
   rc = pmk_invert_stream(*c->gs, sio, c->precision, c->tuning.variant, c->tuning.warps_per_block, false, c->stream,
@@ -755,7 +752,7 @@ int run_invert(pm_ctx* c, PmIO io, float* kernel_ms) {
   PM_CUDA(cudaEventRecord(c->k1, c->stream), "event");
   PM_CUDA(cudaMemcpyAsync(&hc->qread, q, sizeof(PmStreamQ), cudaMemcpyDeviceToHost, c->stream), "queue D2H");
   PM_CUDA(cudaStreamSynchronize(c->stream), "invert kernel");
-  if (hc->qread.err || hc->qread.next != (unsigned long long)io.npix)
+  if (hc->qread.err || hc->qread.next < (unsigned long long)io.npix)
     return fail(PM_EIO, "inversion kernel: queue error %llu, %llu of %lld pixels handed out", hc->qread.err,
                 hc->qread.next, (long long)io.npix);
   if (kernel_ms) cudaEventElapsedTime(kernel_ms, c->k0, c->k1);
@@ -1005,6 +1002,41 @@ extern "C" int pm_autotune(pm_ctx* c, int64_t npix, const float* spectro, const 
   c->tuning = best;
   c->stats = pm_stats{};
   if (out) *out = best;
+  return PM_OK;
+}
+
+extern "C" int pm_selftest_stalled_queue(pm_ctx* c, double limit_ms, int* queue_error, double* elapsed_ms) {
+  if (!c || !queue_error || !elapsed_ms) return fail(PM_EINVAL, "pm_selftest_stalled_queue: NULL argument");
+  if (!(limit_ms > 0 && limit_ms <= 10000)) return fail(PM_EINVAL, "pm_selftest_stalled_queue: limit_ms out of (0, 1e4]");
+  if (c->P.G != 1) return fail(PM_ENOTSUP, "pm_selftest_stalled_queue: one-warp grids only");
+  int rc = stream_resources(c);
+  if (rc != PM_OK) return rc;
+  HostCtl* hc = c->hc;
+  PmStreamQ* q = static_cast<PmStreamQ*>(c->q.p);
+  // an open queue with nothing published and one (never reached) job
+  std::memset(&hc->job, 0, sizeof hc->job);
+  hc->job.npix = 1;
+  std::memset(&hc->qinit, 0, sizeof hc->qinit);
+  PM_CUDA(cudaMemcpyAsync(c->jobs.p, &hc->job, sizeof(PmJob), cudaMemcpyHostToDevice, c->s_kern), "job H2D");
+  PM_CUDA(cudaMemcpyAsync(q, &hc->qinit, sizeof(PmStreamQ), cudaMemcpyHostToDevice, c->s_kern), "queue H2D");
+  c->gs->ngrids = 1;
+  c->gs->g[0] = c->P;
+  PmStreamIO sio{};
+  sio.q = q;
+  sio.jobs = static_cast<const PmJob*>(c->jobs.p);
+  sio.jobs_cap = 1;
+  sio.wait_limit_ns = (long long)(limit_ms * 1e6);
+  PM_CUDA(cudaEventRecord(c->k0, c->s_kern), "event");
+  rc = pmk_invert_stream(*c->gs, sio, c->precision, c->tuning.variant, c->tuning.warps_per_block, false, c->s_kern,
+                         c->num_sms, nullptr);
+  if (rc != PM_OK) return fail(rc, "%s", pmk_last_cuda_error());
+  PM_CUDA(cudaEventRecord(c->k1, c->s_kern), "event");
+  PM_CUDA(cudaMemcpyAsync(&hc->qread, q, sizeof(PmStreamQ), cudaMemcpyDeviceToHost, c->s_kern), "queue D2H");
+  PM_CUDA(cudaStreamSynchronize(c->s_kern), "stalled-queue kernel");
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->k0, c->k1);
+  *queue_error = int(hc->qread.err);
+  *elapsed_ms = ms;
   return PM_OK;
 }
 

@@ -180,7 +180,6 @@ extern "C" int pm_invert_batch_noalloc(const pm_line* line, const pm_config* cfg
   sio.jobs = job_dev;
   sio.jobs_cap = 1;
   sio.first_job = 0;
-  sio.linger_ns = -1;
   sio.wait_limit_ns = 20000000000LL;
   rc = pmk_invert_stream(gs, sio, cfg->precision, 0, 4, false, st, sms, nullptr);
   if (rc != PM_OK) return pmh_fail(rc, pmk_last_cuda_error());
@@ -201,7 +200,7 @@ extern "C" int pm_invert_batch_noalloc(const pm_line* line, const pm_config* cfg
   if ((e = cudaMemcpyAsync(&qread, q, sizeof qread, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
     return cuda_err(e, "queue D2H");
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_err(e, "pm_invert_batch_noalloc");
-  if (qread.err || qread.next != (unsigned long long)npix)
+  if (qread.err || qread.next < (unsigned long long)npix)
     return pmh_fail(PM_EIO, "pm_invert_batch_noalloc: the inversion kernel stopped early");
   return PM_OK;
 }

@@ -60,7 +60,9 @@ struct PmGridSet {
 
 // Ticket queue in device memory.  next: the next ticket to hand out; avail:
 // tickets published (written by the host through the copy engine, after the
-// data they cover); closed: nonzero once no more tickets will be published.
+// data they cover); closed: nonzero once no more tickets will be published (the
+// kernel then ends).  Before a launch on a queue that was closed the host sets
+// next = avail (every published ticket has been inverted) and closed = 0.
 enum { PMQ_ERR_WAIT = 1, PMQ_ERR_JOB = 2 };
 struct PmStreamQ {
   unsigned long long next, avail, closed, err;
@@ -93,7 +95,6 @@ struct PmStreamIO {
   int jobs_cap;
   int pad_;
   long long first_job;      // no ticket left belongs to a job before this one
-  long long linger_ns;      // exit after this long without work (-1: only when closed and drained)
   long long wait_limit_ns;  // longest wait for a ticket before giving up with PMQ_ERR_WAIT
 };
 

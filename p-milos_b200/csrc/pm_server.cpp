@@ -12,11 +12,14 @@
 //  1. admits queued scans in arrival order while a slot and arena space are
 //     free: copy the cube (copy stream), write the job descriptor, then
 //     publish the scan's tickets (PmStreamQ::avail) -- in that stream order;
-//  2. relaunches the persistent kernel if it has exited (it lingers
-//     linger_ms without work) while admitted pixels remain;
-//  3. for every scan whose completion flag is set, copies its results back
+//  2. for every scan whose completion flag is set, copies its results back
 //     (output stream) and, once that copy is done, frees its arena space and
-//     wakes its waiters.
+//     wakes its waiters;
+//  3. runs the persistent kernel: launches it when admitted pixels wait and it
+//     is stopped, and retires it by closing the queue after linger_ms with
+//     nothing in flight (a closed queue ends the kernel once its warps find no
+//     published ticket; the next launch reopens the queue at the first
+//     unpublished ticket).
 // Scans thus join a kernel that is already running, and results leave while
 // other scans are still on the GPU.
 #include <cuda_runtime.h>
@@ -117,8 +120,10 @@ struct pm_server {
   pm_server_config sc{};
   size_t prof[PM_SERVER_MAX_GRIDS] = {};
   cudaStream_t s_kern = nullptr, s_copy = nullptr, s_out = nullptr;
-  cudaEvent_t ev_kernel = nullptr;
-  bool kernel_running = false;
+  cudaEvent_t ev_kernel = nullptr, ev_reset = nullptr;
+  enum { K_STOPPED, K_RUNNING, K_CLOSING } kstate = K_STOPPED;
+  double idle_since = -1;                   // ms; nothing queued or in flight since then
+  unsigned long long* reset_host = nullptr; // pinned: [0] first unpublished ticket at a relaunch, [1] zero
   unsigned char* arena_dev = nullptr;
   Arena* arena = nullptr;
   PmStreamQ* q = nullptr;
@@ -129,7 +134,8 @@ struct pm_server {
   unsigned long long* one_host = nullptr;   // pinned word holding 1
   int* flags_host = nullptr;                // mapped pinned
   int* flags_dev = nullptr;
-  unsigned long long t_next = 0;
+  unsigned long long t_next = 0;      // tickets published
+  unsigned long long t_consumed = 0;  // tickets the stopped kernel(s) reached (all inverted)
   long long next_job = 0;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
@@ -220,14 +226,29 @@ bool admit(pm_server* s, Scan* sc) {
   return true;
 }
 
+// Launch on a stopped kernel: the queue reopens at the first ticket the
+// previous kernel did not reach (it ended only after inverting every published
+// ticket), then the kernel starts on the kernel stream after those copies.
 bool launch(pm_server* s) {
+  s->reset_host[0] = s->t_consumed;
+  s->reset_host[1] = 0;
+  cudaError_t e = cudaMemcpyAsync(&s->q->next, &s->reset_host[0], sizeof(unsigned long long), cudaMemcpyHostToDevice,
+                                  s->s_copy);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&s->q->closed, &s->reset_host[1], sizeof(unsigned long long), cudaMemcpyHostToDevice,
+                        s->s_copy);
+  if (e == cudaSuccess) e = cudaEventRecord(s->ev_reset, s->s_copy);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(s->s_kern, s->ev_reset, 0);
+  if (e != cudaSuccess) {
+    fail_all(s, "queue reopen", e);
+    return false;
+  }
   PmStreamIO sio{};
   sio.q = s->q;
   sio.jobs = s->jobs_dev;
   sio.jobs_cap = kRing;
   sio.first_job = s->oldest_job();
-  sio.linger_ns = (long long)(s->sc.linger_ms * 1e6);
-  sio.wait_limit_ns = sio.linger_ns + 30000000000LL;
+  sio.wait_limit_ns = (long long)(std::max(1000.0, 2 * s->sc.linger_ms) * 1e6) + 30000000000LL;
   const int rc = pmk_invert_stream(*s->gs, sio, s->precision, s->variant, 4, s->ngrids > 1, s->s_kern, s->num_sms,
                                    nullptr);
   if (rc != PM_OK) {
@@ -242,8 +263,21 @@ bool launch(pm_server* s) {
     return false;
   }
   cudaEventRecord(s->ev_kernel, s->s_kern);
-  s->kernel_running = true;
+  s->kstate = pm_server::K_RUNNING;
+  s->idle_since = -1;
   ++s->launches;
+  return true;
+}
+
+// Close the queue: the running kernel ends once its warps find nothing published.
+bool close_queue(pm_server* s) {
+  const cudaError_t e = cudaMemcpyAsync(&s->q->closed, s->one_host, sizeof(unsigned long long),
+                                        cudaMemcpyHostToDevice, s->s_copy);
+  if (e != cudaSuccess) {
+    fail_all(s, "queue close", e);
+    return false;
+  }
+  s->kstate = pm_server::K_CLOSING;
   return true;
 }
 
@@ -284,8 +318,8 @@ void serve(pm_server* s) {
     bool progress = false;
     if (s->error == PM_OK) {
       // 1. admission, in arrival order
-      while (!s->queued.empty() && int(s->active.size()) < s->sc.max_inflight &&
-             s->next_job - s->oldest_job() < kRing) {
+      while (s->kstate != pm_server::K_CLOSING && !s->queued.empty() &&
+             int(s->active.size()) < s->sc.max_inflight && s->next_job - s->oldest_job() < kRing) {
         Scan* sc = s->queued.front();
         size_t off = 0;
         if (!s->arena->alloc(sc->bytes, &off)) break;
@@ -315,42 +349,54 @@ void serve(pm_server* s) {
         }
         ++i;
       }
-      // 3. the persistent kernel: relaunched while admitted pixels remain
-      if (s->error == PM_OK && s->kernel_running) {
+      // 3. the persistent kernel
+      if (s->error == PM_OK && s->kstate != pm_server::K_STOPPED) {
         const cudaError_t e = cudaEventQuery(s->ev_kernel);
         if (e == cudaSuccess) {
-          s->kernel_running = false;
-        } else if (e != cudaErrorNotReady) {
-          fail_all(s, "inversion kernel", e);
-        }
-      }
-      if (s->error == PM_OK && !s->kernel_running) {
-        bool pending = false;
-        for (const Scan* sc : s->active) pending = pending || sc->state == Scan::ADMITTED;
-        // (a scan still ADMITTED here has pixels no kernel has handed out)
-        if (pending) {
-          // read the queue's error word after a finished launch
+          // ended: normally after a close; otherwise its wait limit ran out
           PmStreamQ qh{};
-          if (s->launches > 0 &&
-              cudaMemcpyAsync(&qh, s->q, sizeof qh, cudaMemcpyDeviceToHost, s->s_kern) == cudaSuccess &&
-              cudaStreamSynchronize(s->s_kern) == cudaSuccess && qh.err) {
+          const bool read = cudaMemcpyAsync(&qh, s->q, sizeof qh, cudaMemcpyDeviceToHost, s->s_kern) == cudaSuccess &&
+                            cudaStreamSynchronize(s->s_kern) == cudaSuccess;
+          if (!read || qh.err || s->kstate != pm_server::K_CLOSING) {
             s->error = PM_EIO;
-            std::snprintf(s->error_msg, sizeof s->error_msg, "streamed kernel stopped (error %llu)", qh.err);
+            std::snprintf(s->error_msg, sizeof s->error_msg, "streamed kernel stopped (queue error %llu)", qh.err);
             for (Scan* sc : s->active) {
               sc->info.rc = PM_EIO;
               sc->state = Scan::DONE;
             }
             s->active.clear();
             s->cv_done.notify_all();
-          } else if (launch(s)) {
+          } else {
+            s->kstate = pm_server::K_STOPPED;
+            s->t_consumed = s->t_next;
             progress = true;
           }
+        } else if (e != cudaErrorNotReady) {
+          fail_all(s, "inversion kernel", e);
+        }
+      }
+      if (s->error == PM_OK && s->kstate == pm_server::K_STOPPED) {
+        bool pending = false;
+        for (const Scan* sc : s->active) pending = pending || sc->state == Scan::ADMITTED;
+        if (pending && launch(s)) progress = true;
+      } else if (s->error == PM_OK && s->kstate == pm_server::K_RUNNING) {
+        if (s->active.empty() && s->queued.empty()) {
+          const double now = s->now_ms();
+          if (s->idle_since < 0) s->idle_since = now;
+          else if (now - s->idle_since >= s->sc.linger_ms || s->stop) {
+            if (close_queue(s)) progress = true;
+          }
+        } else {
+          s->idle_since = -1;
         }
       }
     }
-    if (s->stop && s->queued.empty() && s->active.empty()) break;
+    if (s->stop && s->queued.empty() && s->active.empty() &&
+        (s->kstate == pm_server::K_STOPPED || s->error != PM_OK))
+      break;
     if (!progress) {
-      if (s->active.empty() && (s->queued.empty() || s->error != PM_OK)) {
+      if (s->active.empty() && (s->queued.empty() || s->error != PM_OK) &&
+          (s->kstate == pm_server::K_STOPPED || s->error != PM_OK)) {
         if (s->stop) break;
         s->cv_work.wait(lk);
       } else {
@@ -363,8 +409,8 @@ void serve(pm_server* s) {
 }
 
 void release(pm_server* s) {
-  if (s->s_copy && s->q && s->one_host) {
-    // an idle kernel may still linger: close the queue so that it exits now
+  if (s->s_copy && s->q && s->one_host && s->kstate != pm_server::K_STOPPED) {
+    // a kernel still running (after an error): close the queue so that it ends
     cudaMemcpyAsync(&s->q->closed, s->one_host, sizeof(unsigned long long), cudaMemcpyHostToDevice, s->s_copy);
   }
   for (cudaStream_t st : {s->s_copy, s->s_kern, s->s_out})
@@ -375,11 +421,13 @@ void release(pm_server* s) {
   }
   s->scans.clear();
   if (s->ev_kernel) cudaEventDestroy(s->ev_kernel);
+  if (s->ev_reset) cudaEventDestroy(s->ev_reset);
   for (cudaStream_t st : {s->s_copy, s->s_kern, s->s_out})
     if (st) cudaStreamDestroy(st);
   for (void* p : {(void*)s->arena_dev, (void*)s->q, (void*)s->jobs_dev, (void*)s->done_dev})
     if (p) cudaFree(p);
-  for (void* p : {(void*)s->jobs_host, (void*)s->avail_host, (void*)s->one_host, (void*)s->flags_host})
+  for (void* p : {(void*)s->jobs_host, (void*)s->avail_host, (void*)s->one_host, (void*)s->flags_host,
+                  (void*)s->reset_host})
     if (p) cudaFreeHost(p);
   delete s->arena;
   delete s->gs;
@@ -456,6 +504,7 @@ extern "C" int pm_server_create(const pm_line* line, const pm_config* const* gri
   SRV_CUDA(cudaStreamCreateWithFlags(&s->s_copy, cudaStreamNonBlocking), "stream");
   SRV_CUDA(cudaStreamCreateWithFlags(&s->s_out, cudaStreamNonBlocking), "stream");
   SRV_CUDA(cudaEventCreateWithFlags(&s->ev_kernel, cudaEventDisableTiming), "event");
+  SRV_CUDA(cudaEventCreateWithFlags(&s->ev_reset, cudaEventDisableTiming), "event");
   SRV_CUDA(cudaMalloc(&p, sc->hbm_budget_bytes), "arena (hbm_budget_bytes)");
   s->arena_dev = static_cast<unsigned char*>(p);
   s->arena = new (std::nothrow) Arena(sc->hbm_budget_bytes);
@@ -474,6 +523,8 @@ extern "C" int pm_server_create(const pm_line* line, const pm_config* const* gri
   SRV_CUDA(cudaHostAlloc(&p, sizeof(unsigned long long), cudaHostAllocDefault), "pinned word");
   s->one_host = static_cast<unsigned long long*>(p);
   *s->one_host = 1;
+  SRV_CUDA(cudaHostAlloc(&p, 2 * sizeof(unsigned long long), cudaHostAllocDefault), "pinned words");
+  s->reset_host = static_cast<unsigned long long*>(p);
   SRV_CUDA(cudaHostAlloc(&p, sizeof(int) * kRing, cudaHostAllocMapped), "mapped flags");
   s->flags_host = static_cast<int*>(p);
   std::memset(s->flags_host, 0, sizeof(int) * kRing);

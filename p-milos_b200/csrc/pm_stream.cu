@@ -8,12 +8,12 @@ namespace {
 // tickets; the host publishes tickets in stream order after the data they cover
 // has been copied (a copy engine writes PmStreamQ::avail), and appends scans
 // ("jobs": a run of tickets with its own buffers and wavelength grid) to a ring
-// of descriptors.  A warp takes the next ticket with a compare-and-swap below
-// avail, so a ticket is never handed out before it is published and none is
-// lost when the kernel exits.  Waits are bounded: a batch kernel exits once the
-// host has closed the queue and it is drained (or sets err after
-// wait_limit_ns); a serving kernel also exits after linger_ns without work and
-// the host relaunches it when new work arrives.
+// of descriptors.  A warp takes the next ticket with one atomicAdd and owns it:
+// if it is not yet published, the warp waits for its publication, so a ticket
+// is never handed out twice nor lost.  The kernel ends when the host closes the
+// queue (PmStreamQ::closed, written after the last publication): warps holding
+// tickets beyond the final count exit.  Waits are bounded: after wait_limit_ns
+// without its ticket a warp sets PMQ_ERR_WAIT and exits.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p) {
   unsigned long long v;
@@ -28,33 +28,24 @@ __device__ __forceinline__ long long global_ns() {
 }
 
 // Next ticket, or -1 when the kernel should exit.
-__device__ long long next_ticket(PmStreamQ* q, long long linger_ns, long long limit_ns) {
-  unsigned long long n = ld_acquire(&q->next);
-  long long idle_since = -1;
+__device__ long long next_ticket(PmStreamQ* q, long long limit_ns) {
+  const unsigned long long t = atomicAdd(&q->next, 1ull);
+  long long since = -1;
   unsigned sleep = 32;
   while (true) {
-    const unsigned long long avail = ld_acquire(&q->avail);
-    if (n < avail) {
-      const unsigned long long old = atomicCAS(&q->next, n, n + 1);
-      if (old == n) return (long long)n;
-      n = old;
-      continue;
-    }
+    if (t < ld_acquire(&q->avail)) return (long long)t;
     if (ld_acquire(&q->closed)) {
-      // closed is written after the last avail: re-read it once
-      if (n >= ld_acquire(&q->avail)) return -1;
-      continue;
+      // closed is written after the last publication: one more look
+      return t < ld_acquire(&q->avail) ? (long long)t : -1;
     }
     const long long now = global_ns();
-    if (idle_since < 0) idle_since = now;
-    if (linger_ns >= 0 && now - idle_since > linger_ns) return -1;
-    if (now - idle_since > limit_ns) {
+    if (since < 0) since = now;
+    if (now - since > limit_ns) {
       atomicExch(&q->err, (unsigned long long)PMQ_ERR_WAIT);
       return -1;
     }
     __nanosleep(sleep);
     sleep = sleep < 2048 ? 2 * sleep : 2048;
-    n = ld_acquire(&q->next);
   }
 }
 
@@ -78,7 +69,7 @@ __global__ void __launch_bounds__(128, MINB) invert_stream_kernel(const __grid_c
   long long k = sio.first_job;
   while (true) {
     long long t = 0;
-    if (lane == 0) t = next_ticket(sio.q, sio.linger_ns, sio.wait_limit_ns);
+    if (lane == 0) t = next_ticket(sio.q, sio.wait_limit_ns);
     t = __shfl_sync(kFull, t, 0);
     if (t < 0) break;
     // the job of ticket t: jobs are appended in ticket order, so it is at or

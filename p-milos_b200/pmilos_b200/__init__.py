@@ -33,6 +33,7 @@ __all__ = [
     "psf_from_table", "grid_from_malla", "parse_lines_entry", "read_grid_file", "read_lines_file",
     "read_model_file", "read_psf_file", "read_trol_file", "PREC_FP64", "PREC_FP32", "SOLVE_DEFAULT",
     "SOLVE_EIGEN", "SOLVE_CHOLESKY", "SLIGHT_NONE", "SLIGHT_SHARED", "SLIGHT_PER_PIXEL", "Server", "Grid",
+    "fits_header", "ingest_fits",
 ]
 
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
@@ -53,7 +54,8 @@ EXPORTED_SYMBOLS = (
     "pm_line_from_quantum", "pm_psf_gaussian", "pm_psf_interpolate", "pm_ctx_create", "pm_ctx_destroy",
     "pm_invert_batch", "pm_synth_batch", "pm_lm_mils", "pm_invert_batch_noalloc", "pm_get_stats", "pm_last_error",
     "pm_abi_version", "pm_get_tuning", "pm_set_tuning", "pm_autotune", "pm_server_create", "pm_server_submit",
-    "pm_server_wait", "pm_server_get_stats", "pm_server_destroy",
+    "pm_server_wait", "pm_server_get_stats", "pm_server_destroy", "pm_selftest_stalled_queue",
+    "pm_fits_parse_header", "pm_fits_reorder",
 )
 SERVER_MAX_GRIDS = 4
 SERVER_MAX_INFLIGHT = 256
@@ -96,6 +98,14 @@ class _Config(ctypes.Structure):
 class _Tuning(ctypes.Structure):
     _fields_ = [("variant", ctypes.c_int), ("staging_depth", ctypes.c_int), ("warps_per_block", ctypes.c_int),
                 ("graphs", ctypes.c_int)]
+
+
+class _FitsCube(ctypes.Structure):
+    _fields_ = [("naxis", ctypes.c_int), ("naxes", ctypes.c_int64 * 4), ("axis_row", ctypes.c_int),
+                ("axis_col", ctypes.c_int), ("axis_lambda", ctypes.c_int), ("axis_stokes", ctypes.c_int),
+                ("from_ctype", ctypes.c_int), ("nrows", ctypes.c_int64), ("ncols", ctypes.c_int64),
+                ("npix", ctypes.c_int64), ("nlambda", ctypes.c_int), ("data_offset", ctypes.c_int64),
+                ("data_bytes", ctypes.c_int64)]
 
 
 class _ServerConfig(ctypes.Structure):
@@ -157,6 +167,10 @@ def load_library(path: str | None = None):
     L.pm_server_wait.argtypes = [vp, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(_ScanInfo)]
     L.pm_server_get_stats.argtypes = [vp, ctypes.POINTER(_ServerStats)]
     L.pm_server_destroy.argtypes = [vp]
+    L.pm_selftest_stalled_queue.argtypes = [vp, ctypes.c_double, ctypes.POINTER(ctypes.c_int),
+                                            ctypes.POINTER(ctypes.c_double)]
+    L.pm_fits_parse_header.argtypes = [vp, ctypes.c_size_t, ctypes.POINTER(_FitsCube)]
+    L.pm_fits_reorder.argtypes = [ctypes.POINTER(_FitsCube), vp, vp, vp]
     L.pm_last_error.restype = ctypes.c_char_p
     L.pm_abi_version.restype = ctypes.c_int
     if path is None:
@@ -442,6 +456,14 @@ class Inverter:
                                   mode, ctypes.byref(g), int(reps), ctypes.byref(t)))
         return {k: getattr(t, k) for k, _ in _Tuning._fields_}
 
+    def selftest_stalled_queue(self, limit_ms: float = 50.0) -> tuple[int, float]:
+        """Launch the streamed kernel on a queue nothing publishes to: returns
+        (queue error word, kernel ms); 1 = the bounded wait gave up by itself."""
+        err = ctypes.c_int()
+        ms = ctypes.c_double()
+        _check(self.L.pm_selftest_stalled_queue(self.ctx, float(limit_ms), ctypes.byref(err), ctypes.byref(ms)))
+        return err.value, ms.value
+
     def stats(self) -> dict:
         s = _Stats()
         _check(self.L.pm_get_stats(self.ctx, ctypes.byref(s)))
@@ -565,3 +587,40 @@ class Server:
 
     def __exit__(self, *exc):
         self.close()
+
+
+# ---- cube ingest ----
+def _fits_struct(raw) -> "_FitsCube":
+    buf = np.frombuffer(raw, dtype=np.uint8) if not isinstance(raw, np.ndarray) else raw.view(np.uint8).ravel()
+    info = _FitsCube()
+    _check(load_library().pm_fits_parse_header(buf.ctypes.data, buf.size, ctypes.byref(info)))
+    return info
+
+
+def fits_header(raw) -> dict:
+    """Parse a FITS spectro cube's primary header (bytes of the file, at least up
+    to END): axis sizes, the axis of each role, pixels, wavelengths, data block."""
+    info = _fits_struct(raw)
+    out = {k: getattr(info, k) for k, _ in _FitsCube._fields_}
+    out["naxes"] = list(info.naxes)
+    return out
+
+
+def ingest_fits(source, stream=None):
+    """A FITS spectro cube (a path or the file's bytes) as a CUDA float32 tensor
+    [npix][4][nlambda]: the data block is copied to the device as stored and
+    reordered there by pm_fits_reorder."""
+    import torch
+
+    raw = np.fromfile(source, dtype=np.uint8) if isinstance(source, (str, os.PathLike)) else \
+        np.frombuffer(source, dtype=np.uint8)
+    info = _fits_struct(raw)
+    o, n = int(info.data_offset), int(info.data_bytes)
+    if raw.size < o + n:
+        raise PmError(-22, f"the FITS data block needs {o + n} bytes, the file has {raw.size}")
+    data = torch.from_numpy(np.array(raw[o:o + n], copy=True)).to("cuda", non_blocking=False)
+    cube = torch.empty((int(info.npix), 4, int(info.nlambda)), dtype=torch.float32, device="cuda")
+    st = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    _check(load_library().pm_fits_reorder(ctypes.byref(info), data.data_ptr(), cube.data_ptr(), ctypes.c_void_p(st)))
+    torch.cuda.current_stream().synchronize() if stream is None else None
+    return cube

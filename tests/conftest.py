@@ -11,18 +11,14 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
 def pytest_configure(config):
+    """Register the gpu marker; build the CUDA library and the oracle if they are
+    missing or stale (nvcc/gcc only) before any test module loads them."""
     config.addinivalue_line("markers", "gpu: needs a B200 (runs the CUDA library)")
-
-
-@pytest.fixture(scope="session", autouse=True)
-def _built():
-    """Build the CUDA library and the oracle if they are missing (nvcc/gcc only)."""
     from pmilos_b200 import _build
     import pyoracle
 
     _build.build()
     pyoracle.build()
-    yield
 
 
 @pytest.fixture(scope="session")

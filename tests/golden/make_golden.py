@@ -15,6 +15,9 @@ Writes
                       plus mil_sinrf + me_der outputs at 12 models
   ref_psf.npz         the reference's fgauss_WL and interpolationLinearPSF on the
                       configuration grids (host precompute pinning)
+  fits_cases.npz      the reference's FITS cube reader (readFitsSpectroImage over
+                      a CFITSIO read shim) on small cubes in eight axis orders,
+                      with and without CTYPE cards: file bytes and output
   ref_cases_wide.npz  the same per-case content on grids wider than one warp:
                       w112 (112 points of Fe I 6302 at 21.5 mA, 25 mA PSF, the
                       large-cube configuration) and w49 (the known-answer test's
@@ -143,6 +146,36 @@ def case(cfg, seed, npix=48, nsynth=12):
     return out
 
 
+# FITS cubes in several axis orders, with and without CTYPE cards: (order of
+# roles for FITS axes 1..4, CTYPEs written?).  R = rows, C = cols, L = wavelength,
+# S = Stokes.
+FITS_ORDERS = [("LSRC", True), ("SLRC", True), ("RCLS", True), ("CRSL", True), ("LRSC", True),
+               ("LSRC", False), ("RCLS", False), ("SRLC", False)]
+CTYPE_OF = {"R": "HPLN-TAN", "C": "HPLT-TAN", "L": "WAVE-GRI", "S": "STOKES"}
+
+
+def fits_cases(tmpdir):
+    """The reference's reader on small synthetic cubes: the file bytes and its
+    output (pmilos' forParallel layout) per axis order."""
+    rng = np.random.default_rng(77)
+    size = {"R": 9, "C": 11, "L": 7, "S": 4}
+    out = {}
+    for k, (order, with_ctype) in enumerate(FITS_ORDERS):
+        dims = [size[r] for r in order]
+        data = rng.normal(size=dims[::-1]).astype(np.float32)
+        ct = [CTYPE_OF[r] for r in order] if with_ctype else None
+        raw = po.fits_bytes(data, ct)
+        path = os.path.join(tmpdir, f"cube{k}.fits")
+        open(path, "wb").write(raw)
+        cube, rows, cols = po.reference_fits_read(path, size["L"], size["R"] * size["C"])
+        out[f"f{k}_bytes"] = np.frombuffer(raw, dtype=np.uint8)
+        out[f"f{k}_ref"] = cube
+        out[f"f{k}_order"] = np.array(order)
+        out[f"f{k}_ctype"] = np.array(with_ctype)
+        out[f"f{k}_rows_cols"] = np.array([rows, cols])
+    return out
+
+
 def psf_pins():
     ref = po.Reference(po.LineSetup(*grid(-350.0, 25.0, 375.0, 6173.3354)[1:], 6173.3354, TRIPLET, None, 9), "f64")
     out = {}
@@ -189,6 +222,11 @@ def main():
         np.savez_compressed(os.path.join(HERE, "ref_cases.npz"), **cases)
         np.savez_compressed(os.path.join(HERE, "ref_psf.npz"), **psf_pins())
         files += ["kat_synthesis.npz", "ref_cases.npz", "ref_psf.npz"]
+    import tempfile
+
+    with tempfile.TemporaryDirectory() as td:
+        np.savez_compressed(os.path.join(HERE, "fits_cases.npz"), **fits_cases(td))
+    files.append("fits_cases.npz")
     wide = {}
     for cfg in (112, 49):
         for k, v in case(cfg, cfg, npix=16, nsynth=4).items():

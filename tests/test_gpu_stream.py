@@ -113,3 +113,17 @@ def test_small_calls_replay_a_captured_graph():
         # lm_mils, the batch of one, takes the graph path too
         rc, model, spectra, chi, it = inv.lm_mils(c["obs"][7], c["guess"], slight=c["slight"])
         assert np.array_equal(model, ref["models"][7]) and it == ref["iters"][7]
+
+
+def test_stalled_queue_wait_is_bounded_and_reported():
+    """A producer that never publishes cannot hang the device: the persistent
+    kernel's wait gives up after its limit, says so in the queue's error word,
+    and the context inverts normally afterwards."""
+    c = case(1)
+    with inverter(c, pm.PREC_FP32) as inv:
+        err, ms = inv.selftest_stalled_queue(50.0)
+        assert err == 1
+        assert 40.0 <= ms < 2000.0
+        ref = inv.invert(c["obs"], c["guess"])
+        inv.tuning = {"graphs": 0, "staging_depth": 4}
+        _same(inv.invert(c["obs"], c["guess"]), ref)
