@@ -283,6 +283,7 @@ def main():
     ap.add_argument("--plain-requests", type=int, default=12,
                     help="served stream: scans of the same schedule timed on the plain FP64 server")
     ap.add_argument("--budget-gb", type=float, default=24.0, help="served stream: device arena of the server")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch tuning")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -358,10 +359,11 @@ def main():
     sl_d = None if sl_h is None else torch.as_tensor(sl_h, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     # the project's autotuner picks the launch tuning on a sample of this cube (untimed)
-    ns = min(w.npix, 32768)
-    sample = obs[:ns] if obs is not None else obs_d[:ns].cpu().numpy()
-    tuning = inv32.autotune(sample, w.guess, slight=sl_h, reps=2)
-    cfg_desc["tuning"] = tuning
+    if not args.no_autotune:
+        ns = min(w.npix, 32768)
+        sample = obs[:ns] if obs is not None else obs_d[:ns].cpu().numpy()
+        inv32.autotune(sample, w.guess, slight=sl_h, reps=2)
+    cfg_desc["tuning"] = inv32.tuning
 
     def barrier():
         if dist is not None:

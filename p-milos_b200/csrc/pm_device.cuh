@@ -303,6 +303,13 @@ struct alignas(16) WarpSmem {
   R ls[NL][kLaneStatePad];    // synthesis state the response functions need, per lane
   ModelTerms<R> mt;           // per-model terms of the last synthesis (uniform)
   double model[11], trial[11];
+  // the streamed kernel's place in the ticket stream: kept here rather than in
+  // registers while the LM loop runs
+  const PmJob* job;
+  unsigned long long pix;
+  long long job_k;
+  int grid_cur;
+  int pad_;
 };
 
 // The 16-byte vector loads of psf_rows and rf_correlate need every per-warp
@@ -998,8 +1005,10 @@ __device__ __forceinline__ void classical_finish(const PmParams& P, const double
   if (isnan(m[6])) m[6] = 1;
 }
 
-// Classical estimates of a one-warp pixel (lane = wavelength).
-__device__ void classical(const PmParams& P, const float O[4], int lane, bool valid, double* m) {
+// Classical estimates of a one-warp pixel (lane = wavelength).  Out of line: it
+// runs once per pixel, and keeping it out of the LM loop's code keeps that code
+// compact in the instruction cache.
+__device__ __noinline__ void classical(const PmParams& P, const float O[4], int lane, bool valid, double* m) {
   const int nl = P.nl;
   const unsigned neg = __ballot_sync(kFull, valid && O[0] < 0.0f);
   const unsigned validm = (nl >= 32) ? kFull : ((1u << nl) - 1u);
@@ -1048,40 +1057,51 @@ __device__ __forceinline__ WarpSmem<R>& warp_smem(unsigned char* raw, int warp) 
   return reinterpret_cast<WarpSmem<R>*>(raw + sizeof(BlockSmem<R>))[warp];
 }
 
-// Where one pixel's data and results live.
-struct PixIO {
-  const float* obs;          // [4][nl]
-  const float* sl_pix;       // per-pixel stray light [4][nl], or null
-  double* model_out;         // [11]
-  float* chisq_out;
-  int* iters_out;
-  int* status_out;           // nullable
-  float* spectra_out;        // [4][nl], nullable
-  unsigned long long* ctr;   // statistics counters (PMC_*)
-};
+// A pointer field of a job descriptor, read from L2 (the host may have written
+// the descriptor while the kernel runs).
+template <typename T>
+__device__ __forceinline__ T* ld_ptr(T* const* p) {
+  return reinterpret_cast<T*>(__ldcg(reinterpret_cast<const unsigned long long*>(p)));
+}
 
-// lm_mils for one pixel on one warp (milosUtils.c:466-635), preceded by the
-// classical estimates (milos.c:958-983).  The profiles may have been written by
-// a copy engine while the kernel runs, so they are read from L2.
+// lm_mils for one pixel on one warp (milosUtils.c:466-635), starting from the
+// classical estimates (milos.c:958-983): those of the pre-pass kernel when the
+// whole cube was on the device before the launch, else computed here.  The
+// profiles may have been written by a copy engine while the kernel runs, so
+// they are read from L2.
+// Pixel sm.pix of job *sm.job.  The job, the pixel index and the buffer
+// pointers are read from shared memory and the descriptor where they are used,
+// so that none of them occupies registers across the LM loop.
 template <typename R, int KT>
 __device__ __forceinline__ void invert_pixel(const PmParams& P, const BlockSmem<R>& bs, WarpSmem<R>& sm, int lane,
-                                             const PixIO& px) {
+                                             unsigned long long* ctr) {
   const bool valid = lane < P.nl;
   double* m = sm.model;
   double* trial = sm.trial;
-  const float* sl_pix = px.sl_pix;
+  const PmJob* jp = sm.job;
+  size_t p = sm.pix;
+  size_t base = p * 4 * P.nl;
+  const float* sl_pix = nullptr;
+  if (P.slight_mode == PM_SLIGHT_PER_PIXEL) {
+    const float* sl = ld_ptr(&jp->slight);
+    if (sl) sl_pix = sl + base;
+  }
+  const float* obs = ld_ptr(&jp->spectro) + base;
+  const double* model_in = ld_ptr(&jp->model_in);
 
   float O[4];
   R isig[4];
   int ghosts = 0;
 #pragma unroll
   for (int s = 0; s < 4; ++s) {
-    O[s] = valid ? __ldcg(px.obs + s * P.nl + lane) : 0.0f;
+    O[s] = valid ? __ldcg(obs + s * P.nl + lane) : 0.0f;
     const bool g = valid && O[s] <= -1.0f;
     ghosts += __popc(__ballot_sync(kFull, g));
     isig[s] = R(1.0 / (g ? kGhostSigma : P.noise));
   }
-  {
+  if (model_in) {
+    if (lane < 11) m[lane] = __ldcg(model_in + p * 11 + lane);
+  } else {
     double g[11];
 #pragma unroll
     for (int i = 0; i < 11; ++i) g[i] = P.guess[i];
@@ -1170,18 +1190,23 @@ __device__ __forceinline__ void invert_pixel(const PmParams& P, const BlockSmem<
     if (!finite) status = PM_PIX_NONFINITE;
   }
   // outputs
-  if (lane < 11) px.model_out[lane] = m[lane];
+  jp = *reinterpret_cast<const PmJob* const volatile*>(&sm.job);
+  p = *reinterpret_cast<const volatile unsigned long long*>(&sm.pix);
+  base = p * 4 * P.nl;
+  if (lane < 11) ld_ptr(&jp->models)[p * 11 + lane] = m[lane];
   if (lane == 0) {
-    *px.chisq_out = float(ochi);
-    *px.iters_out = iter;
-    if (px.status_out) *px.status_out = status;
-    atomicAdd(&px.ctr[PMC_ITERS], (unsigned long long)(iter > 0 ? iter : 0));
-    atomicAdd(&px.ctr[PMC_ACCEPTED], (unsigned long long)accepted);
-    if (fallbacks) atomicAdd(&px.ctr[PMC_FALLBACK], (unsigned long long)fallbacks);
+    ld_ptr(&jp->chisq)[p] = float(ochi);
+    ld_ptr(&jp->iters)[p] = iter;
+    int* st = ld_ptr(&jp->status);
+    if (st) st[p] = status;
+    atomicAdd(&ctr[PMC_ITERS], (unsigned long long)(iter > 0 ? iter : 0));
+    atomicAdd(&ctr[PMC_ACCEPTED], (unsigned long long)accepted);
+    if (fallbacks) atomicAdd(&ctr[PMC_FALLBACK], (unsigned long long)fallbacks);
   }
-  if (px.spectra_out && valid) {
+  float* spectra = ld_ptr(&jp->spectra);
+  if (spectra && valid) {
 #pragma unroll
-    for (int s = 0; s < 4; ++s) px.spectra_out[s * P.nl + lane] = float(S[s]);
+    for (int s = 0; s < 4; ++s) spectra[base + s * P.nl + lane] = float(S[s]);
   }
   __syncwarp();
 }

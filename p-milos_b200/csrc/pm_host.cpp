@@ -596,6 +596,7 @@ int run_graph_small(pm_ctx* c, int64_t n, const float* spectro, const float* sli
   job.iters = static_cast<int*>(c->iters.p);
   job.status = want_status ? static_cast<int*>(c->status.p) : nullptr;
   job.spectra = want_spectra ? static_cast<float*>(c->spectra.p) : nullptr;
+  job.model_in = c->P.classical ? static_cast<const double*>(c->models.p) : nullptr;
   std::memset(&hc->qinit, 0, sizeof hc->qinit);
   hc->qinit.avail = (unsigned long long)n;
   hc->qinit.closed = 1;
@@ -627,7 +628,10 @@ int run_graph_small(pm_ctx* c, int64_t n, const float* spectro, const float* sli
     if (e == cudaSuccess) e = cudaMemcpyAsync(c->jobs.p, &hc->job, sizeof(PmJob), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(q, &hc->qinit, sizeof(PmStreamQ), cudaMemcpyHostToDevice, s);
     int krc = PM_OK;
-    if (e == cudaSuccess) {
+    if (e == cudaSuccess && c->P.classical)
+      krc = pmk_classical_prepass(c->P, static_cast<const float*>(c->spectro.p), static_cast<double*>(c->models.p), n,
+                                  s, c->num_sms);
+    if (e == cudaSuccess && krc == PM_OK) {
       PmStreamIO sio{};
       sio.q = q;
       sio.jobs = static_cast<const PmJob*>(c->jobs.p);
@@ -731,6 +735,7 @@ int run_invert(pm_ctx* c, PmIO io, float* kernel_ms) {
   job.iters = io.iters_out;
   job.status = io.status_out;
   job.spectra = io.spectra_out;
+  job.model_in = c->P.classical ? io.models_out : nullptr;  // written by the pre-pass below
   std::memset(&hc->qinit, 0, sizeof hc->qinit);
   hc->qinit.avail = (unsigned long long)io.npix;
   hc->qinit.closed = 1;
@@ -746,6 +751,10 @@ int run_invert(pm_ctx* c, PmIO io, float* kernel_ms) {
   sio.first_job = 0;
   sio.wait_limit_ns = 20000000000LL;
   PM_CUDA(cudaEventRecord(c->k0, c->stream), "event");
+  if (c->P.classical) {
+    rc = pmk_classical_prepass(c->P, io.spectro, io.models_out, io.npix, c->stream, c->num_sms);
+    if (rc != PM_OK) return fail(rc, "%s", pmk_last_cuda_error());
+  }
   rc = pmk_invert_stream(*c->gs, sio, c->precision, c->tuning.variant, c->tuning.warps_per_block, false, c->stream,
                          c->num_sms, nullptr);
   if (rc != PM_OK) return fail(rc, "%s", pmk_last_cuda_error());

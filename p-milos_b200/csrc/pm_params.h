@@ -85,6 +85,7 @@ struct PmJob {
   float* spectra;           // nullable
   unsigned long long* done; // device counter of finished pixels (zeroed before publication), nullable
   int* host_flag;           // mapped host word set to 1 when the last pixel is done, nullable
+  const double* model_in;   // [npix][11] starting models of the classical pre-pass, nullable
 };
 
 static_assert(sizeof(PmGridSet) + 64 <= 32764, "kernel parameter block of the streamed kernel exceeds 32 KB");
@@ -121,6 +122,10 @@ int pmk_synth(const PmParams& P, const PmIO& io, int precision, void* stream);
 // Grids of more than 32 wavelengths (pm_wide.cu), called by pmk_invert / pmk_synth.
 int pmk_invert_wide(const PmParams& P, const PmIO& io, int precision, void* stream, int num_sms, float* kernel_ms);
 int pmk_synth_wide(const PmParams& P, const PmIO& io, int precision, void* stream);
+// Classical estimates of npix pixels (one-warp grid) into models [npix][11]:
+// the starting models of a launch whose cube is on the device before it starts.
+int pmk_classical_prepass(const PmParams& P, const float* spectro, double* models, int64_t npix, void* stream,
+                          int num_sms);
 // Streamed inversion: every grid of GS has the same nterms and nl <= 32.
 // multi: grids differ between jobs (dynamic grid index) rather than one grid.
 int pmk_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, int precision, int variant, int warps_per_block,

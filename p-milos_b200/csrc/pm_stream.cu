@@ -49,14 +49,19 @@ __device__ long long next_ticket(PmStreamQ* q, long long limit_ns) {
   }
 }
 
-template <typename T>
-__device__ __forceinline__ T* ld_ptr(T* const* p) {
-  return reinterpret_cast<T*>(__ldcg(reinterpret_cast<const unsigned long long*>(p)));
-}
+
+// The grids a launch serves, by value: all PMK_MAX_GRIDS slots for a server's
+// mixed launch, one slot otherwise (a 7 KB rather than 28 KB parameter block).
+template <int NG>
+struct GridParams {
+  int ngrids;
+  int pad_;
+  PmParams g[NG];
+};
 
 template <typename R, int KT, int MINB, bool MULTI>
-__global__ void __launch_bounds__(128, MINB) invert_stream_kernel(const __grid_constant__ PmGridSet GS,
-                                                                    const PmStreamIO sio) {
+__global__ void __launch_bounds__(128, MINB) invert_stream_kernel(
+    const __grid_constant__ GridParams<MULTI ? PMK_MAX_GRIDS : 1> GS, const PmStreamIO sio) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int NG = MULTI ? PMK_MAX_GRIDS : 1;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -65,8 +70,11 @@ __global__ void __launch_bounds__(128, MINB) invert_stream_kernel(const __grid_c
 #pragma unroll 1
   for (int g = 0; g < NG && g < GS.ngrids; ++g) load_taps<R>(GS.g[g], bs[g]);
   __syncthreads();
-  int cur = -1;             // grid of the previous pixel: the padded rows are re-zeroed on a change
-  long long k = sio.first_job;
+  if (lane == 0) {
+    sm.job_k = sio.first_job;
+    sm.grid_cur = -1;  // grid of the previous pixel: the padded rows are re-zeroed on a change
+  }
+  __syncwarp();
   while (true) {
     long long t = 0;
     if (lane == 0) t = next_ticket(sio.q, sio.wait_limit_ns);
@@ -76,6 +84,7 @@ __global__ void __launch_bounds__(128, MINB) invert_stream_kernel(const __grid_c
     // after this warp's previous one
     const PmJob* jp = nullptr;
     unsigned long long t0 = 0;
+    long long k = sm.job_k;
     for (int guard = 0; guard <= sio.jobs_cap; ++guard, ++k) {
       const PmJob* c = sio.jobs + (k % sio.jobs_cap);
       const unsigned long long c0 = __ldcg(&c->t0);
@@ -92,31 +101,25 @@ __global__ void __launch_bounds__(128, MINB) invert_stream_kernel(const __grid_c
     }
     const int gi = MULTI ? __ldcg(&jp->grid) : 0;
     const PmParams& P = GS.g[gi];
-    if (gi != cur) {
+    if (gi != sm.grid_cur) {
       for (int e = lane; e < 4 * XSR; e += 32) (&sm.xs[0][0])[e] = R(0);
-      cur = gi;
       __syncwarp();
+      if (lane == 0) sm.grid_cur = gi;
     }
-    const unsigned long long p = (unsigned long long)t - t0;
-    const size_t base = size_t(p) * 4 * P.nl;
-    const float* slight = ld_ptr(&jp->slight);
-    float* spectra = ld_ptr(&jp->spectra);
-    int* status = ld_ptr(&jp->status);
-    PixIO px;
-    px.obs = ld_ptr(&jp->spectro) + base;
-    px.sl_pix = (P.slight_mode == PM_SLIGHT_PER_PIXEL && slight) ? slight + base : nullptr;
-    px.model_out = ld_ptr(&jp->models) + size_t(p) * 11;
-    px.chisq_out = ld_ptr(&jp->chisq) + p;
-    px.iters_out = ld_ptr(&jp->iters) + p;
-    px.status_out = status ? status + p : nullptr;
-    px.spectra_out = spectra ? spectra + base : nullptr;
-    px.ctr = sio.q->ctr;
-    invert_pixel<R, KT>(P, bs[gi], sm, lane, px);
     if (lane == 0) {
-      unsigned long long* done = ld_ptr(&jp->done);
-      int* flag = ld_ptr(&jp->host_flag);
-      __threadfence();  // this pixel's results before its count
-      if (done) {
+      sm.job_k = k;
+      sm.job = jp;
+      sm.pix = (unsigned long long)t - t0;
+    }
+    __syncwarp();
+    invert_pixel<R, KT>(P, bs[gi], sm, lane, sio.q->ctr);
+    jp = *reinterpret_cast<const PmJob* const volatile*>(&sm.job);
+    unsigned long long* done = ld_ptr(&jp->done);
+    if (done) {
+      __threadfence();  // every lane: its part of this pixel's results before the count
+      __syncwarp();
+      if (lane == 0) {
+        int* flag = ld_ptr(&jp->host_flag);
         const unsigned long long np = __ldcg(reinterpret_cast<const unsigned long long*>(&jp->npix));
         if (atomicAdd(done, 1ull) + 1 == np && flag) {
           __threadfence_system();
@@ -129,6 +132,32 @@ __global__ void __launch_bounds__(128, MINB) invert_stream_kernel(const __grid_c
 }
 
 
+// Classical estimates (estimacionesClasicas + the NaN fixes of milos.c:975-983),
+// one warp per pixel, written to models as the starting models of the streamed
+// kernel when the cube is on the device before the launch.
+__global__ void __launch_bounds__(256) classical_prepass_kernel(const __grid_constant__ PmParams P,
+                                                                const float* spectro, double* models,
+                                                                long long npix) {
+  const int lane = threadIdx.x & 31;
+  const bool valid = lane < P.nl;
+  const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long pix = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); pix < npix; pix += nwarps) {
+    const size_t base = size_t(pix) * 4 * P.nl;
+    float O[4];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) O[s] = valid ? spectro[base + s * P.nl + lane] : 0.0f;
+    double g[11];
+#pragma unroll
+    for (int i = 0; i < 11; ++i) g[i] = P.guess[i];
+    classical(P, O, lane, valid, g);
+    double mine = g[0];
+#pragma unroll
+    for (int i = 1; i < 11; ++i)
+      if (lane == i) mine = g[i];
+    if (lane < 11) models[size_t(pix) * 11 + lane] = mine;
+  }
+}
+
 template <typename R, int KT, int MINB, bool MULTI>
 int launch_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, cudaStream_t st, int num_sms,
                          size_t* smem_out, int wpb) {
@@ -136,12 +165,16 @@ int launch_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, cudaStream_
   const size_t smem = (MULTI ? PMK_MAX_GRIDS : 1) * sizeof(BlockSmem<R>) + sizeof(WarpSmem<R>) * (threads / 32);
   if (smem_out) *smem_out = smem;
   auto kern = invert_stream_kernel<R, KT, MINB, MULTI>;
+  constexpr int NG = MULTI ? PMK_MAX_GRIDS : 1;
+  GridParams<NG> gp;  // copied into the launch
+  gp.ngrids = GS.ngrids < NG ? GS.ngrids : NG;
+  for (int g = 0; g < gp.ngrids; ++g) gp.g[g] = GS.g[g];
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return snprintf(pmk_g_err, sizeof pmk_g_err, "%s", cudaGetErrorString(e)), PM_EIO;
   int per_sm = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
   if (e != cudaSuccess || per_sm < 1) return snprintf(pmk_g_err, sizeof pmk_g_err, "occupancy: %s", cudaGetErrorString(e)), PM_EIO;
-  kern<<<unsigned(per_sm * num_sms), threads, smem, st>>>(GS, sio);
+  kern<<<unsigned(per_sm * num_sms), threads, smem, st>>>(gp, sio);
   e = cudaGetLastError();
   if (e != cudaSuccess) return snprintf(pmk_g_err, sizeof pmk_g_err, "stream launch: %s", cudaGetErrorString(e)), PM_EIO;
   return PM_OK;
@@ -190,3 +223,18 @@ int pmk_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, int precision,
   return PM_ENOTSUP;
 }
 
+
+int pmk_classical_prepass(const PmParams& P, const float* spectro, double* models, int64_t npix, void* stream,
+                          int num_sms) {
+  if (P.G != 1) {
+    snprintf(pmk_g_err, sizeof pmk_g_err, "classical pre-pass: one-warp grids only");
+    return PM_EINVAL;
+  }
+  long long blocks = (npix + 7) / 8;
+  if (blocks > (long long)num_sms * 16) blocks = (long long)num_sms * 16;
+  if (blocks < 1) blocks = 1;
+  classical_prepass_kernel<<<unsigned(blocks), 256, 0, static_cast<cudaStream_t>(stream)>>>(P, spectro, models, npix);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return snprintf(pmk_g_err, sizeof pmk_g_err, "classical launch: %s", cudaGetErrorString(e)), PM_EIO;
+  return PM_OK;
+}
