@@ -310,6 +310,11 @@ int pm_server_create(const pm_line *line, const pm_config *const *grids, const p
  * scan's id; PM_ERANGE if the scan alone exceeds the arena. */
 int pm_server_submit(pm_server *srv, int grid, int64_t npix, const float *spectro, pm_model *models_out,
                      float *chisq_out, int *iters_out, int *status_out, uint64_t *id_out);
+/* The same for a cube already in this GPU's memory (for instance from
+ * pm_fits_reorder): nothing is copied in and the cube takes no arena space; the
+ * device array must stay valid until the scan is done. */
+int pm_server_submit_device(pm_server *srv, int grid, int64_t npix, const float *spectro_dev, pm_model *models_out,
+                            float *chisq_out, int *iters_out, int *status_out, uint64_t *id_out);
 /* Block until scan `id` is done (its results are in the host arrays) or
  * timeout_s passes (PM_ETIMEDOUT).  info (nullable) gets its timings. */
 int pm_server_wait(pm_server *srv, uint64_t id, double timeout_s, pm_scan_info *info);

@@ -101,7 +101,7 @@ struct SmallStage {
 struct pm_ctx {
   PmParams P;
   int precision = PM_PREC_FP32;
-  pm_tuning tuning{0, 8, 4, 1};
+  pm_tuning tuning{1, 8, 4, 1};
   int device = 0;
   int num_sms = 148;
   cudaStream_t stream = nullptr;

@@ -98,6 +98,7 @@ struct Scan {
   int grid = 0;
   int64_t npix = 0;
   const float* spectro = nullptr;
+  bool device_input = false;  // spectro is caller-owned device memory (no copy, no arena space)
   pm_model* models_out = nullptr;
   float* chisq_out = nullptr;
   int* iters_out = nullptr;
@@ -115,7 +116,7 @@ thread_local char g_err[256];
 }  // namespace
 
 struct pm_server {
-  int device = 0, num_sms = 148, precision = PM_PREC_FP32, variant = 0, ngrids = 0;
+  int device = 0, num_sms = 148, precision = PM_PREC_FP32, variant = 1, ngrids = 0;
   PmGridSet* gs = nullptr;
   pm_server_config sc{};
   size_t prof[PM_SERVER_MAX_GRIDS] = {};
@@ -195,7 +196,7 @@ bool admit(pm_server* s, Scan* sc) {
   J.t0 = s->t_next;
   J.npix = sc->npix;
   J.grid = sc->grid;
-  J.spectro = reinterpret_cast<const float*>(base);
+  J.spectro = sc->device_input ? sc->spectro : reinterpret_cast<const float*>(base);
   J.models = reinterpret_cast<double*>(base + sc->o_models);
   J.chisq = reinterpret_cast<float*>(base + sc->o_chisq);
   J.iters = reinterpret_cast<int*>(base + sc->o_iters);
@@ -204,7 +205,7 @@ bool admit(pm_server* s, Scan* sc) {
   J.host_flag = s->flags_dev + slot;
   reinterpret_cast<volatile int*>(s->flags_host)[slot] = 0;
   cudaError_t e = cudaMemsetAsync(s->done_dev + slot, 0, sizeof(unsigned long long), s->s_copy);
-  if (e == cudaSuccess)
+  if (e == cudaSuccess && !sc->device_input)
     e = cudaMemcpyAsync(base, sc->spectro, prof * size_t(sc->npix), cudaMemcpyHostToDevice, s->s_copy);
   if (e == cudaSuccess) e = cudaMemcpyAsync(s->jobs_dev + slot, &J, sizeof J, cudaMemcpyHostToDevice, s->s_copy);
   s->avail_host[slot] = s->t_next + (unsigned long long)sc->npix;
@@ -541,8 +542,10 @@ extern "C" int pm_server_create(const pm_line* line, const pm_config* const* gri
   return PM_OK;
 }
 
-extern "C" int pm_server_submit(pm_server* s, int grid, int64_t npix, const float* spectro, pm_model* models_out,
-                                float* chisq_out, int* iters_out, int* status_out, uint64_t* id_out) {
+namespace {
+
+int submit(pm_server* s, int grid, int64_t npix, const float* spectro, bool device_input, pm_model* models_out,
+           float* chisq_out, int* iters_out, int* status_out, uint64_t* id_out) {
   if (!s || !spectro || !models_out || !chisq_out || !iters_out || !id_out)
     return sfail(PM_EINVAL, "pm_server_submit: NULL argument");
   if (grid < 0 || grid >= s->ngrids) return sfail(PM_EINVAL, "pm_server_submit: no such grid");
@@ -553,11 +556,12 @@ extern "C" int pm_server_submit(pm_server* s, int grid, int64_t npix, const floa
   sc->grid = grid;
   sc->npix = npix;
   sc->spectro = spectro;
+  sc->device_input = device_input;
   sc->models_out = models_out;
   sc->chisq_out = chisq_out;
   sc->iters_out = iters_out;
   sc->status_out = status_out;
-  sc->o_models = round_up(s->prof[grid] * n);
+  sc->o_models = device_input ? 0 : round_up(s->prof[grid] * n);
   sc->o_chisq = sc->o_models + round_up(sizeof(pm_model) * n);
   sc->o_iters = sc->o_chisq + round_up(sizeof(float) * n);
   sc->o_status = sc->o_iters + round_up(sizeof(int) * n);
@@ -583,6 +587,19 @@ extern "C" int pm_server_submit(pm_server* s, int grid, int64_t npix, const floa
   }
   s->cv_work.notify_one();
   return PM_OK;
+}
+
+}  // namespace
+
+extern "C" int pm_server_submit(pm_server* s, int grid, int64_t npix, const float* spectro, pm_model* models_out,
+                                float* chisq_out, int* iters_out, int* status_out, uint64_t* id_out) {
+  return submit(s, grid, npix, spectro, false, models_out, chisq_out, iters_out, status_out, id_out);
+}
+
+extern "C" int pm_server_submit_device(pm_server* s, int grid, int64_t npix, const float* spectro_dev,
+                                       pm_model* models_out, float* chisq_out, int* iters_out, int* status_out,
+                                       uint64_t* id_out) {
+  return submit(s, grid, npix, spectro_dev, true, models_out, chisq_out, iters_out, status_out, id_out);
 }
 
 extern "C" int pm_server_wait(pm_server* s, uint64_t id, double timeout_s, pm_scan_info* info) {

@@ -55,7 +55,7 @@ EXPORTED_SYMBOLS = (
     "pm_invert_batch", "pm_synth_batch", "pm_lm_mils", "pm_invert_batch_noalloc", "pm_get_stats", "pm_last_error",
     "pm_abi_version", "pm_get_tuning", "pm_set_tuning", "pm_autotune", "pm_server_create", "pm_server_submit",
     "pm_server_wait", "pm_server_get_stats", "pm_server_destroy", "pm_selftest_stalled_queue",
-    "pm_fits_parse_header", "pm_fits_reorder",
+    "pm_fits_parse_header", "pm_fits_reorder", "pm_server_submit_device",
 )
 SERVER_MAX_GRIDS = 4
 SERVER_MAX_INFLIGHT = 256
@@ -164,6 +164,7 @@ def load_library(path: str | None = None):
                                    ctypes.POINTER(_Model), ctypes.c_int, ctypes.POINTER(_ServerConfig),
                                    ctypes.POINTER(vp)]
     L.pm_server_submit.argtypes = [vp, ctypes.c_int, i64, F, vp, vp, vp, vp, ctypes.POINTER(ctypes.c_uint64)]
+    L.pm_server_submit_device.argtypes = [vp, ctypes.c_int, i64, F, vp, vp, vp, vp, ctypes.POINTER(ctypes.c_uint64)]
     L.pm_server_wait.argtypes = [vp, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(_ScanInfo)]
     L.pm_server_get_stats.argtypes = [vp, ctypes.POINTER(_ServerStats)]
     L.pm_server_destroy.argtypes = [vp]
@@ -536,22 +537,33 @@ class Server:
         self._pending = {}
 
     def submit(self, grid: int, spectro, want_status: bool = True) -> int:
-        obs = spectro if (isinstance(spectro, np.ndarray) and spectro.dtype == np.float32 and
-                          spectro.flags.c_contiguous) else np.ascontiguousarray(spectro, dtype=np.float32)
+        """Queue a scan: a host array, or a CUDA float32 tensor already on this GPU
+        (used in place; keep it unchanged until the scan is done)."""
         if not 0 <= grid < len(self.nl):
             raise PmError(-22, f"no grid {grid} (the server holds {len(self.nl)})")
         nl = self.nl[grid]
-        if obs.size % (4 * nl):
+        on_device = _is_torch(spectro) and spectro.is_cuda
+        if on_device:
+            import torch
+
+            if spectro.dtype != torch.float32 or not spectro.is_contiguous():
+                raise TypeError("a device scan must be a contiguous float32 CUDA tensor")
+            obs, size, ptr = spectro, spectro.numel(), spectro.data_ptr()
+        else:
+            obs = spectro if (isinstance(spectro, np.ndarray) and spectro.dtype == np.float32 and
+                              spectro.flags.c_contiguous) else np.ascontiguousarray(spectro, dtype=np.float32)
+            size, ptr = obs.size, obs.ctypes.data
+        if size % (4 * nl):
             raise ValueError(f"grid {grid} has {nl} wavelengths: spectro must be [npix][4][{nl}]")
-        npix = obs.size // (4 * nl)
+        npix = size // (4 * nl)
         models = np.zeros((npix, 11))
         chi = np.zeros(npix, dtype=np.float32)
         its = np.zeros(npix, dtype=np.int32)
         stt = np.zeros(npix, dtype=np.int32) if want_status else None
         sid = ctypes.c_uint64()
-        _check(self.L.pm_server_submit(self.srv, int(grid), npix, obs.ctypes.data, models.ctypes.data,
-                                       chi.ctypes.data, its.ctypes.data, None if stt is None else stt.ctypes.data,
-                                       ctypes.byref(sid)))
+        fn = self.L.pm_server_submit_device if on_device else self.L.pm_server_submit
+        _check(fn(self.srv, int(grid), npix, ptr, models.ctypes.data, chi.ctypes.data, its.ctypes.data,
+                  None if stt is None else stt.ctypes.data, ctypes.byref(sid)))
         self._pending[sid.value] = (obs, models, chi, its, stt)
         return sid.value
 
