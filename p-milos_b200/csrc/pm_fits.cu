@@ -15,6 +15,8 @@
 // applies the generic branch's mapping to every order.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -69,69 +71,75 @@ bool card_string(const char* card, char* out, size_t cap) {
 }
 
 // out[((pixel * 4 + s) * nl) + l] = byteswap(in[l*st_l + s*st_s + row*st_r + col*st_c]),
-// pixel = col * rows + row.  Wavelength is the fastest axis of the output; when
-// it is also the fastest of the input (the reference's default order) every
-// thread copies one element with coalesced reads and writes; otherwise a 32 x
-// 32 tile of (wavelength, the input's fastest axis) goes through shared memory
-// so that both sides stay coalesced.
+// pixel = col * rows + row, i.e. out = sum over axes of coordinate * ost[axis].
+// Three forms, all reading and writing coalesced, HBM-bound:
+//  * identity (the reference's default order: wavelength, Stokes, rows,
+//    columns): a flat byte swap, 16 bytes per thread and step;
+//  * wavelength contiguous in the input: one warp per output row (pixel, Stokes);
+//  * otherwise a 32 x 32 tile of (the input's contiguous axis, wavelength)
+//    through shared memory; every index inside a tile is a linear function of
+//    the tile's corner, so there is no division per element.
 struct Reorder {
   long long n[4];    // axis sizes
   long long st[4];   // element strides of the axes in the input
+  long long ost[4];  // element strides of the axes in the output
   int ax_row, ax_col, ax_l, ax_s;
   long long rows, nl, total;
 };
 
-__device__ __forceinline__ float swap_be(unsigned int u) { return __uint_as_float(__byte_perm(u, 0, 0x0123)); }
+__device__ __forceinline__ unsigned int swap32(unsigned int u) { return __byte_perm(u, 0, 0x0123); }
+__device__ __forceinline__ float swap_be(unsigned int u) { return __uint_as_float(swap32(u)); }
 
-__global__ void __launch_bounds__(256) reorder_direct(const Reorder R, const unsigned int* __restrict__ in,
-                                                     float* __restrict__ out) {
-  // wavelength is axis 0 of the input: walk the output linearly
+__global__ void __launch_bounds__(256) reorder_identity(const uint4* __restrict__ in, uint4* __restrict__ out,
+                                                       long long n4) {
   const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long o = (long long)blockIdx.x * blockDim.x + threadIdx.x; o < R.total; o += stride) {
-    const long long l = o % R.nl;
-    const long long ps = o / R.nl;
-    const long long s = ps & 3, pixel = ps >> 2;
-    const long long row = pixel % R.rows, col = pixel / R.rows;
-    const long long i = l + s * R.st[R.ax_s] + row * R.st[R.ax_row] + col * R.st[R.ax_col];
-    out[o] = swap_be(__ldg(in + i));
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride) {
+    uint4 v = __ldg(in + i);
+    v.x = swap32(v.x);
+    v.y = swap32(v.y);
+    v.z = swap32(v.z);
+    v.w = swap32(v.w);
+    out[i] = v;
   }
 }
 
-// Tiled form: axis f (stride 1 in the input, not wavelength) x wavelength.
-// blockIdx.x: tiles of (f, wavelength); blockIdx.y: the two remaining axes.
+__global__ void __launch_bounds__(256) reorder_rows(const Reorder R, const unsigned int* __restrict__ in,
+                                                   float* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const long long nrows_out = R.total / R.nl;
+  const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long r = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < nrows_out; r += nwarps) {
+    const long long s = r & 3, pixel = r >> 2;
+    const long long row = pixel % R.rows, col = pixel / R.rows;
+    const long long ib = s * R.st[R.ax_s] + row * R.st[R.ax_row] + col * R.st[R.ax_col];
+    for (long long l = lane; l < R.nl; l += 32) out[r * R.nl + l] = swap_be(__ldg(in + ib + l));
+  }
+}
+
+// blockIdx.x: tiles of (f, wavelength) x the two remaining axes g, h
 __global__ void __launch_bounds__(256) reorder_tiled(const Reorder R, int f, int g, int h,
                                                     const unsigned int* __restrict__ in, float* __restrict__ out) {
   __shared__ float tile[32][33];
   const long long tf = (R.n[f] + 31) / 32;
   const long long tl = (R.nl + 31) / 32;
   const long long ntile = tf * tl;
-  const long long gh = R.n[g] * R.n[h];
-  for (long long t = blockIdx.x; t < ntile * gh; t += gridDim.x) {
+  const long long total_tiles = ntile * R.n[g] * R.n[h];
+  const int x = threadIdx.x & 31;
+  const long long st_l = R.st[R.ax_l], ost_f = R.ost[f];
+  for (long long t = blockIdx.x; t < total_tiles; t += gridDim.x) {
     const long long tile_id = t % ntile, rest = t / ntile;
     const long long f0 = (tile_id % tf) * 32, l0 = (tile_id / tf) * 32;
-    const long long cg = rest % R.n[g], chh = rest / R.n[g];
-    const long long base = cg * R.st[g] + chh * R.st[h];
-    // load: threads along f (the input's contiguous axis)
-    for (int k = threadIdx.x >> 5; k < 32; k += blockDim.x >> 5) {
-      const long long fi = f0 + (threadIdx.x & 31), li = l0 + k;
-      float v = 0.f;
-      if (fi < R.n[f] && li < R.nl) v = swap_be(__ldg(in + base + fi + li * R.st[R.ax_l]));
-      tile[k][threadIdx.x & 31] = v;
-    }
+    const long long cg = rest % R.n[g], ch = rest / R.n[g];
+    const long long ib = cg * R.st[g] + ch * R.st[h] + f0 + l0 * st_l;
+    const long long ob = cg * R.ost[g] + ch * R.ost[h] + f0 * ost_f + l0;
+    const int fx = int(R.n[f] - f0 < 32 ? R.n[f] - f0 : 32), lx = int(R.nl - l0 < 32 ? R.nl - l0 : 32);
+    // load: lanes along f, the input's contiguous axis
+    for (int k = threadIdx.x >> 5; k < lx; k += blockDim.x >> 5)
+      if (x < fx) tile[k][x] = swap_be(__ldg(in + ib + x + k * st_l));
     __syncthreads();
-    // store: threads along wavelength (the output's contiguous axis)
-    for (int k = threadIdx.x >> 5; k < 32; k += blockDim.x >> 5) {
-      const long long fi = f0 + k, li = l0 + (threadIdx.x & 31);
-      if (fi < R.n[f] && li < R.nl) {
-        long long c[4];
-        c[f] = fi;
-        c[g] = cg;
-        c[h] = chh;
-        c[R.ax_l] = li;
-        const long long pixel = c[R.ax_col] * R.rows + c[R.ax_row];
-        out[(pixel * 4 + c[R.ax_s]) * R.nl + li] = tile[threadIdx.x & 31][k];
-      }
-    }
+    // store: lanes along wavelength, the output's contiguous axis
+    for (int k = threadIdx.x >> 5; k < fx; k += blockDim.x >> 5)
+      if (x < lx) out[ob + k * ost_f + x] = tile[x][k];
     __syncthreads();
   }
 }
@@ -235,17 +243,31 @@ extern "C" int pm_fits_reorder(const pm_fits_cube* info, const void* data_dev, f
   R.nl = info->nlambda;
   R.total = st;
   const int roles = (1 << R.ax_row) | (1 << R.ax_col) | (1 << R.ax_l) | (1 << R.ax_s);
-  if (roles != 15 || R.n[R.ax_s] != 4 || R.rows * info->ncols != info->npix || R.nl < 1)
+  if (roles != 15 || R.n[R.ax_s] != 4 || R.rows * info->ncols != info->npix || R.nl < 1 ||
+      R.n[R.ax_l] != R.nl || R.n[R.ax_row] != R.rows)
     return pmh_fail(PM_EINVAL, "pm_fits_reorder: inconsistent cube description");
+  R.ost[R.ax_l] = 1;
+  R.ost[R.ax_s] = R.nl;
+  R.ost[R.ax_row] = 4 * R.nl;
+  R.ost[R.ax_col] = 4 * R.nl * R.rows;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const auto* in = static_cast<const unsigned int*>(data_dev);
-  if (R.ax_l == 0) {
-    long long blocks = (R.total + 255) / 256;
-    if (blocks > (long long)sms * 16) blocks = (long long)sms * 16;
-    reorder_direct<<<unsigned(blocks), 256, 0, s>>>(R, in, cube_dev);
+  const long long cap = (long long)sms * 16;
+  bool identity = true;
+  for (int a = 0; a < 4; ++a) identity = identity && R.st[a] == R.ost[a];
+  const bool aligned = (reinterpret_cast<uintptr_t>(data_dev) % 16 == 0) &&
+                       (reinterpret_cast<uintptr_t>(cube_dev) % 16 == 0);
+  if (identity && aligned) {
+    const long long n4 = R.total / 4;  // the Stokes axis makes the element count a multiple of 4
+    const long long blocks = std::min(cap, (n4 + 255) / 256);
+    reorder_identity<<<unsigned(std::max(1LL, blocks)), 256, 0, s>>>(reinterpret_cast<const uint4*>(data_dev),
+                                                                   reinterpret_cast<uint4*>(cube_dev), n4);
+  } else if (R.ax_l == 0) {
+    const long long blocks = std::min(cap, (R.total / R.nl + 7) / 8);
+    reorder_rows<<<unsigned(std::max(1LL, blocks)), 256, 0, s>>>(R, in, cube_dev);
   } else {
     // f: the input's contiguous axis (axis 0); g, h: the two other non-wavelength axes
     const int f = 0;
@@ -256,8 +278,7 @@ extern "C" int pm_fits_reorder(const pm_fits_cube* info, const void* data_dev, f
         else h = a;
       }
     const long long work = ((R.n[f] + 31) / 32) * ((R.nl + 31) / 32) * R.n[g] * R.n[h];
-    long long blocks = work < (long long)sms * 16 ? work : (long long)sms * 16;
-    reorder_tiled<<<unsigned(blocks), 256, 0, s>>>(R, f, g, h, in, cube_dev);
+    reorder_tiled<<<unsigned(std::max(1LL, std::min(cap, work))), 256, 0, s>>>(R, f, g, h, in, cube_dev);
   }
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
