@@ -151,9 +151,10 @@ typedef struct pm_ctx pm_ctx;
 typedef struct pm_tuning {
   int variant;          /* FP32 register budget per thread: 0 = 168 (3 blocks of 4 warps per SM),
                            1 = 128 (4 blocks per SM, a few spills) */
-  int staging_depth;    /* host-buffer calls on grids of <= 32 wavelengths: the cube is copied in this
-                           many pieces while the inversion kernel already runs (1..PM_STAGING_MAX);
-                           0 = copy everything, then launch */
+  int staging_depth;    /* host-buffer calls on grids of <= 32 wavelengths: the cube goes in this many
+                           pieces, each inverted by its own launch while the next one is copied in
+                           and the previous one's results are copied out (1..PM_STAGING_MAX);
+                           0 = copy everything, then launch once */
   int warps_per_block;  /* pixels (one warp each) per block of the one-warp kernels: 1, 2 or 4 */
   int graphs;           /* 1: host-buffer calls of at most PM_GRAPH_MAX_PIXELS pixels on grids of <= 32
                            wavelengths (pm_lm_mils among them) stage through pinned memory and replay a
@@ -329,7 +330,7 @@ int pm_set_tuning(pm_ctx *ctx, const pm_tuning *in);
  * pm_invert_batch with PM_MEM_HOST, so copies and kernel are both timed) once per
  * candidate tuning and repetition, and keeps the fastest tuning in the context.
  * Candidates: variant {0, 1} x warps_per_block {1, 2, 4} x staging_depth
- * {0, 4, 16}.  *out (nullable) receives the choice.  No counterpart in the
+ * {0, 2, 4}.  *out (nullable) receives the choice.  No counterpart in the
  * reference. */
 int pm_autotune(pm_ctx *ctx, int64_t npix, const float *spectro, const float *slight, int slight_mode,
                 const pm_model *guess, int reps, pm_tuning *out);

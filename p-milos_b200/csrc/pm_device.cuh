@@ -1005,10 +1005,8 @@ __device__ __forceinline__ void classical_finish(const PmParams& P, const double
   if (isnan(m[6])) m[6] = 1;
 }
 
-// Classical estimates of a one-warp pixel (lane = wavelength).  Out of line: it
-// runs once per pixel, and keeping it out of the LM loop's code keeps that code
-// compact in the instruction cache.
-__device__ __noinline__ void classical(const PmParams& P, const float O[4], int lane, bool valid, double* m) {
+// Classical estimates of a one-warp pixel (lane = wavelength).
+__device__ __forceinline__ void classical(const PmParams& P, const float O[4], int lane, bool valid, double* m) {
   const int nl = P.nl;
   const unsigned neg = __ballot_sync(kFull, valid && O[0] < 0.0f);
   const unsigned validm = (nl >= 32) ? kFull : ((1u << nl) - 1u);

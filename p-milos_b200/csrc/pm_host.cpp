@@ -65,11 +65,13 @@ struct DevBuf {
 
 // Pinned host words the streamed calls copy from and read back into.
 struct HostCtl {
-  unsigned long long avail[PM_STAGING_MAX];  // published ticket counts, one per piece
   unsigned long long one;                    // 1: the value of PmStreamQ::closed
   PmJob job;
   PmStreamQ qinit;                           // queue state before a fully published launch
   PmStreamQ qread;                           // queue state after the kernel (counters, err)
+  PmJob piece_job[PM_STAGING_MAX];           // pipelined host-buffer calls: one launch per piece
+  PmStreamQ piece_qinit[PM_STAGING_MAX];
+  PmStreamQ piece_qread[PM_STAGING_MAX];
 };
 
 // A captured CUDA graph of a whole small host-buffer call (uploads from pinned
@@ -111,6 +113,7 @@ struct pm_ctx {
   cudaStream_t s_kern = nullptr, s_copy = nullptr;
   cudaEvent_t ev_start = nullptr, ev_q = nullptr, ev_done = nullptr, t0 = nullptr, t1 = nullptr, k0 = nullptr,
               k1 = nullptr;
+  cudaEvent_t ev_piece[PM_STAGING_MAX] = {};  // a piece of a pipelined call is on the device
   DevBuf q, jobs;
   HostCtl* hc = nullptr;
   PmGridSet* gs = nullptr;  // kernel parameters of the streamed kernel (the context's one grid)
@@ -419,6 +422,8 @@ extern "C" int pm_ctx_destroy(pm_ctx* c) {
     b->release();
   for (cudaEvent_t ev : {c->ev_start, c->ev_q, c->ev_done, c->t0, c->t1, c->k0, c->k1})
     if (ev) cudaEventDestroy(ev);
+  for (cudaEvent_t ev : c->ev_piece)
+    if (ev) cudaEventDestroy(ev);
   if (c->s_kern) cudaStreamDestroy(c->s_kern);
   if (c->s_copy) cudaStreamDestroy(c->s_copy);
   if (c->hc) cudaFreeHost(c->hc);
@@ -440,6 +445,7 @@ int stream_resources(pm_ctx* c) {
   for (cudaEvent_t* ev : {&c->ev_start, &c->ev_q, &c->ev_done})
     PM_CUDA(cudaEventCreateWithFlags(ev, cudaEventDisableTiming), "event create");
   for (cudaEvent_t* ev : {&c->t0, &c->t1, &c->k0, &c->k1}) PM_CUDA(cudaEventCreate(ev), "event create");
+  for (cudaEvent_t& ev : c->ev_piece) PM_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event create");
   int rc = c->q.ensure(sizeof(PmStreamQ));
   if (rc == PM_OK) rc = c->jobs.ensure(sizeof(PmJob));
   if (rc != PM_OK) return rc;
@@ -453,11 +459,13 @@ int stream_resources(pm_ctx* c) {
   return PM_OK;
 }
 
-// One resident chunk of a host-buffer inversion, streamed: the persistent
-// kernel starts at once and inverts the pixels of each piece as soon as the
-// copy engine has brought it in (pieces are published through the ticket
-// queue); the results come back after the kernel.  Pieces hold a multiple of
-// 32 pixels, so no 128-byte line of the cube spans two pieces.
+// One resident chunk of a host-buffer inversion, pipelined in `staging_depth`
+// pieces (multiples of 32 pixels, so no 128-byte line of the cube spans two):
+// the copy stream brings piece k + 1 in while the kernel stream inverts piece k
+// (classical pre-pass, then the streamed kernel with the piece fully published)
+// and copies piece k's results back.  Each piece is its own launch because a
+// pre-pass cannot run beside a persistent kernel that holds the SMs, and making
+// the estimates inside the LM kernel costs more than the copies this hides.
 int run_streamed(pm_ctx* c, int64_t n, const float* spectro, const float* slight, int slight_mode,
                  pm_model* models_out, float* chisq_out, int* iters_out, float* best_fit_out, int* status_out,
                  float* kernel_ms, float* total_ms) {
@@ -466,30 +474,7 @@ int run_streamed(pm_ctx* c, int64_t n, const float* spectro, const float* slight
   const int nl = c->P.nl;
   const size_t prof = sizeof(float) * 4 * nl;
   HostCtl* hc = c->hc;
-  PmJob& job = hc->job;
-  std::memset(&job, 0, sizeof job);
-  job.t0 = 0;
-  job.npix = n;
-  job.grid = 0;
-  job.spectro = static_cast<const float*>(c->spectro.p);
-  job.slight = slight_mode == PM_SLIGHT_PER_PIXEL ? static_cast<const float*>(c->slight.p) : nullptr;
-  job.models = static_cast<double*>(c->models.p);
-  job.chisq = static_cast<float*>(c->chisq.p);
-  job.iters = static_cast<int*>(c->iters.p);
-  job.status = status_out ? static_cast<int*>(c->status.p) : nullptr;
-  job.spectra = best_fit_out ? static_cast<float*>(c->spectra.p) : nullptr;
   PmStreamQ* q = static_cast<PmStreamQ*>(c->q.p);
-
-  // order after the caller's earlier work on its stream
-  PM_CUDA(cudaEventRecord(c->ev_start, c->stream), "event");
-  PM_CUDA(cudaStreamWaitEvent(c->s_copy, c->ev_start, 0), "wait");
-  PM_CUDA(cudaStreamWaitEvent(c->s_kern, c->ev_start, 0), "wait");
-  PM_CUDA(cudaEventRecord(c->t0, c->s_copy), "event");
-  PM_CUDA(cudaMemsetAsync(q, 0, sizeof(PmStreamQ), c->s_copy), "queue reset");
-  PM_CUDA(cudaMemcpyAsync(c->jobs.p, &job, sizeof(PmJob), cudaMemcpyHostToDevice, c->s_copy), "job H2D");
-  PM_CUDA(cudaEventRecord(c->ev_q, c->s_copy), "event");
-  PM_CUDA(cudaStreamWaitEvent(c->s_kern, c->ev_q, 0), "wait");
-
   c->gs->ngrids = 1;
   c->gs->g[0] = c->P;
   PmStreamIO sio{};
@@ -497,67 +482,90 @@ int run_streamed(pm_ctx* c, int64_t n, const float* spectro, const float* slight
   sio.jobs = static_cast<const PmJob*>(c->jobs.p);
   sio.jobs_cap = 1;
   sio.first_job = 0;
-  sio.wait_limit_ns = 20000000000LL;  // 20 s without a published piece: give up (PMQ_ERR_WAIT)
-  PM_CUDA(cudaEventRecord(c->k0, c->s_kern), "event");
-  rc = pmk_invert_stream(*c->gs, sio, c->precision, c->tuning.variant, c->tuning.warps_per_block, false, c->s_kern,
-                         c->num_sms, nullptr);
-  if (rc != PM_OK) {
-    cudaStreamSynchronize(c->s_copy);
-    return fail(rc, "%s", pmk_last_cuda_error());
-  }
-  PM_CUDA(cudaEventRecord(c->k1, c->s_kern), "event");
+  sio.wait_limit_ns = 20000000000LL;
 
   const int pieces = std::max(1, std::min(c->tuning.staging_depth, PM_STAGING_MAX));
   int64_t per = (n + pieces - 1) / pieces;
   per = std::max<int64_t>(32, (per + 31) / 32 * 32);
-  int i = 0;
-  cudaError_t ce = cudaSuccess;
-  for (int64_t p0 = 0; p0 < n && ce == cudaSuccess; p0 += per, ++i) {
-    const int64_t m = std::min(per, n - p0);
-    ce = cudaMemcpyAsync(static_cast<char*>(c->spectro.p) + prof * p0, spectro + p0 * 4 * nl, prof * m,
-                         cudaMemcpyHostToDevice, c->s_copy);
-    if (ce == cudaSuccess && slight_mode == PM_SLIGHT_PER_PIXEL)
-      ce = cudaMemcpyAsync(static_cast<char*>(c->slight.p) + prof * p0, slight + p0 * 4 * nl, prof * m,
-                           cudaMemcpyHostToDevice, c->s_copy);
-    hc->avail[i] = (unsigned long long)(p0 + m);
-    if (ce == cudaSuccess)
-      ce = cudaMemcpyAsync(&q->avail, &hc->avail[i], sizeof(unsigned long long), cudaMemcpyHostToDevice,
-                           c->s_copy);
+  const int np = int((n + per - 1) / per);
+
+  // order after the caller's earlier work on its stream
+  PM_CUDA(cudaEventRecord(c->ev_start, c->stream), "event");
+  PM_CUDA(cudaStreamWaitEvent(c->s_copy, c->ev_start, 0), "wait");
+  PM_CUDA(cudaStreamWaitEvent(c->s_kern, c->ev_start, 0), "wait");
+  PM_CUDA(cudaEventRecord(c->t0, c->s_copy), "event");
+  for (int i = 0; i < np; ++i) {
+    const int64_t p0 = i * per, m = std::min(per, n - p0);
+    PM_CUDA(cudaMemcpyAsync(static_cast<char*>(c->spectro.p) + prof * p0, spectro + p0 * 4 * nl, prof * m,
+                            cudaMemcpyHostToDevice, c->s_copy),
+            "spectro H2D");
+    if (slight_mode == PM_SLIGHT_PER_PIXEL)
+      PM_CUDA(cudaMemcpyAsync(static_cast<char*>(c->slight.p) + prof * p0, slight + p0 * 4 * nl, prof * m,
+                              cudaMemcpyHostToDevice, c->s_copy),
+              "slight H2D");
+    PM_CUDA(cudaEventRecord(c->ev_piece[i], c->s_copy), "event");
   }
-  // closed after the last piece (and after a failed copy, so that the kernel ends)
-  const cudaError_t ce2 = cudaMemcpyAsync(&q->closed, &hc->one, sizeof(unsigned long long), cudaMemcpyHostToDevice,
-                                          c->s_copy);
-  if (ce != cudaSuccess || ce2 != cudaSuccess) {
-    cudaStreamSynchronize(c->s_kern);
-    return cuda_fail(ce != cudaSuccess ? ce : ce2, "streamed H2D");
+  for (int i = 0; i < np; ++i) {
+    const int64_t p0 = i * per, m = std::min(per, n - p0);
+    PmJob& job = hc->piece_job[i];
+    std::memset(&job, 0, sizeof job);
+    job.npix = m;
+    job.spectro = static_cast<const float*>(c->spectro.p) + p0 * 4 * nl;
+    job.slight = slight_mode == PM_SLIGHT_PER_PIXEL ? static_cast<const float*>(c->slight.p) + p0 * 4 * nl : nullptr;
+    job.models = static_cast<double*>(c->models.p) + p0 * 11;
+    job.chisq = static_cast<float*>(c->chisq.p) + p0;
+    job.iters = static_cast<int*>(c->iters.p) + p0;
+    job.status = status_out ? static_cast<int*>(c->status.p) + p0 : nullptr;
+    job.spectra = best_fit_out ? static_cast<float*>(c->spectra.p) + p0 * 4 * nl : nullptr;
+    job.model_in = c->P.classical ? job.models : nullptr;  // written by the pre-pass below
+    std::memset(&hc->piece_qinit[i], 0, sizeof(PmStreamQ));
+    hc->piece_qinit[i].avail = (unsigned long long)m;
+    hc->piece_qinit[i].closed = 1;
+    PM_CUDA(cudaStreamWaitEvent(c->s_kern, c->ev_piece[i], 0), "wait");
+    PM_CUDA(cudaMemcpyAsync(c->jobs.p, &job, sizeof job, cudaMemcpyHostToDevice, c->s_kern), "job H2D");
+    PM_CUDA(cudaMemcpyAsync(q, &hc->piece_qinit[i], sizeof(PmStreamQ), cudaMemcpyHostToDevice, c->s_kern),
+            "queue H2D");
+    if (i == 0) PM_CUDA(cudaEventRecord(c->k0, c->s_kern), "event");
+    if (c->P.classical) {
+      rc = pmk_classical_prepass(c->P, job.spectro, job.models, m, c->s_kern, c->num_sms);
+      if (rc != PM_OK) return fail(rc, "%s", pmk_last_cuda_error());
+    }
+    rc = pmk_invert_stream(*c->gs, sio, c->precision, c->tuning.variant, c->tuning.warps_per_block, false, c->s_kern,
+                           c->num_sms, nullptr);
+    if (rc != PM_OK) return fail(rc, "%s", pmk_last_cuda_error());
+    if (i == np - 1) PM_CUDA(cudaEventRecord(c->k1, c->s_kern), "event");
+    PM_CUDA(cudaMemcpyAsync(models_out + p0, job.models, sizeof(pm_model) * m, cudaMemcpyDeviceToHost, c->s_kern),
+            "models D2H");
+    PM_CUDA(cudaMemcpyAsync(chisq_out + p0, job.chisq, sizeof(float) * m, cudaMemcpyDeviceToHost, c->s_kern),
+            "chisq D2H");
+    PM_CUDA(cudaMemcpyAsync(iters_out + p0, job.iters, sizeof(int) * m, cudaMemcpyDeviceToHost, c->s_kern),
+            "iters D2H");
+    if (best_fit_out)
+      PM_CUDA(cudaMemcpyAsync(best_fit_out + p0 * 4 * nl, job.spectra, prof * m, cudaMemcpyDeviceToHost, c->s_kern),
+              "best fit D2H");
+    if (status_out)
+      PM_CUDA(cudaMemcpyAsync(status_out + p0, job.status, sizeof(int) * m, cudaMemcpyDeviceToHost, c->s_kern),
+              "status D2H");
+    PM_CUDA(cudaMemcpyAsync(&hc->piece_qread[i], q, sizeof(PmStreamQ), cudaMemcpyDeviceToHost, c->s_kern),
+            "queue D2H");
   }
-  PM_CUDA(cudaMemcpyAsync(models_out, c->models.p, sizeof(pm_model) * n, cudaMemcpyDeviceToHost, c->s_kern),
-          "models D2H");
-  PM_CUDA(cudaMemcpyAsync(chisq_out, c->chisq.p, sizeof(float) * n, cudaMemcpyDeviceToHost, c->s_kern), "chisq D2H");
-  PM_CUDA(cudaMemcpyAsync(iters_out, c->iters.p, sizeof(int) * n, cudaMemcpyDeviceToHost, c->s_kern), "iters D2H");
-  if (best_fit_out)
-    PM_CUDA(cudaMemcpyAsync(best_fit_out, c->spectra.p, prof * n, cudaMemcpyDeviceToHost, c->s_kern),
-            "best fit D2H");
-  if (status_out)
-    PM_CUDA(cudaMemcpyAsync(status_out, c->status.p, sizeof(int) * n, cudaMemcpyDeviceToHost, c->s_kern),
-            "status D2H");
-  PM_CUDA(cudaMemcpyAsync(&hc->qread, q, sizeof(PmStreamQ), cudaMemcpyDeviceToHost, c->s_kern), "queue D2H");
   PM_CUDA(cudaEventRecord(c->t1, c->s_kern), "event");
   PM_CUDA(cudaEventRecord(c->ev_done, c->s_kern), "event");
   PM_CUDA(cudaStreamWaitEvent(c->stream, c->ev_done, 0), "wait");
-  PM_CUDA(cudaEventSynchronize(c->t1), "streamed inversion");
-  PM_CUDA(cudaStreamSynchronize(c->s_copy), "streamed H2D");
-  if (hc->qread.err)
-    return fail(PM_EIO, "streamed inversion: %s", hc->qread.err == PMQ_ERR_WAIT ? "a piece never arrived (wait limit)"
-                                                                                : "ticket without a job");
-  if (hc->qread.next < (unsigned long long)n)
-    return fail(PM_EIO, "streamed inversion: %llu of %lld pixels handed out", hc->qread.next, (long long)n);
+  PM_CUDA(cudaEventSynchronize(c->t1), "pipelined inversion");
+  for (int i = 0; i < np; ++i) {
+    const PmStreamQ& r = hc->piece_qread[i];
+    const int64_t m = std::min(per, n - int64_t(i) * per);
+    if (r.err || r.next < (unsigned long long)m)
+      return fail(PM_EIO, "pipelined inversion, piece %d: queue error %llu, %llu of %lld pixels handed out", i, r.err,
+                  r.next, (long long)m);
+    c->stats.iterations += int64_t(r.ctr[PMC_ITERS]);
+    c->stats.accepted += int64_t(r.ctr[PMC_ACCEPTED]);
+    c->stats.eigen_fallbacks += int64_t(r.ctr[PMC_FALLBACK]);
+  }
   cudaEventElapsedTime(kernel_ms, c->k0, c->k1);
   cudaEventElapsedTime(total_ms, c->t0, c->t1);
   c->stats.pixels += n;
-  c->stats.iterations += int64_t(hc->qread.ctr[PMC_ITERS]);
-  c->stats.accepted += int64_t(hc->qread.ctr[PMC_ACCEPTED]);
-  c->stats.eigen_fallbacks += int64_t(hc->qread.ctr[PMC_FALLBACK]);
   return PM_OK;
 }
 
@@ -981,7 +989,7 @@ extern "C" int pm_autotune(pm_ctx* c, int64_t npix, const float* spectro, const 
   for (int variant : {0, 1}) {
     if (!fp32 && variant != c->tuning.variant) continue;  // the FP64 kernel has one register budget
     for (int wpb : {1, 2, 4})
-      for (int depth : {0, 4, 16}) {
+      for (int depth : {0, 2, 4}) {
         if (c->P.G != 1 && depth != 0) continue;  // multi-warp grids are not streamed
         cands.push_back(pm_tuning{variant, depth, wpb, c->tuning.graphs});
       }

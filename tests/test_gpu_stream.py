@@ -1,13 +1,13 @@
-"""Streamed host-buffer inversion and the launch tunings.
+"""Host-buffer pipelining, the launch tunings and graph replay.
 
-Every one-warp inversion runs the streamed kernel: device-buffer calls publish
-all pixels before the launch; host-buffer calls launch first and publish the
-cube piece by piece as the copy engine brings it in (pm_tuning.staging_depth
-pieces).  Staging depth and pixels per block do not change the compiled code,
-so results are bit-identical across them and equal to the device-buffer call.
-The two register budgets (pm_tuning.variant) are separately compiled kernels
-whose floating-point contractions may differ in the last bits: between them the
-stated FP32 tolerance applies.
+Every one-warp inversion runs the streamed kernel.  Device-buffer calls publish
+all pixels before one launch; host-buffer calls split the cube into
+pm_tuning.staging_depth pieces, each inverted by its own launch while the next
+one is copied in.  Staging depth and pixels per block do not change the compiled
+code, so results are bit-identical across them and equal to the device-buffer
+call.  The two register budgets (pm_tuning.variant) are separately compiled
+kernels whose floating-point contractions may differ in the last bits: between
+them the stated FP32 tolerance applies.
 """
 import numpy as np
 import pytest
@@ -74,7 +74,7 @@ def test_autotune_picks_a_valid_tuning_and_keeps_results():
         ref = inv.invert(c["obs"], c["guess"])
         t = inv.autotune(np.tile(c["obs"], (64, 1, 1)), c["guess"], reps=1)
         assert t == inv.tuning
-        assert t["variant"] in (0, 1) and t["warps_per_block"] in (1, 2, 4) and t["staging_depth"] in (0, 4, 16)
+        assert t["variant"] in (0, 1) and t["warps_per_block"] in (1, 2, 4) and t["staging_depth"] in (0, 2, 4)
         _same(inv.invert(c["obs"], c["guess"]), ref)
 
 
