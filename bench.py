@@ -173,6 +173,81 @@ def host_cores() -> int:
         return os.cpu_count() or 1
 
 
+# ---- cube ingest ----
+def bench_ingest(args, rank: int):
+    """pm_fits_reorder on a 512 x 512 x 4 x 112 float32 cube (470 MB) written in
+    three axis orders; bytes/s = 2 x data block (read + write) per launch."""
+    import ctypes
+
+    import torch
+
+    import pmilos_b200 as pm
+    from pmilos_b200.files import cube_fits_bytes
+
+    size = {"R": 512, "C": 512, "L": 112, "S": 4}
+    role = {"R": "HPLN-TAN", "C": "HPLT-TAN", "L": "WAVE-GRI", "S": "STOKES"}
+    L = pm.load_library()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    hbm_peak = json.load(open(peaks_path))["hbm_gbs"] if os.path.exists(peaks_path) else 6650.0
+    rows = {}
+    e2e = None
+    for order in ("LSRC", "LRSC", "RCLS"):
+        dims = [size[r] for r in order]
+        data = np.random.default_rng(1).standard_normal(dims[::-1], dtype=np.float32)
+        raw = cube_fits_bytes(data, [role[r] for r in order])
+        info = pm._fits_struct(np.frombuffer(raw, dtype=np.uint8))
+        o, n = int(info.data_offset), int(info.data_bytes)
+        host = torch.from_numpy(np.frombuffer(raw, dtype=np.uint8)[o:o + n].copy()).pin_memory()
+        dev = host.to("cuda")
+        out = torch.empty((int(info.npix), 4, int(info.nlambda)), dtype=torch.float32, device="cuda")
+        st = torch.cuda.current_stream().cuda_stream
+
+        def launch():
+            rc = L.pm_fits_reorder(ctypes.byref(info), dev.data_ptr(), out.data_ptr(), ctypes.c_void_p(st))
+            if rc != 0:
+                raise RuntimeError(L.pm_last_error().decode())
+
+        for _ in range(max(3, args.warmup)):
+            launch()
+        ts, te = [], []
+        for _ in range(args.steps):
+            flush.fill_(1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            launch()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+            # end to end: the data block from pinned host memory, then the reorder
+            e0.record()
+            dev.copy_(host, non_blocking=True)
+            launch()
+            e1.record()
+            torch.cuda.synchronize()
+            te.append(e0.elapsed_time(e1))
+        ms, ms_e2e = float(np.median(ts)), float(np.median(te))
+        rows[order] = {"ms": ms, "gbs": 2 * n / ms / 1e6, "frac": 2 * n / ms / 1e6 / hbm_peak,
+                       "e2e_ms": ms_e2e, "bytes_per_launch": 2 * n}
+        if order == "LSRC":
+            e2e = n / ms_e2e / 1e6
+    v = rows["LSRC"]
+    if rank == 0:
+        print(json.dumps({
+            "metric": "FITS cube ingest (byte swap + reorder) on 1 B200", "value": v["gbs"], "unit": "GB/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": v["ms"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": "512 x 512 pixels x 4 Stokes x 112 wavelengths float32 (470 MB), axis orders "
+                                   "(wavelength, Stokes, rows, columns) = the reference's default, "
+                                   "(wavelength, rows, Stokes, columns), (rows, columns, wavelength, Stokes)",
+                       "l2": "flushed between timed launches (256 MiB write)"},
+            "e2e": {"value": e2e, "unit": "GB/s of data block", "h2d_bytes_per_step": rows["LSRC"]["bytes_per_launch"] // 2,
+                    "d2h_bytes_per_step": 0},
+            "roofline": {"bound": "hbm", "achieved": v["gbs"], "peak": hbm_peak, "unit": "GB/s", "frac": v["frac"],
+                         "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs"},
+            "orders": rows, "gpu_launches": len(rows) * (args.steps * 2 + max(3, args.warmup))}), flush=True)
+
+
 # ---- served stream (configuration 3) ----
 SIZES = (256 * 256, 512 * 512, 1024 * 1024, 2048 * 2048)
 
@@ -284,6 +359,8 @@ def main():
                     help="served stream: scans of the same schedule timed on the plain FP64 server")
     ap.add_argument("--budget-gb", type=float, default=24.0, help="served stream: device arena of the server")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch tuning")
+    ap.add_argument("--ingest", action="store_true",
+                    help="time the FITS cube ingest (512x512 pixels x 112 wavelengths, three axis orders)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -335,6 +412,8 @@ def main():
         return
 
     torch.cuda.set_device(local)
+    if args.ingest:
+        return bench_ingest(args, rank)
     if args.config == 3:
         return bench_served(args, rank, world, metric)
     dist = None
@@ -449,10 +528,12 @@ def main():
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     hbm_peak = json.load(open(peaks_path))["hbm_gbs"] if os.path.exists(peaks_path) else 6650.0
     hbm_bytes = w.npix * args.steps * (16 * w.nl + 11 * 8 + 8)
-    # DRAM bytes per pixel of the FP32 inversion kernel from one ncu capture
-    # (profiles/invert_kernel_fp32_config1.md: 80.2 MB for 131,072 pixels of the
-    # configuration-1 workload), scaled to this launch by its pixel count
-    traffic = 612.0 * w.npix if (args.config == 1 and w.nl == 30) else None
+    # DRAM bytes per pixel of the FP32 inversion kernel from one ncu capture of a
+    # smaller cube of the same workload, scaled to this launch by its pixel count:
+    # profiles/invert_stream_kernel_fp32_config1.md (351.5 MB for 524,288 pixels)
+    # and profiles/invert_wide_kernel_fp32_config4.md (132.7 MB for 65,536 pixels)
+    traffic = {1: 670.4, 4: 2025.0}.get(args.config) if w.nl in (30, 112) else None
+    traffic = traffic * w.npix if traffic else None
     roofline = {"bound": "fp32", "achieved": round(achieved, 3), "peak": round(peak_fp32, 2), "unit": "TFLOP/s",
                 "frac": round(achieved / peak_fp32, 4), "traffic": traffic,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per pixel, scaled",

@@ -76,9 +76,10 @@ bool card_string(const char* card, char* out, size_t cap) {
 //  * identity (the reference's default order: wavelength, Stokes, rows,
 //    columns): a flat byte swap, 16 bytes per thread and step;
 //  * wavelength contiguous in the input: one warp per output row (pixel, Stokes);
-//  * otherwise a 32 x 32 tile of (the input's contiguous axis, wavelength)
+//  * otherwise 32 x 32 tiles of (the input's contiguous axis, wavelength)
 //    through shared memory; every index inside a tile is a linear function of
-//    the tile's corner, so there is no division per element.
+//    the tile's corner, and consecutive tiles of a block differ by constant
+//    offsets, so there is no division per element or per tile.
 struct Reorder {
   long long n[4];    // axis sizes
   long long st[4];   // element strides of the axes in the input
@@ -116,31 +117,33 @@ __global__ void __launch_bounds__(256) reorder_rows(const Reorder R, const unsig
   }
 }
 
-// blockIdx.x: tiles of (f, wavelength) x the two remaining axes g, h
+// Work item = (wavelength tile, g, h); a block walks the item's tiles along f in
+// order, so the only per-tile index arithmetic is two additions.
 __global__ void __launch_bounds__(256) reorder_tiled(const Reorder R, int f, int g, int h,
                                                     const unsigned int* __restrict__ in, float* __restrict__ out) {
   __shared__ float tile[32][33];
-  const long long tf = (R.n[f] + 31) / 32;
   const long long tl = (R.nl + 31) / 32;
-  const long long ntile = tf * tl;
-  const long long total_tiles = ntile * R.n[g] * R.n[h];
+  const long long items = tl * R.n[g] * R.n[h];
   const int x = threadIdx.x & 31;
-  const long long st_l = R.st[R.ax_l], ost_f = R.ost[f];
-  for (long long t = blockIdx.x; t < total_tiles; t += gridDim.x) {
-    const long long tile_id = t % ntile, rest = t / ntile;
-    const long long f0 = (tile_id % tf) * 32, l0 = (tile_id / tf) * 32;
+  const long long st_l = R.st[R.ax_l], ost_f = R.ost[f], nf = R.n[f];
+  for (long long it = blockIdx.x; it < items; it += gridDim.x) {
+    const long long lt = it % tl, rest = it / tl;
     const long long cg = rest % R.n[g], ch = rest / R.n[g];
-    const long long ib = cg * R.st[g] + ch * R.st[h] + f0 + l0 * st_l;
-    const long long ob = cg * R.ost[g] + ch * R.ost[h] + f0 * ost_f + l0;
-    const int fx = int(R.n[f] - f0 < 32 ? R.n[f] - f0 : 32), lx = int(R.nl - l0 < 32 ? R.nl - l0 : 32);
-    // load: lanes along f, the input's contiguous axis
-    for (int k = threadIdx.x >> 5; k < lx; k += blockDim.x >> 5)
-      if (x < fx) tile[k][x] = swap_be(__ldg(in + ib + x + k * st_l));
-    __syncthreads();
-    // store: lanes along wavelength, the output's contiguous axis
-    for (int k = threadIdx.x >> 5; k < fx; k += blockDim.x >> 5)
-      if (x < lx) out[ob + k * ost_f + x] = tile[x][k];
-    __syncthreads();
+    const long long l0 = lt * 32;
+    const int lx = int(R.nl - l0 < 32 ? R.nl - l0 : 32);
+    long long ib = cg * R.st[g] + ch * R.st[h] + l0 * st_l;
+    long long ob = cg * R.ost[g] + ch * R.ost[h] + l0;
+    for (long long f0 = 0; f0 < nf; f0 += 32, ib += 32, ob += 32 * ost_f) {
+      const int fx = int(nf - f0 < 32 ? nf - f0 : 32);
+      // load: lanes along f, the input's contiguous axis
+      for (int k = threadIdx.x >> 5; k < lx; k += blockDim.x >> 5)
+        if (x < fx) tile[k][x] = swap_be(__ldg(in + ib + x + k * st_l));
+      __syncthreads();
+      // store: lanes along wavelength, the output's contiguous axis
+      for (int k = threadIdx.x >> 5; k < fx; k += blockDim.x >> 5)
+        if (x < lx) out[ob + k * ost_f + x] = tile[x][k];
+      __syncthreads();
+    }
   }
 }
 
@@ -277,7 +280,7 @@ extern "C" int pm_fits_reorder(const pm_fits_cube* info, const void* data_dev, f
         if (g < 0) g = a;
         else h = a;
       }
-    const long long work = ((R.n[f] + 31) / 32) * ((R.nl + 31) / 32) * R.n[g] * R.n[h];
+    const long long work = ((R.nl + 31) / 32) * R.n[g] * R.n[h];
     reorder_tiled<<<unsigned(std::max(1LL, std::min(cap, work))), 256, 0, s>>>(R, f, g, h, in, cube_dev);
   }
   const cudaError_t e = cudaGetLastError();

@@ -181,3 +181,21 @@ def read_trol_file(path: str) -> dict:
         cfg["psf_file"] = None
         cfg["psf_fwhm"] = fw if fw != 0 and not math.isnan(fw) else None
     return cfg
+
+
+def cube_fits_bytes(data: np.ndarray, ctypes_: list | None = None) -> bytes:
+    """A spectro cube as a FITS file (primary HDU, BITPIX = -32, big-endian):
+    ``data`` is a float32 array of numpy shape (NAXIS4, NAXIS3, NAXIS2, NAXIS1);
+    ``ctypes_`` gives CTYPE1..4 ('WAVE-GRI', 'STOKES', 'HPLN-TAN', 'HPLT-TAN' in
+    the reference's default order), or None for a header without them."""
+    dims = list(data.shape[::-1])
+    cards = ["SIMPLE  =                    T", "BITPIX  =                  -32", f"NAXIS   = {len(dims):20d}"]
+    cards += [f"NAXIS{i + 1}  = {d:20d}" for i, d in enumerate(dims)]
+    if ctypes_:
+        cards += [f"CTYPE{i + 1}  = '{c:<8s}'" for i, c in enumerate(ctypes_)]
+    cards.append("END")
+    hdr = "".join(c.ljust(80) for c in cards).encode("ascii")
+    hdr += b" " * (-len(hdr) % 2880)
+    body = np.ascontiguousarray(data, dtype=">f4").tobytes()
+    body += b"\0" * (-len(body) % 2880)
+    return hdr + body
