@@ -312,7 +312,8 @@ def bench_served(args, rank: int, world: int, metric: str):
         return {"pixels_per_s": pix / ((last - first) / 1000.0), "pixels": int(pix), "scans": len(infos),
                 "wall_ms": last - first, "latency_p50_ms": float(np.percentile(lat, 50)),
                 "latency_p99_ms": float(np.percentile(lat, 99)), "latency_max_ms": float(lat.max()),
-                "kernel_launches": st["kernel_launches"], "arena_peak_gib": st["arena_peak_bytes"] / 2**30,
+                "kernel_launches": st["kernel_launches"], "prepass_launches": st["prepass_launches"],
+                "arena_peak_gib": st["arena_peak_bytes"] / 2**30,
                 "iterations_per_pixel": its / pix}
 
     with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
@@ -336,7 +337,7 @@ def bench_served(args, rank: int, world: int, metric: str):
             "latency_ms": {"p50": fp32["latency_p50_ms"], "p99": fp32["latency_p99_ms"],
                            "max": fp32["latency_max_ms"]},
             "served_fp32": fp32, "plain_fp64": plain, "clocks": clk.summary(),
-            "gpu_launches": fp32["kernel_launches"]}), flush=True)
+            "gpu_launches": fp32["kernel_launches"] + fp32["prepass_launches"]}), flush=True)
 
 
 # ---- main ----

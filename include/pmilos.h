@@ -299,6 +299,7 @@ typedef struct pm_server_stats {
   double latency_p50_ms, latency_p99_ms, latency_max_ms;  /* submit -> results in host memory */
   double busy_ms;           /* first submit -> last completion */
   size_t arena_peak_bytes;
+  int64_t prepass_launches; /* classical pre-pass launches, one per admitted scan on a grid with classical estimates */
 } pm_server_stats;
 
 /* grids[g], guesses[g]: the settings and initial model of grid g (g < ngrids). */

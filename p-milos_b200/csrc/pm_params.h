@@ -128,8 +128,11 @@ int pmk_classical_prepass(const PmParams& P, const float* spectro, double* model
                           int num_sms);
 // Streamed inversion: every grid of GS has the same nterms and nl <= 32.
 // multi: grids differ between jobs (dynamic grid index) rather than one grid.
+// reserve_blocks: launch that many fewer blocks than fit, leaving room on the
+// SMs for short kernels (the classical pre-pass of newly admitted scans) to run
+// beside the persistent kernel.
 int pmk_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, int precision, int variant, int warps_per_block,
-                      bool multi, void* stream, int num_sms, size_t* smem_out);
+                      bool multi, void* stream, int num_sms, size_t* smem_out, int reserve_blocks = 0);
 const char* pmk_last_cuda_error();
 
 // Host helpers (pm_host.cpp) shared with pm_noalloc.cu.

@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(256) classical_prepass_kernel(const __grid_con
 
 template <typename R, int KT, int MINB, bool MULTI>
 int launch_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, cudaStream_t st, int num_sms,
-                         size_t* smem_out, int wpb) {
+                         size_t* smem_out, int wpb, int reserve) {
   const int threads = 32 * wpb;
   const size_t smem = (MULTI ? PMK_MAX_GRIDS : 1) * sizeof(BlockSmem<R>) + sizeof(WarpSmem<R>) * (threads / 32);
   if (smem_out) *smem_out = smem;
@@ -174,7 +174,8 @@ int launch_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, cudaStream_
   int per_sm = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
   if (e != cudaSuccess || per_sm < 1) return snprintf(pmk_g_err, sizeof pmk_g_err, "occupancy: %s", cudaGetErrorString(e)), PM_EIO;
-  kern<<<unsigned(per_sm * num_sms), threads, smem, st>>>(gp, sio);
+  const int blocks = per_sm * num_sms - reserve > 1 ? per_sm * num_sms - reserve : 1;
+  kern<<<unsigned(blocks), threads, smem, st>>>(gp, sio);
   e = cudaGetLastError();
   if (e != cudaSuccess) return snprintf(pmk_g_err, sizeof pmk_g_err, "stream launch: %s", cudaGetErrorString(e)), PM_EIO;
   return PM_OK;
@@ -182,14 +183,14 @@ int launch_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, cudaStream_
 
 template <typename R, int KT>
 int launch_stream_any(const PmGridSet& GS, const PmStreamIO& sio, cudaStream_t st, int num_sms, int variant,
-                      int wpb, bool multi, size_t* smem_out) {
+                      int wpb, bool multi, size_t* smem_out, int reserve) {
   if constexpr (sizeof(R) == 4) {
-    if (multi) return launch_invert_stream<float, KT, 4, true>(GS, sio, st, num_sms, smem_out, wpb);
-    return variant == 1 ? launch_invert_stream<float, KT, 4, false>(GS, sio, st, num_sms, smem_out, wpb)
-                        : launch_invert_stream<float, KT, 3, false>(GS, sio, st, num_sms, smem_out, wpb);
+    if (multi) return launch_invert_stream<float, KT, 4, true>(GS, sio, st, num_sms, smem_out, wpb, reserve);
+    return variant == 1 ? launch_invert_stream<float, KT, 4, false>(GS, sio, st, num_sms, smem_out, wpb, reserve)
+                        : launch_invert_stream<float, KT, 3, false>(GS, sio, st, num_sms, smem_out, wpb, reserve);
   } else {
-    return multi ? launch_invert_stream<double, KT, 1, true>(GS, sio, st, num_sms, smem_out, wpb)
-                 : launch_invert_stream<double, KT, 1, false>(GS, sio, st, num_sms, smem_out, wpb);
+    return multi ? launch_invert_stream<double, KT, 1, true>(GS, sio, st, num_sms, smem_out, wpb, reserve)
+                 : launch_invert_stream<double, KT, 1, false>(GS, sio, st, num_sms, smem_out, wpb, reserve);
   }
 }
 
@@ -197,7 +198,7 @@ int launch_stream_any(const PmGridSet& GS, const PmStreamIO& sio, cudaStream_t s
 }  // namespace
 
 int pmk_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, int precision, int variant, int warps_per_block,
-                      bool multi, void* stream, int num_sms, size_t* smem_out) {
+                      bool multi, void* stream, int num_sms, size_t* smem_out, int reserve_blocks) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int wpb = (warps_per_block == 1 || warps_per_block == 2) ? warps_per_block : 4;
   if (GS.ngrids < 1 || GS.ngrids > PMK_MAX_GRIDS || (!multi && GS.ngrids != 1)) {
@@ -213,11 +214,11 @@ int pmk_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, int precision,
     }
   }
   if (precision == PM_PREC_FP32) {
-    if (K == 9) return launch_stream_any<float, 9>(GS, sio, st, num_sms, variant, wpb, multi, smem_out);
-    if (K == 10) return launch_stream_any<float, 10>(GS, sio, st, num_sms, variant, wpb, multi, smem_out);
+    if (K == 9) return launch_stream_any<float, 9>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve_blocks);
+    if (K == 10) return launch_stream_any<float, 10>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve_blocks);
   } else {
-    if (K == 9) return launch_stream_any<double, 9>(GS, sio, st, num_sms, variant, wpb, multi, smem_out);
-    if (K == 10) return launch_stream_any<double, 10>(GS, sio, st, num_sms, variant, wpb, multi, smem_out);
+    if (K == 9) return launch_stream_any<double, 9>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve_blocks);
+    if (K == 10) return launch_stream_any<double, 10>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve_blocks);
   }
   snprintf(pmk_g_err, sizeof pmk_g_err, "nterms=%d has no compiled kernel", K);
   return PM_ENOTSUP;

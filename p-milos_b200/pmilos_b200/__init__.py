@@ -121,7 +121,7 @@ class _ServerStats(ctypes.Structure):
     _fields_ = [("scans_done", ctypes.c_int64), ("pixels_done", ctypes.c_int64), ("kernel_launches", ctypes.c_int64),
                 ("latency_p50_ms", ctypes.c_double), ("latency_p99_ms", ctypes.c_double),
                 ("latency_max_ms", ctypes.c_double), ("busy_ms", ctypes.c_double),
-                ("arena_peak_bytes", ctypes.c_size_t)]
+                ("arena_peak_bytes", ctypes.c_size_t), ("prepass_launches", ctypes.c_int64)]
 
 
 class _Stats(ctypes.Structure):
