@@ -10,8 +10,13 @@
  * project's own (one context struct instead of ~60 process globals, one fused
  * pass per wavelength instead of one loop per intermediate).
  *
- * Out of scope, as in every workload this project runs: macroturbulence (v_mac
- * > 1e-4 returns an error) and the FFT convolution path.
+ * Macroturbulence follows the reference's direct-convolution branch (a
+ * Gaussian correlated with the PSF, then a circular convolution of every
+ * profile); the FFT convolution path is out of scope.
+ *
+ * Response-function rows from 9 up are, as in the reference, never cleared: a
+ * row the current call does not write (the macroturbulence row while
+ * v_mac <= 1e-4) keeps what an earlier call of the same context left there.
  */
 #include "pm_oracle.h"
 #include "pm_jacobi.h"
@@ -74,6 +79,9 @@ struct pmo_ctx {
   real shift[3][PMO_NCOMP]; /* nupB, nubB, nurB (mil_sinrf.c:153-166) */
   lam_state *ls;
   real *spectra, *spectra_slight, *d_spectra, *vsigma, *slight;
+  real *spectra_mac;   /* synthesis before any convolution (mil_sinrf.c:278-283) */
+  double *gmac, *gmacd; /* macroturbulence kernel and its derivative (GMAC, GMAC_DERIV) */
+  real *circ;          /* circular-convolution result buffer (resultConv) */
 };
 
 int pmo_sizeof_real(void) { return (int)sizeof(real); }
@@ -154,6 +162,10 @@ pmo_ctx *pmo_create(int nlambda, const double *lambda, double lambda0, const dou
   c->d_spectra = (real *)calloc(4 * nlambda * nterms, sizeof(real));
   c->vsigma = (real *)calloc(4 * nlambda, sizeof(real));
   c->slight = (real *)calloc(4 * nlambda, sizeof(real));
+  c->spectra_mac = (real *)calloc(4 * nlambda, sizeof(real));
+  c->gmac = (double *)calloc(nlambda, sizeof(double));
+  c->gmacd = (double *)calloc(nlambda, sizeof(double));
+  c->circ = (real *)calloc(nlambda, sizeof(real));
   /* milos.c:232-233 */
   c->cc = (real)(PMO_PI / 180.0);
   c->cc_2 = c->cc * 2;
@@ -169,6 +181,7 @@ void pmo_destroy(pmo_ctx *c) {
   if (!c) return;
   free(c->lambda); free(c->psf); free(c->pad); free(c->ls);
   free(c->spectra); free(c->spectra_slight); free(c->d_spectra); free(c->vsigma); free(c->slight);
+  free(c->spectra_mac); free(c->gmac); free(c->gmacd); free(c->circ);
   free(c);
 }
 
@@ -242,6 +255,58 @@ static void correlate(const pmo_ctx *c, real *x, int with_ic, real ic) {
 
 static real edge_max(const real *x, int n) { return (x[0] > x[n - 1]) ? x[0] : x[n - 1]; }
 
+/* The same correlation of a double kernel with the PSF, direct_convolution_double
+ * (convolution.c:21-42): the macroturbulence kernel seen through the instrument. */
+static void correlate_d(const pmo_ctx *c, double *x) {
+  const int n = c->nl, half = n / 2;
+  int k, j;
+  for (k = 0; k < n; k++) c->pad[k + half] = x[k];
+  for (k = 0; k < n; k++) {
+    double acc = 0;
+    for (j = 0; j < n; j++) acc += c->psf[j] * c->pad[j + k];
+    x[k] = acc;
+  }
+}
+
+/* ------------------------------------------------------------------ */
+/* Macroturbulence.  fgauss (fgauss.c:16-66): a Gaussian over the grid, */
+/* centred at lambda[nl/2], of sigma = lambda0 v_mac / c, normalised to */
+/* unit sum; its derivative w.r.t. v_mac as me_der.c:419-421 forms it.   */
+/* convCircular (convolution.c:125-153): y[i] = sum_j h[j] x[(i-j) mod  */
+/* n] in double, stored rotated by nl/2 (result[m] = y[(m + nl/2) mod   */
+/* n]) and rounded to REAL.                                             */
+/* ------------------------------------------------------------------ */
+static void mac_kernel(const pmo_ctx *c, double mac, double *g, double *gd) {
+  const int n = c->nl;
+  const double centre = c->lambda[n / 2];
+  const double ild = (c->lambda0 * mac) / PMO_VLIGHT;
+  double cte = 0;
+  int i;
+  for (i = 0; i < n; i++) {
+    const double a = (c->lambda[i] - centre) / ild;
+    const double term = (a * a) / 2;
+    g[i] = (term < 1e30) ? exp(-term) : 0;
+  }
+  for (i = 0; i < n; i++) cte += g[i];
+  for (i = 0; i < n; i++) g[i] /= cte;
+  if (gd)
+    for (i = 0; i < n; i++) {
+      const double a = (c->lambda[i] - centre) / ild;
+      gd[i] = g[i] / mac * (a * a - 1.0);
+    }
+}
+
+static void circular(const pmo_ctx *c, const real *x, const double *h, real *out) {
+  const int n = c->nl, half = n / 2;
+  int i, j;
+  for (i = 0; i < n; i++) {
+    double acc = 0;
+    for (j = 0; j < n; j++) acc += h[j] * x[(i - j + n) % n];
+    c->circ[(i - half + n) % n] = (real)acc;
+  }
+  for (i = 0; i < n; i++) out[i] = c->circ[i];
+}
+
 int pmo_conv(const pmo_ctx *c, double *x, int mode, double ic) {
   real *t = (real *)malloc(sizeof(real) * c->nl);
   int i;
@@ -253,7 +318,7 @@ int pmo_conv(const pmo_ctx *c, double *x, int mode, double ic) {
 }
 
 /* ------------------------------------------------------------------ */
-/* ME synthesis: mil_sinrf.c:46-415 (single line, no macroturbulence). */
+/* ME synthesis: mil_sinrf.c:46-415 (single line).                     */
 /* ------------------------------------------------------------------ */
 static int synthesis(pmo_ctx *c, const double *m, real ah, const real *slight) {
   const int n = c->nl;
@@ -262,7 +327,8 @@ static int synthesis(pmo_ctx *c, const double *m, real ah, const real *slight) {
   double AZI, GM, E0;
   real ulos, parcial, E0_2, cosi_E0_2;
   int i, g, k;
-  if (m[I_MAC] > 0.0001) return -3; /* macroturbulence: out of scope */
+  const int mac_on = m[I_MAC] > 0.0001;
+  if (mac_on && c->K < 10) return -3; /* v_mac > 0 needs its RF row (NTERMS >= 10, milos.c:152-157) */
 
   /* angle terms, mil_sinrf.c:84-103 */
   AZI = m[I_AZ] * c->cc;
@@ -345,10 +411,17 @@ static int synthesis(pmo_ctx *c, const double *m, real ah, const real *slight) {
     c->spectra[i + n] = (dtiaux * (s->g4));
     c->spectra[i + 2 * n] = (dtiaux * (s->g5));
     c->spectra[i + 3 * n] = (dtiaux * (s->g6));
+    for (k = 0; k < 4; k++) c->spectra_mac[i + k * n] = c->spectra[i + k * n];
   }
 
-  /* instrumental profile, mil_sinrf.c:387-402 */
-  if (c->has_psf) {
+  if (mac_on) {
+    /* macroturbulence (mil_sinrf.c:288-357, direct branch): the PSF folds into
+     * the Gaussian, and every profile, I included, is convolved circularly */
+    mac_kernel(c, m[I_MAC], c->gmac, NULL);
+    if (c->has_psf) correlate_d(c, c->gmac);
+    for (k = 0; k < 4; k++) circular(c, c->spectra + k * n, c->gmac, c->spectra + k * n);
+  } else if (c->has_psf) {
+    /* instrumental profile, mil_sinrf.c:387-402 */
     correlate(c, c->spectra, 1, edge_max(c->spectra, n));
     for (k = 1; k < 4; k++) correlate(c, c->spectra + k * n, 0, 0);
   }
@@ -494,14 +567,24 @@ static void response_functions(pmo_ctx *c, const double *m, real ah, const real 
     d[i + n * 7 + (n * K * 3)] = 0;
     d[i + n * 6] = 0;
     d[i + n * 6 + (n * K * 3)] = 0;
-    /* rows >= 9 (the filling-factor row) are rebuilt below when stray light is
-     * present and are zero otherwise */
-    for (k = 9; k < K; k++)
-      for (s = 0; s < 4; s++) d[i + n * k + n * K * s] = 0;
   }
 
-  /* instrumental profile on every RF but S0's, me_der.c:471-496 */
-  if (c->has_psf) {
+  if (m[I_MAC] > 0.0001 && K >= 10) {
+    /* macroturbulence, me_der.c:314-438 (direct branch): row 9 is the circular
+     * convolution of the unconvolved synthesis with the kernel's derivative,
+     * rows 0..8 but S0 are convolved circularly with the kernel; both kernels
+     * pass through the PSF first */
+    mac_kernel(c, m[I_MAC], c->gmac, c->gmacd);
+    if (c->has_psf) {
+      correlate_d(c, c->gmacd);
+      correlate_d(c, c->gmac);
+    }
+    for (s = 0; s < 4; s++) circular(c, c->spectra_mac + n * s, c->gmacd, d + 9 * n + n * K * s);
+    for (s = 0; s < 4; s++)
+      for (k = 0; k < 9; k++)
+        if (k != 7) circular(c, d + n * k + n * K * s, c->gmac, d + n * k + n * K * s);
+  } else if (c->has_psf) {
+    /* instrumental profile on every RF but S0's, me_der.c:471-496 */
     for (k = 0; k < K; k++)
       if (k != 7) correlate(c, d + n * k, 1, edge_max(d + n * k, n));
     for (s = 1; s < 4; s++)

@@ -23,6 +23,10 @@ Writes
                       large-cube configuration) and w49 (the known-answer test's
                       49-point grid with a 60 mA PSF, stray light and the filling
                       factor inverted); 16 pixels each
+  ref_cases_mac.npz   macroturbulence on the 30-point grid: m10 (v_mac inverted,
+                      60 mA PSF), m10n (the same without PSF), m11 (v_mac and
+                      the filling factor inverted, stray light), mfix (v_mac
+                      fixed at 1.2 km/s); 24 pixels and 8 synthesis models each
 The fixtures are what the CPU test-suite compares the oracle restatement and the
 host precompute with, so those tests need neither the reference nor a GPU.
 """
@@ -85,6 +89,70 @@ CASE_SPECS = {
     112: ((-1204.0, 21.5, 1182.5, 6302.4936), 25.0, False),
     49: ((-600.0, 25.0, 600.0, 6173.3356), 60.0, True),
 }
+
+
+# name: PSF FWHM [mA] or None, stray light + filling factor, v_mac inverted
+MAC_SPECS = {
+    "m10": (60.0, False, True),
+    "m10n": (None, False, True),
+    "m11": (60.0, True, True),
+    "mfix": (60.0, False, False),
+}
+
+
+def mac_case(name, npix=24, nsynth=8):
+    """Macroturbulence on the configuration-1 grid: truths with v_mac in
+    U(0.3, 3) km/s, guess v_mac = 1 (1.2 and fixed for mfix)."""
+    fwhm, stray, free = MAC_SPECS[name]
+    rng = np.random.default_rng(sum(ord(ch) for ch in name) + 2000)
+    (ini, step, fin, l0) = CASE_SPECS[1][0]
+    offs, lam = grid(ini, step, fin, l0)
+    psf = None
+    if fwhm is not None:
+        x, y = gauss_table(fwhm)
+        psf = po.Reference(po.LineSetup(lam, l0, TRIPLET, None, 9), "f64").interp_psf(x, y, offs, 0.0)
+    K = 11 if stray else 10
+    fix = [1] * 9 + [1 if free else 0, 1 if stray else 0]
+    guess = GUESS.copy()
+    guess[9] = 1.0 if free else 1.2
+    if stray:
+        guess[10] = 0.9
+    truth = np.zeros((npix, 11))
+    truth[:, 0] = rng.uniform(1, 20, npix)
+    truth[:, 1] = rng.uniform(0, 3000, npix)
+    truth[:, 2] = rng.uniform(-3, 3, npix)
+    truth[:, 3] = rng.uniform(0.02, 0.05, npix)
+    truth[:, 4] = rng.uniform(0.01, 0.5, npix)
+    truth[:, 5] = rng.uniform(0, 180, npix)
+    truth[:, 6] = rng.uniform(0, 180, npix)
+    truth[:, 7] = rng.uniform(0.1, 0.4, npix)
+    truth[:, 8] = rng.uniform(0.4, 0.9, npix)
+    truth[:, 9] = rng.uniform(0.3, 3.0, npix) if free else 1.2
+    truth[:, 10] = 1.0 - rng.uniform(0, 0.3, npix) if stray else 1.0
+    slight = None
+    if stray:
+        r9 = po.Reference(po.LineSetup(lam, l0, TRIPLET, psf, 9), "f64")
+        slight, _ = r9.synth(np.array([13.0, 0.0, 0.2, 0.035, 0.19, 30.0, 30.0, 0.26, 0.74, 0.0, 1.0]), rf=False)
+        slight = slight.astype(np.float32).astype(np.float64)
+    setup = po.LineSetup(lam, l0, TRIPLET, psf, K)
+    out = dict(lam=lam, offs=offs, lambda0=l0, psf=np.zeros(0) if psf is None else psf, truth=truth, guess=guess,
+               fix=np.array(fix, dtype=np.int32), nterms=K, slight=np.zeros(0) if slight is None else slight)
+    ref64 = po.Reference(setup, "f64")
+    obs = np.array([ref64.synth(m, slight, fix=fix, rf=False)[0] for m in truth], dtype=np.float32)
+    obs += rng.normal(0, 1e-3, obs.shape).astype(np.float32)
+    out["obs"] = obs
+    for flav in ("f32", "f64"):
+        ref = po.Reference(setup, flav)
+        noise = float(np.float32(np.float32(1.0 / 1000) ** 2)) if flav == "f32" else (1.0 / 1000) ** 2
+        r = ref.invert(obs, guess, slight=slight, fix=fix, noise=noise)
+        for k in ("models", "chisq", "iters", "spectra"):
+            out[f"{flav}_{k}"] = r[k]
+        models = truth[:nsynth].copy()
+        sp, rf = zip(*[ref.synth(m, slight, fix=fix) for m in models])
+        out[f"{flav}_synth_models"] = models
+        out[f"{flav}_synth"] = np.array(sp)
+        out[f"{flav}_rf"] = np.array(rf)
+    return out
 
 
 def case(cfg, seed, npix=48, nsynth=12):
@@ -208,10 +276,18 @@ def psf_pins():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
-    ap.add_argument("--only", choices=("all", "wide"), default="all")
+    ap.add_argument("--only", choices=("all", "wide", "mac"), default="all")
     a = ap.parse_args()
     os.environ["PM_REFERENCE_SRC"] = os.path.join(a.reference, "src")
     po.build()
+    mac = {}
+    for name in MAC_SPECS:
+        for k, v in mac_case(name).items():
+            mac[f"{name}_{k}"] = v
+    np.savez_compressed(os.path.join(HERE, "ref_cases_mac.npz"), **mac)
+    print("ref_cases_mac.npz", os.path.getsize(os.path.join(HERE, "ref_cases_mac.npz")), "bytes")
+    if a.only == "mac":
+        return
     files = ["ref_cases_wide.npz"]
     if a.only == "all":
         np.savez_compressed(os.path.join(HERE, "kat_synthesis.npz"), **kat(a.reference))

@@ -119,3 +119,56 @@ def test_wide_grids_bit_exact(name, flav):
     r = ora.invert(g("obs"), g("guess"), slight=sl, fix=fix, noise=_noise(flav))
     for k in ("iters", "chisq", "models", "spectra"):
         assert np.array_equal(r[k], g(f"{flav}_{k}")), k
+
+
+MAC = np.load(os.path.join(GOLDEN, "ref_cases_mac.npz"))
+
+
+@pytest.mark.parametrize("flav", ["f32", "f64"])
+@pytest.mark.parametrize("name", ["m10", "m10n", "m11", "mfix"])
+def test_macroturbulence_bit_exact(name, flav):
+    """Macroturbulence (fgauss, the circular convolutions of mil_sinrf and
+    me_der, with and without the PSF, v_mac inverted or fixed, with the filling
+    factor): full inversions on a fresh context (the order the fixture was made
+    in, since the v_mac response row persists between calls as in the
+    reference), then synthesis and every response function, equal the
+    reference's bit for bit."""
+    g = lambda k: MAC[f"{name}_{k}"]
+    setup = po.LineSetup(g("lam"), float(g("lambda0")), np.array([1.0, 2, 1, 1, 2, 2, 0]),
+                         g("psf") if g("psf").size else None, int(g("nterms")))
+    ora = po.Restatement(setup, flav)
+    sl = g("slight") if g("slight").size else None
+    fix = list(g("fix"))
+    r = ora.invert(g("obs"), g("guess"), slight=sl, fix=fix, noise=_noise(flav))
+    for k in ("iters", "chisq", "models", "spectra"):
+        assert np.array_equal(r[k], g(f"{flav}_{k}")), k
+    for m, sp_ref, rf_ref in zip(g(f"{flav}_synth_models"), g(f"{flav}_synth"), g(f"{flav}_rf")):
+        sp, rf = ora.synth(m, sl, fix=fix)
+        assert np.array_equal(sp, sp_ref)
+        assert np.array_equal(rf, rf_ref)
+    if fix[9]:
+        # the fixture exercises the v_mac row: it moved v_mac away from the guess
+        assert np.abs(r["models"][:, 9] - g("guess")[9]).max() > 0.1
+
+
+def test_macroturbulence_row_is_the_derivative():
+    """The v_mac response row against a central difference of the synthesis,
+    for kernels wider than the grid step (v_mac >= 1 km/s: sigma >= 21 mA at
+    25 mA sampling).  The reference differentiates the Gaussian but not its
+    normalisation to unit sum (me_der.c:419-421); that is exact in the limit of
+    a well-sampled kernel and departs from the true derivative as the kernel
+    narrows towards one grid step (the fixture has such models too)."""
+    g = lambda k: MAC[f"m10_{k}"]
+    setup = po.LineSetup(g("lam"), float(g("lambda0")), np.array([1.0, 2, 1, 1, 2, 2, 0]), g("psf"), 10)
+    ora = po.Restatement(setup, "f64")
+    fix = list(g("fix"))
+    wide = [m for m in g("f64_synth_models") if m[9] >= 1.0]
+    assert len(wide) >= 3
+    for m in wide:
+        _, rf = ora.synth(m, fix=fix)
+        h = 1e-5
+        up, dn = m.copy(), m.copy()
+        up[9] += h
+        dn[9] -= h
+        num = (ora.synth(up, fix=fix, rf=False)[0] - ora.synth(dn, fix=fix, rf=False)[0]) / (2 * h)
+        assert np.abs(rf[:, 9] - num).max() < 2e-3 * np.abs(num).max()
