@@ -96,7 +96,7 @@ typedef struct pm_model {
   double az;    /* azimuth [deg] */
   double S0;    /* source function constant */
   double S1;    /* source function gradient */
-  double mac;   /* macroturbulence [km/s] (must be 0 here) */
+  double mac;   /* macroturbulence [km/s]; > 1e-4 broadens the profiles (grids of <= 32 wavelengths) */
   double alfa;  /* filling factor */
 } pm_model;
 
@@ -124,7 +124,9 @@ typedef struct pm_config {
   double toplim;          /* relative chi^2 stop (1e-12 in the reference) */
   int miter;              /* max LM iterations (NumberOfCycles > 0) */
   int fix[11];            /* 1 = parameter is inverted, reference order (defines.h:245) */
-  int nterms;             /* NTERMS: 9, 10 or 11 */
+  int nterms;             /* NTERMS = 11 - !fix[10] - (guess.mac == 0 && !fix[9]) (milos.c:152-157):
+                             9; 10 (filling factor, or v_mac, inverted; or v_mac fixed nonzero); 11.
+                             Checked against the guess when one is given (PM_EINVAL) */
   int logclambda;         /* "Diagonal element acceleration" */
   double mu;              /* heliocentric angle cosine (ah) */
   int classical_estimates;/* run estimacionesClasicas + NaN fixes before LM */
@@ -199,7 +201,9 @@ int pm_invert_batch(pm_ctx *ctx, int64_t npix, const float *spectro, const float
 
 /* Forward synthesis (mil_sinrf) and optionally the response functions (me_der)
  * of npix models, as the reference's synthesis mode (milos.c:601-602) computes
- * them.  rf_out (nullable) is [npix][4][nterms][nlambda]. */
+ * them.  rf_out (nullable) is [npix][4][nterms][nlambda].  A model's v_mac broadens
+ * its profiles on contexts with nterms >= 10; the v_mac row (row 9 when fix[10] = 0
+ * or nterms = 11) is zero for models with v_mac <= 1e-4. */
 int pm_synth_batch(pm_ctx *ctx, int64_t npix, const pm_model *models, const float *slight, int slight_mode,
                    float *spectra_out, float *rf_out, int mem);
 

@@ -22,6 +22,9 @@
 //   psf_rows         direct_convolution(_ic) convolution.c:54-121, mil_sinrf.c:387-402
 //   rf_lane          me_der.c:48-312, funcionComponentFor :536-609
 //   rf_correlate     me_der.c:471-496
+//   mac_*            fgauss fgauss.c:16-66, direct_convolution_double
+//                    convolution.c:21-42, convCircular :125-153, mil_sinrf.c:288-357,
+//                    me_der.c:314-438
 //   normal_eq        covarm2 lib.c:71-116, totalParcialf/Matrixf :237-268
 //   chisq            fchisqr lib.c:126-152
 //   solve_*          mil_svd milosUtils.c:237-271
@@ -309,7 +312,7 @@ struct alignas(16) WarpSmem {
   unsigned long long pix;
   long long job_k;
   int grid_cur;
-  int pad_;
+  int xs_dirty;  // xs holds macroturbulence data: restore its zero padding before psf_rows
 };
 
 // The 16-byte vector loads of psf_rows and rf_correlate need every per-warp
@@ -323,7 +326,7 @@ constexpr bool smem_layout_ok() {
 }
 static_assert(smem_layout_ok<float>(), "shared-memory layout breaks 16-byte vector loads (float)");
 static_assert(smem_layout_ok<double>(), "shared-memory layout breaks 16-byte vector loads (double)");
-static_assert(3 * 10 * 10 * sizeof(double) <= sizeof(float) * NL * TRS, "eigen scratch exceeds the transpose buffer");
+static_assert(3 * 12 * 12 * sizeof(double) <= sizeof(float) * NL * TRS, "eigen scratch exceeds the transpose buffer");
 
 template <typename R>
 __device__ __forceinline__ void load_taps(const PmParams& P, BlockSmem<R>& bs) {
@@ -379,11 +382,137 @@ __device__ __forceinline__ void psf_rows(const PmParams& P, WarpSmem<R>& sm, int
   __syncwarp();
 }
 
-// Synthesis of the model at this lane's wavelength, PSF and stray light included.
-// S gets the final (mixed) profile, Su the profile before the stray-light mix.
-// The per-model terms and this lane's synthesis state are left in shared memory
-// for the response functions, as the reference leaves them in globals.
+// ---------------------------------------------------------------------------
+// Macroturbulence (the direct branch of mil_sinrf.c:288-357 and
+// me_der.c:314-438).  A Gaussian of sigma = lambda0 v_mac / c over the grid,
+// centred at lambda[nl/2] and normalised to unit sum (fgauss, fgauss.c:16-66),
+// is correlated with the PSF when there is one (direct_convolution_double,
+// convolution.c:21-42); every synthesized profile (Stokes I included, with no
+// continuum padding) and every response function but S0's is then convolved
+// with it circularly, and the v_mac row is the circular convolution of the
+// unconvolved synthesis with the Gaussian's derivative in the form of
+// me_der.c:419-421 (GMAC / v_mac ((x / sigma)^2 - 1): the normalisation is not
+// differentiated).  convCircular (convolution.c:125-153) returns its result
+// rotated by nl/2: out[m] = sum_t x[t] k[(m + nl/2 - t) mod nl].
+//
+// While a model with v_mac > 1e-4 is current, the per-warp rows xs (the padded
+// input of psf_rows otherwise) hold the unconvolved synthesis [4][32] and the
+// kernel and its derivative, each tripled (entry u = k[u mod nl], u < 96) so
+// that the circular index m + nl/2 - t + nl is a plain offset; xs_dirty makes
+// the next psf_rows restore the zero padding first.
+// ---------------------------------------------------------------------------
+constexpr double kMacMin = 0.0001;
+constexpr int kMacSu = 0, kMacK = 4 * NL, kMacD = 7 * NL;
+static_assert(kMacD + 3 * NL <= 4 * XSR, "macroturbulence data exceed the padded rows");
+
+// Lane k's value of the kernel (and of its derivative with DERIV), through the
+// PSF; scratch: 64 doubles.
+template <bool DERIV>
+__device__ __forceinline__ void mac_kernel(const PmParams& P, double mac, int lane, bool valid, double* scratch,
+                                           double& g, double& gd) {
+  const double x = valid ? P.dl[lane] - P.dl[P.half] : 0.0;  // lambda_k - lambda[nl/2], exactly
+  const double ild = (P.lambda0 * mac) / kVLight;
+  const double a = x / ild;
+  const double term = (a * a) / 2;
+  g = (valid && term < 1e30) ? exp(-term) : 0.0;
+  g = g / warp_sum(g);
+  gd = DERIV ? g / mac * (a * a - 1.0) : 0.0;
+  if (P.has_psf) {
+    __syncwarp();
+    scratch[lane] = g;
+    if (DERIV) scratch[NL + lane] = gd;
+    __syncwarp();
+    double acc = 0.0, accd = 0.0;
+    for (int j = 0; j < P.nl; ++j) {
+      const int t = lane + j - P.half;
+      if (t >= 0 && t < P.nl) {
+        acc = fma(P.taps_d[j], scratch[t], acc);
+        if (DERIV) accd = fma(P.taps_d[j], scratch[NL + t], accd);
+      }
+    }
+    __syncwarp();
+    g = valid ? acc : 0.0;
+    gd = valid ? accd : 0.0;
+  }
+}
+
+// dst[u] = k[u mod nl] for u < 96, k[l] held by lane l.
 template <typename R>
+__device__ __forceinline__ void mac_triple(const PmParams& P, double k, int lane, R* dst) {
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const int u = lane + NL * q;
+    const double v = __shfl_sync(kFull, k, u % P.nl);
+    dst[u] = R(v);
+  }
+}
+
+// The kernel of v_mac (and its derivative with DERIV) into xs; tr is scratch.
+template <typename R, bool DERIV>
+__device__ __forceinline__ void mac_prepare(const PmParams& P, WarpSmem<R>& sm, double mac, int lane, bool valid) {
+  double g, gd;
+  mac_kernel<DERIV>(P, mac, lane, valid, reinterpret_cast<double*>(sm.tr), g, gd);
+  R* xf = &sm.xs[0][0];
+  mac_triple<R>(P, g, lane, xf + kMacK);
+  if (DERIV) mac_triple<R>(P, gd, lane, xf + kMacD);
+  if (lane == 0) sm.xs_dirty = 1;
+  __syncwarp();
+}
+
+// out[s] at this lane's wavelength m: sum_t x[s][t] k[(m + nl/2 - t) mod nl] for
+// the four unconvolved rows x of xs and the tripled kernel k3.
+template <typename R>
+__device__ __forceinline__ void mac_circular4(const PmParams& P, const R* xf, const R* k3, int lane, R out[4]) {
+  R acc[4] = {R(0), R(0), R(0), R(0)};
+  const R* kb = k3 + lane + P.half + P.nl;
+#pragma unroll 2
+  for (int t = 0; t < P.nl; ++t) {
+    const R kk = kb[-t];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) acc[s] = fma(xf[kMacSu + s * NL + t], kk, acc[s]);
+  }
+#pragma unroll
+  for (int s = 0; s < 4; ++s) out[s] = acc[s];
+}
+
+// The 32 response-function profiles (one per lane, rows of tr) convolved
+// circularly with the kernel in xs, in place.
+template <typename R>
+__device__ __forceinline__ void mac_rf_circular(const PmParams& P, WarpSmem<R>& sm, int lane) {
+  __syncwarp();
+  R* row = sm.tr + lane * TRS;
+  const R* k3 = &sm.xs[0][0] + kMacK + P.half + P.nl;
+  R acc[NL];
+#pragma unroll
+  for (int m = 0; m < NL; ++m) acc[m] = 0;
+#pragma unroll 1
+  for (int t = 0; t < P.nl; ++t) {
+    const R xt = row[t];
+    const R* kb = k3 - t;
+#pragma unroll
+    for (int m = 0; m < NL; ++m) acc[m] = fma(xt, kb[m], acc[m]);
+  }
+#pragma unroll
+  for (int m = 0; m < NL; ++m) row[m] = acc[m];
+  __syncwarp();
+}
+
+// Zero the padded rows again after macroturbulence data.
+template <typename R>
+__device__ __forceinline__ void xs_restore(WarpSmem<R>& sm, int lane) {
+  for (int e = lane; e < 4 * XSR; e += 32) (&sm.xs[0][0])[e] = R(0);
+  __syncwarp();
+  if (lane == 0) sm.xs_dirty = 0;
+  __syncwarp();
+}
+
+// Synthesis of the model at this lane's wavelength, PSF (or macroturbulence)
+// and stray light included.  S gets the final (mixed) profile, Su the profile
+// before the stray-light mix.  The per-model terms and this lane's synthesis
+// state are left in shared memory for the response functions, as the reference
+// leaves them in globals.  MAC: the kernel has a v_mac response row (NTERMS >=
+// 10), so v_mac may be nonzero.
+template <typename R, bool MAC = false>
 __device__ __forceinline__ void synthesize(const PmParams& P, WarpSmem<R>& sm, const double* m,
                                            const float* sl_pix, int lane, bool valid, R S[4], R Su[4]) {
   ModelTerms<R> T;
@@ -392,7 +521,21 @@ __device__ __forceinline__ void synthesize(const PmParams& P, WarpSmem<R>& sm, c
   synth_lane<R>(P, T, P.dl[valid ? lane : 0], st, S);
   copy16(*reinterpret_cast<LaneState<R>*>(sm.ls[lane]), st);
   if (lane == 0) copy16(sm.mt, T);
-  if (P.has_psf) psf_rows<R>(P, sm, lane, valid, S);
+  const double mac = MAC ? m[9] : 0.0;
+  if (MAC && mac > kMacMin) {
+    R* xf = &sm.xs[0][0];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) xf[kMacSu + s * NL + lane] = valid ? S[s] : R(0);
+    mac_prepare<R, false>(P, sm, mac, lane, valid);
+    R out[4];
+    mac_circular4<R>(P, xf, xf + kMacK, lane, out);
+#pragma unroll
+    for (int s = 0; s < 4; ++s) S[s] = valid ? out[s] : R(0);
+    __syncwarp();
+  } else if (P.has_psf) {
+    if (MAC && sm.xs_dirty) xs_restore<R>(sm, lane);
+    psf_rows<R>(P, sm, lane, valid, S);
+  }
 #pragma unroll
   for (int s = 0; s < 4; ++s) Su[s] = S[s];
   if (P.slight_mode != PM_SLIGHT_NONE) {
@@ -580,7 +723,8 @@ __device__ __forceinline__ void transpose_reduce(T (&v)[N], int lane) {
 // and FijaACeroDerivadasNoNecesarias: d[row][stokes] for rows 0..K-1.
 template <typename R, int KT>
 __device__ __forceinline__ void gather_rf(const PmParams& P, const WarpSmem<R>& sm, int lane, bool valid,
-                                          R alf, const R Sff[4], const float* sl_pix, R (&d)[KT][4]) {
+                                          R alf, const R Sff[4], const float* sl_pix, const R (&dmac)[4],
+                                          R (&d)[KT][4]) {
   const R* col = sm.tr + lane;
 #pragma unroll
   for (int r = 0; r < KT; ++r) {
@@ -590,6 +734,7 @@ __device__ __forceinline__ void gather_rf(const PmParams& P, const WarpSmem<R>& 
       if (r < 7) v = col[(r * 4 + s) * TRS];
       else if (r == 7) v = (s == 0) ? R(1) : R(0);  // S0 (me_der.c:301-306)
       else if (r == 8) v = col[(7 * 4 + s) * TRS];
+      else if (r == 9 && P.mac_row == 9) v = dmac[s];  // zero while v_mac <= 1e-4
       else v = R(0);
       d[r][s] = valid ? v : R(0);
     }
@@ -907,7 +1052,8 @@ __device__ __forceinline__ void apply_delta(const PmParams& P, const double* m, 
     if (P.fix[9]) out[9] = m[9] - dlt[9];
     if (P.fix[10]) out[10] = m[10] - dlt[10];
   } else if constexpr (KT == 10) {
-    if (P.fix[10]) out[10] = m[10] - dlt[9];  // NTERMS == 10: alpha is term 9
+    if (P.fix[9]) out[9] = m[9] - dlt[9];     // NTERMS == 10 with v_mac inverted (then fix[10] == 0)
+    if (P.fix[10]) out[10] = m[10] - dlt[9];  // NTERMS == 10 with alpha inverted (then fix[9] == 0)
   }
 }
 
@@ -1023,11 +1169,17 @@ __device__ __forceinline__ void classical(const PmParams& P, const float O[4], i
   classical_finish(P, v, m);
 }
 
-// Response functions at the current synthesis -> alpha, beta in shared memory.
-template <typename R, int KT>
-__device__ __forceinline__ void rf_and_normal_eq(const PmParams& P, const BlockSmem<R>& bs, WarpSmem<R>& sm,
-                                                 int lane, bool valid, const R S[4], const R Sff[4],
-                                                 const float O[4], const R isig[4], const float* sl_pix) {
+// The response functions of model m at this lane's wavelength (rows 0..K-1,
+// before FijaACeroDerivadasNoNecesarias): me_der's rows, their PSF or
+// macroturbulence convolutions, the v_mac row and the filling-factor terms.
+// m must be the model of the last synthesis.  MAC: compiled with the
+// macroturbulence branch (the grid has a v_mac row; NTERMS >= 10).
+template <typename R, int KT, bool MAC = (KT >= 10)>
+__device__ __forceinline__ void response_rows(const PmParams& P, const BlockSmem<R>& bs, WarpSmem<R>& sm, int lane,
+                                              bool valid, const double* m, const R Sff[4], const float* sl_pix,
+                                              R (&d)[KT][4]) {
+  const bool mac_on = MAC && m[9] > kMacMin;
+  if (mac_on) mac_prepare<R, true>(P, sm, m[9], lane, valid);  // before tr fills up
   R alf;
   {
     ModelTerms<R> T;
@@ -1037,10 +1189,25 @@ __device__ __forceinline__ void rf_and_normal_eq(const PmParams& P, const BlockS
     rf_lane<R, TRS>(P, T, st, sm.tr + lane, valid);
     alf = T.alf;
   }
-  if (P.has_psf) rf_correlate<R>(P, bs, sm, lane);
+  R dmac[4] = {R(0), R(0), R(0), R(0)};
+  if (mac_on) {
+    mac_rf_circular<R>(P, sm, lane);
+    const R* xf = &sm.xs[0][0];
+    mac_circular4<R>(P, xf, xf + kMacD, lane, dmac);
+  } else if (P.has_psf) {
+    rf_correlate<R>(P, bs, sm, lane);
+  }
   __syncwarp();
+  gather_rf<R, KT>(P, sm, lane, valid, alf, Sff, sl_pix, dmac, d);
+}
+
+// Response functions at the current synthesis -> alpha, beta in shared memory.
+template <typename R, int KT, bool MAC>
+__device__ __forceinline__ void rf_and_normal_eq(const PmParams& P, const BlockSmem<R>& bs, WarpSmem<R>& sm,
+                                                 int lane, bool valid, const R S[4], const R Sff[4],
+                                                 const float O[4], const R isig[4], const float* sl_pix) {
   R d[KT][4];
-  gather_rf<R, KT>(P, sm, lane, valid, alf, Sff, sl_pix, d);
+  response_rows<R, KT, MAC>(P, bs, sm, lane, valid, sm.model, Sff, sl_pix, d);
 #pragma unroll
   for (int r = 0; r < KT; ++r)
     if (P.zero_row[r]) {
@@ -1070,7 +1237,8 @@ __device__ __forceinline__ T* ld_ptr(T* const* p) {
 // Pixel sm.pix of job *sm.job.  The job, the pixel index and the buffer
 // pointers are read from shared memory and the descriptor where they are used,
 // so that none of them occupies registers across the LM loop.
-template <typename R, int KT>
+// MAC: compiled with the macroturbulence branch (grids with a v_mac row).
+template <typename R, int KT, bool MAC>
 __device__ __forceinline__ void invert_pixel(const PmParams& P, const BlockSmem<R>& bs, WarpSmem<R>& sm, int lane,
                                              unsigned long long* ctr) {
   const bool valid = lane < P.nl;
@@ -1124,8 +1292,8 @@ __device__ __forceinline__ void invert_pixel(const PmParams& P, const BlockSmem<
   } else {
     {
       R Su[4];
-      synthesize<R>(P, sm, m, sl_pix, lane, valid, S, Su);
-      rf_and_normal_eq<R, KT>(P, bs, sm, lane, valid, S, Su, O, isig, sl_pix);
+      synthesize<R, MAC>(P, sm, m, sl_pix, lane, valid, S, Su);
+      rf_and_normal_eq<R, KT, MAC>(P, bs, sm, lane, valid, S, Su, O, isig, sl_pix);
     }
     ochi = chisq<R>(P, S, O, isig, valid, double(nfree));
     const double chi0 = ochi;
@@ -1159,7 +1327,7 @@ __device__ __forceinline__ void invert_pixel(const PmParams& P, const BlockSmem<
         __syncwarp();
       }
       R Su[4];
-      synthesize<R>(P, sm, trial, sl_pix, lane, valid, S, Su);
+      synthesize<R, MAC>(P, sm, trial, sl_pix, lane, valid, S, Su);
       const double chi = chisq<R>(P, S, O, isig, valid, double(nfree));
       if ((fabs((ochi - chi) * 100 / chi) < P.toplim) || (chi < 0.0001)) {
         stop = true;
@@ -1169,7 +1337,7 @@ __device__ __forceinline__ void invert_pixel(const PmParams& P, const BlockSmem<
         flambda = flambda / (5.0 * factor);
         if (lane < 11) m[lane] = trial[lane];
         __syncwarp();
-        rf_and_normal_eq<R, KT>(P, bs, sm, lane, valid, S, S, O, isig, sl_pix);
+        rf_and_normal_eq<R, KT, MAC>(P, bs, sm, lane, valid, S, S, O, isig, sl_pix);
         ochi = chi;
         ++accepted;
       } else {

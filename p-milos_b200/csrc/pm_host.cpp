@@ -260,14 +260,15 @@ int fill_params(const pm_line* L, const pm_config* c, PmParams& P) {
   if (c->nlambda < 2 || c->nlambda > PMK_NL)
     return fail(PM_ERANGE, "nlambda=%d: this build handles 2..%d wavelengths", c->nlambda, PMK_NL);
   if (!c->lambda) return fail(PM_EINVAL, "lambda grid is NULL");
-  if (c->nterms != 9 && c->nterms != 10)
-    return fail(PM_ENOTSUP, "nterms=%d: supported are 9 and 10 (10 = filling factor inverted)", c->nterms);
-  if (c->fix[9]) return fail(PM_ENOTSUP, "macroturbulence inversion (fix[9]) is outside this implementation");
+  if (c->nterms < 9 || c->nterms > 11) return fail(PM_ENOTSUP, "nterms=%d: supported are 9, 10 and 11", c->nterms);
   {
-    // NTERMS = 11 - !fix[10] - (mac == 0 && !fix[9]) (milos.c:152-157)
-    const int expect = 11 - (c->fix[10] ? 0 : 1) - 1;
-    if (expect != c->nterms)
-      return fail(PM_EINVAL, "nterms=%d inconsistent with fix[10]=%d (expected %d)", c->nterms, c->fix[10], expect);
+    // NTERMS = 11 - !fix[10] - (mac == 0 && !fix[9]) (milos.c:152-157); the
+    // guess's v_mac settles the last term when the guess is known (pmh_check_guess)
+    const int hi = 11 - (c->fix[10] ? 0 : 1);
+    const int lo = hi - (c->fix[9] ? 0 : 1);
+    if (c->nterms < lo || c->nterms > hi)
+      return fail(PM_EINVAL, "nterms=%d inconsistent with fix[9]=%d, fix[10]=%d (expected %d..%d)", c->nterms,
+                  c->fix[9], c->fix[10], lo, hi);
   }
   if (c->miter < 0) return fail(PM_EINVAL, "miter=%d", c->miter);
   if (!(c->noise > 0)) return fail(PM_EINVAL, "noise must be > 0");
@@ -295,7 +296,12 @@ int fill_params(const pm_line* L, const pm_config* c, PmParams& P) {
     if (P.K == 10 && k == 9) P.zero_row[k] = (P.fix[9] == 0 && P.fix[10] == 0);
     else P.zero_row[k] = (P.fix[k] == 0);
   }
-  P.ff_row = (P.K == 10) ? 9 : -1;
+  // me_der.c:499-525: the filling-factor row is 10 with NTERMS 11, else 9 unless
+  // v_mac is inverted; row 9 is v_mac's with NTERMS 11 or 10 and alpha fixed
+  P.ff_row = (P.K == 11) ? 10 : ((P.K == 10 && !P.fix[9]) ? 9 : -1);
+  P.mac_row = (P.K == 11 || (P.K == 10 && !P.fix[10])) ? 9 : -1;
+  if (P.mac_row >= 0 && P.nl > 32)
+    return fail(PM_ENOTSUP, "macroturbulence on grids of more than 32 wavelengths is outside this implementation");
   P.lambda0 = L->lambda0;
   for (int i = 0; i < P.nl; ++i) P.dl[i] = c->lambda[i] - L->lambda0;
   for (int k = 0; k < L->n_pi; ++k) { P.nu[0][k] = L->nup[k]; P.we[0][k] = L->wep[k]; }
@@ -346,11 +352,21 @@ void set_guess(PmParams& P, const pm_model* g) {
   for (int i = 0; i < 11; ++i) P.guess[i] = v[i];
 }
 
+// NTERMS = 11 - !fix[10] - (mac == 0 && !fix[9]) (milos.c:152-157), now that the
+// guess's v_mac is known.
+int check_guess(const PmParams& P, const pm_model* g) {
+  const int expect = 11 - (P.fix[10] ? 0 : 1) - ((g->mac == 0.0 && !P.fix[9]) ? 1 : 0);
+  if (expect != P.K)
+    return fail(PM_EINVAL, "nterms=%d inconsistent with guess v_mac=%g, fix[9]=%d, fix[10]=%d (NTERMS would be %d)", P.K,
+                g->mac, P.fix[9], P.fix[10], expect);
+  return PM_OK;
+}
+
 int set_slight(PmParams& P, const float* slight, int mode, int mem) {
   P.slight_mode = mode;
   if (mode == PM_SLIGHT_NONE) return PM_OK;
   if (!slight) return fail(PM_EINVAL, "slight_mode=%d but slight is NULL", mode);
-  if (P.K != 10) return fail(PM_EINVAL, "stray light requires nterms == 10 (filling factor inverted)");
+  if (P.K < 10) return fail(PM_EINVAL, "stray light requires nterms >= 10 (filling factor or v_mac inverted)");
   if (mode == PM_SLIGHT_SHARED) {
     std::vector<float> h(4 * P.nl);
     if (mem == PM_MEM_DEVICE) {
@@ -373,6 +389,7 @@ int set_slight(PmParams& P, const float* slight, int mode, int mem) {
 // Helpers shared with the other translation units of the library.
 int pmh_fill_params(const pm_line* L, const pm_config* c, PmParams& P) { return fill_params(L, c, P); }
 void pmh_set_guess(PmParams& P, const pm_model* g) { set_guess(P, g); }
+int pmh_check_guess(const PmParams& P, const pm_model* g) { return check_guess(P, g); }
 int pmh_fail(int code, const char* msg) { return fail(code, "%s", msg); }
 
 extern "C" int pm_ctx_create(const pm_line* line, const pm_config* cfg, void* stream, pm_ctx** out) {
@@ -789,7 +806,7 @@ extern "C" int pm_invert_batch(pm_ctx* c, int64_t npix, const float* spectro, co
     return fail(PM_EINVAL, "pm_invert_batch: NULL argument");
   if (npix < 0) return fail(PM_EINVAL, "pm_invert_batch: npix < 0");
   if (mem != PM_MEM_HOST && mem != PM_MEM_DEVICE) return fail(PM_EINVAL, "pm_invert_batch: mem=%d", mem);
-  if (guess->mac != 0.0) return fail(PM_ENOTSUP, "macroturbulence (guess.mac > 0) is outside this implementation");
+  if (int rc = check_guess(c->P, guess); rc != PM_OK) return rc;
   c->stats = pm_stats{};
   if (npix == 0) return PM_OK;
   set_guess(c->P, guess);

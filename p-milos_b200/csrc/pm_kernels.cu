@@ -15,6 +15,7 @@ __global__ void __launch_bounds__(128) synth_kernel(const __grid_constant__ PmPa
   WarpSmem<R>& sm = warp_smem<R>(smem_raw, warp);
   load_taps<R>(P, bs);
   for (int e = lane; e < 4 * XSR; e += 32) (&sm.xs[0][0])[e] = R(0);
+  if (lane == 0) sm.xs_dirty = 0;
   __syncthreads();
   const bool valid = lane < P.nl;
   const int64_t nwarps = int64_t(gridDim.x) * (blockDim.x >> 5);
@@ -24,25 +25,14 @@ __global__ void __launch_bounds__(128) synth_kernel(const __grid_constant__ PmPa
     if (lane < 11) sm.model[lane] = io.models_in[size_t(pix) * 11 + lane];
     __syncwarp();
     R S[4], Su[4];
-    synthesize<R>(P, sm, sm.model, sl_pix, lane, valid, S, Su);
+    synthesize<R, (KT >= 10)>(P, sm, sm.model, sl_pix, lane, valid, S, Su);
     if (valid) {
 #pragma unroll
       for (int s = 0; s < 4; ++s) io.spectra_out[base + s * P.nl + lane] = float(S[s]);
     }
     if (io.rf_out) {
-      R alf;
-      {
-        ModelTerms<R> T;
-        copy16(T, sm.mt);
-        LaneState<R> st;
-        load_lane_state<R>(sm, lane, st);
-        rf_lane<R, TRS>(P, T, st, sm.tr + lane, valid);
-        alf = T.alf;
-      }
-      if (P.has_psf) rf_correlate<R>(P, bs, sm, lane);
-      __syncwarp();
       R d[KT][4];
-      gather_rf<R, KT>(P, sm, lane, valid, alf, Su, sl_pix, d);
+      response_rows<R, KT>(P, bs, sm, lane, valid, sm.model, Su, sl_pix, d);
       __syncwarp();
       if (valid) {
         const size_t rb = size_t(pix) * 4 * KT * P.nl;
@@ -102,9 +92,11 @@ int pmk_synth(const PmParams& P, const PmIO& io, int precision, void* stream) {
   if (precision == PM_PREC_FP32) {
     if (P.K == 9) return launch_synth_any<float, 9>(P, io, st);
     if (P.K == 10) return launch_synth_any<float, 10>(P, io, st);
+    if (P.K == 11) return launch_synth_any<float, 11>(P, io, st);
   } else {
     if (P.K == 9) return launch_synth_any<double, 9>(P, io, st);
     if (P.K == 10) return launch_synth_any<double, 10>(P, io, st);
+    if (P.K == 11) return launch_synth_any<double, 11>(P, io, st);
   }
   snprintf(pmk_g_err, sizeof pmk_g_err, "nterms=%d has no compiled kernel", P.K);
   return PM_ENOTSUP;

@@ -108,7 +108,6 @@ extern "C" int pm_invert_batch_noalloc(const pm_line* line, const pm_config* cfg
                   (long long)npix, PM_NOALLOC_MAX_PIXELS);
     return pmh_fail(PM_ERANGE, msg);
   }
-  if (guess->mac != 0.0) return pmh_fail(PM_ENOTSUP, "macroturbulence (guess.mac > 0) is outside this implementation");
   if (cfg->nlambda > kMaxNl) {
     char msg[160];
     std::snprintf(msg, sizeof msg, "pm_invert_batch_noalloc: %d wavelengths exceed the static scratch (at most %d)",
@@ -118,11 +117,13 @@ extern "C" int pm_invert_batch_noalloc(const pm_line* line, const pm_config* cfg
   PmParams P;
   int rc = pmh_fill_params(line, cfg, P);
   if (rc != PM_OK) return rc;
+  rc = pmh_check_guess(P, guess);
+  if (rc != PM_OK) return rc;
   pmh_set_guess(P, guess);
   P.slight_mode = slight_mode;
   if (slight_mode != PM_SLIGHT_NONE) {
     if (!slight) return pmh_fail(PM_EINVAL, "pm_invert_batch_noalloc: slight_mode set but slight is NULL");
-    if (P.K != 10) return pmh_fail(PM_EINVAL, "stray light requires nterms == 10 (filling factor inverted)");
+    if (P.K < 10) return pmh_fail(PM_EINVAL, "stray light requires nterms >= 10 (filling factor or v_mac inverted)");
     if (slight_mode == PM_SLIGHT_SHARED) {
       for (int i = 0; i < 4 * P.nl; ++i) {
         P.sl_f[i] = slight[i];

@@ -31,6 +31,7 @@ struct PmParams {
   int fix[11];
   int zero_row[PM_NTERMS_MAX];  // FijaACeroDerivadasNoNecesarias (milosUtils.c:199-227)
   int ff_row;      // RF row that holds d/d(filling factor), or -1
+  int mac_row;     // 9 when RF row 9 is d/d(v_mac) (NTERMS 11, or 10 with alpha fixed), else -1
   double lambda0;
   double dl[PMK_NL];                       // lambda_i - lambda0 [A]
   double nu[3][PM_ZEEMAN_MAX];             // splittings: 0 = pi (NUP), 1 = blue (NUB), 2 = NUB mirrored
@@ -138,4 +139,6 @@ const char* pmk_last_cuda_error();
 // Host helpers (pm_host.cpp) shared with pm_noalloc.cu.
 int pmh_fill_params(const pm_line* L, const pm_config* c, PmParams& P);
 void pmh_set_guess(PmParams& P, const pm_model* g);
+// The NTERMS rule of milos.c:152-157 against the guess's v_mac: PM_OK or PM_EINVAL.
+int pmh_check_guess(const PmParams& P, const pm_model* g);
 int pmh_fail(int code, const char* msg);

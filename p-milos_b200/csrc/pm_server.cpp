@@ -479,9 +479,10 @@ extern "C" int pm_server_create(const pm_line* line, const pm_config* const* gri
       release(s);
       return rc;
     }
-    if (guesses[g].mac != 0.0) {
+    rc = pmh_check_guess(s->gs->g[g], &guesses[g]);
+    if (rc != PM_OK) {
       release(s);
-      return sfail(PM_ENOTSUP, "macroturbulence (guess.mac > 0) is outside this implementation");
+      return rc;
     }
     pmh_set_guess(s->gs->g[g], &guesses[g]);
     const PmParams& P = s->gs->g[g];

@@ -59,7 +59,7 @@ struct GridParams {
   PmParams g[NG];
 };
 
-template <typename R, int KT, int MINB, bool MULTI>
+template <typename R, int KT, int MINB, bool MULTI, bool MAC>
 __global__ void __launch_bounds__(128, MINB) invert_stream_kernel(
     const __grid_constant__ GridParams<MULTI ? PMK_MAX_GRIDS : 1> GS, const PmStreamIO sio) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -104,7 +104,10 @@ __global__ void __launch_bounds__(128, MINB) invert_stream_kernel(
     if (gi != sm.grid_cur) {
       for (int e = lane; e < 4 * XSR; e += 32) (&sm.xs[0][0])[e] = R(0);
       __syncwarp();
-      if (lane == 0) sm.grid_cur = gi;
+      if (lane == 0) {
+        sm.grid_cur = gi;
+        sm.xs_dirty = 0;
+      }
     }
     if (lane == 0) {
       sm.job_k = k;
@@ -112,7 +115,7 @@ __global__ void __launch_bounds__(128, MINB) invert_stream_kernel(
       sm.pix = (unsigned long long)t - t0;
     }
     __syncwarp();
-    invert_pixel<R, KT>(P, bs[gi], sm, lane, sio.q->ctr);
+    invert_pixel<R, KT, MAC>(P, bs[gi], sm, lane, sio.q->ctr);
     jp = *reinterpret_cast<const PmJob* const volatile*>(&sm.job);
     unsigned long long* done = ld_ptr(&jp->done);
     if (done) {
@@ -158,13 +161,13 @@ __global__ void __launch_bounds__(256) classical_prepass_kernel(const __grid_con
   }
 }
 
-template <typename R, int KT, int MINB, bool MULTI>
+template <typename R, int KT, int MINB, bool MULTI, bool MAC>
 int launch_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, cudaStream_t st, int num_sms,
                          size_t* smem_out, int wpb, int reserve) {
   const int threads = 32 * wpb;
   const size_t smem = (MULTI ? PMK_MAX_GRIDS : 1) * sizeof(BlockSmem<R>) + sizeof(WarpSmem<R>) * (threads / 32);
   if (smem_out) *smem_out = smem;
-  auto kern = invert_stream_kernel<R, KT, MINB, MULTI>;
+  auto kern = invert_stream_kernel<R, KT, MINB, MULTI, MAC>;
   constexpr int NG = MULTI ? PMK_MAX_GRIDS : 1;
   GridParams<NG> gp;  // copied into the launch
   gp.ngrids = GS.ngrids < NG ? GS.ngrids : NG;
@@ -181,17 +184,30 @@ int launch_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, cudaStream_
   return PM_OK;
 }
 
-template <typename R, int KT>
+// MAC: the macroturbulence branch compiled in (a grid with a v_mac row).
+template <typename R, int KT, bool MAC>
 int launch_stream_any(const PmGridSet& GS, const PmStreamIO& sio, cudaStream_t st, int num_sms, int variant,
                       int wpb, bool multi, size_t* smem_out, int reserve) {
   if constexpr (sizeof(R) == 4) {
-    if (multi) return launch_invert_stream<float, KT, 4, true>(GS, sio, st, num_sms, smem_out, wpb, reserve);
-    return variant == 1 ? launch_invert_stream<float, KT, 4, false>(GS, sio, st, num_sms, smem_out, wpb, reserve)
-                        : launch_invert_stream<float, KT, 3, false>(GS, sio, st, num_sms, smem_out, wpb, reserve);
+    if (multi) return launch_invert_stream<float, KT, 4, true, MAC>(GS, sio, st, num_sms, smem_out, wpb, reserve);
+    return variant == 1 ? launch_invert_stream<float, KT, 4, false, MAC>(GS, sio, st, num_sms, smem_out, wpb, reserve)
+                        : launch_invert_stream<float, KT, 3, false, MAC>(GS, sio, st, num_sms, smem_out, wpb, reserve);
   } else {
-    return multi ? launch_invert_stream<double, KT, 1, true>(GS, sio, st, num_sms, smem_out, wpb, reserve)
-                 : launch_invert_stream<double, KT, 1, false>(GS, sio, st, num_sms, smem_out, wpb, reserve);
+    return multi ? launch_invert_stream<double, KT, 1, true, MAC>(GS, sio, st, num_sms, smem_out, wpb, reserve)
+                 : launch_invert_stream<double, KT, 1, false, MAC>(GS, sio, st, num_sms, smem_out, wpb, reserve);
   }
+}
+
+template <typename R>
+int launch_stream_k(const PmGridSet& GS, const PmStreamIO& sio, cudaStream_t st, int num_sms, int variant, int wpb,
+                    bool multi, size_t* smem_out, int reserve, int K, bool mac) {
+  // NTERMS 9 never has a v_mac row and 11 always has one (milos.c:152-157)
+  if (K == 9) return launch_stream_any<R, 9, false>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve);
+  if (K == 10 && mac) return launch_stream_any<R, 10, true>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve);
+  if (K == 10) return launch_stream_any<R, 10, false>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve);
+  if (K == 11) return launch_stream_any<R, 11, true>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve);
+  snprintf(pmk_g_err, sizeof pmk_g_err, "nterms=%d has no compiled kernel", K);
+  return PM_ENOTSUP;
 }
 
 
@@ -213,15 +229,11 @@ int pmk_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, int precision,
       return PM_ENOTSUP;
     }
   }
-  if (precision == PM_PREC_FP32) {
-    if (K == 9) return launch_stream_any<float, 9>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve_blocks);
-    if (K == 10) return launch_stream_any<float, 10>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve_blocks);
-  } else {
-    if (K == 9) return launch_stream_any<double, 9>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve_blocks);
-    if (K == 10) return launch_stream_any<double, 10>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve_blocks);
-  }
-  snprintf(pmk_g_err, sizeof pmk_g_err, "nterms=%d has no compiled kernel", K);
-  return PM_ENOTSUP;
+  bool mac = false;
+  for (int g = 0; g < GS.ngrids; ++g) mac = mac || GS.g[g].mac_row >= 0;
+  if (precision == PM_PREC_FP32)
+    return launch_stream_k<float>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve_blocks, K, mac);
+  return launch_stream_k<double>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve_blocks, K, mac);
 }
 
 

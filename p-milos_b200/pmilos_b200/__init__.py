@@ -254,7 +254,10 @@ class Inverter:
     Mirrors the inputs lm_mils takes from the control file (.mtrol): weights,
     noise (sigma^2 = 1/SN^2), initial diagonal element, toplim, number of cycles,
     the fix[] switches (reference order eta0, B, vlos, dopp, aa, gm, az, S0, S1,
-    mac, alfa), NTERMS, the diagonal-acceleration switch and mu.
+    mac, alfa), NTERMS, the diagonal-acceleration switch and mu.  NTERMS
+    defaults to 11 - !fix[10] - !fix[9] (milos.c:152-157 with a zero guess
+    v_mac); give it explicitly (10 or 11) for guesses with v_mac fixed at a
+    nonzero value.
     """
 
     def __init__(self, line: LineData, lam, psf=None, *, weights=(1.0, 1.0, 1.0, 1.0), noise=1e-6, ilambda=0.1,
@@ -514,7 +517,9 @@ class Server:
             lam = np.ascontiguousarray(g.lam, dtype=np.float64)
             psf = None if g.psf is None else np.ascontiguousarray(g.psf, dtype=np.float64)
             fix = list(g.fix) if g.fix is not None else [1] * 9 + [0, 0]
-            nterms = g.nterms if g.nterms is not None else 11 - (0 if fix[10] else 1) - (0 if fix[9] else 1)
+            gmac = 0.0 if g.guess is None else float(np.asarray(g.guess, dtype=np.float64)[9])
+            nterms = g.nterms if g.nterms is not None else \
+                11 - (0 if fix[10] else 1) - (0 if (fix[9] or gmac != 0.0) else 1)
             c = _Config()
             c.nlambda = lam.size
             c.lambda_ = _dptr(lam)
