@@ -207,6 +207,23 @@ int pm_invert_batch(pm_ctx *ctx, int64_t npix, const float *spectro, const float
 int pm_synth_batch(pm_ctx *ctx, int64_t npix, const pm_model *models, const float *slight, int slight_mode,
                    float *spectra_out, float *rf_out, int mem);
 
+/* pm_invert_batch / pm_synth_batch with a wavelength grid per pixel: lambda is
+ * [npix][nlambda] absolute wavelengths [A] (float64, in the same memory as
+ * spectro / models).  The reference documents such grids as a 4-D wavelength
+ * FITS file for telecentric and collimated filter set-ups (README "Wavelength
+ * grid file (.fits)"); its reader does not load that form
+ * (readFitsLambdaToArray, utilsFits.c:749-833), so the definition here is: every
+ * pixel is inverted as the reference inverts a cube whose single grid is that
+ * pixel's -- synthesis, macroturbulence kernel and classical estimates on the
+ * pixel's own wavelengths, the context's PSF taps (sampled at the grid step)
+ * for every pixel.  Grids of at most 32 wavelengths (else PM_ENOTSUP); host
+ * buffers are copied in, then inverted (no pipelining). */
+int pm_invert_batch_grids(pm_ctx *ctx, int64_t npix, const float *spectro, const double *lambda,
+                          const float *slight, int slight_mode, const pm_model *guess, pm_model *models_out,
+                          float *chisq_out, int *iters_out, float *best_fit_out, int *status_out, int mem);
+int pm_synth_batch_grids(pm_ctx *ctx, int64_t npix, const pm_model *models, const double *lambda,
+                         const float *slight, int slight_mode, float *spectra_out, float *rf_out, int mem);
+
 /* Batch-of-one form of lm_mils for hosts that keep their per-pixel loop: inverts
  * spectro ([4][nlambda], host memory) starting from *init_model (updated in
  * place); spectra (nullable) gets the last synthesis, *chisqrf and *iter the

@@ -327,3 +327,29 @@ def reference_fits_read(path: str, nlambda: int, npix_cap: int):
         raise RuntimeError(f"reference reader failed ({rc})")
     n = rows.value * cols.value
     return out[: n * 4 * nlambda].reshape(n, 4, nlambda), rows.value, cols.value
+
+
+def reference_fits_straylight(path: str, cap: int = 1 << 20):
+    """readFitsStrayLightFile (oracle/_ref/libpmref_fits.so): (array, nl, ns, nx, ny)."""
+    lib = ctypes.CDLL(os.path.join(REF, "libpmref_fits.so"))
+    lib.pmref_fits_straylight.argtypes = [ctypes.c_char_p, _F, ctypes.c_longlong, _I, _I, _I, _I]
+    out = np.zeros(cap, dtype=np.float32)
+    nl, ns, nx, ny = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    rc = lib.pmref_fits_straylight(path.encode(), _f(out), out.size, ctypes.byref(nl), ctypes.byref(ns),
+                                   ctypes.byref(nx), ctypes.byref(ny))
+    if rc != 0:
+        raise RuntimeError(f"reference stray-light reader failed ({rc})")
+    n = nl.value * ns.value * (nx.value * ny.value if nx.value and ny.value else 1)
+    return out[:n].copy(), nl.value, ns.value, nx.value, ny.value
+
+
+def reference_fits_lambda(path: str, cap: int = 4096):
+    """readFitsLambdaToArray on a 2-D wavelength file: (index_line, lambda)."""
+    lib = ctypes.CDLL(os.path.join(REF, "libpmref_fits.so"))
+    lib.pmref_fits_lambda.argtypes = [ctypes.c_char_p, _D, ctypes.c_int, _I, _I]
+    out = np.zeros(cap)
+    idx, nl = ctypes.c_int(), ctypes.c_int()
+    rc = lib.pmref_fits_lambda(path.encode(), _d(out), cap, ctypes.byref(idx), ctypes.byref(nl))
+    if rc != 0:
+        raise RuntimeError(f"reference wavelength reader failed ({rc})")
+    return idx.value, out[:nl.value].copy()

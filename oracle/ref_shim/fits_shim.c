@@ -196,25 +196,40 @@ static float be_float(const unsigned char* b) {
   return x;
 }
 
+static double be_double(const unsigned char* b) {
+  uint64_t u = 0;
+  for (int i = 0; i < 8; ++i) u = (u << 8) | (uint64_t)b[i];
+  double x;
+  memcpy(&x, &u, 8);
+  return x;
+}
+
 int fits_read_pix(fitsfile* fptr, int datatype, long* fpixel, long nelements, void* nulval, void* array, int* anynul,
                   int* status) {
   (void)nulval;
   if (*status) return *status;
-  if (datatype != TFLOAT || fptr->bitpix != FLOAT_IMG) return *status = BAD_DATATYPE;
+  /* float32 or float64 pixels, converted to the requested float or double as
+   * CFITSIO converts them */
+  if ((datatype != TFLOAT && datatype != TDOUBLE) || (fptr->bitpix != FLOAT_IMG && fptr->bitpix != DOUBLE_IMG))
+    return *status = BAD_DATATYPE;
+  const int width = fptr->bitpix == FLOAT_IMG ? 4 : 8;
   long first = 0, stride = 1;
   for (int i = 0; i < fptr->naxis; ++i) {
     first += (fpixel[i] - 1) * stride;
     stride *= fptr->naxes[i];
   }
   if (first + nelements > stride) return *status = BAD_PIX_NUM;
-  unsigned char* raw = malloc((size_t)nelements * 4);
-  if (fseek(fptr->f, fptr->data_off + 4 * first, SEEK_SET) ||
-      fread(raw, 4, (size_t)nelements, fptr->f) != (size_t)nelements) {
+  unsigned char* raw = malloc((size_t)nelements * width);
+  if (fseek(fptr->f, fptr->data_off + width * first, SEEK_SET) ||
+      fread(raw, width, (size_t)nelements, fptr->f) != (size_t)nelements) {
     free(raw);
     return *status = READ_ERROR;
   }
-  float* out = array;
-  for (long i = 0; i < nelements; ++i) out[i] = be_float(raw + 4 * i);
+  for (long i = 0; i < nelements; ++i) {
+    const double v = width == 4 ? (double)be_float(raw + 4 * i) : be_double(raw + 8 * i);
+    if (datatype == TFLOAT) ((float*)array)[i] = (float)v;
+    else ((double*)array)[i] = v;
+  }
   free(raw);
   if (anynul) *anynul = 0;
   return 0;

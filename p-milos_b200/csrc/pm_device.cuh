@@ -406,11 +406,12 @@ constexpr int kMacSu = 0, kMacK = 4 * NL, kMacD = 7 * NL;
 static_assert(kMacD + 3 * NL <= 4 * XSR, "macroturbulence data exceed the padded rows");
 
 // Lane k's value of the kernel (and of its derivative with DERIV), through the
-// PSF; scratch: 64 doubles.
+// PSF; dl: lane k's wavelength offset lambda_k - lambda0; scratch: 64 doubles.
 template <bool DERIV>
-__device__ __forceinline__ void mac_kernel(const PmParams& P, double mac, int lane, bool valid, double* scratch,
-                                           double& g, double& gd) {
-  const double x = valid ? P.dl[lane] - P.dl[P.half] : 0.0;  // lambda_k - lambda[nl/2], exactly
+__device__ __forceinline__ void mac_kernel(const PmParams& P, double mac, double dl, int lane, bool valid,
+                                           double* scratch, double& g, double& gd) {
+  const double dlc = __shfl_sync(kFull, dl, P.half);
+  const double x = valid ? dl - dlc : 0.0;  // lambda_k - lambda[nl/2], exactly
   const double ild = (P.lambda0 * mac) / kVLight;
   const double a = x / ild;
   const double term = (a * a) / 2;
@@ -449,9 +450,10 @@ __device__ __forceinline__ void mac_triple(const PmParams& P, double k, int lane
 
 // The kernel of v_mac (and its derivative with DERIV) into xs; tr is scratch.
 template <typename R, bool DERIV>
-__device__ __forceinline__ void mac_prepare(const PmParams& P, WarpSmem<R>& sm, double mac, int lane, bool valid) {
+__device__ __forceinline__ void mac_prepare(const PmParams& P, WarpSmem<R>& sm, double mac, double dl, int lane,
+                                            bool valid) {
   double g, gd;
-  mac_kernel<DERIV>(P, mac, lane, valid, reinterpret_cast<double*>(sm.tr), g, gd);
+  mac_kernel<DERIV>(P, mac, dl, lane, valid, reinterpret_cast<double*>(sm.tr), g, gd);
   R* xf = &sm.xs[0][0];
   mac_triple<R>(P, g, lane, xf + kMacK);
   if (DERIV) mac_triple<R>(P, gd, lane, xf + kMacD);
@@ -511,14 +513,15 @@ __device__ __forceinline__ void xs_restore(WarpSmem<R>& sm, int lane) {
 // before the stray-light mix.  The per-model terms and this lane's synthesis
 // state are left in shared memory for the response functions, as the reference
 // leaves them in globals.  MAC: the kernel has a v_mac response row (NTERMS >=
-// 10), so v_mac may be nonzero.
+// 10), so v_mac may be nonzero.  dl: this lane's wavelength offset lambda -
+// lambda0 (the grid's, or the pixel's own).
 template <typename R, bool MAC = false>
 __device__ __forceinline__ void synthesize(const PmParams& P, WarpSmem<R>& sm, const double* m,
-                                           const float* sl_pix, int lane, bool valid, R S[4], R Su[4]) {
+                                           const float* sl_pix, int lane, bool valid, double dl, R S[4], R Su[4]) {
   ModelTerms<R> T;
   LaneState<R> st;
   model_terms<R>(P, m, T);
-  synth_lane<R>(P, T, P.dl[valid ? lane : 0], st, S);
+  synth_lane<R>(P, T, dl, st, S);
   copy16(*reinterpret_cast<LaneState<R>*>(sm.ls[lane]), st);
   if (lane == 0) copy16(sm.mt, T);
   const double mac = MAC ? m[9] : 0.0;
@@ -526,7 +529,7 @@ __device__ __forceinline__ void synthesize(const PmParams& P, WarpSmem<R>& sm, c
     R* xf = &sm.xs[0][0];
 #pragma unroll
     for (int s = 0; s < 4; ++s) xf[kMacSu + s * NL + lane] = valid ? S[s] : R(0);
-    mac_prepare<R, false>(P, sm, mac, lane, valid);
+    mac_prepare<R, false>(P, sm, mac, dl, lane, valid);
     R out[4];
     mac_circular4<R>(P, xf, xf + kMacK, lane, out);
 #pragma unroll
@@ -1087,9 +1090,9 @@ __device__ __forceinline__ void check_model(double* m) {
 // NaN fixes of the drivers (milos.c:976-983), in two halves around the sums over
 // wavelengths (accumulated in FP64): the terms at one wavelength w, between the
 // leading and trailing ghost wavelengths [begin, end), with Ic = I[end - 1] ...
-__device__ __forceinline__ void classical_terms(const PmParams& P, const float O[4], int w, bool valid, int begin,
-                                                int end, double Ic, double (&v)[10]) {
-  const double dl = valid ? P.dl[w] : 0.0;
+__device__ __forceinline__ void classical_terms(const PmParams& P, const float O[4], int w, double dlw, bool valid,
+                                                int begin, int end, double Ic, double (&v)[10]) {
+  const double dl = valid ? dlw : 0.0;  // lambda_w - lambda0
   const bool in = valid && w >= begin && w < end - 1;
   const bool iv = in && O[0] > -1.0f && O[3] > -1.0f;
   const double a = iv ? Ic - double(O[0] + O[3]) : 0.0;
@@ -1151,8 +1154,9 @@ __device__ __forceinline__ void classical_finish(const PmParams& P, const double
   if (isnan(m[6])) m[6] = 1;
 }
 
-// Classical estimates of a one-warp pixel (lane = wavelength).
-__device__ __forceinline__ void classical(const PmParams& P, const float O[4], int lane, bool valid, double* m) {
+// Classical estimates of a one-warp pixel (lane = wavelength, dl its offset).
+__device__ __forceinline__ void classical(const PmParams& P, const float O[4], int lane, bool valid, double dl,
+                                          double* m) {
   const int nl = P.nl;
   const unsigned neg = __ballot_sync(kFull, valid && O[0] < 0.0f);
   const unsigned validm = (nl >= 32) ? kFull : ((1u << nl) - 1u);
@@ -1163,7 +1167,7 @@ __device__ __forceinline__ void classical(const PmParams& P, const float O[4], i
   const int end = 32 - __clz(nonneg);  // one past the last non-negative
   const double Ic = __shfl_sync(kFull, double(O[0]), end - 1);
   double v[10];
-  classical_terms(P, O, lane, valid, begin, end, Ic, v);
+  classical_terms(P, O, lane, dl, valid, begin, end, Ic, v);
 #pragma unroll
   for (int i = 0; i < 10; ++i) v[i] = warp_sum(v[i]);
   classical_finish(P, v, m);
@@ -1176,10 +1180,10 @@ __device__ __forceinline__ void classical(const PmParams& P, const float O[4], i
 // macroturbulence branch (the grid has a v_mac row; NTERMS >= 10).
 template <typename R, int KT, bool MAC = (KT >= 10)>
 __device__ __forceinline__ void response_rows(const PmParams& P, const BlockSmem<R>& bs, WarpSmem<R>& sm, int lane,
-                                              bool valid, const double* m, const R Sff[4], const float* sl_pix,
-                                              R (&d)[KT][4]) {
+                                              bool valid, const double* m, double dl, const R Sff[4],
+                                              const float* sl_pix, R (&d)[KT][4]) {
   const bool mac_on = MAC && m[9] > kMacMin;
-  if (mac_on) mac_prepare<R, true>(P, sm, m[9], lane, valid);  // before tr fills up
+  if (mac_on) mac_prepare<R, true>(P, sm, m[9], dl, lane, valid);  // before tr fills up
   R alf;
   {
     ModelTerms<R> T;
@@ -1204,10 +1208,10 @@ __device__ __forceinline__ void response_rows(const PmParams& P, const BlockSmem
 // Response functions at the current synthesis -> alpha, beta in shared memory.
 template <typename R, int KT, bool MAC>
 __device__ __forceinline__ void rf_and_normal_eq(const PmParams& P, const BlockSmem<R>& bs, WarpSmem<R>& sm,
-                                                 int lane, bool valid, const R S[4], const R Sff[4],
+                                                 int lane, bool valid, double dl, const R S[4], const R Sff[4],
                                                  const float O[4], const R isig[4], const float* sl_pix) {
   R d[KT][4];
-  response_rows<R, KT, MAC>(P, bs, sm, lane, valid, sm.model, Sff, sl_pix, d);
+  response_rows<R, KT, MAC>(P, bs, sm, lane, valid, sm.model, dl, Sff, sl_pix, d);
 #pragma unroll
   for (int r = 0; r < KT; ++r)
     if (P.zero_row[r]) {
@@ -1238,7 +1242,10 @@ __device__ __forceinline__ T* ld_ptr(T* const* p) {
 // pointers are read from shared memory and the descriptor where they are used,
 // so that none of them occupies registers across the LM loop.
 // MAC: compiled with the macroturbulence branch (grids with a v_mac row).
-template <typename R, int KT, bool MAC>
+// PIXGRID: the pixel has its own wavelengths (the job's lambda, [npix][nl]),
+// kept in a register; otherwise the grid's offsets are read from the
+// parameter block where they are used.
+template <typename R, int KT, bool MAC, bool PIXGRID>
 __device__ __forceinline__ void invert_pixel(const PmParams& P, const BlockSmem<R>& bs, WarpSmem<R>& sm, int lane,
                                              unsigned long long* ctr) {
   const bool valid = lane < P.nl;
@@ -1254,6 +1261,12 @@ __device__ __forceinline__ void invert_pixel(const PmParams& P, const BlockSmem<
   }
   const float* obs = ld_ptr(&jp->spectro) + base;
   const double* model_in = ld_ptr(&jp->model_in);
+  double dlp = 0.0;
+  if constexpr (PIXGRID) dlp = valid ? __ldcg(ld_ptr(&jp->lambda) + p * P.nl + lane) - P.lambda0 : 0.0;
+  auto dl = [&]() -> double {
+    if constexpr (PIXGRID) return dlp;
+    else return P.dl[valid ? lane : 0];
+  };
 
   float O[4];
   R isig[4];
@@ -1271,7 +1284,7 @@ __device__ __forceinline__ void invert_pixel(const PmParams& P, const BlockSmem<
     double g[11];
 #pragma unroll
     for (int i = 0; i < 11; ++i) g[i] = P.guess[i];
-    if (P.classical) classical(P, O, lane, valid, g);
+    if (P.classical) classical(P, O, lane, valid, dl(), g);
     double mine = g[0];
 #pragma unroll
     for (int i = 1; i < 11; ++i)
@@ -1292,8 +1305,8 @@ __device__ __forceinline__ void invert_pixel(const PmParams& P, const BlockSmem<
   } else {
     {
       R Su[4];
-      synthesize<R, MAC>(P, sm, m, sl_pix, lane, valid, S, Su);
-      rf_and_normal_eq<R, KT, MAC>(P, bs, sm, lane, valid, S, Su, O, isig, sl_pix);
+      synthesize<R, MAC>(P, sm, m, sl_pix, lane, valid, dl(), S, Su);
+      rf_and_normal_eq<R, KT, MAC>(P, bs, sm, lane, valid, dl(), S, Su, O, isig, sl_pix);
     }
     ochi = chisq<R>(P, S, O, isig, valid, double(nfree));
     const double chi0 = ochi;
@@ -1327,7 +1340,7 @@ __device__ __forceinline__ void invert_pixel(const PmParams& P, const BlockSmem<
         __syncwarp();
       }
       R Su[4];
-      synthesize<R, MAC>(P, sm, trial, sl_pix, lane, valid, S, Su);
+      synthesize<R, MAC>(P, sm, trial, sl_pix, lane, valid, dl(), S, Su);
       const double chi = chisq<R>(P, S, O, isig, valid, double(nfree));
       if ((fabs((ochi - chi) * 100 / chi) < P.toplim) || (chi < 0.0001)) {
         stop = true;
@@ -1337,7 +1350,7 @@ __device__ __forceinline__ void invert_pixel(const PmParams& P, const BlockSmem<
         flambda = flambda / (5.0 * factor);
         if (lane < 11) m[lane] = trial[lane];
         __syncwarp();
-        rf_and_normal_eq<R, KT, MAC>(P, bs, sm, lane, valid, S, S, O, isig, sl_pix);
+        rf_and_normal_eq<R, KT, MAC>(P, bs, sm, lane, valid, dl(), S, S, O, isig, sl_pix);
         ochi = chi;
         ++accepted;
       } else {

@@ -108,7 +108,7 @@ struct pm_ctx {
   int num_sms = 148;
   cudaStream_t stream = nullptr;
   size_t resident_bytes = size_t(8) << 30;  // device staging of one host-mode chunk
-  DevBuf spectro, slight, models, chisq, iters, spectra, status, rf, ctr;
+  DevBuf spectro, slight, models, chisq, iters, spectra, status, rf, ctr, lambda;
   // streamed host-buffer calls: kernel and copy streams, the ticket queue, one job
   cudaStream_t s_kern = nullptr, s_copy = nullptr;
   cudaEvent_t ev_start = nullptr, ev_q = nullptr, ev_done = nullptr, t0 = nullptr, t1 = nullptr, k0 = nullptr,
@@ -761,6 +761,7 @@ int run_invert(pm_ctx* c, PmIO io, float* kernel_ms) {
   job.status = io.status_out;
   job.spectra = io.spectra_out;
   job.model_in = c->P.classical ? io.models_out : nullptr;  // written by the pre-pass below
+  job.lambda = io.lambda_pix;
   std::memset(&hc->qinit, 0, sizeof hc->qinit);
   hc->qinit.avail = (unsigned long long)io.npix;
   hc->qinit.closed = 1;
@@ -777,11 +778,11 @@ int run_invert(pm_ctx* c, PmIO io, float* kernel_ms) {
   sio.wait_limit_ns = 20000000000LL;
   PM_CUDA(cudaEventRecord(c->k0, c->stream), "event");
   if (c->P.classical) {
-    rc = pmk_classical_prepass(c->P, io.spectro, io.models_out, io.npix, c->stream, c->num_sms);
+    rc = pmk_classical_prepass(c->P, io.spectro, io.models_out, io.npix, c->stream, c->num_sms, io.lambda_pix);
     if (rc != PM_OK) return fail(rc, "%s", pmk_last_cuda_error());
   }
   rc = pmk_invert_stream(*c->gs, sio, c->precision, c->tuning.variant, c->tuning.warps_per_block, false, c->stream,
-                         c->num_sms, nullptr);
+                         c->num_sms, nullptr, 0, io.lambda_pix != nullptr);
   if (rc != PM_OK) return fail(rc, "%s", pmk_last_cuda_error());
   PM_CUDA(cudaEventRecord(c->k1, c->stream), "event");
   PM_CUDA(cudaMemcpyAsync(&hc->qread, q, sizeof(PmStreamQ), cudaMemcpyDeviceToHost, c->stream), "queue D2H");
@@ -799,13 +800,19 @@ int run_invert(pm_ctx* c, PmIO io, float* kernel_ms) {
 
 }  // namespace
 
-extern "C" int pm_invert_batch(pm_ctx* c, int64_t npix, const float* spectro, const float* slight, int slight_mode,
-                               const pm_model* guess, pm_model* models_out, float* chisq_out, int* iters_out,
-                               float* best_fit_out, int* status_out, int mem) {
+namespace {
+
+// pm_invert_batch and pm_invert_batch_grids (lambda: per-pixel wavelengths or
+// nullptr).
+int invert_impl(pm_ctx* c, int64_t npix, const float* spectro, const double* lambda, const float* slight,
+                int slight_mode, const pm_model* guess, pm_model* models_out, float* chisq_out, int* iters_out,
+                float* best_fit_out, int* status_out, int mem) {
   if (!c || !spectro || !guess || !models_out || !chisq_out || !iters_out)
     return fail(PM_EINVAL, "pm_invert_batch: NULL argument");
   if (npix < 0) return fail(PM_EINVAL, "pm_invert_batch: npix < 0");
   if (mem != PM_MEM_HOST && mem != PM_MEM_DEVICE) return fail(PM_EINVAL, "pm_invert_batch: mem=%d", mem);
+  if (lambda && c->P.G != 1)
+    return fail(PM_ENOTSUP, "pixel wavelength grids: grids of at most 32 wavelengths (nlambda=%d)", c->P.nl);
   if (int rc = check_guess(c->P, guess); rc != PM_OK) return rc;
   c->stats = pm_stats{};
   if (npix == 0) return PM_OK;
@@ -830,15 +837,17 @@ extern "C" int pm_invert_batch(pm_ctx* c, int64_t npix, const float* spectro, co
     io.spectra_out = best_fit_out;
     io.status_out = status_out;
     io.ctr = static_cast<unsigned long long*>(c->ctr.p);
+    io.lambda_pix = lambda;
     rc = run_invert(c, io, &kms_total);
-  } else if (c->P.G == 1 && c->tuning.graphs && npix <= PM_GRAPH_MAX_PIXELS) {
+  } else if (!lambda && c->P.G == 1 && c->tuning.graphs && npix <= PM_GRAPH_MAX_PIXELS) {
     rc = run_graph_small(c, npix, spectro, slight, slight_mode, models_out, chisq_out, iters_out, best_fit_out,
                          status_out);
     kms_total = float(c->stats.kernel_ms);
   } else {
     // pixels per resident chunk: the device copies of one chunk's inputs and outputs fit resident_bytes
+    const size_t lam_bytes = lambda ? sizeof(double) * nl : 0;  // per pixel
     const size_t per_pixel = prof * (1 + (slight_mode == PM_SLIGHT_PER_PIXEL) + (best_fit_out != nullptr)) +
-                             sizeof(pm_model) + sizeof(float) + 2 * sizeof(int);
+                             sizeof(pm_model) + sizeof(float) + 2 * sizeof(int) + lam_bytes;
     const int64_t chunk = std::min<int64_t>(npix, std::max<int64_t>(32, int64_t(c->resident_bytes / per_pixel)));
     if ((rc = c->spectro.ensure(prof * chunk)) != PM_OK) return rc;
     if (slight_mode == PM_SLIGHT_PER_PIXEL && (rc = c->slight.ensure(prof * chunk)) != PM_OK) return rc;
@@ -847,8 +856,10 @@ extern "C" int pm_invert_batch(pm_ctx* c, int64_t npix, const float* spectro, co
     if ((rc = c->iters.ensure(sizeof(int) * chunk)) != PM_OK) return rc;
     if (best_fit_out && (rc = c->spectra.ensure(prof * chunk)) != PM_OK) return rc;
     if (status_out && (rc = c->status.ensure(sizeof(int) * chunk)) != PM_OK) return rc;
+    if (lambda && (rc = c->lambda.ensure(lam_bytes * chunk)) != PM_OK) return rc;
     pm_stats acc{};
-    const bool streamed = c->P.G == 1 && c->tuning.staging_depth > 0;
+    // per-pixel grids take the copy-then-launch path
+    const bool streamed = !lambda && c->P.G == 1 && c->tuning.staging_depth > 0;
     for (int64_t p0 = 0; p0 < npix && rc == PM_OK && streamed; p0 += chunk) {
       const int64_t n = std::min(chunk, npix - p0);
       float kms = 0, tms = 0;
@@ -865,6 +876,9 @@ extern "C" int pm_invert_batch(pm_ctx* c, int64_t npix, const float* spectro, co
       if (slight_mode == PM_SLIGHT_PER_PIXEL)
         PM_CUDA(cudaMemcpyAsync(c->slight.p, slight + p0 * 4 * nl, prof * n, cudaMemcpyHostToDevice, c->stream),
                 "slight H2D");
+      if (lambda)
+        PM_CUDA(cudaMemcpyAsync(c->lambda.p, lambda + p0 * nl, lam_bytes * n, cudaMemcpyHostToDevice, c->stream),
+                "lambda H2D");
       PmIO io{};
       io.npix = n;
       io.spectro = static_cast<const float*>(c->spectro.p);
@@ -875,6 +889,7 @@ extern "C" int pm_invert_batch(pm_ctx* c, int64_t npix, const float* spectro, co
       io.spectra_out = best_fit_out ? static_cast<float*>(c->spectra.p) : nullptr;
       io.status_out = status_out ? static_cast<int*>(c->status.p) : nullptr;
       io.ctr = static_cast<unsigned long long*>(c->ctr.p);
+      io.lambda_pix = lambda ? static_cast<const double*>(c->lambda.p) : nullptr;
       float kms = 0;
       rc = run_invert(c, io, &kms);
       if (rc != PM_OK) break;
@@ -915,9 +930,31 @@ extern "C" int pm_invert_batch(pm_ctx* c, int64_t npix, const float* spectro, co
   return rc;
 }
 
-extern "C" int pm_synth_batch(pm_ctx* c, int64_t npix, const pm_model* models, const float* slight,
-                              int slight_mode, float* spectra_out, float* rf_out, int mem) {
+}  // namespace
+
+extern "C" int pm_invert_batch(pm_ctx* c, int64_t npix, const float* spectro, const float* slight, int slight_mode,
+                               const pm_model* guess, pm_model* models_out, float* chisq_out, int* iters_out,
+                               float* best_fit_out, int* status_out, int mem) {
+  return invert_impl(c, npix, spectro, nullptr, slight, slight_mode, guess, models_out, chisq_out, iters_out,
+                     best_fit_out, status_out, mem);
+}
+
+extern "C" int pm_invert_batch_grids(pm_ctx* c, int64_t npix, const float* spectro, const double* lambda,
+                                     const float* slight, int slight_mode, const pm_model* guess,
+                                     pm_model* models_out, float* chisq_out, int* iters_out, float* best_fit_out,
+                                     int* status_out, int mem) {
+  if (!lambda) return fail(PM_EINVAL, "pm_invert_batch_grids: lambda is NULL");
+  return invert_impl(c, npix, spectro, lambda, slight, slight_mode, guess, models_out, chisq_out, iters_out,
+                     best_fit_out, status_out, mem);
+}
+
+namespace {
+
+int synth_impl(pm_ctx* c, int64_t npix, const pm_model* models, const double* lambda, const float* slight,
+               int slight_mode, float* spectra_out, float* rf_out, int mem) {
   if (!c || !models || !spectra_out) return fail(PM_EINVAL, "pm_synth_batch: NULL argument");
+  if (lambda && c->P.G != 1)
+    return fail(PM_ENOTSUP, "pixel wavelength grids: grids of at most 32 wavelengths (nlambda=%d)", c->P.nl);
   if (npix < 0) return fail(PM_EINVAL, "pm_synth_batch: npix < 0");
   if (mem != PM_MEM_HOST && mem != PM_MEM_DEVICE) return fail(PM_EINVAL, "pm_synth_batch: mem=%d", mem);
   if (npix == 0) return PM_OK;
@@ -932,6 +969,7 @@ extern "C" int pm_synth_batch(pm_ctx* c, int64_t npix, const pm_model* models, c
     io.slight = slight_mode == PM_SLIGHT_PER_PIXEL ? slight : nullptr;
     io.spectra_out = spectra_out;
     io.rf_out = rf_out;
+    io.lambda_pix = lambda;
     rc = pmk_synth(c->P, io, c->precision, c->stream);
     if (rc != PM_OK) return fail(rc, "%s", pmk_last_cuda_error());
     PM_CUDA(cudaStreamSynchronize(c->stream), "synth kernel");
@@ -941,8 +979,13 @@ extern "C" int pm_synth_batch(pm_ctx* c, int64_t npix, const pm_model* models, c
   if ((rc = c->spectra.ensure(prof * npix)) != PM_OK) return rc;
   if (rf_out && (rc = c->rf.ensure(prof * K * npix)) != PM_OK) return rc;
   if (slight_mode == PM_SLIGHT_PER_PIXEL && (rc = c->slight.ensure(prof * npix)) != PM_OK) return rc;
+  if (lambda && (rc = c->lambda.ensure(sizeof(double) * nl * npix)) != PM_OK) return rc;
   PM_CUDA(cudaMemcpyAsync(c->models.p, models, sizeof(pm_model) * npix, cudaMemcpyHostToDevice, c->stream),
           "models H2D");
+  if (lambda)
+    PM_CUDA(cudaMemcpyAsync(c->lambda.p, lambda, sizeof(double) * nl * npix, cudaMemcpyHostToDevice, c->stream),
+            "lambda H2D");
+  io.lambda_pix = lambda ? static_cast<const double*>(c->lambda.p) : nullptr;
   if (slight_mode == PM_SLIGHT_PER_PIXEL)
     PM_CUDA(cudaMemcpyAsync(c->slight.p, slight, prof * npix, cudaMemcpyHostToDevice, c->stream), "slight H2D");
   io.models_in = static_cast<const double*>(c->models.p);
@@ -956,6 +999,20 @@ extern "C" int pm_synth_batch(pm_ctx* c, int64_t npix, const pm_model* models, c
     PM_CUDA(cudaMemcpyAsync(rf_out, c->rf.p, prof * K * npix, cudaMemcpyDeviceToHost, c->stream), "rf D2H");
   PM_CUDA(cudaStreamSynchronize(c->stream), "synth kernel");
   return PM_OK;
+}
+
+}  // namespace
+
+extern "C" int pm_synth_batch(pm_ctx* c, int64_t npix, const pm_model* models, const float* slight,
+                              int slight_mode, float* spectra_out, float* rf_out, int mem) {
+  return synth_impl(c, npix, models, nullptr, slight, slight_mode, spectra_out, rf_out, mem);
+}
+
+extern "C" int pm_synth_batch_grids(pm_ctx* c, int64_t npix, const pm_model* models, const double* lambda,
+                                    const float* slight, int slight_mode, float* spectra_out, float* rf_out,
+                                    int mem) {
+  if (!lambda) return fail(PM_EINVAL, "pm_synth_batch_grids: lambda is NULL");
+  return synth_impl(c, npix, models, lambda, slight, slight_mode, spectra_out, rf_out, mem);
 }
 
 extern "C" int pm_lm_mils(pm_ctx* c, const float* spectro, pm_model* init_model, float* spectra, float* chisqrf,

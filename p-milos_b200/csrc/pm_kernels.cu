@@ -24,15 +24,16 @@ __global__ void __launch_bounds__(128) synth_kernel(const __grid_constant__ PmPa
     const float* sl_pix = (P.slight_mode == PM_SLIGHT_PER_PIXEL) ? io.slight + base : nullptr;
     if (lane < 11) sm.model[lane] = io.models_in[size_t(pix) * 11 + lane];
     __syncwarp();
+    const double dl = !valid ? 0.0 : (io.lambda_pix ? io.lambda_pix[size_t(pix) * P.nl + lane] - P.lambda0 : P.dl[lane]);
     R S[4], Su[4];
-    synthesize<R, (KT >= 10)>(P, sm, sm.model, sl_pix, lane, valid, S, Su);
+    synthesize<R, (KT >= 10)>(P, sm, sm.model, sl_pix, lane, valid, dl, S, Su);
     if (valid) {
 #pragma unroll
       for (int s = 0; s < 4; ++s) io.spectra_out[base + s * P.nl + lane] = float(S[s]);
     }
     if (io.rf_out) {
       R d[KT][4];
-      response_rows<R, KT>(P, bs, sm, lane, valid, sm.model, Su, sl_pix, d);
+      response_rows<R, KT>(P, bs, sm, lane, valid, sm.model, dl, Su, sl_pix, d);
       __syncwarp();
       if (valid) {
         const size_t rb = size_t(pix) * 4 * KT * P.nl;

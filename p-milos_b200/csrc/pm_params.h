@@ -87,6 +87,7 @@ struct PmJob {
   unsigned long long* done; // device counter of finished pixels (zeroed before publication), nullable
   int* host_flag;           // mapped host word set to 1 when the last pixel is done, nullable
   const double* model_in;   // [npix][11] starting models of the classical pre-pass, nullable
+  const double* lambda;     // [npix][nl] absolute wavelengths of each pixel (pixel grids), else nullptr
 };
 
 static_assert(sizeof(PmGridSet) + 64 <= 32764, "kernel parameter block of the streamed kernel exceeds 32 KB");
@@ -112,6 +113,7 @@ struct PmIO {
   float* rf_out;            // synth kernel: [npix][4][K][nl] (nullable)
   int* status_out;          // [npix] (nullable)
   unsigned long long* ctr;  // PMC_COUNT counters
+  const double* lambda_pix; // [npix][nl] absolute wavelengths of each pixel (nullable: the grid's)
 };
 
 // Kernel variants compiled into the library.
@@ -125,15 +127,18 @@ int pmk_invert_wide(const PmParams& P, const PmIO& io, int precision, void* stre
 int pmk_synth_wide(const PmParams& P, const PmIO& io, int precision, void* stream);
 // Classical estimates of npix pixels (one-warp grid) into models [npix][11]:
 // the starting models of a launch whose cube is on the device before it starts.
+// lambda: [npix][nl] absolute wavelengths of each pixel, or nullptr (the grid's).
 int pmk_classical_prepass(const PmParams& P, const float* spectro, double* models, int64_t npix, void* stream,
-                          int num_sms);
+                          int num_sms, const double* lambda = nullptr);
 // Streamed inversion: every grid of GS has the same nterms and nl <= 32.
 // multi: grids differ between jobs (dynamic grid index) rather than one grid.
 // reserve_blocks: launch that many fewer blocks than fit, leaving room on the
 // SMs for short kernels (the classical pre-pass of newly admitted scans) to run
-// beside the persistent kernel.
+// beside the persistent kernel.  pixgrid: the jobs carry per-pixel wavelengths
+// (PmJob::lambda; one grid, not multi).
 int pmk_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, int precision, int variant, int warps_per_block,
-                      bool multi, void* stream, int num_sms, size_t* smem_out, int reserve_blocks = 0);
+                      bool multi, void* stream, int num_sms, size_t* smem_out, int reserve_blocks = 0,
+                      bool pixgrid = false);
 const char* pmk_last_cuda_error();
 
 // Host helpers (pm_host.cpp) shared with pm_noalloc.cu.

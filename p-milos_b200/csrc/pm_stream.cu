@@ -59,7 +59,7 @@ struct GridParams {
   PmParams g[NG];
 };
 
-template <typename R, int KT, int MINB, bool MULTI, bool MAC>
+template <typename R, int KT, int MINB, bool MULTI, bool MAC, bool PIXGRID>
 __global__ void __launch_bounds__(128, MINB) invert_stream_kernel(
     const __grid_constant__ GridParams<MULTI ? PMK_MAX_GRIDS : 1> GS, const PmStreamIO sio) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(128, MINB) invert_stream_kernel(
       sm.pix = (unsigned long long)t - t0;
     }
     __syncwarp();
-    invert_pixel<R, KT, MAC>(P, bs[gi], sm, lane, sio.q->ctr);
+    invert_pixel<R, KT, MAC, PIXGRID>(P, bs[gi], sm, lane, sio.q->ctr);
     jp = *reinterpret_cast<const PmJob* const volatile*>(&sm.job);
     unsigned long long* done = ld_ptr(&jp->done);
     if (done) {
@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(128, MINB) invert_stream_kernel(
 // kernel when the cube is on the device before the launch.
 __global__ void __launch_bounds__(256) classical_prepass_kernel(const __grid_constant__ PmParams P,
                                                                 const float* spectro, double* models,
-                                                                long long npix) {
+                                                                long long npix, const double* lambda) {
   const int lane = threadIdx.x & 31;
   const bool valid = lane < P.nl;
   const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
@@ -149,10 +149,11 @@ __global__ void __launch_bounds__(256) classical_prepass_kernel(const __grid_con
     float O[4];
 #pragma unroll
     for (int s = 0; s < 4; ++s) O[s] = valid ? spectro[base + s * P.nl + lane] : 0.0f;
+    const double dl = !valid ? 0.0 : (lambda ? lambda[size_t(pix) * P.nl + lane] - P.lambda0 : P.dl[lane]);
     double g[11];
 #pragma unroll
     for (int i = 0; i < 11; ++i) g[i] = P.guess[i];
-    classical(P, O, lane, valid, g);
+    classical(P, O, lane, valid, dl, g);
     double mine = g[0];
 #pragma unroll
     for (int i = 1; i < 11; ++i)
@@ -161,13 +162,13 @@ __global__ void __launch_bounds__(256) classical_prepass_kernel(const __grid_con
   }
 }
 
-template <typename R, int KT, int MINB, bool MULTI, bool MAC>
+template <typename R, int KT, int MINB, bool MULTI, bool MAC, bool PIXGRID = false>
 int launch_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, cudaStream_t st, int num_sms,
                          size_t* smem_out, int wpb, int reserve) {
   const int threads = 32 * wpb;
   const size_t smem = (MULTI ? PMK_MAX_GRIDS : 1) * sizeof(BlockSmem<R>) + sizeof(WarpSmem<R>) * (threads / 32);
   if (smem_out) *smem_out = smem;
-  auto kern = invert_stream_kernel<R, KT, MINB, MULTI, MAC>;
+  auto kern = invert_stream_kernel<R, KT, MINB, MULTI, MAC, PIXGRID>;
   constexpr int NG = MULTI ? PMK_MAX_GRIDS : 1;
   GridParams<NG> gp;  // copied into the launch
   gp.ngrids = GS.ngrids < NG ? GS.ngrids : NG;
@@ -185,9 +186,20 @@ int launch_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, cudaStream_
 }
 
 // MAC: the macroturbulence branch compiled in (a grid with a v_mac row).
+// pixgrid: per-pixel wavelengths (single-grid launches only).
 template <typename R, int KT, bool MAC>
 int launch_stream_any(const PmGridSet& GS, const PmStreamIO& sio, cudaStream_t st, int num_sms, int variant,
-                      int wpb, bool multi, size_t* smem_out, int reserve) {
+                      int wpb, bool multi, size_t* smem_out, int reserve, bool pixgrid) {
+  if (pixgrid) {
+    if (multi) return snprintf(pmk_g_err, sizeof pmk_g_err, "pixel grids: single-grid launches only"), PM_EINVAL;
+    if constexpr (sizeof(R) == 4) {
+      return variant == 1
+                 ? launch_invert_stream<float, KT, 4, false, MAC, true>(GS, sio, st, num_sms, smem_out, wpb, reserve)
+                 : launch_invert_stream<float, KT, 3, false, MAC, true>(GS, sio, st, num_sms, smem_out, wpb, reserve);
+    } else {
+      return launch_invert_stream<double, KT, 1, false, MAC, true>(GS, sio, st, num_sms, smem_out, wpb, reserve);
+    }
+  }
   if constexpr (sizeof(R) == 4) {
     if (multi) return launch_invert_stream<float, KT, 4, true, MAC>(GS, sio, st, num_sms, smem_out, wpb, reserve);
     return variant == 1 ? launch_invert_stream<float, KT, 4, false, MAC>(GS, sio, st, num_sms, smem_out, wpb, reserve)
@@ -200,12 +212,13 @@ int launch_stream_any(const PmGridSet& GS, const PmStreamIO& sio, cudaStream_t s
 
 template <typename R>
 int launch_stream_k(const PmGridSet& GS, const PmStreamIO& sio, cudaStream_t st, int num_sms, int variant, int wpb,
-                    bool multi, size_t* smem_out, int reserve, int K, bool mac) {
+                    bool multi, size_t* smem_out, int reserve, int K, bool mac, bool pg) {
   // NTERMS 9 never has a v_mac row and 11 always has one (milos.c:152-157)
-  if (K == 9) return launch_stream_any<R, 9, false>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve);
-  if (K == 10 && mac) return launch_stream_any<R, 10, true>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve);
-  if (K == 10) return launch_stream_any<R, 10, false>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve);
-  if (K == 11) return launch_stream_any<R, 11, true>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve);
+  if (K == 9) return launch_stream_any<R, 9, false>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve, pg);
+  if (K == 10 && mac)
+    return launch_stream_any<R, 10, true>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve, pg);
+  if (K == 10) return launch_stream_any<R, 10, false>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve, pg);
+  if (K == 11) return launch_stream_any<R, 11, true>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve, pg);
   snprintf(pmk_g_err, sizeof pmk_g_err, "nterms=%d has no compiled kernel", K);
   return PM_ENOTSUP;
 }
@@ -214,7 +227,7 @@ int launch_stream_k(const PmGridSet& GS, const PmStreamIO& sio, cudaStream_t st,
 }  // namespace
 
 int pmk_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, int precision, int variant, int warps_per_block,
-                      bool multi, void* stream, int num_sms, size_t* smem_out, int reserve_blocks) {
+                      bool multi, void* stream, int num_sms, size_t* smem_out, int reserve_blocks, bool pixgrid) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int wpb = (warps_per_block == 1 || warps_per_block == 2) ? warps_per_block : 4;
   if (GS.ngrids < 1 || GS.ngrids > PMK_MAX_GRIDS || (!multi && GS.ngrids != 1)) {
@@ -232,13 +245,13 @@ int pmk_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, int precision,
   bool mac = false;
   for (int g = 0; g < GS.ngrids; ++g) mac = mac || GS.g[g].mac_row >= 0;
   if (precision == PM_PREC_FP32)
-    return launch_stream_k<float>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve_blocks, K, mac);
-  return launch_stream_k<double>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve_blocks, K, mac);
+    return launch_stream_k<float>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve_blocks, K, mac, pixgrid);
+  return launch_stream_k<double>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve_blocks, K, mac, pixgrid);
 }
 
 
 int pmk_classical_prepass(const PmParams& P, const float* spectro, double* models, int64_t npix, void* stream,
-                          int num_sms) {
+                          int num_sms, const double* lambda) {
   if (P.G != 1) {
     snprintf(pmk_g_err, sizeof pmk_g_err, "classical pre-pass: one-warp grids only");
     return PM_EINVAL;
@@ -246,7 +259,7 @@ int pmk_classical_prepass(const PmParams& P, const float* spectro, double* model
   long long blocks = (npix + 7) / 8;
   if (blocks > (long long)num_sms * 16) blocks = (long long)num_sms * 16;
   if (blocks < 1) blocks = 1;
-  classical_prepass_kernel<<<unsigned(blocks), 256, 0, static_cast<cudaStream_t>(stream)>>>(P, spectro, models, npix);
+  classical_prepass_kernel<<<unsigned(blocks), 256, 0, static_cast<cudaStream_t>(stream)>>>(P, spectro, models, npix, lambda);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return snprintf(pmk_g_err, sizeof pmk_g_err, "classical launch: %s", cudaGetErrorString(e)), PM_EIO;
   return PM_OK;

@@ -461,7 +461,7 @@ __global__ void __launch_bounds__(32 * G) classical_wide_kernel(const __grid_con
     double v[10];
     if (begin >= 0) {
       const double Ic = double(io.spectro[base + end - 1]);
-      classical_terms(P, O, t, valid, begin, end, Ic, v);
+      classical_terms(P, O, t, P.dl[valid ? t : 0], valid, begin, end, Ic, v);
       block_sum<G, STR>(red, slot, v);
     }
     if (t < 11) {

@@ -55,7 +55,8 @@ EXPORTED_SYMBOLS = (
     "pm_invert_batch", "pm_synth_batch", "pm_lm_mils", "pm_invert_batch_noalloc", "pm_get_stats", "pm_last_error",
     "pm_abi_version", "pm_get_tuning", "pm_set_tuning", "pm_autotune", "pm_server_create", "pm_server_submit",
     "pm_server_wait", "pm_server_get_stats", "pm_server_destroy", "pm_selftest_stalled_queue",
-    "pm_fits_parse_header", "pm_fits_reorder", "pm_server_submit_device",
+    "pm_fits_parse_header", "pm_fits_reorder", "pm_server_submit_device", "pm_invert_batch_grids",
+    "pm_synth_batch_grids",
 )
 SERVER_MAX_GRIDS = 4
 SERVER_MAX_INFLIGHT = 256
@@ -151,6 +152,9 @@ def load_library(path: str | None = None):
     L.pm_invert_batch.argtypes = [vp, i64, F, F, ctypes.c_int, ctypes.POINTER(_Model), vp, vp, vp, vp, vp,
                                   ctypes.c_int]
     L.pm_synth_batch.argtypes = [vp, i64, vp, F, ctypes.c_int, vp, vp, ctypes.c_int]
+    L.pm_invert_batch_grids.argtypes = [vp, i64, F, vp, F, ctypes.c_int, ctypes.POINTER(_Model), vp, vp, vp, vp, vp,
+                                        ctypes.c_int]
+    L.pm_synth_batch_grids.argtypes = [vp, i64, vp, vp, F, ctypes.c_int, vp, vp, ctypes.c_int]
     L.pm_lm_mils.argtypes = [vp, F, ctypes.POINTER(_Model), vp, ctypes.POINTER(ctypes.c_float), F,
                              ctypes.POINTER(ctypes.c_int)]
     L.pm_invert_batch_noalloc.argtypes = [ctypes.POINTER(_Line), ctypes.POINTER(_Config), i64, F, F, ctypes.c_int,
@@ -302,13 +306,20 @@ class Inverter:
         self.close()
 
     # ---- batched inversion ----
-    def invert(self, spectro, guess, *, slight=None, slight_mode=None, want_spectra=True, want_status=True):
+    def invert(self, spectro, guess, *, slight=None, slight_mode=None, want_spectra=True, want_status=True,
+               lam=None):
         """Invert [npix][4][nl] float32 profiles.  numpy in -> numpy out (host staging);
-        torch CUDA in -> torch CUDA out (no copies)."""
+        torch CUDA in -> torch CUDA out (no copies).  lam: [npix][nl] absolute
+        wavelengths of each pixel (pm_invert_batch_grids) instead of the grid."""
         if _is_torch(spectro):
-            return self._invert_device(spectro, guess, slight, slight_mode, want_spectra, want_status)
+            return self._invert_device(spectro, guess, slight, slight_mode, want_spectra, want_status, lam)
         obs = np.ascontiguousarray(spectro, dtype=np.float32).reshape(-1, 4, self.nl)
         npix = obs.shape[0]
+        lamp = None
+        if lam is not None:
+            lamp = np.ascontiguousarray(lam, dtype=np.float64)
+            if lamp.size != npix * self.nl:
+                raise ValueError("per-pixel wavelengths must be [npix][nl]")
         sl, mode = self._slight_host(slight, slight_mode, npix)
         models = np.zeros((npix, 11), dtype=np.float64)
         chi = np.zeros(npix, dtype=np.float32)
@@ -316,10 +327,13 @@ class Inverter:
         sp = np.zeros((npix, 4, self.nl), dtype=np.float32) if want_spectra else None
         stt = np.zeros(npix, dtype=np.int32) if want_status else None
         g = _model_struct(guess)
-        _check(self.L.pm_invert_batch(self.ctx, npix, obs.ctypes.data, None if sl is None else sl.ctypes.data, mode,
-                                      ctypes.byref(g), models.ctypes.data, chi.ctypes.data, its.ctypes.data,
-                                      None if sp is None else sp.ctypes.data,
-                                      None if stt is None else stt.ctypes.data, MEM_HOST))
+        outs = (ctypes.byref(g), models.ctypes.data, chi.ctypes.data, its.ctypes.data,
+                None if sp is None else sp.ctypes.data, None if stt is None else stt.ctypes.data, MEM_HOST)
+        slp = None if sl is None else sl.ctypes.data
+        if lamp is None:
+            _check(self.L.pm_invert_batch(self.ctx, npix, obs.ctypes.data, slp, mode, *outs))
+        else:
+            _check(self.L.pm_invert_batch_grids(self.ctx, npix, obs.ctypes.data, lamp.ctypes.data, slp, mode, *outs))
         out = {"models": models, "chisq": chi, "iters": its}
         if sp is not None:
             out["spectra"] = sp
@@ -337,7 +351,7 @@ class Inverter:
             raise ValueError("per-pixel stray light must be [npix][4][nl]")
         return sl, mode
 
-    def _invert_device(self, spectro, guess, slight, slight_mode, want_spectra, want_status):
+    def _invert_device(self, spectro, guess, slight, slight_mode, want_spectra, want_status, lam=None):
         import torch
 
         obs = spectro.contiguous().view(-1, 4, self.nl)
@@ -358,9 +372,15 @@ class Inverter:
                 SLIGHT_SHARED if sl.numel() == 4 * self.nl else SLIGHT_PER_PIXEL)
             slp = sl.data_ptr()
         g = _model_struct(guess)
-        _check(self.L.pm_invert_batch(self.ctx, npix, obs.data_ptr(), slp, mode, ctypes.byref(g), models.data_ptr(),
-                                      chi.data_ptr(), its.data_ptr(), None if sp is None else sp.data_ptr(),
-                                      None if stt is None else stt.data_ptr(), MEM_DEVICE))
+        outs = (ctypes.byref(g), models.data_ptr(), chi.data_ptr(), its.data_ptr(),
+                None if sp is None else sp.data_ptr(), None if stt is None else stt.data_ptr(), MEM_DEVICE)
+        if lam is None:
+            _check(self.L.pm_invert_batch(self.ctx, npix, obs.data_ptr(), slp, mode, *outs))
+        else:
+            lamt = lam.contiguous()
+            if lamt.dtype != torch.float64 or not lamt.is_cuda or lamt.numel() != npix * self.nl:
+                raise TypeError("per-pixel wavelengths: a float64 CUDA tensor [npix][nl]")
+            _check(self.L.pm_invert_batch_grids(self.ctx, npix, obs.data_ptr(), lamt.data_ptr(), slp, mode, *outs))
         out = {"models": models, "chisq": chi, "iters": its}
         if sp is not None:
             out["spectra"] = sp
@@ -369,8 +389,9 @@ class Inverter:
         return out
 
     # ---- forward synthesis ----
-    def synth(self, models, *, slight=None, slight_mode=None, rf=False):
-        """Synthesize [npix][11] models -> [npix][4][nl] (+ RFs [npix][4][nterms][nl])."""
+    def synth(self, models, *, slight=None, slight_mode=None, rf=False, lam=None):
+        """Synthesize [npix][11] models -> [npix][4][nl] (+ RFs [npix][4][nterms][nl]).
+        lam: [npix][nl] absolute wavelengths of each pixel (host arrays only)."""
         if _is_torch(models):
             import torch
 
@@ -392,8 +413,15 @@ class Inverter:
         sl, mode = self._slight_host(slight, slight_mode, npix)
         sp = np.zeros((npix, 4, self.nl), dtype=np.float32)
         rfo = np.zeros((npix, 4, self.nterms, self.nl), dtype=np.float32) if rf else None
-        _check(self.L.pm_synth_batch(self.ctx, npix, m.ctypes.data, None if sl is None else sl.ctypes.data, mode,
-                                     sp.ctypes.data, None if rfo is None else rfo.ctypes.data, MEM_HOST))
+        outs = (None if sl is None else sl.ctypes.data, mode, sp.ctypes.data,
+                None if rfo is None else rfo.ctypes.data, MEM_HOST)
+        if lam is None:
+            _check(self.L.pm_synth_batch(self.ctx, npix, m.ctypes.data, *outs))
+        else:
+            lamp = np.ascontiguousarray(lam, dtype=np.float64)
+            if lamp.size != npix * self.nl:
+                raise ValueError("per-pixel wavelengths must be [npix][nl]")
+            _check(self.L.pm_synth_batch_grids(self.ctx, npix, m.ctypes.data, lamp.ctypes.data, *outs))
         return (sp, rfo) if rf else sp
 
     # ---- lm_mils, batch of one ----

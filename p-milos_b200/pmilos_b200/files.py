@@ -10,6 +10,8 @@ reference can point this library at the same files:
 * ``read_model_file``                           -- readInitialModel (readConfig.c:136-191)
 * ``read_trol_file``                            -- readTrolFile (readConfig.c:420-1023), the
   42 positional lines of a .mtrol file
+* ``read_stray_light_fits``                     -- readFitsStrayLightFile (utilsFits.c:881-1199)
+* ``read_wavelength_fits``                      -- readFitsLambdaToArray (utilsFits.c:749-833)
 """
 from __future__ import annotations
 
@@ -199,3 +201,91 @@ def cube_fits_bytes(data: np.ndarray, ctypes_: list | None = None) -> bytes:
     body = np.ascontiguousarray(data, dtype=">f4").tobytes()
     body += b"\0" * (-len(body) % 2880)
     return hdr + body
+
+
+# ---- small FITS arrays (stray light, wavelengths) ----
+def fits_array(raw) -> tuple[list, dict, np.ndarray]:
+    """(naxes, cards, data) of a primary-HDU FITS image of BITPIX -32 or -64:
+    naxes in FITS order (NAXIS1 fastest), data as a float64 numpy array of shape
+    naxes[::-1]."""
+    raw = bytes(raw)
+    cards, pos = {}, 0
+    while True:
+        if pos + 2880 > len(raw):
+            raise ValueError("FITS header without END")
+        block = raw[pos:pos + 2880]
+        pos += 2880
+        done = False
+        for i in range(36):
+            card = block[80 * i:80 * (i + 1)].decode("ascii", "replace")
+            key = card[:8].strip()
+            if key == "END":
+                done = True
+                break
+            if card[8:10] == "= ":
+                val = card[10:].split("/")[0].strip()
+                cards[key] = val.strip("'").strip() if val.startswith("'") else val
+        if done:
+            break
+    bitpix = int(cards["BITPIX"])
+    if bitpix not in (-32, -64):
+        raise ValueError(f"BITPIX {bitpix}: float images only")
+    naxes = [int(cards[f"NAXIS{i + 1}"]) for i in range(int(cards["NAXIS"]))]
+    n = int(np.prod(naxes))
+    dt = ">f4" if bitpix == -32 else ">f8"
+    data = np.frombuffer(raw, dtype=dt, count=n, offset=pos).astype(np.float64)
+    return naxes, cards, data.reshape(naxes[::-1])
+
+
+def read_stray_light_fits(source):
+    """A stray-light FITS file as readFitsStrayLightFile reads it: a 2-D array
+    (nlambda x 4 in either axis order; the longer axis is wavelength) gives one
+    profile [4][nlambda] (float32) for every pixel; a 4-D cube gives a profile
+    per pixel, [npix][4][nlambda] in the cube ingest's pixel order (a CUDA
+    tensor, reordered on the device like an observed cube), for
+    PM_SLIGHT_PER_PIXEL (pmilos.c:1293)."""
+    raw = open(source, "rb").read() if isinstance(source, (str, os.PathLike)) else bytes(source)
+    naxes, _, data = fits_array(raw)
+    if len(naxes) == 2:
+        if naxes[0] >= naxes[1]:  # NAXIS1 = wavelength: stored [stokes][lambda]
+            return np.ascontiguousarray(data, dtype=np.float32)
+        return np.ascontiguousarray(data.T, dtype=np.float32)  # NAXIS1 = Stokes
+    if len(naxes) == 4:
+        from . import ingest_fits
+
+        return ingest_fits(raw)
+    raise ValueError(f"a stray-light file has 2 or 4 axes, not {len(naxes)}")
+
+
+def read_wavelength_fits(source):
+    """A wavelength FITS file.  2-D (NAXIS1 = nlambda, NAXIS2 = 2): the first row
+    holds the line's index in the atomic parameter file, the second the
+    wavelengths [A] -- readFitsLambdaToArray's reading; returns (index, lambda
+    [nlambda]).  4-D: one grid per pixel for pm_invert_batch_grids.  The
+    reference documents this form (README, "Wavelength grid file (.fits)") but
+    its reader does not load it; read here with the axis order of that reader's
+    comment, NAXIS1 = rows, NAXIS2 = columns, NAXIS3 = wavelength, NAXIS4 = 1
+    (or by CTYPE HPLN-TAN / HPLT-TAN / WAVE-GRI when present); returns (None,
+    lambda [npix][nlambda]), pixel = column * rows + row as in the cube ingest."""
+    raw = open(source, "rb").read() if isinstance(source, (str, os.PathLike)) else bytes(source)
+    naxes, cards, data = fits_array(raw)
+    if len(naxes) == 2:
+        flat = data.reshape(-1)
+        nl = naxes[0]
+        return int(flat[nl - 1]), flat[nl:2 * nl].copy()
+    if len(naxes) != 4:
+        raise ValueError(f"a wavelength file has 2 or 4 axes, not {len(naxes)}")
+    role = {"HPLN-TAN": "row", "HPLT-TAN": "col", "WAVE-GRI": "lam"}
+    axes = {}
+    for i in range(4):
+        r = role.get(cards.get(f"CTYPE{i + 1}", ""))
+        if r:
+            axes[r] = i
+    if len(axes) != 3:
+        axes = {"row": 0, "col": 1, "lam": 2}
+    rest = [i for i in range(4) if i not in axes.values()]
+    if naxes[rest[0]] != 1:
+        raise ValueError("the fourth axis of a per-pixel wavelength file has one element")
+    # numpy axis of FITS axis a is 3 - a; target order (col, row, lambda)
+    t = np.transpose(data, (3 - axes["col"], 3 - axes["row"], 3 - axes["lam"], 3 - rest[0]))
+    return None, np.ascontiguousarray(t.reshape(naxes[axes["col"]] * naxes[axes["row"]], naxes[axes["lam"]]))

@@ -23,6 +23,10 @@ Writes
                       large-cube configuration) and w49 (the known-answer test's
                       49-point grid with a 60 mA PSF, stray light and the filling
                       factor inverted); 16 pixels each
+  fits_aux_cases.npz  the reference's stray-light reader (readFitsStrayLightFile)
+                      on 2-D profiles in both axis orders and on 4-D cubes, and
+                      its wavelength reader (readFitsLambdaToArray) on 2-D files
+                      of float64 and float32: file bytes and output
   ref_cases_mac.npz   macroturbulence on the 30-point grid: m10 (v_mac inverted,
                       60 mA PSF), m10n (the same without PSF), m11 (v_mac and
                       the filling factor inverted, stray light), mfix (v_mac
@@ -244,6 +248,60 @@ def fits_cases(tmpdir):
     return out
 
 
+def fits_image_bytes(data: np.ndarray, bitpix: int = -32, ctypes_: list | None = None) -> bytes:
+    """A primary-HDU FITS image of numpy shape (NAXISn, ..., NAXIS1)."""
+    dims = list(data.shape[::-1])
+    cards = ["SIMPLE  =                    T", f"BITPIX  = {bitpix:20d}", f"NAXIS   = {len(dims):20d}"]
+    cards += [f"NAXIS{i + 1}  = {d:20d}" for i, d in enumerate(dims)]
+    if ctypes_:
+        cards += [f"CTYPE{i + 1}  = '{c:<8s}'" for i, c in enumerate(ctypes_)]
+    cards.append("END")
+    hdr = "".join(c.ljust(80) for c in cards).encode("ascii")
+    hdr += b" " * (-len(hdr) % 2880)
+    body = np.ascontiguousarray(data, dtype=">f4" if bitpix == -32 else ">f8").tobytes()
+    body += b"\0" * (-len(body) % 2880)
+    return hdr + body
+
+
+def fits_aux_cases(tmpdir):
+    """The reference's stray-light and wavelength readers on small files."""
+    rng = np.random.default_rng(78)
+    out = {}
+    # stray light, 2-D: (Stokes, lambda) or (lambda, Stokes) in numpy order
+    for k, shape in enumerate([(4, 30), (30, 4), (4, 7), (15, 4)]):
+        data = rng.normal(size=shape).astype(np.float32)
+        raw = fits_image_bytes(data)
+        path = os.path.join(tmpdir, f"sl2d{k}.fits")
+        open(path, "wb").write(raw)
+        arr, nl, ns, nx, ny = po.reference_fits_straylight(path)
+        out[f"s2_{k}_bytes"] = np.frombuffer(raw, dtype=np.uint8)
+        out[f"s2_{k}_ref"] = arr.reshape(ns, nl)
+    # stray light, 4-D cubes (the RCLS order takes the reference's special branch)
+    size = {"R": 5, "C": 6, "L": 7, "S": 4}
+    for k, (order, ct) in enumerate([("LSRC", True), ("SLRC", True), ("CRSL", True), ("LSRC", False)]):
+        dims = [size[r] for r in order]
+        data = rng.normal(size=dims[::-1]).astype(np.float32)
+        raw = fits_image_bytes(data, -32, [CTYPE_OF[r] for r in order] if ct else None)
+        path = os.path.join(tmpdir, f"sl4d{k}.fits")
+        open(path, "wb").write(raw)
+        arr, nl, ns, nx, ny = po.reference_fits_straylight(path)
+        out[f"s4_{k}_bytes"] = np.frombuffer(raw, dtype=np.uint8)
+        out[f"s4_{k}_ref"] = arr.reshape(nx * ny, ns, nl)
+        out[f"s4_{k}_order"] = np.array(order)
+    # wavelength files, 2-D: row 1 the line index, row 2 the wavelengths
+    offs, lam = grid(-350.0, 25.0, 375.0, 6173.3354)
+    for k, bitpix in enumerate((-64, -32)):
+        data = np.stack([np.full(lam.size, 1.0), lam])
+        raw = fits_image_bytes(data, bitpix)
+        path = os.path.join(tmpdir, f"lam{k}.fits")
+        open(path, "wb").write(raw)
+        idx, v = po.reference_fits_lambda(path)
+        out[f"l2_{k}_bytes"] = np.frombuffer(raw, dtype=np.uint8)
+        out[f"l2_{k}_index"] = np.array(idx)
+        out[f"l2_{k}_ref"] = v
+    return out
+
+
 def psf_pins():
     ref = po.Reference(po.LineSetup(*grid(-350.0, 25.0, 375.0, 6173.3354)[1:], 6173.3354, TRIPLET, None, 9), "f64")
     out = {}
@@ -276,10 +334,17 @@ def psf_pins():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
-    ap.add_argument("--only", choices=("all", "wide", "mac"), default="all")
+    ap.add_argument("--only", choices=("all", "wide", "mac", "fits"), default="all")
     a = ap.parse_args()
     os.environ["PM_REFERENCE_SRC"] = os.path.join(a.reference, "src")
     po.build()
+    import tempfile
+
+    with tempfile.TemporaryDirectory() as td:
+        np.savez_compressed(os.path.join(HERE, "fits_aux_cases.npz"), **fits_aux_cases(td))
+    print("fits_aux_cases.npz", os.path.getsize(os.path.join(HERE, "fits_aux_cases.npz")), "bytes")
+    if a.only == "fits":
+        return
     mac = {}
     for name in MAC_SPECS:
         for k, v in mac_case(name).items():

@@ -67,3 +67,47 @@ def test_header_errors():
     three = po.fits_bytes(np.zeros((3, 7, 3, 5), dtype=np.float32), None)  # no 4-plane axis
     with pytest.raises(pm.PmError):
         pm.fits_header(three)
+
+
+AUX = np.load(os.path.join(GOLDEN, "fits_aux_cases.npz"))
+
+
+@pytest.mark.parametrize("k", range(4))
+def test_two_dimensional_stray_light_matches_the_reference_reader(k):
+    """readFitsStrayLightFile on (Stokes, lambda) and (lambda, Stokes) arrays:
+    one profile [4][nlambda]."""
+    from pmilos_b200.files import read_stray_light_fits
+
+    got = read_stray_light_fits(AUX[f"s2_{k}_bytes"].tobytes())
+    assert got.dtype == np.float32
+    assert np.array_equal(got, AUX[f"s2_{k}_ref"])
+
+
+@pytest.mark.parametrize("k", range(2))
+def test_wavelength_file_matches_the_reference_reader(k):
+    """readFitsLambdaToArray on a 2-D file (float64 and float32 pixels): the
+    line index and the wavelengths."""
+    from pmilos_b200.files import read_wavelength_fits
+
+    idx, lam = read_wavelength_fits(AUX[f"l2_{k}_bytes"].tobytes())
+    assert idx == int(AUX[f"l2_{k}_index"])
+    assert np.array_equal(lam, AUX[f"l2_{k}_ref"])
+
+
+def test_per_pixel_wavelength_file_round_trip():
+    """The 4-D (per-pixel) wavelength file, which the reference documents but
+    does not read: NAXIS1 = rows, NAXIS2 = columns, NAXIS3 = wavelength,
+    NAXIS4 = 1, or axes named by CTYPE; pixel = column * rows + row."""
+    from pmilos_b200.files import read_wavelength_fits
+
+    rows, cols, nl = 5, 3, 7
+    lam = 6173.0 + np.random.default_rng(3).uniform(0, 1, (cols * rows, nl))
+    data = lam.reshape(cols, rows, nl).transpose(2, 0, 1)[None]  # numpy order (1, nl, cols, rows)
+    raw = po.fits_bytes(data.astype(np.float32), None)
+    idx, got = read_wavelength_fits(raw)
+    assert idx is None and np.array_equal(got, lam.astype(np.float32).astype(np.float64))
+    # the same grids with named axes in another order: (lambda, 1, rows, cols) as NAXIS1..4
+    data2 = lam.reshape(cols, rows, nl)[:, :, None, :]  # numpy (cols, rows, 1, nl)
+    raw2 = po.fits_bytes(data2.astype(np.float32), ["WAVE-GRI", "LINE", "HPLN-TAN", "HPLT-TAN"])
+    _, got2 = read_wavelength_fits(raw2)
+    assert np.array_equal(got2, got)

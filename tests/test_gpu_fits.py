@@ -35,3 +35,15 @@ def test_reorder_wide_cube(order, tmp_path):
     path.write_bytes(po.fits_bytes(data, ct))
     cube = pm.ingest_fits(str(path)).cpu().numpy()
     assert np.array_equal(cube, po.fits_ingest(data, ct))
+
+
+@pytest.mark.parametrize("k", range(4))
+def test_four_dimensional_stray_light_matches_the_reference_reader(k):
+    """A 4-D stray-light cube (readFitsStrayLightFile, utilsFits.c:936-1180) is
+    ingested on the device like an observed cube: a profile per pixel."""
+    from pmilos_b200.files import read_stray_light_fits
+
+    aux = np.load(os.path.join(GOLDEN, "fits_aux_cases.npz"))
+    got = read_stray_light_fits(aux[f"s4_{k}_bytes"].tobytes())
+    assert got.is_cuda
+    assert np.array_equal(got.cpu().numpy(), aux[f"s4_{k}_ref"])
