@@ -1303,19 +1303,16 @@ __device__ __forceinline__ void invert_pixel(const PmParams& P, const BlockSmem<
 #pragma unroll
     for (int s = 0; s < 4; ++s) S[s] = 0;
   } else {
-    {
-      R Su[4];
-      synthesize<R, MAC>(P, sm, m, sl_pix, lane, valid, dl(), S, Su);
-      rf_and_normal_eq<R, KT, MAC>(P, bs, sm, lane, valid, dl(), S, Su, O, isig, sl_pix);
-    }
-    ochi = chisq<R>(P, S, O, isig, valid, double(nfree));
-    const double chi0 = ochi;
-    double flambda = P.ilambda, factor = 1.0;
+    // The first pass synthesizes the starting model (trial = model) and takes
+    // it as accepted without a step: one copy of the synthesis and of the
+    // response functions in the loop body instead of two (instruction fetch
+    // bounds this kernel), with lm_mils' order of operations unchanged.
+    double chi0 = 0, flambda = P.ilambda, factor = 1.0;
     if (lane < 11) trial[lane] = m[lane];
     __syncwarp();
-    bool stop = false;
-    do {
-      {
+    bool stop = false, first = true;
+    while (true) {
+      if (!first) {
         double dlt[KT];
         bool ok = true;
         double* scratch = reinterpret_cast<double*>(sm.tr);  // the transpose buffer is idle here
@@ -1342,27 +1339,42 @@ __device__ __forceinline__ void invert_pixel(const PmParams& P, const BlockSmem<
       R Su[4];
       synthesize<R, MAC>(P, sm, trial, sl_pix, lane, valid, dl(), S, Su);
       const double chi = chisq<R>(P, S, O, isig, valid, double(nfree));
-      if ((fabs((ochi - chi) * 100 / chi) < P.toplim) || (chi < 0.0001)) {
-        stop = true;
-        status = PM_PIX_CONVERGED;
+      bool accept = true;
+      if (!first) {
+        if ((fabs((ochi - chi) * 100 / chi) < P.toplim) || (chi < 0.0001)) {
+          stop = true;
+          status = PM_PIX_CONVERGED;
+        }
+        accept = chi - ochi < 0.;
       }
-      if (chi - ochi < 0.) {
-        flambda = flambda / (5.0 * factor);
+      if (accept) {
+        if (!first) flambda = flambda / (5.0 * factor);
         if (lane < 11) m[lane] = trial[lane];
         __syncwarp();
-        rf_and_normal_eq<R, KT, MAC>(P, bs, sm, lane, valid, dl(), S, S, O, isig, sl_pix);
+        // the filling-factor row is built from the unmixed synthesis on the
+        // first call of me_der and from the mixed one after a step
+        // (milosUtils.c:537 vs :587)
+        R Sff[4];
+#pragma unroll
+        for (int s = 0; s < 4; ++s) Sff[s] = first ? Su[s] : S[s];
+        rf_and_normal_eq<R, KT, MAC>(P, bs, sm, lane, valid, dl(), S, Sff, O, isig, sl_pix);
         ochi = chi;
-        ++accepted;
+        if (first) chi0 = chi;
+        else ++accepted;
       } else {
         flambda = flambda * 10.0 * factor;
       }
-      if ((flambda > 1e+7) || (flambda < 1e-25)) {
-        if (!stop) status = PM_PIX_LAMBDA;
-        stop = true;
+      if (!first) {
+        if ((flambda > 1e+7) || (flambda < 1e-25)) {
+          if (!stop) status = PM_PIX_LAMBDA;
+          stop = true;
+        }
+        ++iter;
+        if (P.logclambda) factor = double(log10f(float(chi)) / log10f(float(chi0)));
+        if (!(iter < P.miter && !stop)) break;  // lm_mils' do-while: at least one step
       }
-      ++iter;
-      if (P.logclambda) factor = double(log10f(float(chi)) / log10f(float(chi0)));
-    } while (iter < P.miter && !stop);
+      first = false;
+    }
     bool finite = isfinite(ochi);
 #pragma unroll
     for (int i = 0; i < 11; ++i) finite = finite && isfinite(m[i]);
