@@ -360,6 +360,7 @@ def main():
                     help="served stream: scans of the same schedule timed on the plain FP64 server")
     ap.add_argument("--budget-gb", type=float, default=24.0, help="served stream: device arena of the server")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch tuning")
+    ap.add_argument("--tuning", default=None, help="variant,warps_per_block: this launch tuning, no autotuning")
     ap.add_argument("--ingest", action="store_true",
                     help="time the FITS cube ingest (512x512 pixels x 112 wavelengths, three axis orders)")
     args = ap.parse_args()
@@ -439,7 +440,10 @@ def main():
     sl_d = None if sl_h is None else torch.as_tensor(sl_h, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     # the project's autotuner picks the launch tuning on a sample of this cube (untimed)
-    if not args.no_autotune:
+    if args.tuning:
+        v, wpb = (int(x) for x in args.tuning.split(","))
+        inv32.tuning = {"variant": v, "warps_per_block": wpb}
+    elif not args.no_autotune:
         ns = min(w.npix, 32768)
         sample = obs[:ns] if obs is not None else obs_d[:ns].cpu().numpy()
         inv32.autotune(sample, w.guess, slight=sl_h, reps=2)
