@@ -348,64 +348,76 @@ __global__ void __launch_bounds__(32 * G, MINB) invert_wide_kernel(const __grid_
 #pragma unroll
       for (int s = 0; s < 4; ++s) S[s] = 0;
     } else {
-      {
-        R Su[4];
-        synthesize_wide<R, G>(P, sm, m, sl_pix, t, valid, dl_t, omw_t, S, Su);
-        ochi = chisq_wide<R, G>(P, sm, slot, S, O, isig, valid, double(nfree));
-        rf_and_normal_eq_wide<R, KT, G>(P, sm, slot, t, valid, omw_t, S, Su, O, isig, sl_pix);
-      }
-      const double chi0 = ochi;
-      double flambda = P.ilambda, factor = 1.0;
+      // the starting model's synthesis and response functions run as the
+      // loop's first pass (accepted without a step), so that each is inlined
+      // once; lm_mils' order of operations is unchanged
+      double chi0 = 0, flambda = P.ilambda, factor = 1.0;
       if (t < 11) trial[t] = m[t];
       __syncthreads();
-      bool stop = false;
-      do {
-        if (warp == 0) {
-          double dlt[KT];
-          bool ok = true;
-          double* scratch = reinterpret_cast<double*>(&sm.rf[0][0]);  // idle during the solve
-          if (P.solver == PM_SOLVE_CHOLESKY) ok = solve_cholesky<KT>(sm.sv, scratch, lane, flambda, dlt);
-          if (P.solver != PM_SOLVE_CHOLESKY || !ok) {
-            if (P.solver == PM_SOLVE_CHOLESKY) ++fallbacks;
-            solve_eigen<KT>(sm.sv, scratch, lane, flambda);
+      bool stop = false, first = true;
+      while (true) {
+        if (!first) {
+          if (warp == 0) {
+            double dlt[KT];
+            bool ok = true;
+            double* scratch = reinterpret_cast<double*>(&sm.rf[0][0]);  // idle during the solve
+            if (P.solver == PM_SOLVE_CHOLESKY) ok = solve_cholesky<KT>(sm.sv, scratch, lane, flambda, dlt);
+            if (P.solver != PM_SOLVE_CHOLESKY || !ok) {
+              if (P.solver == PM_SOLVE_CHOLESKY) ++fallbacks;
+              solve_eigen<KT>(sm.sv, scratch, lane, flambda);
 #pragma unroll
-            for (int i = 0; i < KT; ++i) dlt[i] = sm.sv.delta[i];
+              for (int i = 0; i < KT; ++i) dlt[i] = sm.sv.delta[i];
+              __syncwarp();
+            }
+            double tt[11];
+#pragma unroll
+            for (int i = 0; i < 11; ++i) tt[i] = trial[i];
+            apply_delta<KT>(P, m, dlt, tt);
+            check_model(tt);
             __syncwarp();
+#pragma unroll
+            for (int i = 0; i < 11; ++i)
+              if (lane == i) trial[i] = tt[i];
           }
-          double tt[11];
-#pragma unroll
-          for (int i = 0; i < 11; ++i) tt[i] = trial[i];
-          apply_delta<KT>(P, m, dlt, tt);
-          check_model(tt);
-          __syncwarp();
-#pragma unroll
-          for (int i = 0; i < 11; ++i)
-            if (lane == i) trial[i] = tt[i];
+          __syncthreads();
         }
-        __syncthreads();
         R Su[4];
         synthesize_wide<R, G>(P, sm, trial, sl_pix, t, valid, dl_t, omw_t, S, Su);
         const double chi = chisq_wide<R, G>(P, sm, slot, S, O, isig, valid, double(nfree));
-        if ((fabs((ochi - chi) * 100 / chi) < P.toplim) || (chi < 0.0001)) {
-          stop = true;
-          status = PM_PIX_CONVERGED;
+        bool accept = true;
+        if (!first) {
+          if ((fabs((ochi - chi) * 100 / chi) < P.toplim) || (chi < 0.0001)) {
+            stop = true;
+            status = PM_PIX_CONVERGED;
+          }
+          accept = chi - ochi < 0.;
         }
-        if (chi - ochi < 0.) {
-          flambda = flambda / (5.0 * factor);
+        if (accept) {
+          if (!first) flambda = flambda / (5.0 * factor);
           if (t < 11) m[t] = trial[t];
-          rf_and_normal_eq_wide<R, KT, G>(P, sm, slot, t, valid, omw_t, S, S, O, isig, sl_pix);
+          // the filling-factor row: unmixed synthesis first, mixed after a step
+          // (milosUtils.c:537 vs :587)
+          R Sff[4];
+#pragma unroll
+          for (int s = 0; s < 4; ++s) Sff[s] = first ? Su[s] : S[s];
+          rf_and_normal_eq_wide<R, KT, G>(P, sm, slot, t, valid, omw_t, S, Sff, O, isig, sl_pix);
           ochi = chi;
-          ++accepted;
+          if (first) chi0 = chi;
+          else ++accepted;
         } else {
           flambda = flambda * 10.0 * factor;
         }
-        if ((flambda > 1e+7) || (flambda < 1e-25)) {
-          if (!stop) status = PM_PIX_LAMBDA;
-          stop = true;
+        if (!first) {
+          if ((flambda > 1e+7) || (flambda < 1e-25)) {
+            if (!stop) status = PM_PIX_LAMBDA;
+            stop = true;
+          }
+          ++iter;
+          if (P.logclambda) factor = double(log10f(float(chi)) / log10f(float(chi0)));
+          if (!(iter < P.miter && !stop)) break;  // lm_mils' do-while: at least one step
         }
-        ++iter;
-        if (P.logclambda) factor = double(log10f(float(chi)) / log10f(float(chi0)));
-      } while (iter < P.miter && !stop);
+        first = false;
+      }
       __syncthreads();  // the last accepted model in m is visible to every thread
       bool finite = isfinite(ochi);
 #pragma unroll
