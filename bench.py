@@ -535,9 +535,9 @@ def main():
     hbm_bytes = w.npix * args.steps * (16 * w.nl + 11 * 8 + 8)
     # DRAM bytes per pixel of the FP32 inversion kernel from one ncu capture of a
     # smaller cube of the same workload, scaled to this launch by its pixel count:
-    # profiles/invert_stream_kernel_fp32_config1.md (351.5 MB for 524,288 pixels)
-    # and profiles/invert_wide_kernel_fp32_config4.md (132.7 MB for 65,536 pixels)
-    traffic = {1: 670.4, 4: 2025.0}.get(args.config) if w.nl in (30, 112) else None
+    # 355.2 MB for 524,288 pixels of the 30-point grid (dram__bytes_read.sum +
+    # dram__bytes_write.sum), 132.7 MB for 65,536 pixels of the 112-point grid
+    traffic = {1: 677.5, 4: 2025.0}.get(args.config) if w.nl in (30, 112) else None
     traffic = traffic * w.npix if traffic else None
     roofline = {"bound": "fp32", "achieved": round(achieved, 3), "peak": round(peak_fp32, 2), "unit": "TFLOP/s",
                 "frac": round(achieved / peak_fp32, 4), "traffic": traffic,
