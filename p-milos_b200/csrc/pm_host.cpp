@@ -72,6 +72,7 @@ struct HostCtl {
   PmJob piece_job[PM_STAGING_MAX];           // pipelined host-buffer calls: one launch per piece
   PmStreamQ piece_qinit[PM_STAGING_MAX];
   PmStreamQ piece_qread[PM_STAGING_MAX];
+  unsigned long long wide_ctr[2][PMC_COUNT];  // counters of the two buffer sets of a wide-grid call
 };
 
 // A captured CUDA graph of a whole small host-buffer call (uploads from pinned
@@ -107,7 +108,9 @@ struct pm_ctx {
   int device = 0;
   int num_sms = 148;
   cudaStream_t stream = nullptr;
-  size_t resident_bytes = size_t(8) << 30;  // device staging of one host-mode chunk
+  // device staging of a host-buffer call (8 GiB; PMILOS_RESIDENT_MB at context
+  // creation overrides it): larger cubes go in chunks
+  size_t resident_bytes = size_t(8) << 30;
   DevBuf spectro, slight, models, chisq, iters, spectra, status, rf, ctr, lambda;
   // streamed host-buffer calls: kernel and copy streams, the ticket queue, one job
   cudaStream_t s_kern = nullptr, s_copy = nullptr;
@@ -418,6 +421,8 @@ extern "C" int pm_ctx_create(const pm_line* line, const pm_config* cfg, void* st
   }
   c->num_sms = prop.multiProcessorCount;
   if (const char* v = std::getenv("PMILOS_VARIANT")) c->tuning.variant = std::atoi(v);
+  if (const char* v = std::getenv("PMILOS_RESIDENT_MB"))
+    if (std::atoll(v) > 0) c->resident_bytes = size_t(std::atoll(v)) << 20;
   if (const char* v = std::getenv("PMILOS_STAGING")) c->tuning.staging_depth = std::atoi(v);
   rc = c->ctr.ensure(sizeof(unsigned long long) * PMC_COUNT);
   if (rc != PM_OK) {
@@ -583,6 +588,102 @@ int run_streamed(pm_ctx* c, int64_t n, const float* spectro, const float* slight
   cudaEventElapsedTime(kernel_ms, c->k0, c->k1);
   cudaEventElapsedTime(total_ms, c->t0, c->t1);
   c->stats.pixels += n;
+  return PM_OK;
+}
+
+// A host-buffer call on a grid wider than one warp, in chunks through two
+// device buffer sets: the copy stream brings chunk k + 1 into one set while the
+// kernel stream inverts chunk k in the other (classical pre-pass + LM kernel),
+// and chunk k's results leave on the copy stream once its kernel is done.  A set
+// is refilled only after its results are out (stream order on the copy
+// stream), and a kernel starts only after its chunk is in (event).  Each set's
+// work counter is reset per launch; its statistics counters add up over the
+// set's launches and are read once at the end.
+int run_wide_pipelined(pm_ctx* c, int64_t npix, int64_t chunk, const float* spectro, const float* slight,
+                       int slight_mode, pm_model* models_out, float* chisq_out, int* iters_out, float* best_fit_out,
+                       int* status_out, float* kernel_ms) {
+  int rc = stream_resources(c);
+  if (rc != PM_OK) return rc;
+  const int nl = c->P.nl;
+  const size_t prof = sizeof(float) * 4 * nl;
+  const bool per_pixel = slight_mode == PM_SLIGHT_PER_PIXEL;
+  if ((rc = c->ctr.ensure(2 * sizeof(unsigned long long) * PMC_COUNT)) != PM_OK) return rc;
+  unsigned long long* ctr = static_cast<unsigned long long*>(c->ctr.p);
+  HostCtl* hc = c->hc;
+  cudaEvent_t ev_in[2] = {c->ev_piece[0], c->ev_piece[1]}, ev_k[2] = {c->ev_piece[2], c->ev_piece[3]};
+  PM_CUDA(cudaEventRecord(c->ev_start, c->stream), "event");
+  PM_CUDA(cudaStreamWaitEvent(c->s_copy, c->ev_start, 0), "wait");
+  PM_CUDA(cudaStreamWaitEvent(c->s_kern, c->ev_start, 0), "wait");
+  PM_CUDA(cudaMemsetAsync(ctr, 0, 2 * sizeof(unsigned long long) * PMC_COUNT, c->s_kern), "counter reset");
+  const int64_t nchunks = (npix + chunk - 1) / chunk;
+  // chunk k's inputs into set k & 1, then the event its kernel waits for
+  auto copy_in = [&](int64_t k) -> int {
+    const int b = int(k & 1);
+    const int64_t p0 = k * chunk, n = std::min(chunk, npix - p0);
+    PM_CUDA(cudaMemcpyAsync(static_cast<char*>(c->spectro.p) + prof * chunk * b, spectro + p0 * 4 * nl, prof * n,
+                            cudaMemcpyHostToDevice, c->s_copy),
+            "spectro H2D");
+    if (per_pixel)
+      PM_CUDA(cudaMemcpyAsync(static_cast<char*>(c->slight.p) + prof * chunk * b, slight + p0 * 4 * nl, prof * n,
+                              cudaMemcpyHostToDevice, c->s_copy),
+              "slight H2D");
+    PM_CUDA(cudaEventRecord(ev_in[b], c->s_copy), "event");
+    return PM_OK;
+  };
+  if ((rc = copy_in(0)) != PM_OK) return rc;
+  for (int64_t k = 0; k < nchunks; ++k) {
+    const int b = int(k & 1);
+    const int64_t p0 = k * chunk, n = std::min(chunk, npix - p0);
+    char* sp = static_cast<char*>(c->spectro.p) + prof * chunk * b;
+    char* sl = per_pixel ? static_cast<char*>(c->slight.p) + prof * chunk * b : nullptr;
+    PmIO io{};
+    io.npix = n;
+    io.spectro = reinterpret_cast<const float*>(sp);
+    io.slight = reinterpret_cast<const float*>(sl);
+    io.models_out = static_cast<double*>(c->models.p) + 11 * chunk * b;
+    io.chisq_out = static_cast<float*>(c->chisq.p) + chunk * b;
+    io.iters_out = static_cast<int*>(c->iters.p) + chunk * b;
+    io.spectra_out = best_fit_out ? reinterpret_cast<float*>(static_cast<char*>(c->spectra.p) + prof * chunk * b)
+                                  : nullptr;
+    io.status_out = status_out ? static_cast<int*>(c->status.p) + chunk * b : nullptr;
+    io.ctr = ctr + PMC_COUNT * b;
+    PM_CUDA(cudaStreamWaitEvent(c->s_kern, ev_in[b], 0), "wait");
+    PM_CUDA(cudaMemsetAsync(io.ctr + PMC_NEXT, 0, sizeof(unsigned long long), c->s_kern), "work counter reset");
+    if (k == 0) PM_CUDA(cudaEventRecord(c->k0, c->s_kern), "event");
+    rc = pmk_invert(c->P, io, c->precision, c->s_kern, c->num_sms, nullptr);
+    if (rc != PM_OK) return fail(rc, "%s", pmk_last_cuda_error());
+    if (k == nchunks - 1) PM_CUDA(cudaEventRecord(c->k1, c->s_kern), "event");
+    PM_CUDA(cudaEventRecord(ev_k[b], c->s_kern), "event");
+    // the next chunk goes in while this one is inverted: its copy is queued
+    // before this chunk's results, which wait for this kernel; its set's previous
+    // results (chunk k - 1) were queued before it
+    if (k + 1 < nchunks && (rc = copy_in(k + 1)) != PM_OK) return rc;
+    PM_CUDA(cudaStreamWaitEvent(c->s_copy, ev_k[b], 0), "wait");
+    PM_CUDA(cudaMemcpyAsync(models_out + p0, io.models_out, sizeof(pm_model) * n, cudaMemcpyDeviceToHost, c->s_copy),
+            "models D2H");
+    PM_CUDA(cudaMemcpyAsync(chisq_out + p0, io.chisq_out, sizeof(float) * n, cudaMemcpyDeviceToHost, c->s_copy),
+            "chisq D2H");
+    PM_CUDA(cudaMemcpyAsync(iters_out + p0, io.iters_out, sizeof(int) * n, cudaMemcpyDeviceToHost, c->s_copy),
+            "iters D2H");
+    if (best_fit_out)
+      PM_CUDA(cudaMemcpyAsync(best_fit_out + p0 * 4 * nl, io.spectra_out, prof * n, cudaMemcpyDeviceToHost, c->s_copy),
+              "best fit D2H");
+    if (status_out)
+      PM_CUDA(cudaMemcpyAsync(status_out + p0, io.status_out, sizeof(int) * n, cudaMemcpyDeviceToHost, c->s_copy),
+              "status D2H");
+  }
+  PM_CUDA(cudaStreamWaitEvent(c->s_copy, c->k1, 0), "wait");
+  PM_CUDA(cudaMemcpyAsync(hc->wide_ctr, ctr, sizeof hc->wide_ctr, cudaMemcpyDeviceToHost, c->s_copy), "counter D2H");
+  PM_CUDA(cudaEventRecord(c->ev_done, c->s_copy), "event");
+  PM_CUDA(cudaStreamWaitEvent(c->stream, c->ev_done, 0), "wait");
+  PM_CUDA(cudaEventSynchronize(c->ev_done), "wide inversion");
+  for (int b = 0; b < 2; ++b) {
+    c->stats.iterations += int64_t(hc->wide_ctr[b][PMC_ITERS]);
+    c->stats.accepted += int64_t(hc->wide_ctr[b][PMC_ACCEPTED]);
+    c->stats.eigen_fallbacks += int64_t(hc->wide_ctr[b][PMC_FALLBACK]);
+  }
+  c->stats.pixels += npix;
+  if (kernel_ms) cudaEventElapsedTime(kernel_ms, c->k0, c->k1);
   return PM_OK;
 }
 
@@ -848,19 +949,29 @@ int invert_impl(pm_ctx* c, int64_t npix, const float* spectro, const double* lam
     const size_t lam_bytes = lambda ? sizeof(double) * nl : 0;  // per pixel
     const size_t per_pixel = prof * (1 + (slight_mode == PM_SLIGHT_PER_PIXEL) + (best_fit_out != nullptr)) +
                              sizeof(pm_model) + sizeof(float) + 2 * sizeof(int) + lam_bytes;
-    const int64_t chunk = std::min<int64_t>(npix, std::max<int64_t>(32, int64_t(c->resident_bytes / per_pixel)));
-    if ((rc = c->spectro.ensure(prof * chunk)) != PM_OK) return rc;
-    if (slight_mode == PM_SLIGHT_PER_PIXEL && (rc = c->slight.ensure(prof * chunk)) != PM_OK) return rc;
-    if ((rc = c->models.ensure(sizeof(pm_model) * chunk)) != PM_OK) return rc;
-    if ((rc = c->chisq.ensure(sizeof(float) * chunk)) != PM_OK) return rc;
-    if ((rc = c->iters.ensure(sizeof(int) * chunk)) != PM_OK) return rc;
-    if (best_fit_out && (rc = c->spectra.ensure(prof * chunk)) != PM_OK) return rc;
-    if (status_out && (rc = c->status.ensure(sizeof(int) * chunk)) != PM_OK) return rc;
+    // wide grids go through two buffer sets (run_wide_pipelined), in at least 8
+    // chunks when the cube is large, so that only the first chunk's copy is not
+    // hidden behind an inversion
+    const int sets = c->P.G != 1 ? 2 : 1;
+    int64_t chunk = std::min<int64_t>(npix, std::max<int64_t>(32, int64_t(c->resident_bytes / (per_pixel * sets))));
+    if (sets == 2 && npix >= 8 * 4096) chunk = std::min<int64_t>(chunk, (npix / 8 + 31) / 32 * 32);
+    const int64_t cap = chunk * sets;
+    if ((rc = c->spectro.ensure(prof * cap)) != PM_OK) return rc;
+    if (slight_mode == PM_SLIGHT_PER_PIXEL && (rc = c->slight.ensure(prof * cap)) != PM_OK) return rc;
+    if ((rc = c->models.ensure(sizeof(pm_model) * cap)) != PM_OK) return rc;
+    if ((rc = c->chisq.ensure(sizeof(float) * cap)) != PM_OK) return rc;
+    if ((rc = c->iters.ensure(sizeof(int) * cap)) != PM_OK) return rc;
+    if (best_fit_out && (rc = c->spectra.ensure(prof * cap)) != PM_OK) return rc;
+    if (status_out && (rc = c->status.ensure(sizeof(int) * cap)) != PM_OK) return rc;
     if (lambda && (rc = c->lambda.ensure(lam_bytes * chunk)) != PM_OK) return rc;
+    if (sets == 2) {
+      rc = run_wide_pipelined(c, npix, chunk, spectro, slight, slight_mode, models_out, chisq_out, iters_out,
+                              best_fit_out, status_out, &kms_total);
+    }
     pm_stats acc{};
     // per-pixel grids take the copy-then-launch path
     const bool streamed = !lambda && c->P.G == 1 && c->tuning.staging_depth > 0;
-    for (int64_t p0 = 0; p0 < npix && rc == PM_OK && streamed; p0 += chunk) {
+    for (int64_t p0 = 0; p0 < npix && rc == PM_OK && sets == 1 && streamed; p0 += chunk) {
       const int64_t n = std::min(chunk, npix - p0);
       float kms = 0, tms = 0;
       rc = run_streamed(c, n, spectro + p0 * 4 * nl, slight_mode == PM_SLIGHT_PER_PIXEL ? slight + p0 * 4 * nl : slight,
@@ -869,7 +980,7 @@ int invert_impl(pm_ctx* c, int64_t npix, const float* spectro, const double* lam
                         &kms, &tms);
       kms_total += kms;
     }
-    for (int64_t p0 = 0; p0 < npix && rc == PM_OK && !streamed; p0 += chunk) {
+    for (int64_t p0 = 0; p0 < npix && rc == PM_OK && sets == 1 && !streamed; p0 += chunk) {
       const int64_t n = std::min(chunk, npix - p0);
       PM_CUDA(cudaMemcpyAsync(c->spectro.p, spectro + p0 * 4 * nl, prof * n, cudaMemcpyHostToDevice, c->stream),
               "spectro H2D");
@@ -913,7 +1024,7 @@ int invert_impl(pm_ctx* c, int64_t npix, const float* spectro, const double* lam
         PM_CUDA(cudaMemcpyAsync(status_out + p0, c->status.p, sizeof(int) * n, cudaMemcpyDeviceToHost, c->stream),
                 "status D2H");
     }
-    if (!streamed) c->stats = acc;
+    if (!streamed && sets == 1) c->stats = acc;
   }
   cudaEventRecord(t1, c->stream);
   cudaEventSynchronize(t1);

@@ -179,3 +179,25 @@ def test_wide_grid_classical_estimates_match_oracle():
                      nterms=c["nterms"], precision=pm.PREC_FP64, miter=0) as inv:
         r = inv.invert(obs, c["guess"])
     assert np.allclose(r["models"], ref["models"], rtol=1e-6, atol=1e-6)
+
+
+def test_host_buffers_in_many_chunks_equal_one_call(monkeypatch):
+    """Host-buffer calls on wide grids run through two device buffer sets, the
+    next chunk's copy overlapping this chunk's inversion: a 1 MB device budget
+    splits 600 pixels into chunks; results equal the single-chunk call and the
+    device-buffer call bit for bit, statistics add up."""
+    import torch
+
+    c, obs, _ = _case_results("w112")
+    big = np.ascontiguousarray(np.tile(obs, (5, 1, 1))[:600])
+    with winverter(c, pm.PREC_FP32) as inv:
+        one = inv.invert(big, c["guess"])
+        dev = inv.invert(torch.as_tensor(big, device="cuda"), c["guess"])
+    monkeypatch.setenv("PMILOS_RESIDENT_MB", "1")
+    with winverter(c, pm.PREC_FP32) as inv:
+        many = inv.invert(big, c["guess"])
+        st = inv.stats()
+    for k in ("models", "chisq", "iters", "spectra", "status"):
+        assert np.array_equal(many[k], one[k]), k
+        assert np.array_equal(dev[k].cpu().numpy(), one[k]), k
+    assert st["pixels"] == 600 and st["iterations"] == int(np.maximum(many["iters"], 0).sum())
