@@ -440,7 +440,7 @@ extern "C" int pm_ctx_destroy(pm_ctx* c) {
   if (c->s_kern) cudaStreamSynchronize(c->s_kern);
   if (c->s_copy) cudaStreamSynchronize(c->s_copy);
   for (DevBuf* b : {&c->spectro, &c->slight, &c->models, &c->chisq, &c->iters, &c->spectra, &c->status, &c->rf,
-                    &c->ctr, &c->q, &c->jobs})
+                    &c->ctr, &c->q, &c->jobs, &c->lambda})
     b->release();
   for (cudaEvent_t ev : {c->ev_start, c->ev_q, c->ev_done, c->t0, c->t1, c->k0, c->k1})
     if (ev) cudaEventDestroy(ev);
