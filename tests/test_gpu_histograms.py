@@ -1,0 +1,74 @@
+"""Distributions, not just medians: chi^2 and iteration-count histograms of the
+plain FP64 form against the FP64 oracle, and the FP32 form's per-parameter error
+quantiles, on 2048 pixels of configurations 1 and 2 (seeded synthetic cubes with
+the configurations' shapes; profiles synthesized by the oracle, N(0, 1e-3) noise).
+
+Iteration counts are not reproducible even between two builds of the reference
+(its own pin and fast builds agree per pixel on a third to most of the pixels),
+so the iteration histograms are compared by their two-sample Kolmogorov-Smirnov
+distance; chi^2 by its quantiles.  The FP32 form's yardstick is the reference's
+own float build (REAL = float, the oracle's bit-exact restatement of it) on the
+same pixels: its iteration histogram is itself 0.06-0.15 away from the double
+build's.
+"""
+import numpy as np
+import pytest
+
+import pmilos_b200 as pm
+import pyoracle as po
+from gpu_common import LINE_6173, NOISE64, within_tolerance
+from pmilos_b200 import workloads
+
+pytestmark = pytest.mark.gpu
+
+NPIX = 2048
+
+
+def ks(a, b):
+    """Two-sample Kolmogorov-Smirnov distance of two integer samples."""
+    grid = np.arange(min(a.min(), b.min()), max(a.max(), b.max()) + 1)
+    fa = np.searchsorted(np.sort(a), grid, side="right") / a.size
+    fb = np.searchsorted(np.sort(b), grid, side="right") / b.size
+    return float(np.abs(fa - fb).max())
+
+
+def _cube(cfg):
+    w = workloads.config(cfg, npix=NPIX)
+    setup = lambda k: po.LineSetup(w.lam, LINE_6173[0], np.array([1.0, *LINE_6173[1]]), w.psf, k)
+    ora = po.Restatement(setup(w.nterms), "f64")
+    rng = np.random.default_rng(50 + cfg)
+    truth = workloads.truth_models(w, rng)
+    sl = None
+    if cfg == 2:  # the stray-light profile: a B = 0 quiet-Sun atmosphere, as float32
+        sl = po.Restatement(setup(9), "f64").synth(workloads.QUIET_SUN_B0, rf=False)[0]
+        sl = sl.astype(np.float32).astype(np.float64)
+    obs = np.array([ora.synth(m, sl, fix=w.fix, rf=False)[0] for m in truth], dtype=np.float32)
+    obs += rng.normal(0, 1e-3, obs.shape).astype(np.float32)
+    ref = ora.invert(obs, w.guess, slight=sl, fix=w.fix, noise=NOISE64)
+    return w, obs, sl, ref
+
+
+@pytest.mark.parametrize("cfg", [1, 2])
+def test_histograms_and_error_quantiles(cfg):
+    w, obs, sl, ref = _cube(cfg)
+    slf = None if sl is None else sl.astype(np.float32)
+    with pm.Inverter(w.line, w.lam, w.psf, noise=NOISE64, fix=w.fix, nterms=w.nterms, precision=pm.PREC_FP64,
+                     solver=pm.SOLVE_EIGEN) as inv:
+        r64 = inv.invert(obs, w.guess, slight=slf)
+    with pm.Inverter(w.line, w.lam, w.psf, noise=NOISE64, fix=w.fix, nterms=w.nterms,
+                     precision=pm.PREC_FP32) as inv:
+        r32 = inv.invert(obs, w.guess, slight=slf)
+    # plain form: within the parameter tolerance, iteration histograms close, chi^2 quantiles equal
+    ok = within_tolerance(r64["models"], ref["models"])
+    assert ok.mean() >= 0.9
+    assert ks(r64["iters"], ref["iters"]) < 0.08
+    q = [0.1, 0.25, 0.5, 0.75, 0.9]
+    assert np.allclose(np.quantile(r64["chisq"], q), np.quantile(ref["chisq"], q), rtol=2e-3)
+    # batched form: the stated FP32 tolerance, and distributions no further from
+    # the FP64 ones than the reference's float build is
+    dB = np.abs(r32["models"][:, 1] - ref["models"][:, 1])
+    assert np.median(dB) < 1.0 and (dB < 5.0).mean() >= 0.9
+    o32 = po.Restatement(po.LineSetup(w.lam, LINE_6173[0], np.array([1.0, *LINE_6173[1]]), w.psf, w.nterms), "f32")
+    rf32 = o32.invert(obs, w.guess, slight=sl, fix=w.fix, noise=float(np.float32(np.float32(1e-3) ** 2)))
+    assert ks(r32["iters"], ref["iters"]) <= ks(rf32["iters"], ref["iters"]) + 0.05
+    assert np.allclose(np.quantile(r32["chisq"], q), np.quantile(ref["chisq"], q), rtol=1e-2)
