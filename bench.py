@@ -14,7 +14,8 @@ JSON line (rank 0):
            host->device copy of the cube and the device->host copy of models,
            chi^2 and iterations are inside the timed region
   plain    the FP64 plain form on the same cube (eigen solve, and Cholesky)
-  roofline FP32-pipe fraction from the frozen flop model
+  roofline FP32-pipe fraction from the frozen flop model (below: add/sub/mul/div 1,
+           FMA 2, transcendentals 0, per pixel and iteration)
   cpu_baseline  the reference's own C hot path (oracle/_ref, float build,
            -O3) on every host core, forked slabs like pmilos' Scatterv
 
