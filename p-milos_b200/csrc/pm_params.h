@@ -128,8 +128,11 @@ int pmk_synth_wide(const PmParams& P, const PmIO& io, int precision, void* strea
 // Classical estimates of npix pixels (one-warp grid) into models [npix][11]:
 // the starting models of a launch whose cube is on the device before it starts.
 // lambda: [npix][nl] absolute wavelengths of each pixel, or nullptr (the grid's).
+// threads: block size (a multiple of 32, at most 256); beside a persistent
+// kernel, at most that kernel's block size, so that a block fits in the slot one
+// of its blocks leaves free.
 int pmk_classical_prepass(const PmParams& P, const float* spectro, double* models, int64_t npix, void* stream,
-                          int num_sms, const double* lambda = nullptr);
+                          int num_sms, const double* lambda = nullptr, int threads = 256);
 // Streamed inversion: every grid of GS has the same nterms and nl <= 32.
 // multi: grids differ between jobs (dynamic grid index) rather than one grid.
 // reserve_blocks: launch that many fewer blocks than fit, leaving room on the

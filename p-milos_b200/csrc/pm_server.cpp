@@ -215,7 +215,9 @@ bool admit(pm_server* s, Scan* sc) {
   const PmParams& P = s->gs->g[sc->grid];
   if (e == cudaSuccess && P.classical) {
     J.model_in = J.models;
-    if (pmk_classical_prepass(P, J.spectro, J.models, sc->npix, s->s_copy, s->num_sms) != PM_OK)
+    // blocks of the persistent kernel's size (4 warps): one fits the slot a
+    // reserved block leaves free, whatever the pre-pass's register count
+    if (pmk_classical_prepass(P, J.spectro, J.models, sc->npix, s->s_copy, s->num_sms, nullptr, 128) != PM_OK)
       e = cudaErrorLaunchFailure;
     else
       ++s->prepass_launches;

@@ -251,15 +251,21 @@ int pmk_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, int precision,
 
 
 int pmk_classical_prepass(const PmParams& P, const float* spectro, double* models, int64_t npix, void* stream,
-                          int num_sms, const double* lambda) {
+                          int num_sms, const double* lambda, int threads) {
   if (P.G != 1) {
     snprintf(pmk_g_err, sizeof pmk_g_err, "classical pre-pass: one-warp grids only");
     return PM_EINVAL;
   }
-  long long blocks = (npix + 7) / 8;
-  if (blocks > (long long)num_sms * 16) blocks = (long long)num_sms * 16;
+  if (threads < 32 || threads > 256 || threads % 32) {
+    snprintf(pmk_g_err, sizeof pmk_g_err, "classical pre-pass: %d threads per block", threads);
+    return PM_EINVAL;
+  }
+  const int warps = threads / 32;
+  long long blocks = (npix + warps - 1) / warps;
+  if (blocks > (long long)num_sms * 128 / warps) blocks = (long long)num_sms * 128 / warps;
   if (blocks < 1) blocks = 1;
-  classical_prepass_kernel<<<unsigned(blocks), 256, 0, static_cast<cudaStream_t>(stream)>>>(P, spectro, models, npix, lambda);
+  classical_prepass_kernel<<<unsigned(blocks), threads, 0, static_cast<cudaStream_t>(stream)>>>(P, spectro, models,
+                                                                                                 npix, lambda);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return snprintf(pmk_g_err, sizeof pmk_g_err, "classical launch: %s", cudaGetErrorString(e)), PM_EIO;
   return PM_OK;
