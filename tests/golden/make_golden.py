@@ -27,6 +27,10 @@ Writes
                       on 2-D profiles in both axis orders and on 4-D cubes, and
                       its wavelength reader (readFitsLambdaToArray) on 2-D files
                       of float64 and float32: file bytes and output
+  ref_cases_zeeman.npz  a Zeeman multiplet, Fe I 6301.5012 (5P2.0-5D2.0: five pi
+                      and four sigma components per group) on a 30-point grid:
+                      z9 (60 mA PSF), z10 (stray light, filling factor
+                      inverted); 24 pixels and 8 synthesis models each
   ref_cases_mac.npz   macroturbulence on the 30-point grid: m10 (v_mac inverted,
                       60 mA PSF), m10n (the same without PSF), m11 (v_mac and
                       the filling factor inverted, stray light), mfix (v_mac
@@ -142,6 +146,61 @@ def mac_case(name, npix=24, nsynth=8):
     out = dict(lam=lam, offs=offs, lambda0=l0, psf=np.zeros(0) if psf is None else psf, truth=truth, guess=guess,
                fix=np.array(fix, dtype=np.int32), nterms=K, slight=np.zeros(0) if slight is None else slight)
     ref64 = po.Reference(setup, "f64")
+    obs = np.array([ref64.synth(m, slight, fix=fix, rf=False)[0] for m in truth], dtype=np.float32)
+    obs += rng.normal(0, 1e-3, obs.shape).astype(np.float32)
+    out["obs"] = obs
+    for flav in ("f32", "f64"):
+        ref = po.Reference(setup, flav)
+        noise = float(np.float32(np.float32(1.0 / 1000) ** 2)) if flav == "f32" else (1.0 / 1000) ** 2
+        r = ref.invert(obs, guess, slight=slight, fix=fix, noise=noise)
+        for k in ("models", "chisq", "iters", "spectra"):
+            out[f"{flav}_{k}"] = r[k]
+        models = truth[:nsynth].copy()
+        sp, rf = zip(*[ref.synth(m, slight, fix=fix) for m in models])
+        out[f"{flav}_synth_models"] = models
+        out[f"{flav}_synth"] = np.array(sp)
+        out[f"{flav}_rf"] = np.array(rf)
+    return out
+
+
+MULTIPLET = np.array([1.0, 2.0, 1.0, 2.0, 2.0, 2.0, 2.0])  # 5P 2.0 - 5D 2.0
+LAMBDA_6301 = 6301.5012
+
+
+def zeeman_case(name, npix=24, nsynth=8):
+    """A multiplet line (LINES entry 2 of the reference's run directory) with the
+    configuration-1 atmospheres; z10 adds stray light and the filling factor."""
+    stray = name == "z10"
+    rng = np.random.default_rng(sum(ord(ch) for ch in name) + 3000)
+    offs, lam = grid(-350.0, 25.0, 375.0, LAMBDA_6301)
+    x, y = gauss_table(60.0)
+    psf = po.Reference(po.LineSetup(lam, LAMBDA_6301, MULTIPLET, None, 9), "f64").interp_psf(x, y, offs, 0.0)
+    K = 10 if stray else 9
+    fix = [1] * 9 + [0, 1 if stray else 0]
+    guess = GUESS.copy()
+    if stray:
+        guess[10] = 0.9
+    truth = np.zeros((npix, 11))
+    truth[:, 0] = rng.uniform(1, 20, npix)
+    truth[:, 1] = rng.uniform(0, 3000, npix)
+    truth[:, 2] = rng.uniform(-3, 3, npix)
+    truth[:, 3] = rng.uniform(0.02, 0.05, npix)
+    truth[:, 4] = rng.uniform(0.01, 0.5, npix)
+    truth[:, 5] = rng.uniform(0, 180, npix)
+    truth[:, 6] = rng.uniform(0, 180, npix)
+    truth[:, 7] = rng.uniform(0.1, 0.4, npix)
+    truth[:, 8] = rng.uniform(0.4, 0.9, npix)
+    truth[:, 10] = 1.0 - rng.uniform(0, 0.3, npix) if stray else 1.0
+    slight = None
+    if stray:
+        r9 = po.Reference(po.LineSetup(lam, LAMBDA_6301, MULTIPLET, psf, 9), "f64")
+        slight, _ = r9.synth(np.array([13.0, 0.0, 0.2, 0.035, 0.19, 30.0, 30.0, 0.26, 0.74, 0.0, 1.0]), rf=False)
+        slight = slight.astype(np.float32).astype(np.float64)
+    setup = po.LineSetup(lam, LAMBDA_6301, MULTIPLET, psf, K)
+    out = dict(lam=lam, offs=offs, lambda0=LAMBDA_6301, cuantic=MULTIPLET, psf=psf, truth=truth, guess=guess,
+               fix=np.array(fix, dtype=np.int32), nterms=K, slight=np.zeros(0) if slight is None else slight)
+    ref64 = po.Reference(setup, "f64")
+    out["cuantic_pattern"] = ref64.cuantic()
     obs = np.array([ref64.synth(m, slight, fix=fix, rf=False)[0] for m in truth], dtype=np.float32)
     obs += rng.normal(0, 1e-3, obs.shape).astype(np.float32)
     out["obs"] = obs
@@ -334,7 +393,7 @@ def psf_pins():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
-    ap.add_argument("--only", choices=("all", "wide", "mac", "fits"), default="all")
+    ap.add_argument("--only", choices=("all", "wide", "mac", "fits", "zeeman"), default="all")
     a = ap.parse_args()
     os.environ["PM_REFERENCE_SRC"] = os.path.join(a.reference, "src")
     po.build()
@@ -344,6 +403,14 @@ def main():
         np.savez_compressed(os.path.join(HERE, "fits_aux_cases.npz"), **fits_aux_cases(td))
     print("fits_aux_cases.npz", os.path.getsize(os.path.join(HERE, "fits_aux_cases.npz")), "bytes")
     if a.only == "fits":
+        return
+    zee = {}
+    for name in ("z9", "z10"):
+        for k, v in zeeman_case(name).items():
+            zee[f"{name}_{k}"] = v
+    np.savez_compressed(os.path.join(HERE, "ref_cases_zeeman.npz"), **zee)
+    print("ref_cases_zeeman.npz", os.path.getsize(os.path.join(HERE, "ref_cases_zeeman.npz")), "bytes")
+    if a.only == "zeeman":
         return
     mac = {}
     for name in MAC_SPECS:

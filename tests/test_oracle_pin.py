@@ -172,3 +172,26 @@ def test_macroturbulence_row_is_the_derivative():
         dn[9] -= h
         num = (ora.synth(up, fix=fix, rf=False)[0] - ora.synth(dn, fix=fix, rf=False)[0]) / (2 * h)
         assert np.abs(rf[:, 9] - num).max() < 2e-3 * np.abs(num).max()
+
+
+ZEE = np.load(os.path.join(GOLDEN, "ref_cases_zeeman.npz"))
+
+
+@pytest.mark.parametrize("flav", ["f32", "f64"])
+@pytest.mark.parametrize("name", ["z9", "z10"])
+def test_zeeman_multiplet_bit_exact(name, flav):
+    """A multiplet (Fe I 6301.5, five pi and four sigma components per group):
+    inversions, synthesis and every response function equal the reference's,
+    and so does the Zeeman pattern."""
+    g = lambda k: ZEE[f"{name}_{k}"]
+    ora = po.Restatement(po.LineSetup(g("lam"), float(g("lambda0")), g("cuantic"), g("psf"), int(g("nterms"))), flav)
+    sl = g("slight") if g("slight").size else None
+    fix = list(g("fix"))
+    r = ora.invert(g("obs"), g("guess"), slight=sl, fix=fix, noise=_noise(flav))
+    for k in ("iters", "chisq", "models", "spectra"):
+        assert np.array_equal(r[k], g(f"{flav}_{k}")), k
+    for m, sp_ref, rf_ref in zip(g(f"{flav}_synth_models"), g(f"{flav}_synth"), g(f"{flav}_rf")):
+        sp, rf = ora.synth(m, sl, fix=fix)
+        assert np.array_equal(sp, sp_ref)
+        assert np.array_equal(rf, rf_ref)
+    assert np.allclose(ora.cuantic(), g("cuantic_pattern"), rtol=1e-6, atol=1e-12)
