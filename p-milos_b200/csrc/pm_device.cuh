@@ -130,9 +130,12 @@ __device__ __forceinline__ void voigt(R a, R v, R& h, R& f) {
 }
 
 // Per-model terms shared by every wavelength (mil_sinrf.c:84-166, me_der.c:58-63).
-// This build handles the normal Zeeman triplet (one component per group: N_PI =
-// N_SIG = 1, e.g. Fe I 6173 and 6302, 5P1.0-5D0.0); the host rejects multiplets.
-// The FP32 form evaluates these terms in FP32 as well.
+// ZM: the line is a Zeeman multiplet (N_PI or N_SIG > 1, e.g. Fe I 6301.5,
+// 5P2.0-5D2.0); otherwise a normal triplet (one component per group, e.g. Fe I
+// 6173 and 6302, 5P1.0-5D0.0), whose splittings are compile-time operands.  zs is
+// the shift of each group's last component, the one the response functions use
+// (me_der.c:569-600 assigns rather than accumulates over components).  The FP32
+// form evaluates these terms in FP32 as well.
 template <typename R>
 struct alignas(16) ModelTerms {
   R sin_gm, cosi, sinis, cosis, cosis_2, sina, cosa, sinda, cosda, sindi, cosdi, sinis_cosa, sinis_sina;
@@ -141,10 +144,11 @@ struct alignas(16) ModelTerms {
   R zsB[3];  // the same times B
   R auxCte;  // d u / d vlos (me_der.c:545)
   R invE0, sc, ss, cosi_2_E0;  // me_der.c:118-127
+  R parcial, Bm;  // splitting per gauss and Lande unit in Doppler units, and B: the multiplet components
   double E0, B0, B1, ALF;
 };
 
-template <typename R>
+template <typename R, bool ZM = false>
 __device__ __forceinline__ void model_terms(const PmParams& P, const double* m, ModelTerms<R>& T) {
   constexpr bool f32 = sizeof(R) == 4;
   const int lane = threadIdx.x & 31;
@@ -193,8 +197,13 @@ __device__ __forceinline__ void model_terms(const PmParams& P, const double* m, 
   const R parcial = (l0 * l0) * T.invLD * R(kZeeman);
 #pragma unroll
   for (int g = 0; g < 3; ++g) {
-    T.zs[g] = parcial * R(P.nu[g][0]);
+    const int last = ZM ? (g == 0 ? P.n_pi : P.n_sig) - 1 : 0;
+    T.zs[g] = parcial * R(P.nu[g][last]);
     T.zsB[g] = T.zs[g] * R(m[1]);
+  }
+  if constexpr (ZM) {
+    T.parcial = parcial;
+    T.Bm = R(m[1]);
   }
   T.auxCte = (-l0) * T.invLD * R(1.0 / kVLight);
   T.sc = E0 * T.sinis_cosa / R(2);
@@ -227,22 +236,41 @@ static_assert(sizeof(LaneState<float>) == kLaneStatePad * sizeof(float), "LaneSt
 static_assert(sizeof(LaneState<double>) == kLaneStatePad * sizeof(double), "LaneState layout");
 
 // ME synthesis at wavelength offset dl (mil_sinrf.c:117-285): the three Zeeman
-// groups, the propagation matrix, and the Unno-Rachkovsky solution.
-template <typename R>
+// groups (funcionComponentFor_sinrf, mil_sinrf.c:418-449: the strength-weighted
+// sum of every component's Voigt and Faraday-Voigt profiles), the propagation
+// matrix, and the Unno-Rachkovsky solution.
+template <typename R, bool ZM = false>
 __device__ __forceinline__ void synth_lane(const PmParams& P, const ModelTerms<R>& T, double dl, LaneState<R>& s,
                                            R S[4]) {
   const R u = R(dl) * T.invLD - T.ulos;
 #pragma unroll
   for (int g = 0; g < 3; ++g) {
-    const R uu = u - T.zsB[g];
-    R H, F;
-    voigt<R>(T.A, uu, H, F);
-    const R we = R(P.we[g][0]);
-    s.fi[g] = we * H;
-    s.shi[g] = we * F * R(2);
-    s.uu[g] = uu;
-    s.H[g] = H;
-    s.F[g] = F;
+    if constexpr (ZM) {
+      const int n = g == 0 ? P.n_pi : P.n_sig;
+      R fi = 0, shi = 0, uu = 0, H = 0, F = 0;
+      for (int k = 0; k < n; ++k) {
+        uu = u - (T.parcial * R(P.nu[g][k])) * T.Bm;
+        voigt<R>(T.A, uu, H, F);
+        const R we = R(P.we[g][k]);
+        fi = fi + we * H;
+        shi = shi + we * F * R(2);
+      }
+      s.fi[g] = fi;
+      s.shi[g] = shi;
+      s.uu[g] = uu;  // the last component's, for the response functions
+      s.H[g] = H;
+      s.F[g] = F;
+    } else {
+      const R uu = u - T.zsB[g];
+      R H, F;
+      voigt<R>(T.A, uu, H, F);
+      const R we = R(P.we[g][0]);
+      s.fi[g] = we * H;
+      s.shi[g] = we * F * R(2);
+      s.uu[g] = uu;
+      s.H[g] = H;
+      s.F[g] = F;
+    }
   }
   s.parcial1 = s.fi[1] + s.fi[2];
   s.parcial2 = T.E0_2 * (s.fi[0] - s.parcial1 / R(2));
@@ -515,13 +543,13 @@ __device__ __forceinline__ void xs_restore(WarpSmem<R>& sm, int lane) {
 // leaves them in globals.  MAC: the kernel has a v_mac response row (NTERMS >=
 // 10), so v_mac may be nonzero.  dl: this lane's wavelength offset lambda -
 // lambda0 (the grid's, or the pixel's own).
-template <typename R, bool MAC = false>
+template <typename R, bool MAC = false, bool ZM = false>
 __device__ __forceinline__ void synthesize(const PmParams& P, WarpSmem<R>& sm, const double* m,
                                            const float* sl_pix, int lane, bool valid, double dl, R S[4], R Su[4]) {
   ModelTerms<R> T;
   LaneState<R> st;
-  model_terms<R>(P, m, T);
-  synth_lane<R>(P, T, dl, st, S);
+  model_terms<R, ZM>(P, m, T);
+  synth_lane<R, ZM>(P, T, dl, st, S);
   copy16(*reinterpret_cast<LaneState<R>*>(sm.ls[lane]), st);
   if (lane == 0) copy16(sm.mt, T);
   const double mac = MAC ? m[9] : 0.0;
@@ -561,13 +589,13 @@ __device__ __forceinline__ void load_lane_state(const WarpSmem<R>& sm, int lane,
 // stored at col[p * STRIDE]: p = r*4 + s for rows r = 0..6 (eta0, B, vlos, dopp,
 // a, gamma, azimuth) and r = 7 holding RF row 8 (S1).  Row 7 of the reference
 // (S0: I = 1, Q = U = V = 0) is not convolved and is added in registers later.
-template <typename R, int STRIDE>
+template <typename R, int STRIDE, bool ZM = false>
 __device__ __forceinline__ void rf_lane(const PmParams& P, const ModelTerms<R>& T, const LaneState<R>& st, R* col,
                                         bool valid) {
   R dfi[3][4], dshi[3][4];
 #pragma unroll
   for (int g = 0; g < 3; ++g) {
-    const R we = R(P.we[g][0]);
+    const R we = R(P.we[g][ZM ? (g == 0 ? P.n_pi : P.n_sig) - 1 : 0]);  // the last component's
     const R uu = st.uu[g], H = st.H[g], F = st.F[g];
     const R dH_u = ((R(4) * T.A * F) - (R(2) * uu * H)) * we;
     const R dF_u = (R(kRsqrtPi) - T.A * H - R(2) * uu * F) * we;
@@ -1178,7 +1206,7 @@ __device__ __forceinline__ void classical(const PmParams& P, const float O[4], i
 // macroturbulence convolutions, the v_mac row and the filling-factor terms.
 // m must be the model of the last synthesis.  MAC: compiled with the
 // macroturbulence branch (the grid has a v_mac row; NTERMS >= 10).
-template <typename R, int KT, bool MAC = (KT >= 10)>
+template <typename R, int KT, bool MAC = (KT >= 10), bool ZM = false>
 __device__ __forceinline__ void response_rows(const PmParams& P, const BlockSmem<R>& bs, WarpSmem<R>& sm, int lane,
                                               bool valid, const double* m, double dl, const R Sff[4],
                                               const float* sl_pix, R (&d)[KT][4]) {
@@ -1190,7 +1218,7 @@ __device__ __forceinline__ void response_rows(const PmParams& P, const BlockSmem
     copy16(T, sm.mt);
     LaneState<R> st;
     load_lane_state<R>(sm, lane, st);
-    rf_lane<R, TRS>(P, T, st, sm.tr + lane, valid);
+    rf_lane<R, TRS, ZM>(P, T, st, sm.tr + lane, valid);
     alf = T.alf;
   }
   R dmac[4] = {R(0), R(0), R(0), R(0)};
@@ -1206,12 +1234,12 @@ __device__ __forceinline__ void response_rows(const PmParams& P, const BlockSmem
 }
 
 // Response functions at the current synthesis -> alpha, beta in shared memory.
-template <typename R, int KT, bool MAC>
+template <typename R, int KT, bool MAC, bool ZM>
 __device__ __forceinline__ void rf_and_normal_eq(const PmParams& P, const BlockSmem<R>& bs, WarpSmem<R>& sm,
                                                  int lane, bool valid, double dl, const R S[4], const R Sff[4],
                                                  const float O[4], const R isig[4], const float* sl_pix) {
   R d[KT][4];
-  response_rows<R, KT, MAC>(P, bs, sm, lane, valid, sm.model, dl, Sff, sl_pix, d);
+  response_rows<R, KT, MAC, ZM>(P, bs, sm, lane, valid, sm.model, dl, Sff, sl_pix, d);
 #pragma unroll
   for (int r = 0; r < KT; ++r)
     if (P.zero_row[r]) {
@@ -1245,7 +1273,8 @@ __device__ __forceinline__ T* ld_ptr(T* const* p) {
 // PIXGRID: the pixel has its own wavelengths (the job's lambda, [npix][nl]),
 // kept in a register; otherwise the grid's offsets are read from the
 // parameter block where they are used.
-template <typename R, int KT, bool MAC, bool PIXGRID>
+// ZM: the line is a Zeeman multiplet.
+template <typename R, int KT, bool MAC, bool PIXGRID, bool ZM = false>
 __device__ __forceinline__ void invert_pixel(const PmParams& P, const BlockSmem<R>& bs, WarpSmem<R>& sm, int lane,
                                              unsigned long long* ctr) {
   const bool valid = lane < P.nl;
@@ -1337,7 +1366,7 @@ __device__ __forceinline__ void invert_pixel(const PmParams& P, const BlockSmem<
         __syncwarp();
       }
       R Su[4];
-      synthesize<R, MAC>(P, sm, trial, sl_pix, lane, valid, dl(), S, Su);
+      synthesize<R, MAC, ZM>(P, sm, trial, sl_pix, lane, valid, dl(), S, Su);
       const double chi = chisq<R>(P, S, O, isig, valid, double(nfree));
       bool accept = true;
       if (!first) {
@@ -1357,7 +1386,7 @@ __device__ __forceinline__ void invert_pixel(const PmParams& P, const BlockSmem<
         R Sff[4];
 #pragma unroll
         for (int s = 0; s < 4; ++s) Sff[s] = first ? Su[s] : S[s];
-        rf_and_normal_eq<R, KT, MAC>(P, bs, sm, lane, valid, dl(), S, Sff, O, isig, sl_pix);
+        rf_and_normal_eq<R, KT, MAC, ZM>(P, bs, sm, lane, valid, dl(), S, Sff, O, isig, sl_pix);
         ochi = chi;
         if (first) chi0 = chi;
         else ++accepted;

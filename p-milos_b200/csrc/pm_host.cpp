@@ -276,9 +276,9 @@ int fill_params(const pm_line* L, const pm_config* c, PmParams& P) {
   if (c->miter < 0) return fail(PM_EINVAL, "miter=%d", c->miter);
   if (!(c->noise > 0)) return fail(PM_EINVAL, "noise must be > 0");
   if (c->precision != PM_PREC_FP32 && c->precision != PM_PREC_FP64) return fail(PM_EINVAL, "precision");
-  if (L->n_pi != 1 || L->n_sig != 1)
-    return fail(PM_ENOTSUP, "only normal Zeeman triplets (N_PI = N_SIG = 1) are compiled in; got %d/%d", L->n_pi,
-                L->n_sig);
+  if (L->n_pi < 1 || L->n_sig < 1 || L->n_pi > PM_ZEEMAN_MAX || L->n_sig > PM_ZEEMAN_MAX)
+    return fail(PM_EINVAL, "Zeeman pattern with %d pi and %d sigma components (1..%d per group)", L->n_pi,
+                L->n_sig, PM_ZEEMAN_MAX);
   P.nl = c->nlambda;
   P.half = c->nlambda / 2;
   P.K = c->nterms;
@@ -305,6 +305,9 @@ int fill_params(const pm_line* L, const pm_config* c, PmParams& P) {
   P.mac_row = (P.K == 11 || (P.K == 10 && !P.fix[10])) ? 9 : -1;
   if (P.mac_row >= 0 && P.nl > 32)
     return fail(PM_ENOTSUP, "macroturbulence on grids of more than 32 wavelengths is outside this implementation");
+  if ((L->n_pi > 1 || L->n_sig > 1) && (P.nl > 32 || P.mac_row >= 0))
+    return fail(PM_ENOTSUP, "Zeeman multiplets are compiled for grids of at most 32 wavelengths without "
+                            "macroturbulence");
   P.lambda0 = L->lambda0;
   for (int i = 0; i < P.nl; ++i) P.dl[i] = c->lambda[i] - L->lambda0;
   for (int k = 0; k < L->n_pi; ++k) { P.nu[0][k] = L->nup[k]; P.we[0][k] = L->wep[k]; }

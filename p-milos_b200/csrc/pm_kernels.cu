@@ -7,7 +7,7 @@
 char pmk_g_err[256];
 
 namespace {
-template <typename R, int KT>
+template <typename R, int KT, bool ZM>
 __global__ void __launch_bounds__(128) synth_kernel(const __grid_constant__ PmParams P, const PmIO io) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -26,14 +26,14 @@ __global__ void __launch_bounds__(128) synth_kernel(const __grid_constant__ PmPa
     __syncwarp();
     const double dl = !valid ? 0.0 : (io.lambda_pix ? io.lambda_pix[size_t(pix) * P.nl + lane] - P.lambda0 : P.dl[lane]);
     R S[4], Su[4];
-    synthesize<R, (KT >= 10)>(P, sm, sm.model, sl_pix, lane, valid, dl, S, Su);
+    synthesize<R, (KT >= 10), ZM>(P, sm, sm.model, sl_pix, lane, valid, dl, S, Su);
     if (valid) {
 #pragma unroll
       for (int s = 0; s < 4; ++s) io.spectra_out[base + s * P.nl + lane] = float(S[s]);
     }
     if (io.rf_out) {
       R d[KT][4];
-      response_rows<R, KT>(P, bs, sm, lane, valid, sm.model, dl, Su, sl_pix, d);
+      response_rows<R, KT, (KT >= 10), ZM>(P, bs, sm, lane, valid, sm.model, dl, Su, sl_pix, d);
       __syncwarp();
       if (valid) {
         const size_t rb = size_t(pix) * 4 * KT * P.nl;
@@ -48,11 +48,11 @@ __global__ void __launch_bounds__(128) synth_kernel(const __grid_constant__ PmPa
 }
 
 
-template <typename R, int KT>
+template <typename R, int KT, bool ZM>
 int launch_synth(const PmParams& P, const PmIO& io, cudaStream_t st) {
   const int threads = 128;
   const size_t smem = sizeof(BlockSmem<R>) + sizeof(WarpSmem<R>) * (threads / 32);
-  auto kern = synth_kernel<R, KT>;
+  auto kern = synth_kernel<R, KT, ZM>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return snprintf(pmk_g_err, sizeof pmk_g_err, "%s", cudaGetErrorString(e)), PM_EIO;
   int64_t blocks = (io.npix + 3) / 4;
@@ -68,7 +68,8 @@ int launch_synth(const PmParams& P, const PmIO& io, cudaStream_t st) {
 template <typename R, int KT>
 int launch_synth_any(const PmParams& P, const PmIO& io, cudaStream_t st) {
   if (P.G != 1) return pmk_synth_wide(P, io, sizeof(R) == 4 ? PM_PREC_FP32 : PM_PREC_FP64, st);
-  return launch_synth<R, KT>(P, io, st);
+  if (P.n_pi > 1 || P.n_sig > 1) return launch_synth<R, KT, true>(P, io, st);  // a Zeeman multiplet
+  return launch_synth<R, KT, false>(P, io, st);
 }
 
 }  // namespace

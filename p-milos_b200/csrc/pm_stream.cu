@@ -59,7 +59,7 @@ struct GridParams {
   PmParams g[NG];
 };
 
-template <typename R, int KT, int MINB, bool MULTI, bool MAC, bool PIXGRID>
+template <typename R, int KT, int MINB, bool MULTI, bool MAC, bool PIXGRID, bool ZM = false>
 __global__ void __launch_bounds__(128, MINB) invert_stream_kernel(
     const __grid_constant__ GridParams<MULTI ? PMK_MAX_GRIDS : 1> GS, const PmStreamIO sio) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(128, MINB) invert_stream_kernel(
       sm.pix = (unsigned long long)t - t0;
     }
     __syncwarp();
-    invert_pixel<R, KT, MAC, PIXGRID>(P, bs[gi], sm, lane, sio.q->ctr);
+    invert_pixel<R, KT, MAC, PIXGRID, ZM>(P, bs[gi], sm, lane, sio.q->ctr);
     jp = *reinterpret_cast<const PmJob* const volatile*>(&sm.job);
     unsigned long long* done = ld_ptr(&jp->done);
     if (done) {
@@ -162,13 +162,13 @@ __global__ void __launch_bounds__(256) classical_prepass_kernel(const __grid_con
   }
 }
 
-template <typename R, int KT, int MINB, bool MULTI, bool MAC, bool PIXGRID = false>
+template <typename R, int KT, int MINB, bool MULTI, bool MAC, bool PIXGRID = false, bool ZM = false>
 int launch_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, cudaStream_t st, int num_sms,
                          size_t* smem_out, int wpb, int reserve) {
   const int threads = 32 * wpb;
   const size_t smem = (MULTI ? PMK_MAX_GRIDS : 1) * sizeof(BlockSmem<R>) + sizeof(WarpSmem<R>) * (threads / 32);
   if (smem_out) *smem_out = smem;
-  auto kern = invert_stream_kernel<R, KT, MINB, MULTI, MAC, PIXGRID>;
+  auto kern = invert_stream_kernel<R, KT, MINB, MULTI, MAC, PIXGRID, ZM>;
   constexpr int NG = MULTI ? PMK_MAX_GRIDS : 1;
   GridParams<NG> gp;  // copied into the launch
   gp.ngrids = GS.ngrids < NG ? GS.ngrids : NG;
@@ -242,8 +242,29 @@ int pmk_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, int precision,
       return PM_ENOTSUP;
     }
   }
-  bool mac = false;
-  for (int g = 0; g < GS.ngrids; ++g) mac = mac || GS.g[g].mac_row >= 0;
+  bool mac = false, zm = false;
+  for (int g = 0; g < GS.ngrids; ++g) {
+    mac = mac || GS.g[g].mac_row >= 0;
+    zm = zm || GS.g[g].n_pi > 1 || GS.g[g].n_sig > 1;
+  }
+  if (zm) {
+    // Zeeman multiplets: one grid, shared wavelengths, no macroturbulence row;
+    // the FP32 form with the 128-register budget
+    if (multi || pixgrid || mac || K > 10) {
+      snprintf(pmk_g_err, sizeof pmk_g_err,
+               "Zeeman multiplets: single-grid calls on a shared grid without macroturbulence only");
+      return PM_ENOTSUP;
+    }
+    if (precision == PM_PREC_FP32)
+      return K == 9 ? launch_invert_stream<float, 9, 4, false, false, false, true>(GS, sio, st, num_sms, smem_out,
+                                                                                    wpb, reserve_blocks)
+                    : launch_invert_stream<float, 10, 4, false, false, false, true>(GS, sio, st, num_sms, smem_out,
+                                                                                     wpb, reserve_blocks);
+    return K == 9 ? launch_invert_stream<double, 9, 1, false, false, false, true>(GS, sio, st, num_sms, smem_out, wpb,
+                                                                                   reserve_blocks)
+                  : launch_invert_stream<double, 10, 1, false, false, false, true>(GS, sio, st, num_sms, smem_out,
+                                                                                    wpb, reserve_blocks);
+  }
   if (precision == PM_PREC_FP32)
     return launch_stream_k<float>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve_blocks, K, mac, pixgrid);
   return launch_stream_k<double>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve_blocks, K, mac, pixgrid);
