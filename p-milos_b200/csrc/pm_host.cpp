@@ -305,9 +305,8 @@ int fill_params(const pm_line* L, const pm_config* c, PmParams& P) {
   P.mac_row = (P.K == 11 || (P.K == 10 && !P.fix[10])) ? 9 : -1;
   if (P.mac_row >= 0 && P.nl > 32)
     return fail(PM_ENOTSUP, "macroturbulence on grids of more than 32 wavelengths is outside this implementation");
-  if ((L->n_pi > 1 || L->n_sig > 1) && (P.nl > 32 || P.mac_row >= 0))
-    return fail(PM_ENOTSUP, "Zeeman multiplets are compiled for grids of at most 32 wavelengths without "
-                            "macroturbulence");
+  if ((L->n_pi > 1 || L->n_sig > 1) && P.mac_row >= 0)
+    return fail(PM_ENOTSUP, "Zeeman multiplets are compiled without macroturbulence");
   P.lambda0 = L->lambda0;
   for (int i = 0; i < P.nl; ++i) P.dl[i] = c->lambda[i] - L->lambda0;
   for (int k = 0; k < L->n_pi; ++k) { P.nu[0][k] = L->nup[k]; P.we[0][k] = L->wep[k]; }

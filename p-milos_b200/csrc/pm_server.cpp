@@ -492,10 +492,6 @@ extern "C" int pm_server_create(const pm_line* line, const pm_config* const* gri
       release(s);
       return sfail(PM_ENOTSUP, "pm_server_create: served grids have at most 32 wavelengths");
     }
-    if (ngrids > 1 && (P.n_pi > 1 || P.n_sig > 1)) {
-      release(s);
-      return sfail(PM_ENOTSUP, "pm_server_create: a Zeeman multiplet is served alone (one grid per server)");
-    }
     if (grids[g]->precision != grids[0]->precision || P.K != s->gs->g[0].K) {
       release(s);
       return sfail(PM_EINVAL, "pm_server_create: grids differ in precision or nterms");

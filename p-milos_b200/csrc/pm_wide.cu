@@ -117,14 +117,14 @@ __device__ __forceinline__ void psf_wide(const PmParams& P, WideSmem<R, G>& sm, 
   for (int q = 1; q < 4; ++q) S[q] = valid ? acc[q] : R(0);
 }
 
-template <typename R, int G>
+template <typename R, int G, bool ZM>
 __device__ __forceinline__ void synthesize_wide(const PmParams& P, WideSmem<R, G>& sm, const double* m,
                                                 const float* sl_pix, int t, bool valid, double dl_t, R omw_t,
                                                 R S[4], R Su[4]) {
   ModelTerms<R> T;
   LaneState<R> st;
-  model_terms<R>(P, m, T);
-  synth_lane<R>(P, T, dl_t, st, S);
+  model_terms<R, ZM>(P, m, T);
+  synth_lane<R, ZM>(P, T, dl_t, st, S);
   copy16(*reinterpret_cast<LaneState<R>*>(sm.ls[t]), st);
   if (t == 0) copy16(sm.mt, T);
   if (P.has_psf) psf_wide<R, G>(P, sm, t, valid, omw_t, S);
@@ -184,7 +184,7 @@ __device__ __forceinline__ void rf_correlate_wide(const PmParams& P, const WideS
 // Response functions of the last synthesis at this thread's wavelength, after
 // correlation, stray light and filling factor (as gather_rf): d[row][stokes].
 // Sff is the spectrum the filling-factor row is built from.
-template <typename R, int KT, int G>
+template <typename R, int KT, int G, bool ZM>
 __device__ __forceinline__ void rf_wide(const PmParams& P, WideSmem<R, G>& sm, int t, bool valid, R omw_t,
                                         const R Sff[4], const float* sl_pix, R (&d)[KT][4]) {
   R alf;
@@ -193,7 +193,7 @@ __device__ __forceinline__ void rf_wide(const PmParams& P, WideSmem<R, G>& sm, i
     copy16(T, sm.mt);
     LaneState<R> st;
     copy16(st, *reinterpret_cast<const LaneState<R>*>(sm.ls[t]));
-    rf_lane<R, 1>(P, T, st, sm.rf[t], valid);
+    rf_lane<R, 1, ZM>(P, T, st, sm.rf[t], valid);
     alf = T.alf;
   }
   __syncthreads();
@@ -287,12 +287,12 @@ __device__ __forceinline__ double chisq_wide(const PmParams& P, WideSmem<R, G>& 
   return acc[0] / nfree;
 }
 
-template <typename R, int KT, int G>
+template <typename R, int KT, int G, bool ZM>
 __device__ __forceinline__ void rf_and_normal_eq_wide(const PmParams& P, WideSmem<R, G>& sm, int& slot, int t,
                                                       bool valid, R omw_t, const R S[4], const R Sff[4],
                                                       const float O[4], const R isig[4], const float* sl_pix) {
   R d[KT][4];
-  rf_wide<R, KT, G>(P, sm, t, valid, omw_t, Sff, sl_pix, d);
+  rf_wide<R, KT, G, ZM>(P, sm, t, valid, omw_t, Sff, sl_pix, d);
 #pragma unroll
   for (int r = 0; r < KT; ++r)
     if (P.zero_row[r]) {
@@ -304,7 +304,8 @@ __device__ __forceinline__ void rf_and_normal_eq_wide(const PmParams& P, WideSme
 
 // lm_mils over pixels of a wide grid: the control flow of invert_pixel with
 // block-wide reductions; the solve and the trial model come from warp 0.
-template <typename R, int KT, int G, int MINB>
+// ZM: the line is a Zeeman multiplet (a separate instance, as in the one-warp kernel).
+template <typename R, int KT, int G, int MINB, bool ZM>
 __global__ void __launch_bounds__(32 * G, MINB) invert_wide_kernel(const __grid_constant__ PmParams P,
                                                                      const PmIO io) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -382,7 +383,7 @@ __global__ void __launch_bounds__(32 * G, MINB) invert_wide_kernel(const __grid_
           __syncthreads();
         }
         R Su[4];
-        synthesize_wide<R, G>(P, sm, trial, sl_pix, t, valid, dl_t, omw_t, S, Su);
+        synthesize_wide<R, G, ZM>(P, sm, trial, sl_pix, t, valid, dl_t, omw_t, S, Su);
         const double chi = chisq_wide<R, G>(P, sm, slot, S, O, isig, valid, double(nfree));
         bool accept = true;
         if (!first) {
@@ -400,7 +401,7 @@ __global__ void __launch_bounds__(32 * G, MINB) invert_wide_kernel(const __grid_
           R Sff[4];
 #pragma unroll
           for (int s = 0; s < 4; ++s) Sff[s] = first ? Su[s] : S[s];
-          rf_and_normal_eq_wide<R, KT, G>(P, sm, slot, t, valid, omw_t, S, Sff, O, isig, sl_pix);
+          rf_and_normal_eq_wide<R, KT, G, ZM>(P, sm, slot, t, valid, omw_t, S, Sff, O, isig, sl_pix);
           ochi = chi;
           if (first) chi0 = chi;
           else ++accepted;
@@ -491,7 +492,7 @@ __global__ void __launch_bounds__(32 * G) classical_wide_kernel(const __grid_con
 }
 
 // Synthesis (and response functions) of given models on a wide grid.
-template <typename R, int KT, int G>
+template <typename R, int KT, int G, bool ZM>
 __global__ void __launch_bounds__(32 * G) synth_wide_kernel(const __grid_constant__ PmParams P, const PmIO io) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WideSmem<R, G>& sm = *reinterpret_cast<WideSmem<R, G>*>(smem_raw);
@@ -505,7 +506,7 @@ __global__ void __launch_bounds__(32 * G) synth_wide_kernel(const __grid_constan
     if (t < 11) sm.model[t] = io.models_in[size_t(pix) * 11 + t];
     __syncthreads();
     R S[4], Su[4];
-    synthesize_wide<R, G>(P, sm, sm.model, sl_pix, t, valid, dl_t, omw_t, S, Su);
+    synthesize_wide<R, G, ZM>(P, sm, sm.model, sl_pix, t, valid, dl_t, omw_t, S, Su);
     if (valid) {
 #pragma unroll
       for (int s = 0; s < 4; ++s) io.spectra_out[base + s * P.nl + t] = float(S[s]);
@@ -513,7 +514,7 @@ __global__ void __launch_bounds__(32 * G) synth_wide_kernel(const __grid_constan
     if (io.rf_out) {
       __syncthreads();  // the model terms from thread 0
       R d[KT][4];
-      rf_wide<R, KT, G>(P, sm, t, valid, omw_t, Su, sl_pix, d);
+      rf_wide<R, KT, G, ZM>(P, sm, t, valid, omw_t, Su, sl_pix, d);
       if (valid) {
         const size_t rb = size_t(pix) * 4 * KT * P.nl;
 #pragma unroll
@@ -531,7 +532,8 @@ template <typename R, int KT, int G, int MINB>
 int launch_invert_wide(const PmParams& P, const PmIO& io, cudaStream_t st, int num_sms, float* kernel_ms) {
   const int threads = 32 * G;
   const size_t smem = sizeof(WideSmem<R, G>);
-  auto kern = invert_wide_kernel<R, KT, G, MINB>;
+  auto kern = (P.n_pi > 1 || P.n_sig > 1) ? invert_wide_kernel<R, KT, G, MINB, true>
+                                           : invert_wide_kernel<R, KT, G, MINB, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return snprintf(pmk_g_err, sizeof pmk_g_err, "%s", cudaGetErrorString(e)), PM_EIO;
   int per_sm = 0;
@@ -568,7 +570,7 @@ template <typename R, int KT, int G>
 int launch_synth_wide(const PmParams& P, const PmIO& io, cudaStream_t st) {
   const int threads = 32 * G;
   const size_t smem = sizeof(WideSmem<R, G>);
-  auto kern = synth_wide_kernel<R, KT, G>;
+  auto kern = (P.n_pi > 1 || P.n_sig > 1) ? synth_wide_kernel<R, KT, G, true> : synth_wide_kernel<R, KT, G, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return snprintf(pmk_g_err, sizeof pmk_g_err, "%s", cudaGetErrorString(e)), PM_EIO;
   int64_t blocks = io.npix;

@@ -28,9 +28,11 @@ Writes
                       its wavelength reader (readFitsLambdaToArray) on 2-D files
                       of float64 and float32: file bytes and output
   ref_cases_zeeman.npz  a Zeeman multiplet, Fe I 6301.5012 (5P2.0-5D2.0: five pi
-                      and four sigma components per group) on a 30-point grid:
-                      z9 (60 mA PSF), z10 (stray light, filling factor
-                      inverted); 24 pixels and 8 synthesis models each
+                      and four sigma components per group), 60 mA PSF: z9 and
+                      z10 on a 30-point grid, zw9 on 49 points and zw10 on 112
+                      points (25 mA steps); the *10 cases add stray light and
+                      invert the filling factor; 24 pixels and 8 synthesis
+                      models each (16 and 4 on the wide grids)
   ref_cases_mac.npz   macroturbulence on the 30-point grid: m10 (v_mac inverted,
                       60 mA PSF), m10n (the same without PSF), m11 (v_mac and
                       the filling factor inverted, stray light), mfix (v_mac
@@ -165,14 +167,16 @@ def mac_case(name, npix=24, nsynth=8):
 
 MULTIPLET = np.array([1.0, 2.0, 1.0, 2.0, 2.0, 2.0, 2.0])  # 5P 2.0 - 5D 2.0
 LAMBDA_6301 = 6301.5012
+ZEEMAN_GRIDS = {"z9": (-350.0, 25.0, 375.0), "z10": (-350.0, 25.0, 375.0),
+                "zw9": (-600.0, 25.0, 600.0), "zw10": (-1387.5, 25.0, 1387.5)}
 
 
 def zeeman_case(name, npix=24, nsynth=8):
     """A multiplet line (LINES entry 2 of the reference's run directory) with the
-    configuration-1 atmospheres; z10 adds stray light and the filling factor."""
-    stray = name == "z10"
+    configuration-1 atmospheres; the *10 cases add stray light and the filling factor."""
+    stray = name.endswith("10")
     rng = np.random.default_rng(sum(ord(ch) for ch in name) + 3000)
-    offs, lam = grid(-350.0, 25.0, 375.0, LAMBDA_6301)
+    offs, lam = grid(*ZEEMAN_GRIDS[name], LAMBDA_6301)
     x, y = gauss_table(60.0)
     psf = po.Reference(po.LineSetup(lam, LAMBDA_6301, MULTIPLET, None, 9), "f64").interp_psf(x, y, offs, 0.0)
     K = 10 if stray else 9
@@ -405,8 +409,8 @@ def main():
     if a.only == "fits":
         return
     zee = {}
-    for name in ("z9", "z10"):
-        for k, v in zeeman_case(name).items():
+    for name in ZEEMAN_GRIDS:
+        for k, v in zeeman_case(name, *((16, 4) if name.startswith("zw") else (24, 8))).items():
             zee[f"{name}_{k}"] = v
     np.savez_compressed(os.path.join(HERE, "ref_cases_zeeman.npz"), **zee)
     print("ref_cases_zeeman.npz", os.path.getsize(os.path.join(HERE, "ref_cases_zeeman.npz")), "bytes")

@@ -1,8 +1,11 @@
 """A Zeeman multiplet on the GPU: Fe I 6301.5012 (5P2.0-5D2.0; five pi and four
-sigma components per group) on a 30-point grid, from
-tests/golden/ref_cases_zeeman.npz (made by running the reference): z9 (60 mA PSF,
-nine parameters), z10 (stray light, filling factor inverted).  The oracle equals
-the reference bit for bit on these cases (tests/test_oracle_pin.py).
+sigma components per group), from tests/golden/ref_cases_zeeman.npz (made by
+running the reference), 60 mA PSF: z9 (30 wavelengths, nine parameters), z10
+(30 wavelengths, stray light, filling factor inverted), zw9 (49 wavelengths: two
+warps per pixel) and zw10 (112 wavelengths, four warps per pixel, stray light).
+The oracle equals the reference bit for bit on these cases
+(tests/test_oracle_pin.py).  Inversions run on the fixture's pixels plus 40
+pixels synthesized by the FP64 oracle with N(0, 1e-3) noise.
 """
 import os
 
@@ -17,6 +20,7 @@ from gpu_common import NOISE64, within_tolerance
 pytestmark = pytest.mark.gpu
 
 ZEE = np.load(os.path.join(GOLDEN, "ref_cases_zeeman.npz"))
+NAMES = ["z9", "z10", "zw9", "zw10"]
 LINE = pm.LineData(6301.5012, (2.0, 1.0, 2.0, 2.0, 2.0, 2.0))
 STEP = np.array([0.1, 10.0, 0.01, 1e-3, 1e-2, 1.0, 1.0, 1e-2, 1e-2, 1e-2, 1e-2])
 
@@ -52,7 +56,17 @@ def _models(c, n, seed):
     return np.concatenate([c["models"], m])
 
 
-@pytest.mark.parametrize("name", ["z9", "z10"])
+def _observed(c, seed):
+    """The fixture's profiles and 40 more from fresh models, as float32."""
+    rng = np.random.default_rng(seed)
+    ora = zora(c)
+    extra = np.array([ora.synth(m, c["slight"], fix=c["fix"], rf=False)[0] for m in _models(c, 40, seed)[-40:]],
+                     dtype=np.float32)
+    extra += rng.normal(0, 1e-3, extra.shape).astype(np.float32)
+    return np.concatenate([c["obs"], extra])
+
+
+@pytest.mark.parametrize("name", NAMES)
 def test_fp64_synthesis_and_rf_match_oracle(name):
     c = zcase(name)
     models = _models(c, 40, 21)
@@ -66,19 +80,20 @@ def test_fp64_synthesis_and_rf_match_oracle(name):
         assert (np.abs(rf[i] - rf_ref) / scale).max() < 1e-5, i
 
 
-def test_fp32_synthesis_close_to_fp64_oracle():
+@pytest.mark.parametrize("name", ["z9", "zw10"])
+def test_fp32_synthesis_close_to_fp64_oracle(name):
     """The FP32 criterion of the other lines: profiles within 2e-6 of FP64, each
     response function no worse than the reference's own float build, or within
     1% of its row maximum, or within 1e-6 over a typical step."""
-    c = zcase("z9")
+    c = zcase(name)
     models = _models(c, 40, 22)
     with zinv(c, pm.PREC_FP32) as inv:
-        sp, rf = inv.synth(models, rf=True)
+        sp, rf = inv.synth(models, slight=c["slight"], rf=True)
     o64, o32 = zora(c, "f64"), zora(c, "f32")
     worst = 0.0
     for i in range(models.shape[0]):
-        s_ref, rf_ref = o64.synth(models[i], fix=c["fix"])
-        _, rf_r32 = o32.synth(models[i], fix=c["fix"])
+        s_ref, rf_ref = o64.synth(models[i], c["slight"], fix=c["fix"])
+        _, rf_r32 = o32.synth(models[i], c["slight"], fix=c["fix"])
         worst = max(worst, np.abs(sp[i] - s_ref).max())
         rowmax = np.abs(rf_ref).max(axis=-1)
         e_gpu = np.abs(rf[i] - rf_ref).max(axis=-1)
@@ -88,44 +103,106 @@ def test_fp32_synthesis_close_to_fp64_oracle():
     assert worst < 2e-6
 
 
-@pytest.mark.parametrize("name", ["z9", "z10"])
+@pytest.mark.parametrize("name", NAMES)
 def test_plain_fp64_inversion_matches_oracle(name):
     c = zcase(name)
-    ref = zora(c).invert(c["obs"], c["guess"], slight=c["slight"], fix=c["fix"], noise=NOISE64)
+    obs = _observed(c, 31)
+    ref = zora(c).invert(obs, c["guess"], slight=c["slight"], fix=c["fix"], noise=NOISE64)
     with zinv(c, pm.PREC_FP64, pm.SOLVE_EIGEN) as inv:
-        r = inv.invert(c["obs"], c["guess"], slight=c["slight"])
+        r = inv.invert(obs, c["guess"], slight=c["slight"])
     ok = within_tolerance(r["models"], ref["models"])
     assert ok.mean() >= 0.85, f"only {ok.mean():.2%} of pixels within tolerance"
     assert np.abs(r["spectra"][ok] - ref["spectra"][ok]).max() < 1e-5
     assert abs(np.median(r["iters"]) - np.median(ref["iters"])) <= 3
 
 
-@pytest.mark.parametrize("name", ["z9", "z10"])
+@pytest.mark.parametrize("name", NAMES)
 def test_fp32_inversion_against_fp64_oracle(name):
     c = zcase(name)
-    ref = zora(c).invert(c["obs"], c["guess"], slight=c["slight"], fix=c["fix"], noise=NOISE64)
+    obs = _observed(c, 32)
+    ref = zora(c).invert(obs, c["guess"], slight=c["slight"], fix=c["fix"], noise=NOISE64)
     with zinv(c, pm.PREC_FP32) as inv:
-        r = inv.invert(c["obs"], c["guess"], slight=c["slight"])
+        r = inv.invert(obs, c["guess"], slight=c["slight"])
     dB = np.abs(r["models"][:, 1] - ref["models"][:, 1])
     assert np.median(dB) < 1.0 and (dB < 5.0).mean() >= 0.85
     assert np.all(r["status"] >= 0)
 
 
-def test_multiplet_limits():
-    """Multiplets are compiled for one-warp grids without macroturbulence, and a
-    server holds one alone (then with the batch entry point's kernel)."""
+def _pixel_grids(base, n, seed):
+    """The grid stretched by up to 1e-3 and shifted by up to +-20 mA per pixel."""
+    rng = np.random.default_rng(seed)
+    l0 = LINE.lambda0
+    scale = 1.0 + rng.uniform(-1e-3, 1e-3, n)
+    shift = rng.uniform(-0.020, 0.020, n)
+    return l0 + (base[None, :] - l0) * scale[:, None] + shift[:, None]
+
+
+def test_multiplet_on_each_pixels_grid():
+    """Per-pixel wavelength grids with the multiplet: synthesis and the FP64
+    inversion of every pixel against the oracle on the pixel's own grid (with the
+    context's PSF taps), the FP32 inversion within the stated tolerance."""
     c = zcase("z9")
-    wide = np.linspace(6300.9, 6302.1, 49)
-    with pytest.raises(pm.PmError) as e:
-        pm.Inverter(LINE, wide, None, noise=NOISE64, fix=c["fix"], nterms=9)
-    assert e.value.code == -95  # PM_ENOTSUP
+    n = 48
+    lam = _pixel_grids(c["lam"], n, 41)
+    oras = [po.Restatement(po.LineSetup(l, LINE.lambda0, c["cuantic"], c["psf"], 9), "f64") for l in lam]
+    models = _models(c, n, 42)[-n:]
+    with zinv(c, pm.PREC_FP64) as inv:
+        sp, rf = inv.synth(models, rf=True, lam=lam)
+    for o, m, s_gpu, r_gpu in zip(oras, models, sp, rf):
+        s_ref, rf_ref = o.synth(m, fix=c["fix"])
+        assert np.abs(s_gpu - s_ref).max() < 1e-6
+        scale = np.abs(rf_ref).max(axis=-1, keepdims=True) + 1e-30
+        assert (np.abs(r_gpu - rf_ref) / scale).max() < 1e-5
+    rng = np.random.default_rng(43)
+    obs = np.array([o.synth(m, fix=c["fix"], rf=False)[0] for o, m in zip(oras, models)], dtype=np.float32)
+    obs += rng.normal(0, 1e-3, obs.shape).astype(np.float32)
+    ref = np.concatenate([o.invert(obs[i:i + 1], c["guess"], fix=c["fix"], noise=NOISE64)["models"]
+                          for i, o in enumerate(oras)])
+    with zinv(c, pm.PREC_FP64, pm.SOLVE_EIGEN) as inv:
+        r64 = inv.invert(obs, c["guess"], lam=lam)
+    with zinv(c, pm.PREC_FP32) as inv:
+        r32 = inv.invert(obs, c["guess"], lam=lam)
+    assert within_tolerance(r64["models"], ref).mean() >= 0.85
+    dB = np.abs(r32["models"][:, 1] - ref[:, 1])
+    assert np.median(dB) < 1.0 and (dB < 5.0).mean() >= 0.85
+
+
+def test_server_serves_multiplet_grids_together():
+    """Two multiplet grids in one server (30 points at 25 mA, 15 points at 50 mA):
+    a scan gives the same results alone and among scans of the other grid, bit
+    for bit, and the FP32 batch entry point's within the stated tolerance."""
+    c = zcase("z9")
+    lam15 = c["lam"][::2]
+    psf15 = pm.psf_gaussian(60.0, lam15)
+    g0 = pm.Grid(lam=c["lam"], psf=c["psf"], guess=c["guess"], noise=NOISE64, fix=c["fix"], nterms=9)
+    g1 = pm.Grid(lam=lam15, psf=psf15, guess=c["guess"], noise=NOISE64, fix=c["fix"], nterms=9)
+    obs0 = _observed(c, 44)
+    ora15 = po.Restatement(po.LineSetup(lam15, LINE.lambda0, c["cuantic"], psf15, 9), "f64")
+    rng = np.random.default_rng(45)
+    obs1 = np.array([ora15.synth(m, fix=c["fix"], rf=False)[0] for m in _models(c, 64, 46)[-64:]], dtype=np.float32)
+    obs1 += rng.normal(0, 1e-3, obs1.shape).astype(np.float32)
+    with pm.Server(LINE, [g0, g1], hbm_budget_bytes=1 << 28) as srv:
+        alone = srv.wait(srv.submit(0, obs0))
+        ids = [srv.submit(1, obs1), srv.submit(0, obs0), srv.submit(1, obs1)]
+        res = [srv.wait(i) for i in ids]
+    for k in ("models", "chisq", "iters", "status"):
+        assert np.array_equal(res[1][k], alone[k]), k
+        assert np.array_equal(res[2][k], res[0][k]), k
+    for g, obs, r in ((g0, obs0, alone), (g1, obs1, res[0])):
+        with pm.Inverter(LINE, g.lam, g.psf, noise=NOISE64, fix=c["fix"], nterms=9, precision=pm.PREC_FP32) as inv:
+            b = inv.invert(obs, c["guess"])
+        dB = np.abs(r["models"][:, 1] - b["models"][:, 1])
+        assert np.median(dB) < 1.0 and (dB < 5.0).mean() >= 0.85
+
+
+def test_multiplet_limits():
+    """Multiplets are compiled without macroturbulence; a server with one grid
+    inverts with the batch entry point's kernel."""
+    c = zcase("z9")
     with pytest.raises(pm.PmError) as e:
         pm.Inverter(LINE, c["lam"], c["psf"], noise=NOISE64, fix=[1] * 10 + [0], nterms=10)
-    assert e.value.code == -95
+    assert e.value.code == -95  # PM_ENOTSUP
     g = pm.Grid(lam=c["lam"], psf=c["psf"], guess=c["guess"], noise=NOISE64, fix=c["fix"], nterms=9)
-    with pytest.raises(pm.PmError) as e:
-        pm.Server(LINE, [g, g], hbm_budget_bytes=1 << 28)
-    assert e.value.code == -95
     with pm.Server(LINE, [g], hbm_budget_bytes=1 << 28) as srv:
         r = srv.wait(srv.submit(0, np.ascontiguousarray(c["obs"])))
     with zinv(c, pm.PREC_FP32) as inv:
