@@ -96,7 +96,7 @@ typedef struct pm_model {
   double az;    /* azimuth [deg] */
   double S0;    /* source function constant */
   double S1;    /* source function gradient */
-  double mac;   /* macroturbulence [km/s]; > 1e-4 broadens the profiles (grids of <= 32 wavelengths) */
+  double mac;   /* macroturbulence [km/s]; > 1e-4 broadens the profiles */
   double alfa;  /* filling factor */
 } pm_model;
 

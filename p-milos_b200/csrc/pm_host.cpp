@@ -303,8 +303,6 @@ int fill_params(const pm_line* L, const pm_config* c, PmParams& P) {
   // v_mac is inverted; row 9 is v_mac's with NTERMS 11 or 10 and alpha fixed
   P.ff_row = (P.K == 11) ? 10 : ((P.K == 10 && !P.fix[9]) ? 9 : -1);
   P.mac_row = (P.K == 11 || (P.K == 10 && !P.fix[10])) ? 9 : -1;
-  if (P.mac_row >= 0 && P.nl > 32)
-    return fail(PM_ENOTSUP, "macroturbulence on grids of more than 32 wavelengths is outside this implementation");
   if ((L->n_pi > 1 || L->n_sig > 1) && P.mac_row >= 0)
     return fail(PM_ENOTSUP, "Zeeman multiplets are compiled without macroturbulence");
   P.lambda0 = L->lambda0;

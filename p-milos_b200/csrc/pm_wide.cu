@@ -33,7 +33,7 @@ constexpr bool wide_layout_ok() {
   using W = WideSmem<R, G>;
   return offsetof(W, xs) % 16 == 0 && offsetof(W, rf) % 16 == 0 && offsetof(W, ls) % 16 == 0 &&
          offsetof(W, mt) % 16 == 0 && (W::RS * sizeof(R)) % 16 == 0 && (4 * sizeof(R)) % 16 == 0 &&
-         sizeof(W::rf) >= eigen_scratch_doubles<10>() * sizeof(double);
+         sizeof(W::rf) >= eigen_scratch_doubles<11>() * sizeof(double) && sizeof(W) % 16 == 0;
 }
 static_assert(wide_layout_ok<float, 2>() && wide_layout_ok<float, 4>(), "wide shared-memory layout (float)");
 static_assert(wide_layout_ok<double, 2>() && wide_layout_ok<double, 4>(), "wide shared-memory layout (double)");
@@ -117,7 +117,123 @@ __device__ __forceinline__ void psf_wide(const PmParams& P, WideSmem<R, G>& sm, 
   for (int q = 1; q < 4; ++q) S[q] = valid ? acc[q] : R(0);
 }
 
-template <typename R, int G, bool ZM>
+// ---------------------------------------------------------------------------
+// Macroturbulence on a wide grid (the direct branch of mil_sinrf.c:288-357 and
+// me_der.c:314-438, as the one-warp mac_* helpers do it): thread t builds the
+// Gaussian's value at wavelength t, the block normalises it to unit sum (summed
+// in wavelength order, as fgauss does), correlates it with the PSF when there
+// is one (direct_convolution_double, all nl taps, FP64), and the profiles,
+// every response function but S0's and the v_mac row are circular convolutions
+// with it, rotated by nl/2 as convCircular returns them.  The data live in
+// dynamic shared memory after WideSmem, in the macroturbulence instances only.
+// ---------------------------------------------------------------------------
+template <typename R, int G>
+struct alignas(16) MacSmem {
+  static constexpr int NT = 32 * G;
+  double s[2][NT];  // the Gaussian (and its derivative) in FP64 while they are built
+  R k[3 * NT];      // the kernel, tripled: k[u] = kernel[u mod nl] for u < 3 nl
+  R kd[3 * NT];     // the same for the derivative in v_mac
+};
+
+template <typename R, int G>
+__device__ __forceinline__ MacSmem<R, G>& mac_smem(WideSmem<R, G>& sm) {
+  return *reinterpret_cast<MacSmem<R, G>*>(reinterpret_cast<unsigned char*>(&sm) + sizeof(WideSmem<R, G>));
+}
+
+// The kernel of v_mac (and with DERIV its derivative, in the form of
+// me_der.c:419-421) into MacSmem::k (kd).  Every thread of the block calls it;
+// the caller puts a barrier between it and the reads of k / kd.
+template <typename R, int G, bool DERIV>
+__device__ __forceinline__ void mac_kernel_wide(const PmParams& P, WideSmem<R, G>& sm, double mac, int t, bool valid,
+                                                double dl_t) {
+  MacSmem<R, G>& mx = mac_smem(sm);
+  const int nl = P.nl;
+  const double x = valid ? dl_t - P.dl[P.half] : 0.0;  // lambda_t - lambda[nl/2], exactly
+  const double ild = (P.lambda0 * mac) / kVLight;
+  const double a = x / ild;
+  const double term = (a * a) / 2;
+  double g = (valid && term < 1e30) ? exp(-term) : 0.0;
+  mx.s[0][t] = g;
+  __syncthreads();
+  double sum = 0.0;
+  for (int u = 0; u < nl; ++u) sum += mx.s[0][u];
+  g = g / sum;
+  double gd = DERIV ? g / mac * (a * a - 1.0) : 0.0;
+  if (P.has_psf) {
+    __syncthreads();  // every thread has its sum
+    mx.s[0][t] = g;
+    if (DERIV) mx.s[1][t] = gd;
+    __syncthreads();
+    double acc = 0.0, accd = 0.0;
+    for (int j = 0; j < nl; ++j) {
+      const int u = t + j - P.half;
+      if (u >= 0 && u < nl) {
+        acc = fma(P.taps_d[j], mx.s[0][u], acc);
+        if (DERIV) accd = fma(P.taps_d[j], mx.s[1][u], accd);
+      }
+    }
+    g = acc;
+    gd = accd;
+  }
+  if (valid) {
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      mx.k[t + q * nl] = R(g);
+      if (DERIV) mx.kd[t + q * nl] = R(gd);
+    }
+  }
+}
+
+// out[s] at wavelength t: sum_u xs[u][s] k3[(t + nl/2 - u) mod nl] over the
+// unconvolved synthesis in xs; k3 is a tripled kernel of MacSmem.
+template <typename R, int G>
+__device__ __forceinline__ void mac_circular_wide(const PmParams& P, const WideSmem<R, G>& sm, const R* k3, int t,
+                                                  bool valid, R out[4]) {
+  R acc[4] = {R(0), R(0), R(0), R(0)};
+  const R* kb = k3 + (valid ? t : 0) + P.half + P.nl;
+#pragma unroll 2
+  for (int u = 0; u < P.nl; ++u) {
+    const R kk = kb[-u];
+    R x[4];
+    load4<R>(sm.xs[u], x);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[q] = fma(x[q], kk, acc[q]);
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) out[q] = valid ? acc[q] : R(0);
+}
+
+// The 32 response-function profiles of the rows sm.rf[u] convolved circularly
+// with the kernel, at wavelength t.
+template <typename R, int G>
+__device__ __forceinline__ void mac_rf_wide(const PmParams& P, WideSmem<R, G>& sm, int t, bool valid, R (&v)[32]) {
+  constexpr int VEC = WideSmem<R, G>::VEC;
+#pragma unroll
+  for (int p = 0; p < 32; ++p) v[p] = 0;
+  const R* kb = mac_smem(sm).k + (valid ? t : 0) + P.half + P.nl;
+#pragma unroll 1
+  for (int u = 0; u < P.nl; ++u) {
+    const R g = kb[-u];
+    const R* row = sm.rf[u];
+#pragma unroll
+    for (int p = 0; p < 32; p += VEC) {
+      if constexpr (VEC == 4) {
+        const float4 q = *reinterpret_cast<const float4*>(row + p);
+        v[p] = fma(q.x, g, v[p]);
+        v[p + 1] = fma(q.y, g, v[p + 1]);
+        v[p + 2] = fma(q.z, g, v[p + 2]);
+        v[p + 3] = fma(q.w, g, v[p + 3]);
+      } else {
+        const double2 q = *reinterpret_cast<const double2*>(row + p);
+        v[p] = fma(q.x, g, v[p]);
+        v[p + 1] = fma(q.y, g, v[p + 1]);
+      }
+    }
+  }
+}
+
+// MAC: compiled with the macroturbulence branch (the grid has a v_mac row).
+template <typename R, int G, bool ZM, bool MAC>
 __device__ __forceinline__ void synthesize_wide(const PmParams& P, WideSmem<R, G>& sm, const double* m,
                                                 const float* sl_pix, int t, bool valid, double dl_t, R omw_t,
                                                 R S[4], R Su[4]) {
@@ -127,7 +243,17 @@ __device__ __forceinline__ void synthesize_wide(const PmParams& P, WideSmem<R, G
   synth_lane<R, ZM>(P, T, dl_t, st, S);
   copy16(*reinterpret_cast<LaneState<R>*>(sm.ls[t]), st);
   if (t == 0) copy16(sm.mt, T);
-  if (P.has_psf) psf_wide<R, G>(P, sm, t, valid, omw_t, S);
+  const double mac = MAC ? m[9] : 0.0;
+  if (MAC && mac > kMacMin) {
+    // every profile (Stokes I with no continuum padding) convolved circularly;
+    // xs keeps the unconvolved synthesis for the v_mac row
+    if (valid) store4<R>(sm.xs[t], S);
+    mac_kernel_wide<R, G, false>(P, sm, mac, t, valid, dl_t);
+    __syncthreads();
+    mac_circular_wide<R, G>(P, sm, mac_smem(sm).k, t, valid, S);
+  } else if (P.has_psf) {
+    psf_wide<R, G>(P, sm, t, valid, omw_t, S);
+  }
 #pragma unroll
   for (int s = 0; s < 4; ++s) Su[s] = S[s];
   if (P.slight_mode != PM_SLIGHT_NONE) {
@@ -184,9 +310,14 @@ __device__ __forceinline__ void rf_correlate_wide(const PmParams& P, const WideS
 // Response functions of the last synthesis at this thread's wavelength, after
 // correlation, stray light and filling factor (as gather_rf): d[row][stokes].
 // Sff is the spectrum the filling-factor row is built from.
-template <typename R, int KT, int G, bool ZM>
+// mac: v_mac of the model of the last synthesis (MAC instances); dl_t: this
+// thread's wavelength offset.
+template <typename R, int KT, int G, bool ZM, bool MAC>
 __device__ __forceinline__ void rf_wide(const PmParams& P, WideSmem<R, G>& sm, int t, bool valid, R omw_t,
-                                        const R Sff[4], const float* sl_pix, R (&d)[KT][4]) {
+                                        const R Sff[4], const float* sl_pix, double mac, double dl_t,
+                                        R (&d)[KT][4]) {
+  const bool mac_on = MAC && mac > kMacMin;
+  if (mac_on) mac_kernel_wide<R, G, true>(P, sm, mac, t, valid, dl_t);
   R alf;
   {
     ModelTerms<R> T;
@@ -198,7 +329,11 @@ __device__ __forceinline__ void rf_wide(const PmParams& P, WideSmem<R, G>& sm, i
   }
   __syncthreads();
   R v[32];
-  if (P.has_psf) {
+  R dmac[4] = {R(0), R(0), R(0), R(0)};
+  if (mac_on) {
+    mac_rf_wide<R, G>(P, sm, t, valid, v);
+    mac_circular_wide<R, G>(P, sm, mac_smem(sm).kd, t, valid, dmac);
+  } else if (P.has_psf) {
     rf_correlate_wide<R, G>(P, sm, t, omw_t, v);
   } else {
 #pragma unroll
@@ -212,6 +347,7 @@ __device__ __forceinline__ void rf_wide(const PmParams& P, WideSmem<R, G>& sm, i
       if (r < 7) x = v[r * 4 + s];
       else if (r == 7) x = (s == 0) ? R(1) : R(0);  // S0 (me_der.c:301-306)
       else if (r == 8) x = v[7 * 4 + s];
+      else if (MAC && r == 9 && P.mac_row == 9) x = dmac[s];  // zero while v_mac <= 1e-4
       else x = R(0);
       d[r][s] = valid ? x : R(0);
     }
@@ -287,12 +423,13 @@ __device__ __forceinline__ double chisq_wide(const PmParams& P, WideSmem<R, G>& 
   return acc[0] / nfree;
 }
 
-template <typename R, int KT, int G, bool ZM>
+template <typename R, int KT, int G, bool ZM, bool MAC>
 __device__ __forceinline__ void rf_and_normal_eq_wide(const PmParams& P, WideSmem<R, G>& sm, int& slot, int t,
                                                       bool valid, R omw_t, const R S[4], const R Sff[4],
-                                                      const float O[4], const R isig[4], const float* sl_pix) {
+                                                      const float O[4], const R isig[4], const float* sl_pix,
+                                                      double mac, double dl_t) {
   R d[KT][4];
-  rf_wide<R, KT, G, ZM>(P, sm, t, valid, omw_t, Sff, sl_pix, d);
+  rf_wide<R, KT, G, ZM, MAC>(P, sm, t, valid, omw_t, Sff, sl_pix, mac, dl_t, d);
 #pragma unroll
   for (int r = 0; r < KT; ++r)
     if (P.zero_row[r]) {
@@ -304,8 +441,9 @@ __device__ __forceinline__ void rf_and_normal_eq_wide(const PmParams& P, WideSme
 
 // lm_mils over pixels of a wide grid: the control flow of invert_pixel with
 // block-wide reductions; the solve and the trial model come from warp 0.
-// ZM: the line is a Zeeman multiplet (a separate instance, as in the one-warp kernel).
-template <typename R, int KT, int G, int MINB, bool ZM>
+// ZM: the line is a Zeeman multiplet (a separate instance, as in the one-warp
+// kernel); MAC: the grid has a v_mac row (dynamic shared memory holds MacSmem).
+template <typename R, int KT, int G, int MINB, bool ZM, bool MAC>
 __global__ void __launch_bounds__(32 * G, MINB) invert_wide_kernel(const __grid_constant__ PmParams P,
                                                                      const PmIO io) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -383,7 +521,7 @@ __global__ void __launch_bounds__(32 * G, MINB) invert_wide_kernel(const __grid_
           __syncthreads();
         }
         R Su[4];
-        synthesize_wide<R, G, ZM>(P, sm, trial, sl_pix, t, valid, dl_t, omw_t, S, Su);
+        synthesize_wide<R, G, ZM, MAC>(P, sm, trial, sl_pix, t, valid, dl_t, omw_t, S, Su);
         const double chi = chisq_wide<R, G>(P, sm, slot, S, O, isig, valid, double(nfree));
         bool accept = true;
         if (!first) {
@@ -401,7 +539,8 @@ __global__ void __launch_bounds__(32 * G, MINB) invert_wide_kernel(const __grid_
           R Sff[4];
 #pragma unroll
           for (int s = 0; s < 4; ++s) Sff[s] = first ? Su[s] : S[s];
-          rf_and_normal_eq_wide<R, KT, G, ZM>(P, sm, slot, t, valid, omw_t, S, Sff, O, isig, sl_pix);
+          rf_and_normal_eq_wide<R, KT, G, ZM, MAC>(P, sm, slot, t, valid, omw_t, S, Sff, O, isig, sl_pix,
+                                                   MAC ? trial[9] : 0.0, dl_t);
           ochi = chi;
           if (first) chi0 = chi;
           else ++accepted;
@@ -492,7 +631,7 @@ __global__ void __launch_bounds__(32 * G) classical_wide_kernel(const __grid_con
 }
 
 // Synthesis (and response functions) of given models on a wide grid.
-template <typename R, int KT, int G, bool ZM>
+template <typename R, int KT, int G, bool ZM, bool MAC>
 __global__ void __launch_bounds__(32 * G) synth_wide_kernel(const __grid_constant__ PmParams P, const PmIO io) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WideSmem<R, G>& sm = *reinterpret_cast<WideSmem<R, G>*>(smem_raw);
@@ -506,7 +645,7 @@ __global__ void __launch_bounds__(32 * G) synth_wide_kernel(const __grid_constan
     if (t < 11) sm.model[t] = io.models_in[size_t(pix) * 11 + t];
     __syncthreads();
     R S[4], Su[4];
-    synthesize_wide<R, G, ZM>(P, sm, sm.model, sl_pix, t, valid, dl_t, omw_t, S, Su);
+    synthesize_wide<R, G, ZM, MAC>(P, sm, sm.model, sl_pix, t, valid, dl_t, omw_t, S, Su);
     if (valid) {
 #pragma unroll
       for (int s = 0; s < 4; ++s) io.spectra_out[base + s * P.nl + t] = float(S[s]);
@@ -514,7 +653,7 @@ __global__ void __launch_bounds__(32 * G) synth_wide_kernel(const __grid_constan
     if (io.rf_out) {
       __syncthreads();  // the model terms from thread 0
       R d[KT][4];
-      rf_wide<R, KT, G, ZM>(P, sm, t, valid, omw_t, Su, sl_pix, d);
+      rf_wide<R, KT, G, ZM, MAC>(P, sm, t, valid, omw_t, Su, sl_pix, MAC ? sm.model[9] : 0.0, dl_t, d);
       if (valid) {
         const size_t rb = size_t(pix) * 4 * KT * P.nl;
 #pragma unroll
@@ -531,9 +670,22 @@ __global__ void __launch_bounds__(32 * G) synth_wide_kernel(const __grid_constan
 template <typename R, int KT, int G, int MINB>
 int launch_invert_wide(const PmParams& P, const PmIO& io, cudaStream_t st, int num_sms, float* kernel_ms) {
   const int threads = 32 * G;
-  const size_t smem = sizeof(WideSmem<R, G>);
-  auto kern = (P.n_pi > 1 || P.n_sig > 1) ? invert_wide_kernel<R, KT, G, MINB, true>
-                                           : invert_wide_kernel<R, KT, G, MINB, false>;
+  const bool mac = P.mac_row >= 0, zm = P.n_pi > 1 || P.n_sig > 1;
+  size_t smem = sizeof(WideSmem<R, G>);
+  void (*kern)(const PmParams, const PmIO) = nullptr;
+  if constexpr (KT >= 10) {
+    if (mac && !zm) {
+      kern = invert_wide_kernel<R, KT, G, MINB, false, true>;
+      smem += sizeof(MacSmem<R, G>);
+    }
+  }
+  if constexpr (KT <= 10) {
+    if (!mac) kern = zm ? invert_wide_kernel<R, KT, G, MINB, true, false> : invert_wide_kernel<R, KT, G, MINB, false, false>;
+  }
+  if (!kern)
+    return snprintf(pmk_g_err, sizeof pmk_g_err, "no wide kernel for nterms=%d (v_mac row %d, multiplet %d)", KT,
+                    int(mac), int(zm)),
+           PM_ENOTSUP;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return snprintf(pmk_g_err, sizeof pmk_g_err, "%s", cudaGetErrorString(e)), PM_EIO;
   int per_sm = 0;
@@ -569,8 +721,22 @@ int launch_invert_wide(const PmParams& P, const PmIO& io, cudaStream_t st, int n
 template <typename R, int KT, int G>
 int launch_synth_wide(const PmParams& P, const PmIO& io, cudaStream_t st) {
   const int threads = 32 * G;
-  const size_t smem = sizeof(WideSmem<R, G>);
-  auto kern = (P.n_pi > 1 || P.n_sig > 1) ? synth_wide_kernel<R, KT, G, true> : synth_wide_kernel<R, KT, G, false>;
+  const bool mac = P.mac_row >= 0, zm = P.n_pi > 1 || P.n_sig > 1;
+  size_t smem = sizeof(WideSmem<R, G>);
+  void (*kern)(const PmParams, const PmIO) = nullptr;
+  if constexpr (KT >= 10) {
+    if (mac && !zm) {
+      kern = synth_wide_kernel<R, KT, G, false, true>;
+      smem += sizeof(MacSmem<R, G>);
+    }
+  }
+  if constexpr (KT <= 10) {
+    if (!mac) kern = zm ? synth_wide_kernel<R, KT, G, true, false> : synth_wide_kernel<R, KT, G, false, false>;
+  }
+  if (!kern)
+    return snprintf(pmk_g_err, sizeof pmk_g_err, "no wide kernel for nterms=%d (v_mac row %d, multiplet %d)", KT,
+                    int(mac), int(zm)),
+           PM_ENOTSUP;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return snprintf(pmk_g_err, sizeof pmk_g_err, "%s", cudaGetErrorString(e)), PM_EIO;
   int64_t blocks = io.npix;
@@ -593,11 +759,15 @@ int pmk_invert_wide(const PmParams& P, const PmIO& io, int precision, void* stre
                              : launch_invert_wide<double, 9, 2, 1>(P, io, st, num_sms, kernel_ms);
     if (P.K == 10) return f32 ? launch_invert_wide<float, 10, 2, 8>(P, io, st, num_sms, kernel_ms)
                               : launch_invert_wide<double, 10, 2, 1>(P, io, st, num_sms, kernel_ms);
+    if (P.K == 11) return f32 ? launch_invert_wide<float, 11, 2, 8>(P, io, st, num_sms, kernel_ms)
+                              : launch_invert_wide<double, 11, 2, 1>(P, io, st, num_sms, kernel_ms);
   } else if (P.G == 4) {
     if (P.K == 9) return f32 ? launch_invert_wide<float, 9, 4, 4>(P, io, st, num_sms, kernel_ms)
                              : launch_invert_wide<double, 9, 4, 1>(P, io, st, num_sms, kernel_ms);
     if (P.K == 10) return f32 ? launch_invert_wide<float, 10, 4, 4>(P, io, st, num_sms, kernel_ms)
                               : launch_invert_wide<double, 10, 4, 1>(P, io, st, num_sms, kernel_ms);
+    if (P.K == 11) return f32 ? launch_invert_wide<float, 11, 4, 4>(P, io, st, num_sms, kernel_ms)
+                              : launch_invert_wide<double, 11, 4, 1>(P, io, st, num_sms, kernel_ms);
   }
   snprintf(pmk_g_err, sizeof pmk_g_err, "no wide kernel for nl=%d (G=%d), nterms=%d", P.nl, P.G, P.K);
   return PM_ENOTSUP;
@@ -609,9 +779,11 @@ int pmk_synth_wide(const PmParams& P, const PmIO& io, int precision, void* strea
   if (P.G == 2) {
     if (P.K == 9) return f32 ? launch_synth_wide<float, 9, 2>(P, io, st) : launch_synth_wide<double, 9, 2>(P, io, st);
     if (P.K == 10) return f32 ? launch_synth_wide<float, 10, 2>(P, io, st) : launch_synth_wide<double, 10, 2>(P, io, st);
+    if (P.K == 11) return f32 ? launch_synth_wide<float, 11, 2>(P, io, st) : launch_synth_wide<double, 11, 2>(P, io, st);
   } else if (P.G == 4) {
     if (P.K == 9) return f32 ? launch_synth_wide<float, 9, 4>(P, io, st) : launch_synth_wide<double, 9, 4>(P, io, st);
     if (P.K == 10) return f32 ? launch_synth_wide<float, 10, 4>(P, io, st) : launch_synth_wide<double, 10, 4>(P, io, st);
+    if (P.K == 11) return f32 ? launch_synth_wide<float, 11, 4>(P, io, st) : launch_synth_wide<double, 11, 4>(P, io, st);
   }
   snprintf(pmk_g_err, sizeof pmk_g_err, "no wide kernel for nl=%d (G=%d), nterms=%d", P.nl, P.G, P.K);
   return PM_ENOTSUP;

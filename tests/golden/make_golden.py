@@ -36,7 +36,9 @@ Writes
   ref_cases_mac.npz   macroturbulence on the 30-point grid: m10 (v_mac inverted,
                       60 mA PSF), m10n (the same without PSF), m11 (v_mac and
                       the filling factor inverted, stray light), mfix (v_mac
-                      fixed at 1.2 km/s); 24 pixels and 8 synthesis models each
+                      fixed at 1.2 km/s); 24 pixels and 8 synthesis models each;
+                      and on wider grids: mw10 (as m10, 49 points) and mw11 (as
+                      m11, 112 points), 16 pixels and 4 models each
 The fixtures are what the CPU test-suite compares the oracle restatement and the
 host precompute with, so those tests need neither the reference nor a GPU.
 """
@@ -107,15 +109,22 @@ MAC_SPECS = {
     "m10n": (None, False, True),
     "m11": (60.0, True, True),
     "mfix": (60.0, False, False),
+    "mw10": (60.0, False, True),
+    "mw11": (60.0, True, True),
 }
+# grids of the cases that are not on the configuration-1 grid (25 mA steps)
+MAC_GRIDS = {"mw10": (-600.0, 25.0, 600.0), "mw11": (-1387.5, 25.0, 1387.5)}
 
 
 def mac_case(name, npix=24, nsynth=8):
-    """Macroturbulence on the configuration-1 grid: truths with v_mac in
-    U(0.3, 3) km/s, guess v_mac = 1 (1.2 and fixed for mfix)."""
+    """Macroturbulence on the configuration-1 grid (49 and 112 points for the mw
+    cases): truths with v_mac in U(0.3, 3) km/s, guess v_mac = 1 (1.2 and fixed
+    for mfix)."""
     fwhm, stray, free = MAC_SPECS[name]
     rng = np.random.default_rng(sum(ord(ch) for ch in name) + 2000)
     (ini, step, fin, l0) = CASE_SPECS[1][0]
+    if name in MAC_GRIDS:
+        ini, step, fin = MAC_GRIDS[name]
     offs, lam = grid(ini, step, fin, l0)
     psf = None
     if fwhm is not None:
@@ -418,7 +427,7 @@ def main():
         return
     mac = {}
     for name in MAC_SPECS:
-        for k, v in mac_case(name).items():
+        for k, v in mac_case(name, *((16, 4) if name in MAC_GRIDS else (24, 8))).items():
             mac[f"{name}_{k}"] = v
     np.savez_compressed(os.path.join(HERE, "ref_cases_mac.npz"), **mac)
     print("ref_cases_mac.npz", os.path.getsize(os.path.join(HERE, "ref_cases_mac.npz")), "bytes")

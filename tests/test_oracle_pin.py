@@ -125,11 +125,11 @@ MAC = np.load(os.path.join(GOLDEN, "ref_cases_mac.npz"))
 
 
 @pytest.mark.parametrize("flav", ["f32", "f64"])
-@pytest.mark.parametrize("name", ["m10", "m10n", "m11", "mfix"])
+@pytest.mark.parametrize("name", ["m10", "m10n", "m11", "mfix", "mw10", "mw11"])
 def test_macroturbulence_bit_exact(name, flav):
     """Macroturbulence (fgauss, the circular convolutions of mil_sinrf and
     me_der, with and without the PSF, v_mac inverted or fixed, with the filling
-    factor): full inversions on a fresh context (the order the fixture was made
+    factor; on 30, 49 and 112 wavelengths): full inversions on a fresh context (the order the fixture was made
     in, since the v_mac response row persists between calls as in the
     reference), then synthesis and every response function, equal the
     reference's bit for bit."""
