@@ -101,9 +101,8 @@ typedef struct pm_model {
 } pm_model;
 
 /* Spectral line: what create_cuantic (create_cuantic.c:24-294) and wlines[1]
- * provide to the reference.  Strengths and splittings are per Zeeman group.
- * Multiplets (n_pi or n_sig > 1) run without macroturbulence (NTERMS 9, or 10
- * with the filling factor); with a v_mac row they are PM_ENOTSUP. */
+ * provide to the reference.  Strengths and splittings are per Zeeman group
+ * (normal triplets and multiplets alike). */
 typedef struct pm_line {
   double lambda0;   /* line centre [A] (wlines[1]) */
   int n_pi;         /* components in the pi group (N_PI) */

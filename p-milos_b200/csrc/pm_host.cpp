@@ -303,8 +303,6 @@ int fill_params(const pm_line* L, const pm_config* c, PmParams& P) {
   // v_mac is inverted; row 9 is v_mac's with NTERMS 11 or 10 and alpha fixed
   P.ff_row = (P.K == 11) ? 10 : ((P.K == 10 && !P.fix[9]) ? 9 : -1);
   P.mac_row = (P.K == 11 || (P.K == 10 && !P.fix[10])) ? 9 : -1;
-  if ((L->n_pi > 1 || L->n_sig > 1) && P.mac_row >= 0)
-    return fail(PM_ENOTSUP, "Zeeman multiplets are compiled without macroturbulence");
   P.lambda0 = L->lambda0;
   for (int i = 0; i < P.nl; ++i) P.dl[i] = c->lambda[i] - L->lambda0;
   for (int k = 0; k < L->n_pi; ++k) { P.nu[0][k] = L->nup[k]; P.we[0][k] = L->wep[k]; }

@@ -142,10 +142,10 @@ int pmk_classical_prepass(const PmParams& P, const float* spectro, double* model
 int pmk_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, int precision, int variant, int warps_per_block,
                       bool multi, void* stream, int num_sms, size_t* smem_out, int reserve_blocks = 0,
                       bool pixgrid = false);
-// The same for a Zeeman multiplet without a macroturbulence row (pm_stream_zm.cu):
-// its own kernel instances, so the triplet kernels keep their register budget.
+// The same for a Zeeman multiplet (pm_stream_zm.cu): its own kernel instances, so
+// the triplet kernels keep their register budget.  mac: a grid has a v_mac row.
 int pmk_invert_stream_zm(const PmGridSet& GS, const PmStreamIO& sio, int precision, int warps_per_block, bool multi,
-                         void* stream, int num_sms, size_t* smem_out, int reserve_blocks, bool pixgrid);
+                         void* stream, int num_sms, size_t* smem_out, int reserve_blocks, bool pixgrid, bool mac);
 const char* pmk_last_cuda_error();
 
 // Host helpers (pm_host.cpp) shared with pm_noalloc.cu.

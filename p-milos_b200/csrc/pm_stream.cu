@@ -94,13 +94,9 @@ int pmk_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, int precision,
     mac = mac || GS.g[g].mac_row >= 0;
     zm = zm || GS.g[g].n_pi > 1 || GS.g[g].n_sig > 1;
   }
-  if (zm) {
-    if (mac) {
-      snprintf(pmk_g_err, sizeof pmk_g_err, "Zeeman multiplets: no macroturbulence row");
-      return PM_ENOTSUP;
-    }
-    return pmk_invert_stream_zm(GS, sio, precision, wpb, multi, stream, num_sms, smem_out, reserve_blocks, pixgrid);
-  }
+  if (zm)
+    return pmk_invert_stream_zm(GS, sio, precision, wpb, multi, stream, num_sms, smem_out, reserve_blocks, pixgrid,
+                                mac);
   if (precision == PM_PREC_FP32)
     return launch_stream_k<float>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve_blocks, K, mac, pixgrid);
   return launch_stream_k<double>(GS, sio, st, num_sms, variant, wpb, multi, smem_out, reserve_blocks, K, mac, pixgrid);

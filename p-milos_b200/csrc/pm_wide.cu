@@ -674,8 +674,8 @@ int launch_invert_wide(const PmParams& P, const PmIO& io, cudaStream_t st, int n
   size_t smem = sizeof(WideSmem<R, G>);
   void (*kern)(const PmParams, const PmIO) = nullptr;
   if constexpr (KT >= 10) {
-    if (mac && !zm) {
-      kern = invert_wide_kernel<R, KT, G, MINB, false, true>;
+    if (mac) {
+      kern = zm ? invert_wide_kernel<R, KT, G, MINB, true, true> : invert_wide_kernel<R, KT, G, MINB, false, true>;
       smem += sizeof(MacSmem<R, G>);
     }
   }
@@ -725,8 +725,8 @@ int launch_synth_wide(const PmParams& P, const PmIO& io, cudaStream_t st) {
   size_t smem = sizeof(WideSmem<R, G>);
   void (*kern)(const PmParams, const PmIO) = nullptr;
   if constexpr (KT >= 10) {
-    if (mac && !zm) {
-      kern = synth_wide_kernel<R, KT, G, false, true>;
+    if (mac) {
+      kern = zm ? synth_wide_kernel<R, KT, G, true, true> : synth_wide_kernel<R, KT, G, false, true>;
       smem += sizeof(MacSmem<R, G>);
     }
   }

@@ -31,8 +31,10 @@ Writes
                       and four sigma components per group), 60 mA PSF: z9 and
                       z10 on a 30-point grid, zw9 on 49 points and zw10 on 112
                       points (25 mA steps); the *10 cases add stray light and
-                      invert the filling factor; 24 pixels and 8 synthesis
-                      models each (16 and 4 on the wide grids)
+                      invert the filling factor; with v_mac inverted: zm10 on
+                      30 points and zmw11 on 112 (stray light and filling
+                      factor too); 24 pixels and 8 synthesis models each (16
+                      and 4 on the wide grids)
   ref_cases_mac.npz   macroturbulence on the 30-point grid: m10 (v_mac inverted,
                       60 mA PSF), m10n (the same without PSF), m11 (v_mac and
                       the filling factor inverted, stray light), mfix (v_mac
@@ -176,21 +178,26 @@ def mac_case(name, npix=24, nsynth=8):
 
 MULTIPLET = np.array([1.0, 2.0, 1.0, 2.0, 2.0, 2.0, 2.0])  # 5P 2.0 - 5D 2.0
 LAMBDA_6301 = 6301.5012
-ZEEMAN_GRIDS = {"z9": (-350.0, 25.0, 375.0), "z10": (-350.0, 25.0, 375.0),
-                "zw9": (-600.0, 25.0, 600.0), "zw10": (-1387.5, 25.0, 1387.5)}
+G30, G49, G112 = (-350.0, 25.0, 375.0), (-600.0, 25.0, 600.0), (-1387.5, 25.0, 1387.5)
+# name: grid, stray light + filling factor, v_mac inverted
+ZEEMAN_SPECS = {"z9": (G30, False, False), "z10": (G30, True, False), "zw9": (G49, False, False),
+                "zw10": (G112, True, False), "zm10": (G30, False, True), "zmw11": (G112, True, True)}
 
 
 def zeeman_case(name, npix=24, nsynth=8):
     """A multiplet line (LINES entry 2 of the reference's run directory) with the
-    configuration-1 atmospheres; the *10 cases add stray light and the filling factor."""
-    stray = name.endswith("10")
+    configuration-1 atmospheres; stray light and the filling factor, and v_mac
+    in U(0.3, 3) km/s inverted from a guess of 1, as ZEEMAN_SPECS says."""
+    grid_spec, stray, mac = ZEEMAN_SPECS[name]
     rng = np.random.default_rng(sum(ord(ch) for ch in name) + 3000)
-    offs, lam = grid(*ZEEMAN_GRIDS[name], LAMBDA_6301)
+    offs, lam = grid(*grid_spec, LAMBDA_6301)
     x, y = gauss_table(60.0)
     psf = po.Reference(po.LineSetup(lam, LAMBDA_6301, MULTIPLET, None, 9), "f64").interp_psf(x, y, offs, 0.0)
-    K = 10 if stray else 9
-    fix = [1] * 9 + [0, 1 if stray else 0]
+    K = 9 + int(stray) + int(mac)
+    fix = [1] * 9 + [1 if mac else 0, 1 if stray else 0]
     guess = GUESS.copy()
+    if mac:
+        guess[9] = 1.0
     if stray:
         guess[10] = 0.9
     truth = np.zeros((npix, 11))
@@ -203,6 +210,8 @@ def zeeman_case(name, npix=24, nsynth=8):
     truth[:, 6] = rng.uniform(0, 180, npix)
     truth[:, 7] = rng.uniform(0.1, 0.4, npix)
     truth[:, 8] = rng.uniform(0.4, 0.9, npix)
+    if mac:
+        truth[:, 9] = rng.uniform(0.3, 3.0, npix)
     truth[:, 10] = 1.0 - rng.uniform(0, 0.3, npix) if stray else 1.0
     slight = None
     if stray:
@@ -418,8 +427,8 @@ def main():
     if a.only == "fits":
         return
     zee = {}
-    for name in ZEEMAN_GRIDS:
-        for k, v in zeeman_case(name, *((16, 4) if name.startswith("zw") else (24, 8))).items():
+    for name in ZEEMAN_SPECS:
+        for k, v in zeeman_case(name, *((24, 8) if ZEEMAN_SPECS[name][0] == G30 else (16, 4))).items():
             zee[f"{name}_{k}"] = v
     np.savez_compressed(os.path.join(HERE, "ref_cases_zeeman.npz"), **zee)
     print("ref_cases_zeeman.npz", os.path.getsize(os.path.join(HERE, "ref_cases_zeeman.npz")), "bytes")

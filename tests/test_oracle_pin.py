@@ -178,11 +178,12 @@ ZEE = np.load(os.path.join(GOLDEN, "ref_cases_zeeman.npz"))
 
 
 @pytest.mark.parametrize("flav", ["f32", "f64"])
-@pytest.mark.parametrize("name", ["z9", "z10", "zw9", "zw10"])
+@pytest.mark.parametrize("name", ["z9", "z10", "zw9", "zw10", "zm10", "zmw11"])
 def test_zeeman_multiplet_bit_exact(name, flav):
     """A multiplet (Fe I 6301.5, five pi and four sigma components per group) on
-    30, 49 and 112 wavelengths: inversions, synthesis and every response
-    function equal the reference's, and so does the Zeeman pattern."""
+    30, 49 and 112 wavelengths, with and without macroturbulence: inversions (on
+    a fresh context, the order the fixture was made in), synthesis and every
+    response function equal the reference's, and so does the Zeeman pattern."""
     g = lambda k: ZEE[f"{name}_{k}"]
     ora = po.Restatement(po.LineSetup(g("lam"), float(g("lambda0")), g("cuantic"), g("psf"), int(g("nterms"))), flav)
     sl = g("slight") if g("slight").size else None
