@@ -217,8 +217,8 @@ int pm_synth_batch(pm_ctx *ctx, int64_t npix, const pm_model *models, const floa
  * pixel is inverted as the reference inverts a cube whose single grid is that
  * pixel's -- synthesis, macroturbulence kernel and classical estimates on the
  * pixel's own wavelengths, the context's PSF taps (sampled at the grid step)
- * for every pixel.  Grids of at most 32 wavelengths (else PM_ENOTSUP); host
- * buffers are copied in, then inverted (no pipelining). */
+ * for every pixel.  Every grid width (2..PM_NL_MAX); host buffers are copied
+ * in, then inverted, chunk by chunk (no pipelining). */
 int pm_invert_batch_grids(pm_ctx *ctx, int64_t npix, const float *spectro, const double *lambda,
                           const float *slight, int slight_mode, const pm_model *guess, pm_model *models_out,
                           float *chisq_out, int *iters_out, float *best_fit_out, int *status_out, int mem);

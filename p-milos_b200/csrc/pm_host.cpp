@@ -910,8 +910,6 @@ int invert_impl(pm_ctx* c, int64_t npix, const float* spectro, const double* lam
     return fail(PM_EINVAL, "pm_invert_batch: NULL argument");
   if (npix < 0) return fail(PM_EINVAL, "pm_invert_batch: npix < 0");
   if (mem != PM_MEM_HOST && mem != PM_MEM_DEVICE) return fail(PM_EINVAL, "pm_invert_batch: mem=%d", mem);
-  if (lambda && c->P.G != 1)
-    return fail(PM_ENOTSUP, "pixel wavelength grids: grids of at most 32 wavelengths (nlambda=%d)", c->P.nl);
   if (int rc = check_guess(c->P, guess); rc != PM_OK) return rc;
   c->stats = pm_stats{};
   if (npix == 0) return PM_OK;
@@ -949,8 +947,8 @@ int invert_impl(pm_ctx* c, int64_t npix, const float* spectro, const double* lam
                              sizeof(pm_model) + sizeof(float) + 2 * sizeof(int) + lam_bytes;
     // wide grids go through two buffer sets (run_wide_pipelined), in at least 8
     // chunks when the cube is large, so that only the first chunk's copy is not
-    // hidden behind an inversion
-    const int sets = c->P.G != 1 ? 2 : 1;
+    // hidden behind an inversion; per-pixel grids copy, then launch, chunk by chunk
+    const int sets = (c->P.G != 1 && !lambda) ? 2 : 1;
     int64_t chunk = std::min<int64_t>(npix, std::max<int64_t>(32, int64_t(c->resident_bytes / (per_pixel * sets))));
     if (sets == 2 && npix >= 8 * 4096) chunk = std::min<int64_t>(chunk, (npix / 8 + 31) / 32 * 32);
     const int64_t cap = chunk * sets;
@@ -1062,8 +1060,6 @@ namespace {
 int synth_impl(pm_ctx* c, int64_t npix, const pm_model* models, const double* lambda, const float* slight,
                int slight_mode, float* spectra_out, float* rf_out, int mem) {
   if (!c || !models || !spectra_out) return fail(PM_EINVAL, "pm_synth_batch: NULL argument");
-  if (lambda && c->P.G != 1)
-    return fail(PM_ENOTSUP, "pixel wavelength grids: grids of at most 32 wavelengths (nlambda=%d)", c->P.nl);
   if (npix < 0) return fail(PM_EINVAL, "pm_synth_batch: npix < 0");
   if (mem != PM_MEM_HOST && mem != PM_MEM_DEVICE) return fail(PM_EINVAL, "pm_synth_batch: mem=%d", mem);
   if (npix == 0) return PM_OK;

@@ -125,6 +125,12 @@ int pmk_synth(const PmParams& P, const PmIO& io, int precision, void* stream);
 // Grids of more than 32 wavelengths (pm_wide.cu), called by pmk_invert / pmk_synth.
 int pmk_invert_wide(const PmParams& P, const PmIO& io, int precision, void* stream, int num_sms, float* kernel_ms);
 int pmk_synth_wide(const PmParams& P, const PmIO& io, int precision, void* stream);
+// Their instances for multiplets, macroturbulence and per-pixel grids, by
+// precision (pm_wide_x32.cu, pm_wide_x64.cu).
+int pmk_invert_wide_x32(const PmParams& P, const PmIO& io, void* stream, int num_sms, float* kernel_ms);
+int pmk_invert_wide_x64(const PmParams& P, const PmIO& io, void* stream, int num_sms, float* kernel_ms);
+int pmk_synth_wide_x32(const PmParams& P, const PmIO& io, void* stream);
+int pmk_synth_wide_x64(const PmParams& P, const PmIO& io, void* stream);
 // Classical estimates of npix pixels (one-warp grid) into models [npix][11]:
 // the starting models of a launch whose cube is on the device before it starts.
 // lambda: [npix][nl] absolute wavelengths of each pixel, or nullptr (the grid's).

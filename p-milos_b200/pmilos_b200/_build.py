@@ -14,8 +14,8 @@ ROOT = os.path.dirname(PKG_DIR)                  # p-milos_b200/
 CSRC = os.path.join(ROOT, "csrc")
 OBJ = os.path.join(ROOT, "_build")
 OUT = os.path.join(ROOT, "libpmilos_b200.so")
-SOURCES = ("pm_kernels.cu", "pm_wide.cu", "pm_stream.cu", "pm_stream_zm.cu", "pm_noalloc.cu", "pm_fits.cu",
-           "pm_host.cpp", "pm_server.cpp")
+SOURCES = ("pm_kernels.cu", "pm_wide.cu", "pm_wide_x32.cu", "pm_wide_x64.cu", "pm_stream.cu", "pm_stream_zm.cu",
+           "pm_noalloc.cu", "pm_fits.cu", "pm_host.cpp", "pm_server.cpp")
 ARCH = "-gencode=arch=compute_100a,code=sm_100a"
 FLAGS = ["-std=c++17", "-O3", ARCH, "-lineinfo", "-Xcompiler", "-fPIC"]
 

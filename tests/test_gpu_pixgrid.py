@@ -1,16 +1,21 @@
 """Per-pixel wavelength grids (pm_invert_batch_grids / pm_synth_batch_grids).
 
-Every pixel has its own 30-point grid: the configuration-1 grid stretched by up
-to 1e-3 and shifted by up to +-20 mA, as a telecentric Fabry-Perot's cavity
-errors shift it across the field.  The expected result of a pixel is the
-oracle's (the reference's, bit for bit) inversion of that pixel on a single grid
-equal to its own, with the context's PSF taps.
+Every pixel has its own grid: the configuration-1 grid (30 points; 112 points of
+tests/golden/ref_cases_wide.npz, 49 points with macroturbulence of
+ref_cases_mac.npz for the wide-grid kernels) stretched by up to 1e-3 and shifted
+by up to +-20 mA, as a telecentric Fabry-Perot's cavity errors shift it across
+the field.  The expected result of a pixel is the oracle's (the reference's, bit
+for bit) inversion of that pixel on a single grid equal to its own, with the
+context's PSF taps.
 """
+import os
+
 import numpy as np
 import pytest
 
 import pmilos_b200 as pm
 import pyoracle as po
+from conftest import GOLDEN
 from gpu_common import LINE_6173, NOISE64, case, within_tolerance
 
 pytestmark = pytest.mark.gpu
@@ -18,9 +23,8 @@ pytestmark = pytest.mark.gpu
 CUANTIC = np.array([1.0, *LINE_6173[1]])
 
 
-def grids(base, n, seed):
+def grids(base, n, seed, l0=LINE_6173[0]):
     rng = np.random.default_rng(seed)
-    l0 = LINE_6173[0]
     scale = 1.0 + rng.uniform(-1e-3, 1e-3, n)
     shift = rng.uniform(-0.020, 0.020, n)
     return l0 + (base[None, :] - l0) * scale[:, None] + shift[:, None]
@@ -138,8 +142,79 @@ def test_device_buffers_and_errors():
         assert np.array_equal(dev["iters"].cpu().numpy(), host["iters"])
         with pytest.raises(ValueError):
             inv.invert(c["obs"], c["guess"], lam=lam[:-1])
-    wide = np.linspace(6172.5, 6174.0, 49)
-    with pm.Inverter(pm.LineData(*LINE_6173), wide, None, noise=NOISE64, fix=c["fix"], nterms=9) as inv:
-        with pytest.raises(pm.PmError) as e:
-            inv.invert(np.zeros((2, 4, 49), np.float32), c["guess"], lam=np.tile(wide, (2, 1)))
-        assert e.value.code == -95  # PM_ENOTSUP
+
+
+# ---- grids wider than one warp ----
+TRIPLET = (2.0, 1.0, 1.0, 2.0, 2.0, 0.0)
+
+
+def wide_case(name):
+    """w112: the 112-point configuration-4 grid (Fe I 6302.4936, 25 mA PSF, nine
+    parameters); mw10: 49 points with v_mac inverted (Fe I 6173.3354, 60 mA PSF)."""
+    src = np.load(os.path.join(GOLDEN, "ref_cases_wide.npz" if name == "w112" else "ref_cases_mac.npz"))
+    g = lambda k: src[f"{name}_{k}"]
+    return dict(lam=g("lam"), l0=float(g("lambda0")), psf=g("psf"), fix=list(g("fix")), nterms=int(g("nterms")),
+                guess=g("guess"), mac=name == "mw10")
+
+
+def wide_inverter(c, precision, solver=pm.SOLVE_DEFAULT):
+    return pm.Inverter(pm.LineData(c["l0"], TRIPLET), c["lam"], c["psf"], noise=NOISE64, fix=c["fix"],
+                       nterms=c["nterms"], precision=precision, solver=solver)
+
+
+def wide_oracles(c, lam, flav="f64"):
+    return [po.Restatement(po.LineSetup(l, c["l0"], np.array([1.0, *TRIPLET]), c["psf"], c["nterms"]), flav)
+            for l in lam]
+
+
+@pytest.mark.parametrize("name", ["w112", "mw10"])
+def test_wide_synthesis_on_each_pixels_grid(name):
+    """Two and four warps per pixel: the synthesis and every response function
+    (the v_mac row and its kernel, centred on the pixel's own middle wavelength,
+    included) on each pixel's grid."""
+    c = wide_case(name)
+    n = 32
+    lam = grids(c["lam"], n, 21, c["l0"])
+    models = truths(n, 22, c["mac"])
+    with wide_inverter(c, pm.PREC_FP64) as inv:
+        sp, rf = inv.synth(models, rf=True, lam=lam)
+    for o, m, s_gpu, r_gpu in zip(wide_oracles(c, lam), models, sp, rf):
+        s_ref, rf_ref = o.synth(m, fix=c["fix"])
+        assert np.abs(s_gpu - s_ref).max() < 1e-6
+        scale = np.abs(rf_ref).max(axis=-1, keepdims=True) + 1e-30
+        assert (np.abs(r_gpu - rf_ref) / scale).max() < 1e-5
+
+
+@pytest.mark.parametrize("prec", [pm.PREC_FP64, pm.PREC_FP32])
+def test_wide_inversion_on_each_pixels_grid(prec):
+    c = wide_case("w112")
+    n = 64
+    lam = grids(c["lam"], n, 23, c["l0"])
+    oras = wide_oracles(c, lam)
+    obs = observed(oras, truths(n, 24), c["fix"], 25)
+    ref = np.concatenate([o.invert(obs[i:i + 1], c["guess"], fix=c["fix"], noise=NOISE64)["models"]
+                          for i, o in enumerate(oras)])
+    with wide_inverter(c, prec, pm.SOLVE_EIGEN if prec == pm.PREC_FP64 else pm.SOLVE_DEFAULT) as inv:
+        r = inv.invert(obs, c["guess"], lam=lam)
+        shared = inv.invert(obs, c["guess"])
+    if prec == pm.PREC_FP64:
+        assert within_tolerance(r["models"], ref).mean() >= 0.9
+    else:
+        dB = np.abs(r["models"][:, 1] - ref[:, 1])
+        assert np.median(dB) < 1.0 and (dB < 5.0).mean() >= 0.9
+    # the shifts matter: on the shared grid the same profiles give other models
+    assert within_tolerance(shared["models"], ref).mean() < 0.5
+
+
+def test_wide_device_and_host_buffers_agree():
+    import torch
+
+    c = wide_case("w112")
+    n = 40
+    lam = grids(c["lam"], n, 26, c["l0"])
+    obs = observed(wide_oracles(c, lam), truths(n, 27), c["fix"], 28)
+    with wide_inverter(c, pm.PREC_FP32) as inv:
+        host = inv.invert(obs, c["guess"], lam=lam)
+        dev = inv.invert(torch.from_numpy(obs).cuda(), c["guess"], lam=torch.from_numpy(lam).cuda())
+    for k in ("models", "iters", "chisq"):
+        assert np.array_equal(dev[k].cpu().numpy(), host[k]), k
