@@ -21,7 +21,10 @@
 //     published ticket; the next launch reopens the queue at the first
 //     unpublished ticket).
 // Scans thus join a kernel that is already running, and results leave while
-// other scans are still on the GPU.
+// other scans are still on the GPU.  Grids of more than 32 wavelengths (all of
+// a server's grids, or none) have no persistent kernel: each admitted scan is
+// one launch of the wide kernel after its copy-in, and an event on the kernel
+// stream takes the place of the completion flag.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -111,6 +114,7 @@ struct Scan {
   long long job = -1;
   enum State { QUEUED, ADMITTED, COPYING_OUT, DONE } state = QUEUED;
   cudaEvent_t ev_out = nullptr;
+  cudaEvent_t ev_kernel = nullptr;  // grids wider than one warp: the scan's own launch has ended
   pm_scan_info info{};
 };
 
@@ -125,6 +129,12 @@ struct pm_server {
   size_t prof[PM_SERVER_MAX_GRIDS] = {};
   cudaStream_t s_kern = nullptr, s_copy = nullptr, s_out = nullptr;
   cudaEvent_t ev_kernel = nullptr, ev_reset = nullptr;
+  // grids of more than 32 wavelengths: no persistent kernel; each admitted scan
+  // is one launch of the wide kernel, after its copy-in (ev_copied), with its
+  // pixel and iteration counters in ctr_dev
+  bool wide = false;
+  cudaEvent_t ev_copied = nullptr;
+  unsigned long long* ctr_dev = nullptr;
   enum { K_STOPPED, K_RUNNING, K_CLOSING } kstate = K_STOPPED;
   double idle_since = -1;                   // ms; nothing queued or in flight since then
   unsigned long long* reset_host = nullptr; // pinned: [0] first unpublished ticket at a relaunch, [1] zero
@@ -189,7 +199,50 @@ void fail_all(pm_server* s, const char* what, cudaError_t e) {
   s->cv_done.notify_all();
 }
 
+// Grids of more than 32 wavelengths: the scan's copy-in on the copy stream, then
+// its own launch of the wide kernel (classical estimates included) on the
+// kernel stream, then an event the scheduler polls.  Launches run one after
+// another on the kernel stream; copies in and out overlap them.
+bool admit_wide(pm_server* s, Scan* sc) {
+  const size_t prof = s->prof[sc->grid];
+  unsigned char* base = s->arena_dev + sc->off;
+  const PmParams& P = s->gs->g[sc->grid];
+  PmIO io{};
+  io.npix = sc->npix;
+  io.spectro = sc->device_input ? sc->spectro : reinterpret_cast<const float*>(base);
+  io.models_out = reinterpret_cast<double*>(base + sc->o_models);
+  io.chisq_out = reinterpret_cast<float*>(base + sc->o_chisq);
+  io.iters_out = reinterpret_cast<int*>(base + sc->o_iters);
+  io.status_out = reinterpret_cast<int*>(base + sc->o_status);
+  io.ctr = s->ctr_dev;
+  cudaError_t e = cudaSuccess;
+  if (!sc->device_input)
+    e = cudaMemcpyAsync(base, sc->spectro, prof * size_t(sc->npix), cudaMemcpyHostToDevice, s->s_copy);
+  if (e == cudaSuccess) e = cudaEventRecord(s->ev_copied, s->s_copy);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(s->s_kern, s->ev_copied, 0);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s->ctr_dev, 0, sizeof(unsigned long long) * PMC_COUNT, s->s_kern);
+  if (e == cudaSuccess && !sc->ev_kernel) e = cudaEventCreateWithFlags(&sc->ev_kernel, cudaEventDisableTiming);
+  if (e == cudaSuccess) {
+    if (pmk_invert(P, io, s->precision, s->s_kern, s->num_sms, nullptr) != PM_OK) e = cudaErrorLaunchFailure;
+    else e = cudaEventRecord(sc->ev_kernel, s->s_kern);
+  }
+  if (e != cudaSuccess) {
+    sc->info.rc = PM_EIO;
+    sc->state = Scan::DONE;
+    fail_all(s, "scan launch", e);
+    return false;
+  }
+  ++s->launches;
+  if (P.classical) ++s->prepass_launches;
+  sc->job = s->next_job++;  // keeps the in-flight bound of the admission loop
+  sc->state = Scan::ADMITTED;
+  sc->info.admit_ms = s->now_ms();
+  s->active.push_back(sc);
+  return true;
+}
+
 bool admit(pm_server* s, Scan* sc) {
+  if (s->wide) return admit_wide(s, sc);
   const size_t prof = s->prof[sc->grid];
   const long long k = s->next_job;
   const int slot = int(k % kRing);
@@ -348,7 +401,16 @@ void serve(pm_server* s) {
       for (size_t i = 0; i < s->active.size() && s->error == PM_OK;) {
         Scan* sc = s->active[i];
         const int slot = int(sc->job % kRing);
-        if (sc->state == Scan::ADMITTED && reinterpret_cast<volatile int*>(s->flags_host)[slot] == 1) {
+        bool inverted = false;
+        if (sc->state == Scan::ADMITTED && s->wide) {
+          const cudaError_t e = cudaEventQuery(sc->ev_kernel);
+          if (e == cudaSuccess) inverted = true;
+          else if (e != cudaErrorNotReady) fail_all(s, "inversion kernel", e);
+        } else if (sc->state == Scan::ADMITTED) {
+          inverted = reinterpret_cast<volatile int*>(s->flags_host)[slot] == 1;
+        }
+        if (s->error != PM_OK) break;
+        if (inverted) {
           copy_out(s, sc);
           progress = true;
         }
@@ -391,7 +453,7 @@ void serve(pm_server* s) {
           fail_all(s, "inversion kernel", e);
         }
       }
-      if (s->error == PM_OK && s->kstate == pm_server::K_STOPPED) {
+      if (s->error == PM_OK && s->kstate == pm_server::K_STOPPED && !s->wide) {
         bool pending = false;
         for (const Scan* sc : s->active) pending = pending || sc->state == Scan::ADMITTED;
         if (pending && launch(s)) progress = true;
@@ -433,14 +495,16 @@ void release(pm_server* s) {
     if (st) cudaStreamSynchronize(st);
   for (auto& kv : s->scans) {
     if (kv.second->ev_out) cudaEventDestroy(kv.second->ev_out);
+    if (kv.second->ev_kernel) cudaEventDestroy(kv.second->ev_kernel);
     delete kv.second;
   }
   s->scans.clear();
   if (s->ev_kernel) cudaEventDestroy(s->ev_kernel);
   if (s->ev_reset) cudaEventDestroy(s->ev_reset);
+  if (s->ev_copied) cudaEventDestroy(s->ev_copied);
   for (cudaStream_t st : {s->s_copy, s->s_kern, s->s_out})
     if (st) cudaStreamDestroy(st);
-  for (void* p : {(void*)s->arena_dev, (void*)s->q, (void*)s->jobs_dev, (void*)s->done_dev})
+  for (void* p : {(void*)s->arena_dev, (void*)s->q, (void*)s->jobs_dev, (void*)s->done_dev, (void*)s->ctr_dev})
     if (p) cudaFree(p);
   for (void* p : {(void*)s->jobs_host, (void*)s->avail_host, (void*)s->one_host, (void*)s->flags_host,
                   (void*)s->reset_host})
@@ -488,9 +552,10 @@ extern "C" int pm_server_create(const pm_line* line, const pm_config* const* gri
     }
     pmh_set_guess(s->gs->g[g], &guesses[g]);
     const PmParams& P = s->gs->g[g];
-    if (P.G != 1) {
+    if ((P.G != 1) != (s->gs->g[0].G != 1)) {
       release(s);
-      return sfail(PM_ENOTSUP, "pm_server_create: served grids have at most 32 wavelengths");
+      return sfail(PM_ENOTSUP, "pm_server_create: grids of at most 32 wavelengths and wider ones are served by "
+                               "separate servers");
     }
     if (grids[g]->precision != grids[0]->precision || P.K != s->gs->g[0].K) {
       release(s);
@@ -499,6 +564,7 @@ extern "C" int pm_server_create(const pm_line* line, const pm_config* const* gri
     s->prof[g] = sizeof(float) * 4 * size_t(P.nl);
   }
   s->precision = grids[0]->precision;
+  s->wide = s->gs->g[0].G != 1;
   if (const char* v = std::getenv("PMILOS_VARIANT")) s->variant = std::atoi(v) == 1 ? 1 : 0;
   cudaDeviceProp prop;
   cudaError_t e = cudaGetDevice(&s->device);
@@ -522,6 +588,9 @@ extern "C" int pm_server_create(const pm_line* line, const pm_config* const* gri
   SRV_CUDA(cudaStreamCreateWithFlags(&s->s_out, cudaStreamNonBlocking), "stream");
   SRV_CUDA(cudaEventCreateWithFlags(&s->ev_kernel, cudaEventDisableTiming), "event");
   SRV_CUDA(cudaEventCreateWithFlags(&s->ev_reset, cudaEventDisableTiming), "event");
+  SRV_CUDA(cudaEventCreateWithFlags(&s->ev_copied, cudaEventDisableTiming), "event");
+  SRV_CUDA(cudaMalloc(&p, sizeof(unsigned long long) * PMC_COUNT), "counters");
+  s->ctr_dev = static_cast<unsigned long long*>(p);
   SRV_CUDA(cudaMalloc(&p, sc->hbm_budget_bytes), "arena (hbm_budget_bytes)");
   s->arena_dev = static_cast<unsigned char*>(p);
   s->arena = new (std::nothrow) Arena(sc->hbm_budget_bytes);
@@ -632,6 +701,7 @@ extern "C" int pm_server_wait(pm_server* s, uint64_t id, double timeout_s, pm_sc
   const int rc = sc->info.rc;
   s->scans.erase(it);
   if (sc->ev_out) cudaEventDestroy(sc->ev_out);
+  if (sc->ev_kernel) cudaEventDestroy(sc->ev_kernel);
   delete sc;
   if (rc != PM_OK) return pmh_fail(rc, s->error_msg);
   return PM_OK;

@@ -6,10 +6,13 @@ with a 60 mA Gaussian PSF, nine free parameters, FP32.  Observed profiles are
 synthesized by this library's FP64 path with seeded atmospheres (70% weak-field,
 30% strong-field) and N(0, 1e-3) noise.
 """
+import os
+
 import numpy as np
 import pytest
 
 import pmilos_b200 as pm
+from conftest import GOLDEN
 from gpu_common import NOISE64, within_tolerance
 from pmilos_b200 import workloads
 
@@ -131,3 +134,64 @@ def test_wait_timeout_and_unknown_id(cubes):
             srv.wait(sid)
         with pytest.raises(pm.PmError):
             srv.submit(7, cubes[(0, 700, 5)])
+
+
+# ---- grids of more than 32 wavelengths: one launch of the wide kernel per scan ----
+WIDE_LINE = pm.LineData(6302.4936, (2.0, 1.0, 1.0, 2.0, 2.0, 0.0))
+FIX9 = [1] * 9 + [0, 0]
+
+
+def wide_grids():
+    """The 112-point configuration-4 grid with its PSF (tests/golden/ref_cases_wide.npz)
+    and every second point of it (56 points, 50 mA steps, a 25 mA Gaussian PSF)."""
+    w = np.load(os.path.join(GOLDEN, "ref_cases_wide.npz"))
+    lam, psf, guess = w["w112_lam"], w["w112_psf"], w["w112_guess"]
+    lam56 = lam[::2].copy()
+    return [pm.Grid(lam=lam, psf=psf, guess=guess, noise=NOISE64, fix=FIX9, nterms=9),
+            pm.Grid(lam=lam56, psf=pm.psf_gaussian(25.0, lam56), guess=guess, noise=NOISE64, fix=FIX9, nterms=9)]
+
+
+def wide_cube(g, npix, seed):
+    """Profiles of seeded atmospheres synthesized in FP64 on the grid, N(0, 1e-3) noise."""
+    rng = np.random.default_rng(seed)
+    m = np.zeros((npix, 11))
+    m[:, 0] = rng.uniform(1, 20, npix)
+    m[:, 1] = rng.uniform(0, 3000, npix)
+    m[:, 2] = rng.uniform(-3, 3, npix)
+    m[:, 3] = rng.uniform(0.02, 0.05, npix)
+    m[:, 4] = rng.uniform(0.01, 0.5, npix)
+    m[:, 5] = rng.uniform(0, 180, npix)
+    m[:, 6] = rng.uniform(0, 180, npix)
+    m[:, 7] = rng.uniform(0.1, 0.4, npix)
+    m[:, 8] = rng.uniform(0.4, 0.9, npix)
+    m[:, 10] = 1.0
+    with pm.Inverter(WIDE_LINE, g.lam, g.psf, noise=NOISE64, fix=FIX9, nterms=9, precision=pm.PREC_FP64) as inv:
+        obs = inv.synth(m)
+    return np.ascontiguousarray(obs + rng.normal(0, 1e-3, obs.shape), dtype=np.float32)
+
+
+def test_wide_grid_scans_equal_the_batch_entry_point():
+    """Each scan on a wide grid is one launch of the wide kernel after its copy-in:
+    its results equal pm_invert_batch's on the same cube bit for bit, whatever
+    else is queued, and every scan completes."""
+    G = wide_grids()
+    cubes = [wide_cube(G[0], 3000, 71), wide_cube(G[1], 2000, 72), wide_cube(G[0], 500, 73)]
+    order = [(0, 0), (1, 1), (0, 2), (1, 1)]
+    with pm.Server(WIDE_LINE, G, hbm_budget_bytes=1 << 30, max_inflight=8) as srv:
+        ids = [srv.submit(g, cubes[c]) for g, c in order]
+        res = [srv.wait(i) for i in ids]
+        st = srv.stats()
+    for (g, c), r in zip(order, res):
+        with pm.Inverter(WIDE_LINE, G[g].lam, G[g].psf, noise=NOISE64, fix=FIX9, nterms=9,
+                         precision=pm.PREC_FP32) as inv:
+            b = inv.invert(cubes[c], G[g].guess)
+        _eq(r, b)
+    assert st["scans_done"] == 4 and st["kernel_launches"] == 4
+    assert st["pixels_done"] == 3000 + 2000 + 500 + 2000
+
+
+def test_one_warp_and_wide_grids_are_served_apart():
+    G = wide_grids()
+    with pytest.raises(pm.PmError) as e:
+        pm.Server(WIDE_LINE, [G[0], grids()[2]], hbm_budget_bytes=1 << 28)
+    assert e.value.code == -95  # PM_ENOTSUP
