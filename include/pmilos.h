@@ -345,6 +345,15 @@ int pm_server_submit_device(pm_server *srv, int grid, int64_t npix, const float 
 /* Block until scan `id` is done (its results are in the host arrays) or
  * timeout_s passes (PM_ETIMEDOUT).  info (nullable) gets its timings. */
 int pm_server_wait(pm_server *srv, uint64_t id, double timeout_s, pm_scan_info *info);
+/* Stray light of a served grid, as the reference's real-time loop applies its
+ * StrayLightFile to every new cube (pmilos.c:2151-2167, :2288-2296):
+ * PM_SLIGHT_SHARED, one [4][nlambda] profile for every pixel; PM_SLIGHT_PER_PIXEL,
+ * a [npix][4][nlambda] cube in the pixel order of the grid's scans, kept on the
+ * device, after which every scan on the grid has exactly npix pixels (else
+ * pm_server_submit returns PM_EINVAL); PM_SLIGHT_NONE removes it.  Host memory;
+ * the grid's nterms must be >= 10.  Only before the first pm_server_submit
+ * (PM_EINVAL afterwards). */
+int pm_server_set_slight(pm_server *srv, int grid, const float *slight, int slight_mode, int64_t npix);
 int pm_server_get_stats(pm_server *srv, pm_server_stats *out);
 /* Finishes every queued scan, then stops the scheduler and frees the device state. */
 int pm_server_destroy(pm_server *srv);

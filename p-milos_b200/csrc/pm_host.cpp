@@ -392,6 +392,7 @@ int pmh_fill_params(const pm_line* L, const pm_config* c, PmParams& P) { return 
 void pmh_set_guess(PmParams& P, const pm_model* g) { set_guess(P, g); }
 int pmh_check_guess(const PmParams& P, const pm_model* g) { return check_guess(P, g); }
 int pmh_fail(int code, const char* msg) { return fail(code, "%s", msg); }
+int pmh_set_slight(PmParams& P, const float* slight, int mode) { return set_slight(P, slight, mode, PM_MEM_HOST); }
 
 extern "C" int pm_ctx_create(const pm_line* line, const pm_config* cfg, void* stream, pm_ctx** out) {
   if (!line || !cfg || !out) return fail(PM_EINVAL, "pm_ctx_create: NULL argument");

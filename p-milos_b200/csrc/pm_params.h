@@ -157,6 +157,8 @@ const char* pmk_last_cuda_error();
 // Host helpers (pm_host.cpp) shared with pm_noalloc.cu.
 int pmh_fill_params(const pm_line* L, const pm_config* c, PmParams& P);
 void pmh_set_guess(PmParams& P, const pm_model* g);
+// The stray-light profile or mode of a grid (host memory), as pm_invert_batch sets it.
+int pmh_set_slight(PmParams& P, const float* slight, int mode);
 // The NTERMS rule of milos.c:152-157 against the guess's v_mac: PM_OK or PM_EINVAL.
 int pmh_check_guess(const PmParams& P, const pm_model* g);
 int pmh_fail(int code, const char* msg);

@@ -127,6 +127,8 @@ struct pm_server {
   PmGridSet* gs = nullptr;
   pm_server_config sc{};
   size_t prof[PM_SERVER_MAX_GRIDS] = {};
+  float* slight_dev[PM_SERVER_MAX_GRIDS] = {};   // PM_SLIGHT_PER_PIXEL grids: the resident cube
+  int64_t slight_npix[PM_SERVER_MAX_GRIDS] = {};  // and its pixel count (every scan on the grid has it)
   cudaStream_t s_kern = nullptr, s_copy = nullptr, s_out = nullptr;
   cudaEvent_t ev_kernel = nullptr, ev_reset = nullptr;
   // grids of more than 32 wavelengths: no persistent kernel; each admitted scan
@@ -210,6 +212,7 @@ bool admit_wide(pm_server* s, Scan* sc) {
   PmIO io{};
   io.npix = sc->npix;
   io.spectro = sc->device_input ? sc->spectro : reinterpret_cast<const float*>(base);
+  io.slight = s->slight_dev[sc->grid];
   io.models_out = reinterpret_cast<double*>(base + sc->o_models);
   io.chisq_out = reinterpret_cast<float*>(base + sc->o_chisq);
   io.iters_out = reinterpret_cast<int*>(base + sc->o_iters);
@@ -253,6 +256,7 @@ bool admit(pm_server* s, Scan* sc) {
   J.npix = sc->npix;
   J.grid = sc->grid;
   J.spectro = sc->device_input ? sc->spectro : reinterpret_cast<const float*>(base);
+  J.slight = s->slight_dev[sc->grid];
   J.models = reinterpret_cast<double*>(base + sc->o_models);
   J.chisq = reinterpret_cast<float*>(base + sc->o_chisq);
   J.iters = reinterpret_cast<int*>(base + sc->o_iters);
@@ -506,6 +510,8 @@ void release(pm_server* s) {
     if (st) cudaStreamDestroy(st);
   for (void* p : {(void*)s->arena_dev, (void*)s->q, (void*)s->jobs_dev, (void*)s->done_dev, (void*)s->ctr_dev})
     if (p) cudaFree(p);
+  for (float* p : s->slight_dev)
+    if (p) cudaFree(p);
   for (void* p : {(void*)s->jobs_host, (void*)s->avail_host, (void*)s->one_host, (void*)s->flags_host,
                   (void*)s->reset_host})
     if (p) cudaFreeHost(p);
@@ -635,6 +641,8 @@ int submit(pm_server* s, int grid, int64_t npix, const float* spectro, bool devi
     return sfail(PM_EINVAL, "pm_server_submit: NULL argument");
   if (grid < 0 || grid >= s->ngrids) return sfail(PM_EINVAL, "pm_server_submit: no such grid");
   if (npix < 1) return sfail(PM_EINVAL, "pm_server_submit: npix < 1");
+  if (s->slight_dev[grid] && npix != s->slight_npix[grid])
+    return sfail(PM_EINVAL, "pm_server_submit: the grid's stray-light cube has another pixel count");
   Scan* sc = new (std::nothrow) Scan();
   if (!sc) return sfail(PM_ENOMEM, "pm_server_submit: out of host memory");
   const size_t n = size_t(npix);
@@ -685,6 +693,38 @@ extern "C" int pm_server_submit_device(pm_server* s, int grid, int64_t npix, con
                                        pm_model* models_out, float* chisq_out, int* iters_out, int* status_out,
                                        uint64_t* id_out) {
   return submit(s, grid, npix, spectro_dev, true, models_out, chisq_out, iters_out, status_out, id_out);
+}
+
+extern "C" int pm_server_set_slight(pm_server* s, int grid, const float* slight, int slight_mode, int64_t npix) {
+  if (!s) return sfail(PM_EINVAL, "pm_server_set_slight: NULL server");
+  if (grid < 0 || grid >= s->ngrids) return sfail(PM_EINVAL, "pm_server_set_slight: no such grid");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->next_id != 1) return sfail(PM_EINVAL, "pm_server_set_slight: scans were submitted already");
+  PmParams& P = s->gs->g[grid];
+  if (slight_mode == PM_SLIGHT_PER_PIXEL && (!slight || npix < 1))
+    return sfail(PM_EINVAL, "pm_server_set_slight: a per-pixel cube needs slight and npix >= 1");
+  const int rc = pmh_set_slight(P, slight, slight_mode);
+  if (rc != PM_OK) return rc;
+  if (s->slight_dev[grid]) {
+    cudaFree(s->slight_dev[grid]);
+    s->slight_dev[grid] = nullptr;
+    s->slight_npix[grid] = 0;
+  }
+  if (slight_mode == PM_SLIGHT_PER_PIXEL) {
+    const size_t bytes = s->prof[grid] * size_t(npix);
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e == cudaSuccess) e = cudaMemcpy(p, slight, bytes, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      if (p) cudaFree(p);
+      P.slight_mode = PM_SLIGHT_NONE;
+      return sfail(e == cudaErrorMemoryAllocation ? PM_ENOMEM : PM_EIO, "pm_server_set_slight: %s",
+                   cudaGetErrorString(e));
+    }
+    s->slight_dev[grid] = static_cast<float*>(p);
+    s->slight_npix[grid] = npix;
+  }
+  return PM_OK;
 }
 
 extern "C" int pm_server_wait(pm_server* s, uint64_t id, double timeout_s, pm_scan_info* info) {

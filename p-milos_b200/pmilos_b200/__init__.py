@@ -56,7 +56,7 @@ EXPORTED_SYMBOLS = (
     "pm_abi_version", "pm_get_tuning", "pm_set_tuning", "pm_autotune", "pm_server_create", "pm_server_submit",
     "pm_server_wait", "pm_server_get_stats", "pm_server_destroy", "pm_selftest_stalled_queue",
     "pm_fits_parse_header", "pm_fits_reorder", "pm_server_submit_device", "pm_invert_batch_grids",
-    "pm_synth_batch_grids",
+    "pm_synth_batch_grids", "pm_server_set_slight",
 )
 SERVER_MAX_GRIDS = 4
 SERVER_MAX_INFLIGHT = 256
@@ -170,6 +170,7 @@ def load_library(path: str | None = None):
     L.pm_server_submit.argtypes = [vp, ctypes.c_int, i64, F, vp, vp, vp, vp, ctypes.POINTER(ctypes.c_uint64)]
     L.pm_server_submit_device.argtypes = [vp, ctypes.c_int, i64, F, vp, vp, vp, vp, ctypes.POINTER(ctypes.c_uint64)]
     L.pm_server_wait.argtypes = [vp, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(_ScanInfo)]
+    L.pm_server_set_slight.argtypes = [vp, ctypes.c_int, F, ctypes.c_int, i64]
     L.pm_server_get_stats.argtypes = [vp, ctypes.POINTER(_ServerStats)]
     L.pm_server_destroy.argtypes = [vp]
     L.pm_selftest_stalled_queue.argtypes = [vp, ctypes.c_double, ctypes.POINTER(ctypes.c_int),
@@ -568,6 +569,22 @@ class Server:
                                        ctypes.byref(srv)))
         self.srv = srv
         self._pending = {}
+
+    def set_slight(self, grid: int, slight) -> None:
+        """Stray light of a grid, before the first submit (pm_server_set_slight):
+        a [4][nl] profile for every pixel, a [npix][4][nl] cube (then every scan
+        on the grid has npix pixels, in the cube's pixel order), or None."""
+        if slight is None:
+            _check(self.L.pm_server_set_slight(self.srv, int(grid), None, SLIGHT_NONE, 0))
+            return
+        sl = np.ascontiguousarray(slight, dtype=np.float32)
+        nl = self.nl[grid]
+        if sl.size == 4 * nl:
+            mode, npix = SLIGHT_SHARED, 1
+        else:
+            sl = sl.reshape(-1, 4, nl)
+            mode, npix = SLIGHT_PER_PIXEL, sl.shape[0]
+        _check(self.L.pm_server_set_slight(self.srv, int(grid), sl.ctypes.data, mode, npix))
 
     def submit(self, grid: int, spectro, want_status: bool = True) -> int:
         """Queue a scan: a host array, or a CUDA float32 tensor already on this GPU

@@ -195,3 +195,62 @@ def test_one_warp_and_wide_grids_are_served_apart():
     with pytest.raises(pm.PmError) as e:
         pm.Server(WIDE_LINE, [G[0], grids()[2]], hbm_budget_bytes=1 << 28)
     assert e.value.code == -95  # PM_ENOTSUP
+
+
+# ---- stray light, as the reference's real-time loop applies its StrayLightFile ----
+def test_shared_stray_light_scans_match_the_batch_entry_point():
+    """A one-warp grid with a stray-light profile and the filling factor inverted
+    (the 10-parameter configuration): the served FP32 results against
+    pm_invert_batch's with the same profile, within the stated FP32 tolerance."""
+    w = workloads.config(2, npix=3000)
+    obs = workloads.synthesize(w, rng=np.random.default_rng(81))
+    sl = np.asarray(w.slight, dtype=np.float32)
+    g = pm.Grid(lam=w.lam, psf=w.psf, guess=w.guess, noise=NOISE64, fix=w.fix, nterms=w.nterms)
+    line = pm.LineData(workloads.FE6173, workloads.TRIPLET)
+    with pm.Server(line, [g], hbm_budget_bytes=1 << 28) as srv:
+        srv.set_slight(0, sl)
+        r = srv.wait(srv.submit(0, obs))
+        with pytest.raises(pm.PmError) as e:  # only before the first submit
+            srv.set_slight(0, None)
+        assert e.value.code == -22
+    with pm.Inverter(line, w.lam, w.psf, noise=NOISE64, fix=w.fix, nterms=w.nterms, precision=pm.PREC_FP32) as inv:
+        b = inv.invert(obs, w.guess, slight=sl)
+        unmixed = inv.invert(obs, w.guess)
+    dB = np.abs(r["models"][:, 1] - b["models"][:, 1])
+    assert np.median(dB) < 1.0 and (dB < 5.0).mean() >= 0.9
+    da = np.abs(r["models"][:, 10] - b["models"][:, 10])
+    assert np.median(da) < 1e-3
+    # the profile is applied: without it the filling factors come out otherwise
+    assert np.median(np.abs(unmixed["models"][:, 10] - b["models"][:, 10])) > 10 * max(np.median(da), 1e-6)
+
+
+def test_per_pixel_stray_light_cube_on_a_wide_grid():
+    """A [npix][4][nl] stray-light cube resident in the server (49 wavelengths,
+    two warps per pixel): every scan's results equal pm_invert_batch's with the
+    same cube bit for bit; a scan of another pixel count is refused."""
+    w = np.load(os.path.join(GOLDEN, "ref_cases_wide.npz"))
+    lam, psf, guess, fix = w["w49_lam"], w["w49_psf"], w["w49_guess"], list(w["w49_fix"])
+    l0, nterms = float(w["w49_lambda0"]), int(w["w49_nterms"])
+    line = pm.LineData(l0, (2.0, 1.0, 1.0, 2.0, 2.0, 0.0))
+    rng = np.random.default_rng(82)
+    npix = 1500
+    cube = (w["w49_slight"][None].astype(np.float64) * rng.uniform(0.9, 1.1, (npix, 1, 1))).astype(np.float32)
+    truth = np.repeat(guess[None], npix, axis=0)
+    truth[:, 1] = rng.uniform(0, 3000, npix)
+    truth[:, 2] = rng.uniform(-3, 3, npix)
+    truth[:, 10] = rng.uniform(0.7, 1.0, npix)
+    with pm.Inverter(line, lam, psf, noise=NOISE64, fix=fix, nterms=nterms, precision=pm.PREC_FP64) as inv:
+        obs = inv.synth(truth, slight=cube)
+    obs = np.ascontiguousarray(obs + rng.normal(0, 1e-3, obs.shape), dtype=np.float32)
+    g = pm.Grid(lam=lam, psf=psf, guess=guess, noise=NOISE64, fix=fix, nterms=nterms)
+    with pm.Server(line, [g], hbm_budget_bytes=1 << 28) as srv:
+        srv.set_slight(0, cube)
+        ids = [srv.submit(0, obs), srv.submit(0, obs)]
+        res = [srv.wait(i) for i in ids]
+        with pytest.raises(pm.PmError) as e:
+            srv.submit(0, obs[:100])
+        assert e.value.code == -22  # PM_EINVAL
+    with pm.Inverter(line, lam, psf, noise=NOISE64, fix=fix, nterms=nterms, precision=pm.PREC_FP32) as inv:
+        b = inv.invert(obs, guess, slight=cube)
+    for r in res:
+        _eq(r, b)
