@@ -84,6 +84,7 @@ extern "C" {
 #define PM_PIX_MAXITER 2     /* stopped at miter iterations */
 #define PM_PIX_NFREE (-1)    /* no degrees of freedom (lm_mils returns -1) */
 #define PM_PIX_NONFINITE (-2)/* a non-finite chi^2 or model was produced */
+#define PM_PIX_CLASSICAL 3   /* classical estimates only (pm_config.miter < 0) */
 
 /* Atmosphere model; same field order and types as Init_Model (defines.h:86-98). */
 typedef struct pm_model {
@@ -123,7 +124,10 @@ typedef struct pm_config {
   double noise;           /* per-point variance (noise = 1/SN^2; lm_mils' sigma) */
   double ilambda;         /* initial LM damping (InitialDiagonalElement) */
   double toplim;          /* relative chi^2 stop (1e-12 in the reference) */
-  int miter;              /* max LM iterations (NumberOfCycles > 0) */
+  int miter;              /* max LM iterations (NumberOfCycles > 0); < 0: the classical-estimates-only
+                             mode of NumberOfCycles < 0 (milos.c:399-520): estimacionesClasicas from
+                             the guess with forInitialUse = 0 (S0 = B_los), no NaN fixes, no LM;
+                             iterations and chi^2 0, status PM_PIX_CLASSICAL, best fit zero */
   int fix[11];            /* 1 = parameter is inverted, reference order (defines.h:245) */
   int nterms;             /* NTERMS = 11 - !fix[10] - (guess.mac == 0 && !fix[9]) (milos.c:152-157):
                              9; 10 (filling factor, or v_mac, inverted; or v_mac fixed nonzero); 11.

@@ -758,12 +758,14 @@ static void clamp_model(double *m) {
 }
 
 /* ------------------------------------------------------------------ */
-/* Classical estimates: estimacionesClasicas, milosUtils.c:287-452      */
-/* (forInitialUse = 1).  Weak-field centre-of-gravity B_los, v_los from  */
-/* the I centroid, inclination from sum|V| m / sum V^2, azimuth from the */
-/* Q,U sums with the quadrant rules.                                    */
+/* Classical estimates: estimacionesClasicas, milosUtils.c:287-452.     */
+/* Weak-field centre-of-gravity B_los, v_los from the I centroid,       */
+/* inclination from sum|V| m / sum V^2, azimuth from the Q,U sums with  */
+/* the quadrant rules.  initial_use = forInitialUse: 1 before lm_mils   */
+/* (inclinations within 5 deg of 90 kept off it for B, :395-402), 0 in  */
+/* the classical-estimates-only mode (S0 = B_los, :449-450).            */
 /* ------------------------------------------------------------------ */
-void pmo_classical(const pmo_ctx *c, const float *spectro, double *m) {
+static void classical(const pmo_ctx *c, const float *spectro, double *m, int initial_use) {
   const int n = c->nl;
   const double l0 = c->lambda0;
   const float *sI = spectro, *sQ = spectro + n, *sU = spectro + 2 * n, *sV = spectro + 3 * n;
@@ -806,8 +808,10 @@ void pmo_classical(const pmo_ctx *c, const float *spectro, double *m) {
   tan_gamma = fabs(sqrt(x / y));
   gamma_rad = atan(tan_gamma);
   gamma = gamma_rad * (180 / PMO_PI);
-  if (gamma >= 85 && gamma <= 90) gamma_rad = 85 * (PMO_PI / 180);
-  if (gamma > 90 && gamma <= 95) gamma_rad = 95 * (PMO_PI / 180);
+  if (initial_use) {
+    if (gamma >= 85 && gamma <= 90) gamma_rad = 85 * (PMO_PI / 180);
+    if (gamma > 90 && gamma <= 95) gamma_rad = 95 * (PMO_PI / 180);
+  }
   if (Blos < 0) gamma = (180) - gamma;
   sum_u = sum_q = 0.0;
   for (i = 0; i < n; i++)
@@ -828,7 +832,14 @@ void pmo_classical(const pmo_ctx *c, const float *spectro, double *m) {
   m[I_VLOS] = Vlos;
   m[I_GM] = gamma;
   m[I_AZ] = phi;
+  if (!initial_use) m[I_S0] = Blos;
 }
+
+void pmo_classical(const pmo_ctx *c, const float *spectro, double *m) { classical(c, spectro, m, 1); }
+
+/* The classical-estimates-only mode of the drivers (NumberOfCycles < 0,
+ * milos.c:399-520): forInitialUse = 0, no NaN fixes, no lm_mils. */
+void pmo_classical_only(const pmo_ctx *c, const float *spectro, double *m) { classical(c, spectro, m, 0); }
 
 /* ------------------------------------------------------------------ */
 /* Levenberg-Marquardt driver: lm_mils, milosUtils.c:466-635.          */

@@ -50,6 +50,7 @@ int pmo_synth(pmo_ctx *c, const double *model, const double *slight, double mu, 
 
 /* estimacionesClasicas(..., forInitialUse = 1) on one pixel. */
 void pmo_classical(const pmo_ctx *c, const float *spectro, double *model_inout);
+void pmo_classical_only(const pmo_ctx *c, const float *spectro, double *model_inout);
 
 /* The per-pixel body of milos.c:958-1009: guess copy, optional classical estimates
  * with the NaN fixes, then lm_mils.  Returns lm_mils' return value (1 or -1). */

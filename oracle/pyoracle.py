@@ -90,9 +90,11 @@ class _Lib:
             raise RuntimeError(f"synth failed rc={rc}")
         return sp.reshape(4, nl), (None if ds is None else ds.reshape(4, K, nl))
 
-    def classical(self, spectro, guess):
+    def classical(self, spectro, guess, initial_use=True):
+        """estimacionesClasicas on one pixel from guess: initial_use=True as
+        before lm_mils, False as the classical-estimates-only mode."""
         m = np.ascontiguousarray(guess, dtype=np.float64).copy()
-        self._classical(np.ascontiguousarray(spectro, dtype=np.float32).ravel(), m)
+        self._classical(np.ascontiguousarray(spectro, dtype=np.float32).ravel(), m, initial_use)
         return m
 
     def invert(self, spectro, guess, *, slight=None, slight_per_pixel=False, classical=True, miter=50,
@@ -130,6 +132,7 @@ class Restatement(_Lib):
         L.pmo_destroy.argtypes = [ctypes.c_void_p]
         L.pmo_synth.argtypes = [ctypes.c_void_p, _D, _D, ctypes.c_double, _I, _D, _D]
         L.pmo_classical.argtypes = [ctypes.c_void_p, _F, _D]
+        L.pmo_classical_only.argtypes = [ctypes.c_void_p, _F, _D]
         L.pmo_invert_batch.argtypes = [ctypes.c_void_p, ctypes.c_int, _F, _D, _D, ctypes.c_int, ctypes.c_int,
                                        ctypes.c_int, _D, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                        ctypes.c_double, ctypes.c_double, _I, _D, _F, _I, _F, _I]
@@ -155,8 +158,8 @@ class Restatement(_Lib):
     def _synth(self, m, sl, mu, fx, sp, ds):
         return self.L.pmo_synth(self.ctx, _d(m), _d(sl), mu, _i(fx), _d(sp), _d(ds))
 
-    def _classical(self, obs, m):
-        self.L.pmo_classical(self.ctx, _f(obs), _d(m))
+    def _classical(self, obs, m, initial_use=True):
+        (self.L.pmo_classical if initial_use else self.L.pmo_classical_only)(self.ctx, _f(obs), _d(m))
 
     def _batch(self, npix, obs, g, sl, slpp, cl, miter, w, noise, ilam, logc, toplim, mu, fx, models, chi, its,
                sp, acc):
@@ -200,6 +203,7 @@ class Reference(_Lib):
         L.pmref_setup.argtypes = [ctypes.c_int, _D, ctypes.c_double, _D, _D, ctypes.c_int]
         L.pmref_synth.argtypes = [_D, _D, ctypes.c_double, _I, _D, _D]
         L.pmref_classical.argtypes = [_F, _D]
+        L.pmref_classical_only.argtypes = [_F, _D]
         L.pmref_invert_batch.argtypes = [ctypes.c_int, _F, _D, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D,
                                          ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                          ctypes.c_double, _I, _D, _F, _I, _F]
@@ -223,8 +227,8 @@ class Reference(_Lib):
     def _synth(self, m, sl, mu, fx, sp, ds):
         return self.L.pmref_synth(_d(m), _d(sl), mu, _i(fx), _d(sp), _d(ds))
 
-    def _classical(self, obs, m):
-        self.L.pmref_classical(_f(obs), _d(m))
+    def _classical(self, obs, m, initial_use=True):
+        (self.L.pmref_classical if initial_use else self.L.pmref_classical_only)(_f(obs), _d(m))
 
     def _batch(self, npix, obs, g, sl, slpp, cl, miter, w, noise, ilam, logc, toplim, mu, fx, models, chi, its,
                sp, acc):

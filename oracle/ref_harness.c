@@ -15,6 +15,7 @@
  *                      (milos.c:143-230 globals; create_cuantic, AllocateMemoryDerivedSynthesis)
  *   pmref_synth        mil_sinrf + me_der at one model (synthesis mode, milos.c:601-602)
  *   pmref_classical    estimacionesClasicas (milosUtils.c:287-452)
+ *   pmref_classical_only the same with forInitialUse = 0 (milos.c:486-501)
  *   pmref_invert_pixel the per-pixel body of milos.c:958-1009: guess copy,
  *                      classical estimates, NaN fixes, lm_mils
  *   pmref_invert_batch the same over a contiguous slab of pixels (CPU baseline)
@@ -215,6 +216,16 @@ void pmref_classical(const float *spectro, double *model_inout) {
   Init_Model m;
   model_from(&m, model_inout);
   estimacionesClasicas(h_wlines[1], h_lambda, h_nl, (float *)spectro, &m, 1);
+  model_to(model_inout, &m);
+}
+
+/* The per-pixel body of the classical-estimates-only mode, milos.c:486-501
+ * (NumberOfCycles < 0): the initial model, then estimacionesClasicas with
+ * forInitialUse = 0, nothing else. */
+void pmref_classical_only(const float *spectro, double *model_inout) {
+  Init_Model m;
+  model_from(&m, model_inout);
+  estimacionesClasicas(h_wlines[1], h_lambda, h_nl, (float *)spectro, &m, 0);
   model_to(model_inout, &m);
 }
 

@@ -1115,7 +1115,9 @@ __device__ __forceinline__ void check_model(double* m) {
 }
 
 // estimacionesClasicas (milosUtils.c:287-452, forInitialUse = 1) followed by the
-// NaN fixes of the drivers (milos.c:976-983), in two halves around the sums over
+// NaN fixes of the drivers (milos.c:976-983) -- or, in the classical-estimates-
+// only mode (P.miter < 0, milos.c:486-501), forInitialUse = 0 and no NaN fixes --
+// in two halves around the sums over
 // wavelengths (accumulated in FP64): the terms at one wavelength w, between the
 // leading and trailing ghost wavelengths [begin, end), with Ic = I[end - 1] ...
 __device__ __forceinline__ void classical_terms(const PmParams& P, const float O[4], int w, double dlw, bool valid,
@@ -1147,8 +1149,11 @@ __device__ __forceinline__ void classical_terms(const PmParams& P, const float O
   v[9] = iu ? double(O[1]) : 0.0;
 }
 
-// ... and the estimates from the ten sums.
+// ... and the estimates from the ten sums.  CE: compiled with the classical-
+// estimates-only branch (the pre-pass kernels; the LM kernels never run it).
+template <bool CE = false>
 __device__ __forceinline__ void classical_finish(const PmParams& P, const double (&v)[10], double* m) {
+  const bool ce = CE && P.miter < 0;
   const double x = v[0], y = v[1], xv = v[2], yv = v[3], xm = v[4], ym = v[5];
   const double lp = fabs(y) > 1e-15 ? x / y : 0.0;
   const double lmn = fabs(ym) > 1e-15 ? xm / ym : 0.0;
@@ -1160,8 +1165,10 @@ __device__ __forceinline__ void classical_finish(const PmParams& P, const double
   const double tan_gamma = fabs(sqrt(sx / sy));
   double gamma_rad = atan(tan_gamma);
   double gamma = gamma_rad * (180 / kPi);
-  if (gamma >= 85 && gamma <= 90) gamma_rad = 85 * (kPi / 180);
-  if (gamma > 90 && gamma <= 95) gamma_rad = 95 * (kPi / 180);
+  if (!ce) {  // forInitialUse (milosUtils.c:395-402)
+    if (gamma >= 85 && gamma <= 90) gamma_rad = 85 * (kPi / 180);
+    if (gamma > 90 && gamma <= 95) gamma_rad = 95 * (kPi / 180);
+  }
   if (Blos < 0) gamma = 180 - gamma;
   const double su = v[8], sq = v[9];
   double phi = (atan(su / sq) * 180 / kPi) / 2;
@@ -1176,6 +1183,10 @@ __device__ __forceinline__ void classical_finish(const PmParams& P, const double
   m[2] = Vlos;
   m[5] = gamma;
   m[6] = phi;
+  if (ce) {
+    m[7] = Blos;  // milosUtils.c:449-450
+    return;
+  }
   if (isnan(m[1])) m[1] = 1;
   if (isnan(m[2])) m[2] = 1e-3;
   if (isnan(m[5])) m[5] = 1;
@@ -1183,6 +1194,7 @@ __device__ __forceinline__ void classical_finish(const PmParams& P, const double
 }
 
 // Classical estimates of a one-warp pixel (lane = wavelength, dl its offset).
+template <bool CE = false>
 __device__ __forceinline__ void classical(const PmParams& P, const float O[4], int lane, bool valid, double dl,
                                           double* m) {
   const int nl = P.nl;
@@ -1198,7 +1210,7 @@ __device__ __forceinline__ void classical(const PmParams& P, const float O[4], i
   classical_terms(P, O, lane, dl, valid, begin, end, Ic, v);
 #pragma unroll
   for (int i = 0; i < 10; ++i) v[i] = warp_sum(v[i]);
-  classical_finish(P, v, m);
+  classical_finish<CE>(P, v, m);
 }
 
 // The response functions of model m at this lane's wavelength (rows 0..K-1,

@@ -273,7 +273,6 @@ int fill_params(const pm_line* L, const pm_config* c, PmParams& P) {
       return fail(PM_EINVAL, "nterms=%d inconsistent with fix[9]=%d, fix[10]=%d (expected %d..%d)", c->nterms,
                   c->fix[9], c->fix[10], lo, hi);
   }
-  if (c->miter < 0) return fail(PM_EINVAL, "miter=%d", c->miter);
   if (!(c->noise > 0)) return fail(PM_EINVAL, "noise must be > 0");
   if (c->precision != PM_PREC_FP32 && c->precision != PM_PREC_FP64) return fail(PM_EINVAL, "precision");
   if (L->n_pi < 1 || L->n_sig < 1 || L->n_pi > PM_ZEEMAN_MAX || L->n_sig > PM_ZEEMAN_MAX)
@@ -282,7 +281,7 @@ int fill_params(const pm_line* L, const pm_config* c, PmParams& P) {
   P.nl = c->nlambda;
   P.half = c->nlambda / 2;
   P.K = c->nterms;
-  P.miter = c->miter;
+  P.miter = c->miter;  // < 0: classical estimates alone (NumberOfCycles < 0, milos.c:399-520)
   P.nfree_base = 4 * c->nlambda - c->nterms;
   P.logclambda = c->logclambda;
   P.classical = c->classical_estimates;
@@ -833,7 +832,42 @@ int run_graph_small(pm_ctx* c, int64_t n, const float* spectro, const float* sli
 // One launch over n pixels whose buffers are all device pointers.  One-warp
 // grids: the streamed kernel with every pixel published before the launch (the
 // same compiled code as the pipelined host-buffer path and the server).
+// The classical-estimates-only mode (miter < 0, as NumberOfCycles < 0 in the
+// reference, milos.c:399-520): the estimates from the guess with forInitialUse =
+// 0 and no NaN fixes, no lm_mils; iterations and chi^2 are 0 (the zero-filled
+// vNumIter / vChisqrf that mode writes), status PM_PIX_CLASSICAL, best-fit
+// profiles zero.
+int run_classical_only(pm_ctx* c, const PmIO& io, float* kernel_ms) {
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  cudaEventRecord(a, c->stream);
+  int rc = c->P.G == 1 ? pmk_classical_prepass(c->P, io.spectro, io.models_out, io.npix, c->stream, c->num_sms,
+                                               io.lambda_pix)
+                       : pmk_classical_wide(c->P, io, c->stream, c->num_sms);
+  cudaEventRecord(b, c->stream);
+  if (rc == PM_OK && io.status_out) rc = pmk_fill_int(io.status_out, io.npix, PM_PIX_CLASSICAL, c->stream);
+  if (rc != PM_OK) {
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return fail(rc, "%s", pmk_last_cuda_error());
+  }
+  const size_t n = size_t(io.npix);
+  cudaError_t e = cudaMemsetAsync(io.chisq_out, 0, sizeof(float) * n, c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(io.iters_out, 0, sizeof(int) * n, c->stream);
+  if (e == cudaSuccess && io.spectra_out)
+    e = cudaMemsetAsync(io.spectra_out, 0, sizeof(float) * 4 * c->P.nl * n, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e == cudaSuccess && kernel_ms) e = cudaEventElapsedTime(kernel_ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (e != cudaSuccess) return cuda_fail(e, "classical estimates");
+  c->stats.pixels += io.npix;
+  return PM_OK;
+}
+
 int run_invert(pm_ctx* c, PmIO io, float* kernel_ms) {
+  if (c->P.miter < 0) return run_classical_only(c, io, kernel_ms);
   if (c->P.G != 1) {
     PM_CUDA(cudaMemsetAsync(io.ctr, 0, sizeof(unsigned long long) * PMC_COUNT, c->stream), "counter reset");
     int rc = pmk_invert(c->P, io, c->precision, c->stream, c->num_sms, kernel_ms);
@@ -912,6 +946,7 @@ int invert_impl(pm_ctx* c, int64_t npix, const float* spectro, const double* lam
   if (npix < 0) return fail(PM_EINVAL, "pm_invert_batch: npix < 0");
   if (mem != PM_MEM_HOST && mem != PM_MEM_DEVICE) return fail(PM_EINVAL, "pm_invert_batch: mem=%d", mem);
   if (int rc = check_guess(c->P, guess); rc != PM_OK) return rc;
+  const bool ce_only = c->P.miter < 0;  // classical estimates alone: copy, estimate, copy back
   c->stats = pm_stats{};
   if (npix == 0) return PM_OK;
   set_guess(c->P, guess);
@@ -937,7 +972,7 @@ int invert_impl(pm_ctx* c, int64_t npix, const float* spectro, const double* lam
     io.ctr = static_cast<unsigned long long*>(c->ctr.p);
     io.lambda_pix = lambda;
     rc = run_invert(c, io, &kms_total);
-  } else if (!lambda && c->P.G == 1 && c->tuning.graphs && npix <= PM_GRAPH_MAX_PIXELS) {
+  } else if (!lambda && !ce_only && c->P.G == 1 && c->tuning.graphs && npix <= PM_GRAPH_MAX_PIXELS) {
     rc = run_graph_small(c, npix, spectro, slight, slight_mode, models_out, chisq_out, iters_out, best_fit_out,
                          status_out);
     kms_total = float(c->stats.kernel_ms);
@@ -949,7 +984,7 @@ int invert_impl(pm_ctx* c, int64_t npix, const float* spectro, const double* lam
     // wide grids go through two buffer sets (run_wide_pipelined), in at least 8
     // chunks when the cube is large, so that only the first chunk's copy is not
     // hidden behind an inversion; per-pixel grids copy, then launch, chunk by chunk
-    const int sets = (c->P.G != 1 && !lambda) ? 2 : 1;
+    const int sets = (c->P.G != 1 && !lambda && !ce_only) ? 2 : 1;
     int64_t chunk = std::min<int64_t>(npix, std::max<int64_t>(32, int64_t(c->resident_bytes / (per_pixel * sets))));
     if (sets == 2 && npix >= 8 * 4096) chunk = std::min<int64_t>(chunk, (npix / 8 + 31) / 32 * 32);
     const int64_t cap = chunk * sets;
@@ -967,7 +1002,7 @@ int invert_impl(pm_ctx* c, int64_t npix, const float* spectro, const double* lam
     }
     pm_stats acc{};
     // per-pixel grids take the copy-then-launch path
-    const bool streamed = !lambda && c->P.G == 1 && c->tuning.staging_depth > 0;
+    const bool streamed = !lambda && !ce_only && c->P.G == 1 && c->tuning.staging_depth > 0;
     for (int64_t p0 = 0; p0 < npix && rc == PM_OK && sets == 1 && streamed; p0 += chunk) {
       const int64_t n = std::min(chunk, npix - p0);
       float kms = 0, tms = 0;

@@ -77,6 +77,22 @@ int launch_synth_any(const PmParams& P, const PmIO& io, cudaStream_t st) {
 // Batch inversion kernels launched directly: grids wider than one warp.  Grids
 // of up to 32 wavelengths are inverted by the streamed kernel (pmk_invert_stream)
 // in every call path, so that each pixel's arithmetic is one compiled code.
+namespace {
+__global__ void fill_int_kernel(int* p, long long n, int value) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    p[i] = value;
+}
+}  // namespace
+
+int pmk_fill_int(int* p, int64_t n, int value, void* stream) {
+  if (n <= 0) return PM_OK;
+  const long long blocks = std::min<long long>((n + 255) / 256, 148 * 8);
+  fill_int_kernel<<<unsigned(blocks), 256, 0, static_cast<cudaStream_t>(stream)>>>(p, n, value);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return snprintf(pmk_g_err, sizeof pmk_g_err, "fill launch: %s", cudaGetErrorString(e)), PM_EIO;
+  return PM_OK;
+}
+
 int pmk_invert(const PmParams& P, const PmIO& io, int precision, void* stream, int num_sms, float* kernel_ms) {
   if (P.G == 1) {
     snprintf(pmk_g_err, sizeof pmk_g_err, "one-warp grids are inverted by the streamed kernel");

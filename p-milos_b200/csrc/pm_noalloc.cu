@@ -117,6 +117,7 @@ extern "C" int pm_invert_batch_noalloc(const pm_line* line, const pm_config* cfg
   PmParams P;
   int rc = pmh_fill_params(line, cfg, P);
   if (rc != PM_OK) return rc;
+  if (P.miter < 0) return pmh_fail(PM_EINVAL, "miter < 0: the LM inversion needs miter >= 0");
   rc = pmh_check_guess(P, guess);
   if (rc != PM_OK) return rc;
   pmh_set_guess(P, guess);

@@ -17,7 +17,7 @@ struct PmParams {
   int nl;          // wavelengths
   int half;        // nl / 2: PSF centre tap (convolution.c:64)
   int K;           // NTERMS
-  int miter;
+  int miter;       // < 0: classical estimates alone (NumberOfCycles < 0, milos.c:399-520)
   int nfree_base;  // 4*nl - K (CalculaNfree, lib.c:399-407)
   int logclambda;
   int classical;   // estimacionesClasicas before LM
@@ -125,6 +125,10 @@ int pmk_synth(const PmParams& P, const PmIO& io, int precision, void* stream);
 // Grids of more than 32 wavelengths (pm_wide.cu), called by pmk_invert / pmk_synth.
 int pmk_invert_wide(const PmParams& P, const PmIO& io, int precision, void* stream, int num_sms, float* kernel_ms);
 int pmk_synth_wide(const PmParams& P, const PmIO& io, int precision, void* stream);
+// The classical estimates alone on a wide grid (io.models_out, from the guess).
+int pmk_classical_wide(const PmParams& P, const PmIO& io, void* stream, int num_sms);
+// n ints of p set to value (stream-ordered).
+int pmk_fill_int(int* p, int64_t n, int value, void* stream);
 // Their instances for multiplets, macroturbulence and per-pixel grids, by
 // precision (pm_wide_x32.cu, pm_wide_x64.cu).
 int pmk_invert_wide_x32(const PmParams& P, const PmIO& io, void* stream, int num_sms, float* kernel_ms);

@@ -558,6 +558,10 @@ extern "C" int pm_server_create(const pm_line* line, const pm_config* const* gri
     }
     pmh_set_guess(s->gs->g[g], &guesses[g]);
     const PmParams& P = s->gs->g[g];
+    if (P.miter < 0) {
+      release(s);
+      return sfail(PM_EINVAL, "pm_server_create: miter < 0 (classical estimates only) is not served");
+    }
     if ((P.G != 1) != (s->gs->g[0].G != 1)) {
       release(s);
       return sfail(PM_ENOTSUP, "pm_server_create: grids of at most 32 wavelengths and wider ones are served by "

@@ -19,6 +19,13 @@ int pmk_invert_wide(const PmParams& P, const PmIO& io, int precision, void* stre
              : invert_wide_dispatch<double, true>(P, io, st, num_sms, kernel_ms);
 }
 
+int pmk_classical_wide(const PmParams& P, const PmIO& io, void* stream, int num_sms) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (P.G == 2) return launch_classical_wide<2>(P, io, st, num_sms);
+  if (P.G == 4) return launch_classical_wide<4>(P, io, st, num_sms);
+  return no_wide_kernel(P, io);
+}
+
 int pmk_synth_wide(const PmParams& P, const PmIO& io, int precision, void* stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const bool f32 = precision == PM_PREC_FP32;

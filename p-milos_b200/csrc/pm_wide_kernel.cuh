@@ -637,7 +637,7 @@ __global__ void __launch_bounds__(32 * G) classical_wide_kernel(const __grid_con
       double g[11];
 #pragma unroll
       for (int i = 0; i < 11; ++i) g[i] = P.guess[i];
-      if (begin >= 0) classical_finish(P, v, g);
+      if (begin >= 0) classical_finish<true>(P, v, g);
       double out = g[0];
 #pragma unroll
       for (int i = 1; i < 11; ++i)
@@ -688,6 +688,19 @@ __global__ void __launch_bounds__(32 * G) synth_wide_kernel(const __grid_constan
 
 using WideKernel = void (*)(const PmParams, const PmIO);
 
+// The classical estimates of every pixel into io.models_out, one block of G
+// warps per pixel, up to 64 / G blocks per SM.
+template <int G>
+int launch_classical_wide(const PmParams& P, const PmIO& io, cudaStream_t st, int num_sms) {
+  int64_t cb = io.npix;
+  if (cb > int64_t(num_sms) * (64 / G)) cb = int64_t(num_sms) * (64 / G);
+  if (cb < 1) cb = 1;
+  classical_wide_kernel<G><<<unsigned(cb), 32 * G, 0, st>>>(P, io);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return snprintf(pmk_g_err, sizeof pmk_g_err, "classical launch: %s", cudaGetErrorString(e)), PM_EIO;
+  return PM_OK;
+}
+
 // One compiled instance of the wide inversion: the classical estimates first
 // when the settings ask for them, then the LM kernel with as many blocks as fit.
 template <typename R, int KT, int G, int MINB, bool ZM, bool MAC, bool PIXGRID>
@@ -709,10 +722,8 @@ int launch_invert_wide_inst(const PmParams& P, const PmIO& io, cudaStream_t st, 
     cudaEventRecord(a, st);
   }
   if (P.classical) {
-    int64_t cb = io.npix;
-    if (cb > int64_t(num_sms) * (64 / G)) cb = int64_t(num_sms) * (64 / G);
-    if (cb < 1) cb = 1;
-    classical_wide_kernel<G><<<unsigned(cb), threads, 0, st>>>(P, io);
+    const int rc = launch_classical_wide<G>(P, io, st, num_sms);
+    if (rc != PM_OK) return rc;
   }
   kern<<<unsigned(blocks), threads, smem, st>>>(P, io);
   e = cudaGetLastError();

@@ -412,13 +412,39 @@ def psf_pins():
     return out
 
 
+def classical_only_cases():
+    """The classical-estimates-only mode (NumberOfCycles < 0, milos.c:486-501:
+    estimacionesClasicas with forInitialUse = 0 from the initial model) on the
+    observed cubes of ref_cases.npz (configurations 0, 1, 2) and
+    ref_cases_wide.npz (49 and 112 points), both precisions."""
+    out = {}
+    for fname, names in (("ref_cases.npz", ("c0", "c1", "c2")), ("ref_cases_wide.npz", ("w49", "w112"))):
+        src = np.load(os.path.join(HERE, fname))
+        for name in names:
+            g = lambda k: src[f"{name}_{k}"]
+            lam, obs, guess = g("lam"), g("obs"), g("guess")
+            l0 = float(g("lambda0")) if f"{name}_lambda0" in src.files else CASE_SPECS[int(name[1])][0][3]
+            cu = TRIPLET
+            for flav in ("f32", "f64"):
+                ref = po.Reference(po.LineSetup(lam, l0, cu, None, 9), flav)
+                out[f"{name}_{flav}_models"] = np.array([ref.classical(o, guess, initial_use=False) for o in obs])
+            out[f"{name}_lam"], out[f"{name}_lambda0"], out[f"{name}_guess"] = lam, l0, guess
+            out[f"{name}_obs"] = obs
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
-    ap.add_argument("--only", choices=("all", "wide", "mac", "fits", "zeeman"), default="all")
+    ap.add_argument("--only", choices=("all", "wide", "mac", "fits", "zeeman", "classical"), default="all")
     a = ap.parse_args()
     os.environ["PM_REFERENCE_SRC"] = os.path.join(a.reference, "src")
     po.build()
+    if a.only in ("all", "classical"):
+        np.savez_compressed(os.path.join(HERE, "ref_classical_only.npz"), **classical_only_cases())
+        print("ref_classical_only.npz", os.path.getsize(os.path.join(HERE, "ref_classical_only.npz")), "bytes")
+        if a.only == "classical":
+            return
     import tempfile
 
     with tempfile.TemporaryDirectory() as td:

@@ -196,3 +196,20 @@ def test_zeeman_multiplet_bit_exact(name, flav):
         assert np.array_equal(sp, sp_ref)
         assert np.array_equal(rf, rf_ref)
     assert np.allclose(ora.cuantic(), g("cuantic_pattern"), rtol=1e-6, atol=1e-12)
+
+
+CE = np.load(os.path.join(GOLDEN, "ref_classical_only.npz"))
+
+
+@pytest.mark.parametrize("flav", ["f32", "f64"])
+@pytest.mark.parametrize("name", ["c0", "c1", "c2", "w49", "w112"])
+def test_classical_only_mode_bit_exact(name, flav):
+    """The classical-estimates-only mode (NumberOfCycles < 0, milos.c:486-501):
+    estimacionesClasicas with forInitialUse = 0 (no 85-95 deg inclination clamp
+    for B, S0 = B_los) from the initial model equals the reference's."""
+    g = lambda k: CE[f"{name}_{k}"]
+    cu = np.array([1.0, 2, 1, 1, 2, 2, 0])
+    ora = po.Restatement(po.LineSetup(g("lam"), float(g("lambda0")), cu, None, 9), flav)
+    got = np.array([ora.classical(o, g("guess"), initial_use=False) for o in g("obs")])
+    assert np.array_equal(got, g(f"{flav}_models"))
+    assert not np.array_equal(got[:, 7], np.full(len(got), g("guess")[7]))  # S0 holds B_los
