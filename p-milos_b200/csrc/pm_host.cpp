@@ -433,6 +433,7 @@ extern "C" int pm_ctx_create(const pm_line* line, const pm_config* cfg, void* st
 
 extern "C" int pm_ctx_destroy(pm_ctx* c) {
   if (!c) return PM_OK;
+  PmDeviceGuard dg(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   else cudaDeviceSynchronize();
   if (c->s_kern) cudaStreamSynchronize(c->s_kern);
@@ -943,6 +944,7 @@ int invert_impl(pm_ctx* c, int64_t npix, const float* spectro, const double* lam
                 float* best_fit_out, int* status_out, int mem) {
   if (!c || !spectro || !guess || !models_out || !chisq_out || !iters_out)
     return fail(PM_EINVAL, "pm_invert_batch: NULL argument");
+  PmDeviceGuard dg(c->device);
   if (npix < 0) return fail(PM_EINVAL, "pm_invert_batch: npix < 0");
   if (mem != PM_MEM_HOST && mem != PM_MEM_DEVICE) return fail(PM_EINVAL, "pm_invert_batch: mem=%d", mem);
   if (int rc = check_guess(c->P, guess); rc != PM_OK) return rc;
@@ -1096,6 +1098,7 @@ namespace {
 int synth_impl(pm_ctx* c, int64_t npix, const pm_model* models, const double* lambda, const float* slight,
                int slight_mode, float* spectra_out, float* rf_out, int mem) {
   if (!c || !models || !spectra_out) return fail(PM_EINVAL, "pm_synth_batch: NULL argument");
+  PmDeviceGuard dg(c->device);
   if (npix < 0) return fail(PM_EINVAL, "pm_synth_batch: npix < 0");
   if (mem != PM_MEM_HOST && mem != PM_MEM_DEVICE) return fail(PM_EINVAL, "pm_synth_batch: mem=%d", mem);
   if (npix == 0) return PM_OK;
@@ -1194,6 +1197,7 @@ extern "C" int pm_set_tuning(pm_ctx* c, const pm_tuning* in) {
 extern "C" int pm_autotune(pm_ctx* c, int64_t npix, const float* spectro, const float* slight, int slight_mode,
                            const pm_model* guess, int reps, pm_tuning* out) {
   if (!c || !spectro || !guess) return fail(PM_EINVAL, "pm_autotune: NULL argument");
+  PmDeviceGuard dg(c->device);
   if (npix < 1) return fail(PM_EINVAL, "pm_autotune: npix=%lld", (long long)npix);
   reps = std::max(1, std::min(reps, 16));
   std::vector<pm_model> models(static_cast<size_t>(npix));
@@ -1239,6 +1243,7 @@ extern "C" int pm_autotune(pm_ctx* c, int64_t npix, const float* spectro, const 
 
 extern "C" int pm_selftest_stalled_queue(pm_ctx* c, double limit_ms, int* queue_error, double* elapsed_ms) {
   if (!c || !queue_error || !elapsed_ms) return fail(PM_EINVAL, "pm_selftest_stalled_queue: NULL argument");
+  PmDeviceGuard dg(c->device);
   if (!(limit_ms > 0 && limit_ms <= 10000)) return fail(PM_EINVAL, "pm_selftest_stalled_queue: limit_ms out of (0, 1e4]");
   if (c->P.G != 1) return fail(PM_ENOTSUP, "pm_selftest_stalled_queue: one-warp grids only");
   int rc = stream_resources(c);

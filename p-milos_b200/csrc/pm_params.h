@@ -6,6 +6,7 @@
 // compile-time index becomes a constant operand of the FMA that uses it, with no
 // load instruction at all.  Per-pixel data travels by pointer in PmIO.
 #pragma once
+#include <cuda_runtime.h>
 #include <stdint.h>
 
 #include "../../include/pmilos.h"
@@ -157,6 +158,21 @@ int pmk_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, int precision,
 int pmk_invert_stream_zm(const PmGridSet& GS, const PmStreamIO& sio, int precision, int warps_per_block, bool multi,
                          void* stream, int num_sms, size_t* smem_out, int reserve_blocks, bool pixgrid, bool mac);
 const char* pmk_last_cuda_error();
+
+// Makes dev the calling thread's current device for the guard's scope and puts
+// the caller's back afterwards: every entry point that works on a context or a
+// server runs on that object's GPU whatever the caller's thread has selected.
+struct PmDeviceGuard {
+  int prev = -1;
+  explicit PmDeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess || prev == dev || cudaSetDevice(dev) != cudaSuccess) prev = -1;
+  }
+  ~PmDeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+  PmDeviceGuard(const PmDeviceGuard&) = delete;
+  PmDeviceGuard& operator=(const PmDeviceGuard&) = delete;
+};
 
 // Host helpers (pm_host.cpp) shared with pm_noalloc.cu.
 int pmh_fill_params(const pm_line* L, const pm_config* c, PmParams& P);

@@ -386,6 +386,7 @@ void finish(pm_server* s, Scan* sc) {
 }
 
 void serve(pm_server* s) {
+  cudaSetDevice(s->device);  // a new thread starts on device 0: work on the server's GPU
   std::unique_lock<std::mutex> lk(s->mu);
   while (true) {
     bool progress = false;
@@ -491,6 +492,7 @@ void serve(pm_server* s) {
 }
 
 void release(pm_server* s) {
+  PmDeviceGuard dg(s->device);
   if (s->s_copy && s->q && s->one_host && s->kstate != pm_server::K_STOPPED) {
     // a kernel still running (after an error): close the queue so that it ends
     cudaMemcpyAsync(&s->q->closed, s->one_host, sizeof(unsigned long long), cudaMemcpyHostToDevice, s->s_copy);
@@ -704,6 +706,7 @@ extern "C" int pm_server_set_slight(pm_server* s, int grid, const float* slight,
   if (grid < 0 || grid >= s->ngrids) return sfail(PM_EINVAL, "pm_server_set_slight: no such grid");
   std::lock_guard<std::mutex> lk(s->mu);
   if (s->next_id != 1) return sfail(PM_EINVAL, "pm_server_set_slight: scans were submitted already");
+  PmDeviceGuard dg(s->device);
   PmParams& P = s->gs->g[grid];
   if (slight_mode == PM_SLIGHT_PER_PIXEL && (!slight || npix < 1))
     return sfail(PM_EINVAL, "pm_server_set_slight: a per-pixel cube needs slight and npix >= 1");
