@@ -121,3 +121,27 @@ def test_trol_reader(tmp_path):
     assert c["fix"] == [1, 1, 1, 1, 1, 1, 0, 1, 1, 0, 1]
     assert c["noise"] == pytest.approx(4e-6) and c["ilambda"] == 0.01 and c["logclambda"] == 1
     assert c["mu"] == 1.0 and c["psf_fwhm"] == 60.0
+
+
+def _grid(nl, **kw):
+    lam = 6173.3354 + np.linspace(-0.35, 0.35, nl)
+    return pm.Grid(lam=lam, noise=1e-6, fix=[1] * 9 + [0, 0], nterms=9, **kw)
+
+
+@pytest.mark.skipif(__import__("torch").cuda.is_available(), reason="checks the failure without a GPU")
+def test_server_creation_checks_its_grids_then_needs_a_gpu():
+    """pm_server_create validates the grids before it looks for a device: a
+    classical-estimates-only grid (miter < 0) is refused, grids of at most 32 and
+    of more than 32 wavelengths do not share a server, and a valid set fails
+    loudly without an sm_100 device (there is no CPU path)."""
+    line = pm.LineData(6173.3354, (2.0, 1.0, 1.0, 2.0, 2.0, 0.0))
+    with pytest.raises(pm.PmError) as e:
+        pm.Server(line, [_grid(30, miter=-1)], hbm_budget_bytes=1 << 28)
+    assert e.value.code == -22  # PM_EINVAL
+    with pytest.raises(pm.PmError) as e:
+        pm.Server(line, [_grid(30), _grid(49)], hbm_budget_bytes=1 << 28)
+    assert e.value.code == -95  # PM_ENOTSUP
+    for grids in ([_grid(30), _grid(15)], [_grid(112), _grid(49)]):
+        with pytest.raises(pm.PmError) as e:
+            pm.Server(line, grids, hbm_budget_bytes=1 << 28)
+        assert e.value.code == -19  # PM_ENODEV
