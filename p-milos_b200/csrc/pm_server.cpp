@@ -184,21 +184,27 @@ int sfail(int code, const char* fmt, const char* a = "", const char* b = "") {
   return pmh_fail(code, g_err);
 }
 
-// Device error inside the scheduler: every queued and active scan ends with it.
-void fail_all(pm_server* s, const char* what, cudaError_t e) {
-  s->error = PM_EIO;
-  std::snprintf(s->error_msg, sizeof s->error_msg, "%s: %s", what, cudaGetErrorString(e));
+// An error inside the scheduler: every queued and active scan ends with it.
+void fail_all_code(pm_server* s, int code, const char* msg) {
+  s->error = code;
+  std::snprintf(s->error_msg, sizeof s->error_msg, "%s", msg);
   for (Scan* sc : s->active) {
-    sc->info.rc = PM_EIO;
+    sc->info.rc = code;
     sc->state = Scan::DONE;
   }
   for (Scan* sc : s->queued) {
-    sc->info.rc = PM_EIO;
+    sc->info.rc = code;
     sc->state = Scan::DONE;
   }
   s->active.clear();
   s->queued.clear();
   s->cv_done.notify_all();
+}
+
+void fail_all(pm_server* s, const char* what, cudaError_t e) {
+  char msg[256];
+  std::snprintf(msg, sizeof msg, "%s: %s", what, cudaGetErrorString(e));
+  fail_all_code(s, PM_EIO, msg);
 }
 
 // Grids of more than 32 wavelengths: the scan's copy-in on the copy stream, then
@@ -225,14 +231,16 @@ bool admit_wide(pm_server* s, Scan* sc) {
   if (e == cudaSuccess) e = cudaStreamWaitEvent(s->s_kern, s->ev_copied, 0);
   if (e == cudaSuccess) e = cudaMemsetAsync(s->ctr_dev, 0, sizeof(unsigned long long) * PMC_COUNT, s->s_kern);
   if (e == cudaSuccess && !sc->ev_kernel) e = cudaEventCreateWithFlags(&sc->ev_kernel, cudaEventDisableTiming);
+  int rc = PM_OK;
   if (e == cudaSuccess) {
-    if (pmk_invert(P, io, s->precision, s->s_kern, s->num_sms, nullptr) != PM_OK) e = cudaErrorLaunchFailure;
-    else e = cudaEventRecord(sc->ev_kernel, s->s_kern);
+    rc = pmk_invert(P, io, s->precision, s->s_kern, s->num_sms, nullptr);
+    if (rc == PM_OK) e = cudaEventRecord(sc->ev_kernel, s->s_kern);
   }
-  if (e != cudaSuccess) {
-    sc->info.rc = PM_EIO;
+  if (e != cudaSuccess || rc != PM_OK) {
+    sc->info.rc = rc != PM_OK ? rc : PM_EIO;
     sc->state = Scan::DONE;
-    fail_all(s, "scan launch", e);
+    if (rc != PM_OK) fail_all_code(s, rc, pmk_last_cuda_error());
+    else fail_all(s, "scan launch", e);
     return false;
   }
   ++s->launches;
