@@ -40,7 +40,7 @@
 extern "C" {
 #endif
 
-#define PMILOS_ABI_VERSION 1
+#define PMILOS_ABI_VERSION 2
 
 /* error codes */
 #define PM_OK 0
@@ -54,7 +54,7 @@ extern "C" {
 /* limits */
 #define PM_NL_MAX 128      /* wavelengths per profile */
 #define PM_NTERMS_MAX 11   /* free parameters */
-#define PM_ZEEMAN_MAX 8    /* Zeeman components per group (pi, sigma_b, sigma_r) */
+#define PM_ZEEMAN_MAX 16   /* Zeeman components per group (pi, sigma_b, sigma_r) */
 
 /* buffer residency */
 #define PM_MEM_HOST 0

@@ -46,7 +46,7 @@ SOLVE_DEFAULT, SOLVE_EIGEN, SOLVE_CHOLESKY = 0, 1, 2
 SLIGHT_NONE, SLIGHT_SHARED, SLIGHT_PER_PIXEL = 0, 1, 2
 MEM_HOST, MEM_DEVICE = 0, 1
 PIX_CONVERGED, PIX_LAMBDA, PIX_MAXITER, PIX_NFREE, PIX_NONFINITE = 0, 1, 2, -1, -2
-ZMAX = 8
+ZMAX = 16  # PM_ZEEMAN_MAX
 NL_MAX = 128
 
 # Every symbol include/pmilos.h declares (checked by the CPU test suite).

@@ -56,6 +56,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 sys.path.insert(0, os.path.join(ROOT, "tests"))
+sys.path.insert(0, os.path.join(ROOT, "p-milos_b200"))
 
 import pyoracle as po  # noqa: E402
 from fitsmini import read_fits_f32  # noqa: E402
@@ -412,6 +413,32 @@ def psf_pins():
     return out
 
 
+def lines_cases(reference):
+    """create_cuantic (create_cuantic.c:60-294) of every entry of the reference's
+    run/LINES file: the entry's text and the reference's pattern (N_PI, N_SIG,
+    GL, GU, GEFF, FO, NUB, NUP, NUR, WEB, WEP, WER)."""
+    from pmilos_b200.files import parse_lines_entry
+    out = {}
+    with open(os.path.join(reference, "run", "LINES")) as f:
+        entries = [ln.rstrip("\n") for ln in f if ln.strip()]
+    for text in entries:
+        try:
+            idx, lam0, q = parse_lines_entry(text)
+        except ValueError:
+            # a term letter outside readFileCuanticLines' S, P, D, F, G, H, J
+            # (readConfig.c:46-95 leaves L unset there): entry 5's "7k" is read
+            # with its spectroscopic value, K: L = 7
+            idx, lam0, q = parse_lines_entry(text.replace("7k", "7H"))
+            q = (q[0], q[1], q[2], q[3], 7.0, q[5])
+        lam = lam0 + np.linspace(-0.35, 0.35, 30)
+        ref = po.Reference(po.LineSetup(lam, lam0, np.array([1.0, *q]), None, 9), "f64")
+        out[f"l{idx}_text"] = np.array(text)
+        out[f"l{idx}_lambda0"] = lam0
+        out[f"l{idx}_quantum"] = np.array(q, dtype=np.float64)
+        out[f"l{idx}_pattern"] = ref.cuantic()
+    return out
+
+
 def classical_only_cases():
     """The classical-estimates-only mode (NumberOfCycles < 0, milos.c:486-501:
     estimacionesClasicas with forInitialUse = 0 from the initial model) on the
@@ -436,10 +463,15 @@ def classical_only_cases():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
-    ap.add_argument("--only", choices=("all", "wide", "mac", "fits", "zeeman", "classical"), default="all")
+    ap.add_argument("--only", choices=("all", "wide", "mac", "fits", "zeeman", "classical", "lines"), default="all")
     a = ap.parse_args()
     os.environ["PM_REFERENCE_SRC"] = os.path.join(a.reference, "src")
     po.build()
+    if a.only in ("all", "lines"):
+        np.savez_compressed(os.path.join(HERE, "ref_lines.npz"), **lines_cases(a.reference))
+        print("ref_lines.npz", os.path.getsize(os.path.join(HERE, "ref_lines.npz")), "bytes")
+        if a.only == "lines":
+            return
     if a.only in ("all", "classical"):
         np.savez_compressed(os.path.join(HERE, "ref_classical_only.npz"), **classical_only_cases())
         print("ref_classical_only.npz", os.path.getsize(os.path.join(HERE, "ref_classical_only.npz")), "bytes")

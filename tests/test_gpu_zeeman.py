@@ -234,3 +234,42 @@ def test_single_grid_server_matches_the_batch_entry_point():
         b = inv.invert(c["obs"], c["guess"])
     dB = np.abs(r["models"][:, 1] - b["models"][:, 1])
     assert np.median(dB) < 1.0 and (dB < 5.0).mean() >= 0.85
+
+
+def test_nine_component_line_matches_oracle():
+    """Fe I 15652.857 (7D5.0-7K4.0: nine pi and nine sigma components per group)
+    on 30 wavelengths with a 60 mA PSF: FP64 synthesis and response functions,
+    and FP64 inversions, against the oracle."""
+    lam0, q = 15652.857, (3.0, 2.0, 5.0, 3.0, 7.0, 4.0)
+    lam = lam0 + np.linspace(-0.6, 0.6, 30)
+    psf = pm.psf_gaussian(60.0, lam)
+    line = pm.line_from_quantum(lam0, *q)
+    assert (line._c.n_pi, line._c.n_sig) == (9, 9)
+    fix = [1] * 9 + [0, 0]
+    ora = po.Restatement(po.LineSetup(lam, lam0, np.array([1.0, *q]), psf, 9), "f64")
+    rng = np.random.default_rng(91)
+    n = 48
+    m = np.zeros((n, 11))
+    m[:, 0] = rng.uniform(1, 20, n)
+    m[:, 1] = rng.uniform(0, 2000, n)
+    m[:, 2] = rng.uniform(-3, 3, n)
+    m[:, 3] = rng.uniform(0.05, 0.12, n)
+    m[:, 4] = rng.uniform(0.01, 0.5, n)
+    m[:, 5] = rng.uniform(0, 180, n)
+    m[:, 6] = rng.uniform(0, 180, n)
+    m[:, 7] = rng.uniform(0.1, 0.4, n)
+    m[:, 8] = rng.uniform(0.4, 0.9, n)
+    m[:, 10] = 1.0
+    guess = np.array([8.0, 400.0, 0.0, 0.08, 0.1, 30.0, 30.0, 0.25, 0.75, 0.0, 1.0])
+    with pm.Inverter(line, lam, psf, noise=NOISE64, fix=fix, nterms=9, precision=pm.PREC_FP64,
+                     solver=pm.SOLVE_EIGEN) as inv:
+        sp, rf = inv.synth(m, rf=True)
+        for i in range(n):
+            s_ref, rf_ref = ora.synth(m[i], fix=fix)
+            assert np.abs(sp[i] - s_ref).max() < 1e-6
+            scale = np.abs(rf_ref).max(axis=-1, keepdims=True) + 1e-30
+            assert (np.abs(rf[i] - rf_ref) / scale).max() < 1e-5
+        obs = np.ascontiguousarray(sp + rng.normal(0, 1e-3, sp.shape), dtype=np.float32)
+        r = inv.invert(obs, guess)
+    ref = ora.invert(obs, guess, fix=fix, noise=NOISE64)
+    assert within_tolerance(r["models"], ref["models"]).mean() >= 0.85

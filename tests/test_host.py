@@ -22,7 +22,7 @@ def test_library_exports_every_declared_symbol():
     L = pm.load_library()
     for name in declared:
         assert hasattr(L, name), name
-    assert L.pm_abi_version() == 1
+    assert L.pm_abi_version() == 2
 
 
 def test_zeeman_triplet_matches_oracle():
@@ -145,3 +145,36 @@ def test_server_creation_checks_its_grids_then_needs_a_gpu():
         with pytest.raises(pm.PmError) as e:
             pm.Server(line, grids, hbm_budget_bytes=1 << 28)
         assert e.value.code == -19  # PM_ENODEV
+
+
+LINES = np.load(os.path.join(GOLDEN, "ref_lines.npz"))
+
+
+@pytest.mark.parametrize("idx", range(1, 10))
+def test_zeeman_pattern_of_every_reference_line(idx):
+    """pm_line_from_quantum against the reference's create_cuantic for every
+    entry of its run/LINES: normal triplets and multiplets of up to nine
+    components per group (Fe I 15652.857, 7D5.0-7K4.0)."""
+    g = lambda k: LINES[f"l{idx}_{k}"]
+    c = pm.line_from_quantum(float(g("lambda0")), *g("quantum"))._c
+    ref = g("pattern")
+    npi, nsig = int(ref[0]), int(ref[1])
+    assert (c.n_pi, c.n_sig) == (npi, nsig)
+    mine = [npi, nsig, c.gl, c.gu, c.geff, c.fo, *c.nub[:nsig], *c.nup[:npi], *c.nur[:nsig], *c.web[:nsig],
+            *c.wep[:npi], *c.wer[:nsig]]
+    assert np.allclose(mine, ref, rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("idx", range(1, 10))
+def test_lines_entries_parse_like_the_reference(idx):
+    """The LINES reader gives readFileCuanticLines' quantum numbers; a term
+    letter outside its S, P, D, F, G, H, J (entry 5's "7k", for which the
+    reference leaves L unset) is an error rather than an undefined value."""
+    text = str(LINES[f"l{idx}_text"])
+    if idx == 5:
+        with pytest.raises(ValueError):
+            pm.files.parse_lines_entry(text)
+        return
+    i, lam0, q = pm.files.parse_lines_entry(text)
+    assert i == idx and lam0 == float(LINES[f"l{idx}_lambda0"])
+    assert np.array_equal(np.array(q, dtype=np.float64), LINES[f"l{idx}_quantum"])
