@@ -21,7 +21,9 @@ import re
 
 import numpy as np
 
-_LEVELS = {"S": 0, "P": 1, "D": 2, "F": 3, "G": 4, "H": 5, "J": 6}
+# readFileCuanticLines' letters (readConfig.c:46-95, J for L = 6 as it has it),
+# and the spectroscopic I and K it leaves undecoded (L unset there)
+_LEVELS = {"S": 0, "P": 1, "D": 2, "F": 3, "G": 4, "H": 5, "J": 6, "I": 6, "K": 7}
 _LINE_RE = re.compile(
     r"^\s*(\d+)=(\S+)\s+(\d+)\s+([-+0-9.eE]+)\s+([-+0-9.eE]+)\s+([-+0-9.eE]+)\s+-([0-9.eE+-]+)\s+"
     r"(\d+)([A-Za-z])\s*([0-9.]+)-\s*(\d+)([A-Za-z])\s*([0-9.]+)")

@@ -167,14 +167,9 @@ def test_zeeman_pattern_of_every_reference_line(idx):
 
 @pytest.mark.parametrize("idx", range(1, 10))
 def test_lines_entries_parse_like_the_reference(idx):
-    """The LINES reader gives readFileCuanticLines' quantum numbers; a term
-    letter outside its S, P, D, F, G, H, J (entry 5's "7k", for which the
-    reference leaves L unset) is an error rather than an undefined value."""
+    """The LINES reader gives readFileCuanticLines' quantum numbers; entry 5's
+    "7k", a letter the reference leaves undecoded (L unset), reads as K: L = 7."""
     text = str(LINES[f"l{idx}_text"])
-    if idx == 5:
-        with pytest.raises(ValueError):
-            pm.files.parse_lines_entry(text)
-        return
     i, lam0, q = pm.files.parse_lines_entry(text)
     assert i == idx and lam0 == float(LINES[f"l{idx}_lambda0"])
     assert np.array_equal(np.array(q, dtype=np.float64), LINES[f"l{idx}_quantum"])
