@@ -422,14 +422,8 @@ def lines_cases(reference):
     with open(os.path.join(reference, "run", "LINES")) as f:
         entries = [ln.rstrip("\n") for ln in f if ln.strip()]
     for text in entries:
-        try:
-            idx, lam0, q = parse_lines_entry(text)
-        except ValueError:
-            # a term letter outside readFileCuanticLines' S, P, D, F, G, H, J
-            # (readConfig.c:46-95 leaves L unset there): entry 5's "7k" is read
-            # with its spectroscopic value, K: L = 7
-            idx, lam0, q = parse_lines_entry(text.replace("7k", "7H"))
-            q = (q[0], q[1], q[2], q[3], 7.0, q[5])
+        # entry 5's "7k" reads as K: L = 7 (readFileCuanticLines leaves L unset for it)
+        idx, lam0, q = parse_lines_entry(text)
         lam = lam0 + np.linspace(-0.35, 0.35, 30)
         ref = po.Reference(po.LineSetup(lam, lam0, np.array([1.0, *q]), None, 9), "f64")
         out[f"l{idx}_text"] = np.array(text)
