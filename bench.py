@@ -5,7 +5,11 @@ Workload (one "step"): invert the 256x256-pixel, 30-wavelength, PSF-convolved,
 9-free-parameter cube (benchmark configuration 1; Fe I 6173.3354 A, grid
 -350..375 mA in 25 mA steps, Gaussian PSF FWHM 60 mA through the 1 mA table
 route, sigma = 1e-3 noise, <= 50 LM iterations) with the FP32 batched form.
-Synthetic data: seeded atmospheres synthesized by this library's FP64 path.
+Synthetic data: seeded atmospheres whose profiles are synthesized by the
+reference's own mil_sinrf (its C sources built with REAL = double under oracle/,
+outside every timed region), plus seeded N(0, 1e-3) noise; both arms invert the
+same cube.  Cubes above 4 GB (configuration 4) are synthesized on the device by
+this library's FP64 path instead.
 
 JSON line (rank 0):
   value    pixels/s with the cube resident in HBM (CUDA-event time of the
@@ -19,7 +23,10 @@ JSON line (rank 0):
   cpu_baseline  the reference's own C hot path (oracle/_ref, float build,
            -O3) on every host core, forked slabs like pmilos' Scatterv
 
---impl reference: time only the reference's CPU implementation (rank 0).
+--impl reference: the reference's own C hot path (oracle/_ref, REAL = float, -O3)
+on every host core, one forked process per contiguous slab (pmilos' Scatterv
+partition), inverting the whole cube each step; rank 0 only.  This arm loads no
+library of this package.
 Multi-GPU (torchrun): every rank inverts its own cube (weak scaling, replicas:
 pixels are independent, there is no collective on the data path); time is the
 max over ranks.
@@ -111,48 +118,154 @@ class ClockSampler:
                 "power_w_max": max(pw) if pw else None, "reasons": reasons, "samples": len(rows)}
 
 
-# ---- CPU baseline: the reference's own code on every host core ----
+# ---- the reference's own code on the host cores (input synthesis, CPU baseline, reference arm) ----
 _W = {}
 
 
-def _cpu_worker_init(lib, lam, lambda0, cq, psf, nterms):
+def load_specs():
+    """pmilos_b200/specs.py loaded by file path: the workload definitions
+    without importing the package (the reference arm maps no library of it)."""
+    import importlib.util
+
+    path = os.path.join(ROOT, "p-milos_b200", "pmilos_b200", "specs.py")
+    spec = importlib.util.spec_from_file_location("pm_bench_specs", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+class RefWorkload:
+    """A benchmark configuration built with numpy and the reference's own host
+    routines (interpolationLinearPSF / fgauss_WL through oracle/_ref)."""
+
+    def __init__(self, cfg: int, npix: int | None):
+        import pyoracle as po
+
+        S = load_specs()
+        self.cfg = cfg
+        ini, step, fin, self.lambda0 = S.grid_spec(cfg)
+        self.offs, self.lam = S.grid_from_malla(ini, step, fin, self.lambda0)
+        self.cuantic = np.array([1.0, *S.TRIPLET])
+        self.npix = npix or S.DEFAULT_NPIX[cfg]
+        self.seed = cfg
+        self.nterms, self.fix, self.guess = S.nterms_fix_guess(cfg)
+        self.noise = (1.0 / S.SN) ** 2
+        self.miter = 50
+        flavour = "f64" if po.reference_available("f64") else None
+        lib = po.Reference if flavour else po.Restatement
+        self.synth_kind = "reference" if flavour else "port"
+        route = S.psf_route(cfg)
+        self.psf = None
+        if route is not None:
+            helper = po.Reference(po.LineSetup(self.lam, self.lambda0, self.cuantic, None, self.nterms), "f64") \
+                if flavour else None
+            if route[0] == "table":
+                x, y = S.gaussian_psf_table(route[1])
+                self.psf = helper.interp_psf(x, y, self.offs, 0.0) if helper else None
+            else:
+                nl = self.lam.size
+                self.psf = helper.fgauss_wl(route[1], self.lam[1] - self.lam[0], self.lam[0], self.lam[nl // 2], nl) \
+                    if helper else None
+            if self.psf is None:
+                raise RuntimeError("the reference build (oracle/_ref) is needed for the PSF route")
+        self.slight = None
+        if cfg == 2:  # stray light: the synthesis of a B = 0 atmosphere
+            one = lib(po.LineSetup(self.lam, self.lambda0, self.cuantic, self.psf, self.nterms), "f64")
+            self.slight = one.synth(S.QUIET_SUN_B0, None, fix=self.fix, rf=False)[0].astype(np.float32)
+        self.specs = S
+
+    @property
+    def nl(self) -> int:
+        return int(self.lam.size)
+
+    def setup_args(self):
+        return (self.lam, self.lambda0, self.cuantic, self.psf, self.nterms)
+
+
+def _worker_init(lib, lam, lambda0, cq, psf, nterms):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle as po
 
     setup = po.LineSetup(lam, lambda0, cq, psf, nterms)
-    _W["ref"] = po.Reference(setup, lib) if lib.startswith("f") and po.reference_available(lib) else po.Restatement(
-        setup, lib.replace("port_", ""))
+    if lib.startswith("port_"):
+        _W["ref"] = po.Restatement(setup, lib[5:])
+    else:
+        _W["ref"] = po.Reference(setup, lib)
 
 
-def _cpu_worker_run(args):
-    obs, guess, fix, noise = args
+def _worker_synth(args):
+    truth, slight, fix = args
+    ref = _W["ref"]
+    sl = None if slight is None else np.asarray(slight, dtype=np.float64)
+    return np.array([ref.synth(m, sl, fix=fix, rf=False)[0] for m in truth], dtype=np.float32)
+
+
+def _worker_invert(args):
+    obs, guess, fix, noise, slight = args
     t0 = time.perf_counter()
-    _W["ref"].invert(obs, guess, fix=fix, noise=noise, want_spectra=False)
+    _W["ref"].invert(obs, guess, fix=fix, noise=noise, slight=slight, want_spectra=False)
     return time.perf_counter() - t0
 
 
-def cpu_baseline(w, obs, sample_pixels: int, cores: int):
-    """Time the reference (oracle/_ref float build, -O3) on `cores` processes,
-    contiguous slabs (pmilos.c:1181-1205).  Returns (pixels/s, info)."""
+def reference_cube(rw: RefWorkload, seed: int, cores: int):
+    """Seeded observed cube [npix][4][nl] float32 of configuration rw.cfg: truth
+    atmospheres from specs.truth_models, profiles synthesized by the reference's
+    mil_sinrf (REAL = double) on `cores` spawned processes, then N(0, 1e-3) noise
+    from the same generator."""
     import multiprocessing as mp
 
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import pyoracle as po
+    rng = np.random.default_rng(seed)
+    truth = rw.specs.truth_models(rw.cfg, rw.npix, rng)
+    lib = "f64" if rw.synth_kind == "reference" else "port_f64"
+    parts = np.array_split(truth, max(1, min(cores, rw.npix // 256 or 1)))
+    with mp.get_context("spawn").Pool(min(cores, len(parts)), initializer=_worker_init,
+                                      initargs=(lib, *rw.setup_args())) as pool:
+        obs = np.concatenate(pool.map(_worker_synth, [(t, rw.slight, rw.fix) for t in parts]))
+    obs = obs + rng.normal(0.0, rw.specs.NOISE_SIGMA, obs.shape).astype(np.float32)
+    return np.ascontiguousarray(obs, dtype=np.float32)
 
-    kind = "reference" if po.reference_available("f32_fast") else "port"
-    lib = "f32_fast" if kind == "reference" else "port_f32"
-    n = min(sample_pixels, obs.shape[0])
-    slabs = np.array_split(obs[:n], cores)
-    noise32 = float(np.float32(np.float32(1.0 / 1000) ** 2))
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(cores, initializer=_cpu_worker_init,
-                  initargs=(lib, w.lam, w.line.lambda0, w.line.cuantic_dat(), w.psf, w.nterms)) as pool:
-        pool.map(_cpu_worker_run, [(s[:2], w.guess, w.fix, noise32) for s in slabs])  # warm-up
+
+class ReferencePool:
+    """The reference's inversion (oracle/_ref float build, -O3: the reference
+    makefile's default REAL = float) on `cores` spawned processes; each call
+    inverts contiguous slabs, one per process (pmilos.c:1181-1205)."""
+
+    def __init__(self, rw: RefWorkload, cores: int):
+        import multiprocessing as mp
+
+        import pyoracle as po
+
+        self.kind = "reference" if po.reference_available("f32_fast") else "port"
+        lib = "f32_fast" if self.kind == "reference" else "port_f32"
+        self.rw, self.cores = rw, cores
+        self.noise32 = float(np.float32(np.float32(1.0 / rw.specs.SN) ** 2))
+        self.pool = mp.get_context("spawn").Pool(cores, initializer=_worker_init, initargs=(lib, *rw.setup_args()))
+
+    def run(self, obs: np.ndarray) -> tuple:
+        """Invert obs on every process; returns (wall s, slowest slab s)."""
+        rw = self.rw
+        slabs = np.array_split(obs, self.cores)
         t0 = time.perf_counter()
-        per = pool.map(_cpu_worker_run, [(s, w.guess, w.fix, noise32) for s in slabs])
-        wall = time.perf_counter() - t0
-    info = {"kind": kind, "cores": cores, "sample": f"{n} pixels of the workload in {cores} contiguous slabs",
-            "wall_s": round(wall, 3), "max_slab_s": round(max(per), 3)}
+        per = self.pool.map(_worker_invert, [(sl, rw.guess, rw.fix, self.noise32, rw.slight) for sl in slabs])
+        return time.perf_counter() - t0, max(per)
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+
+def cpu_baseline(rw: RefWorkload, obs, sample_pixels: int, cores: int):
+    """The reference's inversion on `cores` processes over a bounded sample of
+    the cube (contiguous slabs).  Returns (pixels/s, info)."""
+    n = min(sample_pixels, obs.shape[0])
+    ref = ReferencePool(rw, cores)
+    try:
+        ref.run(obs[:2 * cores])  # warm-up
+        wall, slab = ref.run(obs[:n])
+    finally:
+        ref.close()
+    info = {"kind": ref.kind, "cores": cores, "sample": f"{n} pixels of the workload in {cores} contiguous slabs",
+            "wall_s": round(wall, 3), "max_slab_s": round(slab, 3)}
     return n / wall, info
 
 
@@ -341,6 +454,64 @@ def bench_served(args, rank: int, world: int, metric: str):
             "gpu_launches": fp32["kernel_launches"] + fp32["prepass_launches"]}), flush=True)
 
 
+# ---- the batch configurations: description, inputs, reference arm ----
+def describe(rw: RefWorkload, gpus: int) -> dict:
+    psf_desc = "no PSF" if rw.psf is None else "Gaussian PSF"
+    stray_desc = ", stray light mixed at alpha~U(0.7,1)" if rw.cfg == 2 else ""
+    return {"workload": f"ME inversion, benchmark configuration {rw.cfg}: {rw.npix} pixels "
+                        f"({int(np.sqrt(rw.npix))}^2) x 4 Stokes x {rw.nl} wavelengths, Fe I {rw.lambda0} A, "
+                        f"{psf_desc}{stray_desc}, {rw.nterms} free parameters, <= {rw.miter} LM iterations",
+            "pixels_per_step": rw.npix, "nlambda": rw.nl, "nterms": rw.nterms,
+            "parallelism": f"replicas x{gpus}", "l2": "flushed between timed steps (256 MiB write)"}
+
+
+def data_desc(rw: RefWorkload, on_device: bool) -> str:
+    if on_device:
+        return ("synthetic: seeded atmospheres drawn on the device, profiles synthesized by this library's FP64 "
+                "path, N(0, 1e-3) noise")
+    who = "the reference's mil_sinrf (REAL = double)" if rw.synth_kind == "reference" else \
+        "the oracle's restatement of mil_sinrf (FP64)"
+    return f"synthetic: seeded atmospheres (seed {rw.seed}), profiles synthesized by {who}, N(0, 1e-3) noise"
+
+
+def reference_arm(args, rank: int, metric: str):
+    """--impl reference: the reference's own C hot path on every host core,
+    inverting the whole cube (configurations 0-2; a bounded sample of the 30 GB
+    configuration 4) every step, one process per contiguous slab."""
+    if rank != 0:
+        return
+    if args.ingest or args.config == 3:
+        why = "the reference has no serving mode" if args.config == 3 else "the reference reads FITS on the host"
+        print(json.dumps({"impl": "reference", "unavailable": why}), flush=True)
+        return
+    cores = host_cores()
+    rw = RefWorkload(args.config, args.npix)
+    cfg_desc = describe(rw, args.gpus)
+    whole = rw.npix * rw.nl * 16 <= (4 << 30)
+    if not whole:
+        rw.npix = args.cpu_sample or 200 * cores  # a bounded sample of the same distributions
+    obs = reference_cube(rw, rw.seed, cores)
+    ref = ReferencePool(rw, cores)
+    walls = []
+    try:
+        for _ in range(args.warmup + args.steps):
+            walls.append(ref.run(obs)[0])
+    finally:
+        ref.close()
+    t = float(np.mean(walls[args.warmup:]))
+    val = rw.npix / t
+    sample = (f"the whole cube ({rw.npix} pixels) every step, {cores} contiguous slabs" if whole else
+              f"{rw.npix} pixels of the workload's distributions every step, {cores} contiguous slabs")
+    print(json.dumps({"metric": metric, "value": val, "unit": "pixels/s", "impl": "reference",
+                      "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                      "ms_per_step": 1000.0 * t, "higher_is_better": True, "scaling": "weak",
+                      "vs_baseline": None, "dtype": "f32", "data": data_desc(rw, False), "config": cfg_desc,
+                      "cpu_baseline": {"value": val, "unit": "pixels/s", "cores": cores, "kind": ref.kind,
+                                       "sample": sample},
+                      "e2e": {"value": val, "unit": "pixels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+          flush=True)
+
+
 # ---- main ----
 def main():
     ap = argparse.ArgumentParser()
@@ -370,49 +541,24 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
+    metric = "pixels/s inverted on 1 B200"
+    # the reference's own code (oracle/): input synthesis, CPU baseline, reference arm
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    if args.impl == "reference":
+        return reference_arm(args, rank, metric)
+
+    rw = None
+    if not args.ingest and args.config != 3:
+        # inputs first (spawned CPU processes, before any CUDA call)
+        rw = RefWorkload(args.config, args.npix)
+        cfg_desc = describe(rw, args.gpus)
+        big = rw.npix * rw.nl * 16 > (4 << 30)
+        obs = None if big else reference_cube(rw, rw.seed + 1000 * rank, max(1, host_cores() // world))
+
     import torch
 
     import pmilos_b200 as pm
     from pmilos_b200 import workloads
-
-    metric = "pixels/s inverted on 1 B200"
-    w = workloads.config(args.config, npix=args.npix)
-    psf_desc = "no PSF" if w.psf is None else "Gaussian PSF"
-    stray_desc = ", stray light mixed at alpha~U(0.7,1)" if w.cfg == 2 else ""
-    cfg_desc = {"workload": f"ME inversion, benchmark configuration {args.config}: {w.npix} pixels "
-                            f"({int(np.sqrt(w.npix))}^2) x 4 Stokes x {w.nl} wavelengths, Fe I {w.line.lambda0} A, "
-                            f"{psf_desc}{stray_desc}, {w.nterms} free parameters, <= {w.miter} LM iterations",
-                "pixels_per_step": w.npix, "nlambda": w.nl, "nterms": w.nterms,
-                "parallelism": f"replicas x{args.gpus}", "l2": "flushed between timed steps (256 MiB write)"}
-
-    if args.impl == "reference":
-        if rank != 0:
-            return
-        # the reference's CPU path on the host cores; data synthesized by the oracle port
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import pyoracle as po
-
-        rng = np.random.default_rng(w.seed)
-        truth = workloads.truth_models(w, rng)
-        cores = host_cores()
-        n = args.cpu_sample or min(w.npix, (1500 if w.nl <= 32 else 200) * cores)
-        ora = po.Restatement(po.LineSetup(w.lam, w.line.lambda0, w.line.cuantic_dat(), w.psf, w.nterms), "f64")
-        obs = np.array([ora.synth(m, None, fix=w.fix, rf=False)[0] for m in truth[:n]], dtype=np.float32)
-        obs += rng.normal(0, 1e-3, obs.shape).astype(np.float32)
-        vals = []
-        for _ in range(args.warmup + args.steps):
-            v, info = cpu_baseline(w, obs, n, cores)
-            vals.append(v)
-        val = float(np.median(vals[args.warmup:]))
-        print(json.dumps({"metric": metric, "value": val, "unit": "pixels/s", "impl": "reference",
-                          "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-                          "ms_per_step": 1000.0 * w.npix / val, "higher_is_better": True, "scaling": "weak",
-                          "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg_desc,
-                          "cpu_baseline": {"value": val, "unit": "pixels/s", "cores": info["cores"],
-                                           "kind": info["kind"], "sample": info["sample"]},
-                          "e2e": {"value": val, "unit": "pixels/s", "h2d_bytes_per_step": 0,
-                                  "d2h_bytes_per_step": 0}}), flush=True)
-        return
 
     torch.cuda.set_device(local)
     if args.ingest:
@@ -427,15 +573,14 @@ def main():
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
+    w = workloads.config(args.config, npix=args.npix)
+    w.slight = rw.slight  # the reference's synthesis of the B = 0 atmosphere (configuration 2)
     inv32 = pm.Inverter(w.line, w.lam, w.psf, noise=w.noise, fix=w.fix, nterms=w.nterms, precision=pm.PREC_FP32)
     inv64 = pm.Inverter(w.line, w.lam, w.psf, noise=w.noise, fix=w.fix, nterms=w.nterms, precision=pm.PREC_FP64)
-    rng = np.random.default_rng(w.seed + 1000 * rank)
-    if w.npix * w.nl * 16 > (4 << 30):
+    if obs is None:
         # cubes above 4 GB are drawn and synthesized on the device, in chunks
-        obs = None
         obs_d = workloads.synthesize_device(w, inv64, seed=w.seed + 1000 * rank)
     else:
-        obs = workloads.synthesize(w, inv_fp64=inv64, rng=rng)
         obs_d = torch.as_tensor(obs, device="cuda")
     sl_h = None if w.slight is None else np.ascontiguousarray(w.slight, dtype=np.float32)
     sl_d = None if sl_h is None else torch.as_tensor(sl_h, device="cuda")
@@ -448,7 +593,7 @@ def main():
         ns = min(w.npix, 32768)
         sample = obs[:ns] if obs is not None else obs_d[:ns].cpu().numpy()
         inv32.autotune(sample, w.guess, slight=sl_h, reps=2)
-    cfg_desc["tuning"] = inv32.tuning
+    tuning = inv32.tuning
 
     def barrier():
         if dist is not None:
@@ -557,7 +702,7 @@ def main():
         cores = host_cores()
         n = args.cpu_sample or min(w.npix, (1500 if w.nl <= 32 else 200) * cores)
         sample = obs if obs is not None else obs_d[:n].cpu().numpy()
-        v, info = cpu_baseline(w, sample, n, cores)
+        v, info = cpu_baseline(rw, sample, n, cores)
         cpu = {"value": v, "unit": "pixels/s", "cores": info["cores"], "kind": info["kind"],
                "sample": info["sample"]}
 
@@ -565,7 +710,8 @@ def main():
         print(json.dumps({
             "metric": metric, "value": value, "unit": "pixels/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg_desc,
+            "vs_baseline": None, "dtype": "f32", "data": data_desc(rw, obs is None), "config": cfg_desc,
+            "tuning": tuning,
             "e2e": {"value": e2e_v, "unit": "pixels/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     **({"note": e2e_note} if e2e_note else {})},
             "plain": plain, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,

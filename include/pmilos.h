@@ -247,11 +247,15 @@ int pm_lm_mils(pm_ctx *ctx, const float *spectro, pm_model *init_model, float *s
  * staging and the work-queue counters live in one static device array built into
  * the library (about 6.5 MB, held on every GPU that loads the library until the
  * process exits), sized for at most PM_NOALLOC_MAX_PIXELS pixels of up to 32
- * wavelengths per call: larger calls fail with PM_ERANGE.  The first call on a
- * device looks up that array's device address (cudaGetSymbolAddress) and caches
- * it; make that first call before any stream capture.  All calls share the one
- * array: calls whose GPU work overlaps (other host threads, other streams) race
- * and must be serialised by the caller.  stream: a cudaStream_t or NULL. */
+ * wavelengths per call: larger calls fail with PM_ERANGE.  Every call looks up
+ * that array's device address on the current device (cudaGetSymbolAddress,
+ * which allocates nothing), so a cudaDeviceReset between calls does no harm.
+ * The call synchronizes its stream before it returns, on success and on every
+ * error after its first copy was queued: do not call it while that stream is
+ * being captured into a CUDA graph.  All calls share the one array, and it keeps
+ * the last call's contents: calls whose GPU work overlaps (other host threads,
+ * other streams) race and must be serialised by the caller.  stream: a
+ * cudaStream_t or NULL. */
 #define PM_NOALLOC_MAX_PIXELS 4096
 #define PM_NOALLOC_MAX_WAVELENGTHS 32
 int pm_invert_batch_noalloc(const pm_line *line, const pm_config *cfg, int64_t npix, const float *spectro,

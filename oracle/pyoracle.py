@@ -42,15 +42,17 @@ def _i(a):
     return None if a is None else a.ctypes.data_as(_I)
 
 
-def build(quiet: bool = True) -> None:
-    """Compile the restatement (always) and the reference (when its sources exist)."""
+def build(quiet: bool = True, refsrc: str | None = None) -> None:
+    """Compile the restatement (always) and the reference, from its src/
+    directory given as ``refsrc`` or $PM_REFERENCE_SRC (skipped when neither
+    names an existing directory)."""
     import subprocess
 
     targets = ["own"]
-    refsrc = os.environ.get("PM_REFERENCE_SRC", "/root/reference/src")
-    if os.path.isdir(refsrc):
+    refsrc = refsrc or os.environ.get("PM_REFERENCE_SRC")
+    if refsrc and os.path.isdir(refsrc):
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE, f"REFSRC={refsrc}", *targets], check=True,
+    subprocess.run(["make", "-s", "-C", HERE, f"REFSRC={refsrc or ''}", *targets], check=True,
                    stdout=subprocess.DEVNULL if quiet else None)
 
 

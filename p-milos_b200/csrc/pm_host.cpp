@@ -30,8 +30,8 @@ int fail(int code, const char* fmt, ...) {
   return code;
 }
 
-int cuda_fail(cudaError_t e, const char* what) {
-  return fail(PM_EIO, "%s: %s", what, cudaGetErrorString(e));
+int cuda_fail(cudaError_t e, const char* what, int code = PM_EIO) {
+  return fail(code, "%s: %s", what, cudaGetErrorString(e));
 }
 
 #define PM_CUDA(call, what)                       \
@@ -39,6 +39,19 @@ int cuda_fail(cudaError_t e, const char* what) {
     cudaError_t e_ = (call);                      \
     if (e_ != cudaSuccess) return cuda_fail(e_, what); \
   } while (0)
+
+// A start/stop event pair that every return path of its owner releases.
+struct TimingEvents {
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  cudaError_t create() {
+    cudaError_t e = cudaEventCreate(&t0);
+    return e != cudaSuccess ? e : cudaEventCreate(&t1);
+  }
+  ~TimingEvents() {
+    if (t0) cudaEventDestroy(t0);
+    if (t1) cudaEventDestroy(t1);
+  }
+};
 
 // Device buffer that grows on demand.
 struct DevBuf {
@@ -839,20 +852,16 @@ int run_graph_small(pm_ctx* c, int64_t n, const float* spectro, const float* sli
 // vNumIter / vChisqrf that mode writes), status PM_PIX_CLASSICAL, best-fit
 // profiles zero.
 int run_classical_only(pm_ctx* c, const PmIO& io, float* kernel_ms) {
-  cudaEvent_t a, b;
-  cudaEventCreate(&a);
-  cudaEventCreate(&b);
+  TimingEvents ev;
+  PM_CUDA(ev.create(), "classical estimates: events");
+  cudaEvent_t a = ev.t0, b = ev.t1;
   cudaEventRecord(a, c->stream);
   int rc = c->P.G == 1 ? pmk_classical_prepass(c->P, io.spectro, io.models_out, io.npix, c->stream, c->num_sms,
                                                io.lambda_pix)
                        : pmk_classical_wide(c->P, io, c->stream, c->num_sms);
   cudaEventRecord(b, c->stream);
   if (rc == PM_OK && io.status_out) rc = pmk_fill_int(io.status_out, io.npix, PM_PIX_CLASSICAL, c->stream);
-  if (rc != PM_OK) {
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
-    return fail(rc, "%s", pmk_last_cuda_error());
-  }
+  if (rc != PM_OK) return fail(rc, "%s", pmk_last_cuda_error());
   const size_t n = size_t(io.npix);
   cudaError_t e = cudaMemsetAsync(io.chisq_out, 0, sizeof(float) * n, c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(io.iters_out, 0, sizeof(int) * n, c->stream);
@@ -860,8 +869,6 @@ int run_classical_only(pm_ctx* c, const PmIO& io, float* kernel_ms) {
     e = cudaMemsetAsync(io.spectra_out, 0, sizeof(float) * 4 * c->P.nl * n, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e == cudaSuccess && kernel_ms) e = cudaEventElapsedTime(kernel_ms, a, b);
-  cudaEventDestroy(a);
-  cudaEventDestroy(b);
   if (e != cudaSuccess) return cuda_fail(e, "classical estimates");
   c->stats.pixels += io.npix;
   return PM_OK;
@@ -945,6 +952,7 @@ int invert_impl(pm_ctx* c, int64_t npix, const float* spectro, const double* lam
   if (!c || !spectro || !guess || !models_out || !chisq_out || !iters_out)
     return fail(PM_EINVAL, "pm_invert_batch: NULL argument");
   PmDeviceGuard dg(c->device);
+  if (!dg.ok()) return cuda_fail(dg.err, "pm_invert_batch: selecting the context's device", PM_ENODEV);
   if (npix < 0) return fail(PM_EINVAL, "pm_invert_batch: npix < 0");
   if (mem != PM_MEM_HOST && mem != PM_MEM_DEVICE) return fail(PM_EINVAL, "pm_invert_batch: mem=%d", mem);
   if (int rc = check_guess(c->P, guess); rc != PM_OK) return rc;
@@ -956,9 +964,9 @@ int invert_impl(pm_ctx* c, int64_t npix, const float* spectro, const double* lam
   if (rc != PM_OK) return rc;
   const int nl = c->P.nl;
   const size_t prof = sizeof(float) * 4 * nl;
-  cudaEvent_t t0, t1;
-  cudaEventCreate(&t0);
-  cudaEventCreate(&t1);
+  TimingEvents ev;  // destroyed on every return path
+  PM_CUDA(ev.create(), "pm_invert_batch: events");
+  cudaEvent_t t0 = ev.t0, t1 = ev.t1;
   cudaEventRecord(t0, c->stream);
   float kms_total = 0;
   if (mem == PM_MEM_DEVICE) {
@@ -1064,8 +1072,6 @@ int invert_impl(pm_ctx* c, int64_t npix, const float* spectro, const double* lam
   cudaEventSynchronize(t1);
   float tot = 0;
   cudaEventElapsedTime(&tot, t0, t1);
-  cudaEventDestroy(t0);
-  cudaEventDestroy(t1);
   c->stats.kernel_ms = kms_total;
   c->stats.total_ms = tot;
   if (rc == PM_OK) {
@@ -1099,6 +1105,7 @@ int synth_impl(pm_ctx* c, int64_t npix, const pm_model* models, const double* la
                int slight_mode, float* spectra_out, float* rf_out, int mem) {
   if (!c || !models || !spectra_out) return fail(PM_EINVAL, "pm_synth_batch: NULL argument");
   PmDeviceGuard dg(c->device);
+  if (!dg.ok()) return cuda_fail(dg.err, "pm_synth_batch: selecting the context's device", PM_ENODEV);
   if (npix < 0) return fail(PM_EINVAL, "pm_synth_batch: npix < 0");
   if (mem != PM_MEM_HOST && mem != PM_MEM_DEVICE) return fail(PM_EINVAL, "pm_synth_batch: mem=%d", mem);
   if (npix == 0) return PM_OK;
@@ -1198,6 +1205,7 @@ extern "C" int pm_autotune(pm_ctx* c, int64_t npix, const float* spectro, const 
                            const pm_model* guess, int reps, pm_tuning* out) {
   if (!c || !spectro || !guess) return fail(PM_EINVAL, "pm_autotune: NULL argument");
   PmDeviceGuard dg(c->device);
+  if (!dg.ok()) return cuda_fail(dg.err, "pm_autotune: selecting the context's device", PM_ENODEV);
   if (npix < 1) return fail(PM_EINVAL, "pm_autotune: npix=%lld", (long long)npix);
   reps = std::max(1, std::min(reps, 16));
   std::vector<pm_model> models(static_cast<size_t>(npix));
@@ -1244,6 +1252,7 @@ extern "C" int pm_autotune(pm_ctx* c, int64_t npix, const float* spectro, const 
 extern "C" int pm_selftest_stalled_queue(pm_ctx* c, double limit_ms, int* queue_error, double* elapsed_ms) {
   if (!c || !queue_error || !elapsed_ms) return fail(PM_EINVAL, "pm_selftest_stalled_queue: NULL argument");
   PmDeviceGuard dg(c->device);
+  if (!dg.ok()) return cuda_fail(dg.err, "pm_selftest_stalled_queue: selecting the context's device", PM_ENODEV);
   if (!(limit_ms > 0 && limit_ms <= 10000)) return fail(PM_EINVAL, "pm_selftest_stalled_queue: limit_ms out of (0, 1e4]");
   if (c->P.G != 1) return fail(PM_ENOTSUP, "pm_selftest_stalled_queue: one-warp grids only");
   int rc = stream_resources(c);

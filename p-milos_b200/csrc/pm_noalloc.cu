@@ -51,38 +51,42 @@ constexpr size_t kScratchBytes = align256(kOffBest + kMaxPix * kProf);
 // The scratch.  Host code must not use this name as an address: on the host it
 // is a stand-in object, not device memory (a kernel given it would fault, or on
 // systems where the GPU can reach host memory, silently use the wrong memory).
-// The device address comes from cudaGetSymbolAddress, once per device.
+// The device address comes from cudaGetSymbolAddress with the device current.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 namespace {
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
-unsigned char* g_scratch[kMaxDevices] = {};
-int g_sms[kMaxDevices] = {};
+int g_sms[kMaxDevices] = {};  // set-up done once per device: SM count after the architecture check
 
-// Device address of the scratch on the current device, looked up on the first
-// call made on that device (with the device current) and cached.
+// Device address of the scratch on the current device.  The architecture check
+// and the SM count are set up on the first call made on a device (with that
+// device current); the address itself is looked up on every call
+// (cudaGetSymbolAddress allocates nothing), so a context recreated by
+// cudaDeviceReset between calls, which reloads the module, gets the new
+// address rather than a stale one.
 int scratch_for_current_device(unsigned char** out, int* sms) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return pmh_fail(PM_ENODEV, cudaGetErrorString(e));
   if (dev < 0 || dev >= kMaxDevices) return pmh_fail(PM_ERANGE, "device index beyond 63");
-  std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_scratch[dev]) {
-    int major = 0, nsm = 0;
-    e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
-    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (e != cudaSuccess) return pmh_fail(PM_ENODEV, cudaGetErrorString(e));
-    if (major != 10) return pmh_fail(PM_ENODEV, "pm_invert_batch_noalloc: this library is built for sm_100a");
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) return pmh_fail(PM_EIO, e != cudaSuccess ? cudaGetErrorString(e) : "null symbol");
-    g_scratch[dev] = static_cast<unsigned char*>(p);
-    g_sms[dev] = nsm;
+  {
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (!g_sms[dev]) {
+      int major = 0, nsm = 0;
+      e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+      if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+      if (e != cudaSuccess) return pmh_fail(PM_ENODEV, cudaGetErrorString(e));
+      if (major != 10) return pmh_fail(PM_ENODEV, "pm_invert_batch_noalloc: this library is built for sm_100a");
+      g_sms[dev] = nsm;
+    }
+    *sms = g_sms[dev];
   }
-  *out = g_scratch[dev];
-  *sms = g_sms[dev];
+  void* p = nullptr;
+  e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p) return pmh_fail(PM_EIO, e != cudaSuccess ? cudaGetErrorString(e) : "null symbol");
+  *out = static_cast<unsigned char*>(p);
   return PM_OK;
 }
 
@@ -90,6 +94,14 @@ int cuda_err(cudaError_t e, const char* what) {
   char msg[256];
   std::snprintf(msg, sizeof msg, "%s: %s", what, cudaGetErrorString(e));
   return pmh_fail(PM_EIO, msg);
+}
+
+// An error after work was queued on st: wait for that work (it uses the shared
+// scratch) before returning, so that a caller who serialises its calls never
+// has two calls' GPU work on the scratch at once.  The first error is kept.
+int fail_after_queue(cudaStream_t st, int rc) {
+  cudaStreamSynchronize(st);
+  return rc;
 }
 
 }  // namespace
@@ -144,10 +156,10 @@ extern "C" int pm_invert_batch_noalloc(const pm_line* line, const pm_config* cfg
   PmJob* job_dev = reinterpret_cast<PmJob*>(base + kOffJob);
   cudaError_t e;
   if ((e = cudaMemcpyAsync(base + kOffSpectro, spectro, prof * npix, cudaMemcpyHostToDevice, st)) != cudaSuccess)
-    return cuda_err(e, "spectro H2D");
+    return fail_after_queue(st, cuda_err(e, "spectro H2D"));
   if (slight_mode == PM_SLIGHT_PER_PIXEL &&
       (e = cudaMemcpyAsync(base + kOffSlight, slight, prof * npix, cudaMemcpyHostToDevice, st)) != cudaSuccess)
-    return cuda_err(e, "slight H2D");
+    return fail_after_queue(st, cuda_err(e, "slight H2D"));
   PmIO io{};
   io.npix = npix;
   io.models_out = reinterpret_cast<double*>(base + kOffModels);
@@ -171,9 +183,9 @@ extern "C" int pm_invert_batch_noalloc(const pm_line* line, const pm_config* cfg
   qinit.avail = (unsigned long long)npix;
   qinit.closed = 1;
   if ((e = cudaMemcpyAsync(job_dev, &job, sizeof job, cudaMemcpyHostToDevice, st)) != cudaSuccess)
-    return cuda_err(e, "job H2D");
+    return fail_after_queue(st, cuda_err(e, "job H2D"));
   if ((e = cudaMemcpyAsync(q, &qinit, sizeof qinit, cudaMemcpyHostToDevice, st)) != cudaSuccess)
-    return cuda_err(e, "queue H2D");
+    return fail_after_queue(st, cuda_err(e, "queue H2D"));
   PmGridSet gs;
   std::memset(&gs, 0, sizeof gs);
   gs.ngrids = 1;
@@ -186,26 +198,26 @@ extern "C" int pm_invert_batch_noalloc(const pm_line* line, const pm_config* cfg
   sio.wait_limit_ns = 20000000000LL;
   if (P.classical) {
     rc = pmk_classical_prepass(P, job.spectro, io.models_out, npix, st, sms);
-    if (rc != PM_OK) return pmh_fail(rc, pmk_last_cuda_error());
+    if (rc != PM_OK) return fail_after_queue(st, pmh_fail(rc, pmk_last_cuda_error()));
   }
   rc = pmk_invert_stream(gs, sio, cfg->precision, 0, 4, false, st, sms, nullptr);
-  if (rc != PM_OK) return pmh_fail(rc, pmk_last_cuda_error());
+  if (rc != PM_OK) return fail_after_queue(st, pmh_fail(rc, pmk_last_cuda_error()));
   if ((e = cudaMemcpyAsync(models_out, io.models_out, sizeof(pm_model) * npix, cudaMemcpyDeviceToHost, st)) !=
       cudaSuccess)
-    return cuda_err(e, "models D2H");
+    return fail_after_queue(st, cuda_err(e, "models D2H"));
   if ((e = cudaMemcpyAsync(chisq_out, io.chisq_out, sizeof(float) * npix, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
-    return cuda_err(e, "chisq D2H");
+    return fail_after_queue(st, cuda_err(e, "chisq D2H"));
   if ((e = cudaMemcpyAsync(iters_out, io.iters_out, sizeof(int) * npix, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
-    return cuda_err(e, "iters D2H");
+    return fail_after_queue(st, cuda_err(e, "iters D2H"));
   if (status_out &&
       (e = cudaMemcpyAsync(status_out, io.status_out, sizeof(int) * npix, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
-    return cuda_err(e, "status D2H");
+    return fail_after_queue(st, cuda_err(e, "status D2H"));
   if (best_fit_out &&
       (e = cudaMemcpyAsync(best_fit_out, io.spectra_out, prof * npix, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
-    return cuda_err(e, "best fit D2H");
+    return fail_after_queue(st, cuda_err(e, "best fit D2H"));
   PmStreamQ qread{};
   if ((e = cudaMemcpyAsync(&qread, q, sizeof qread, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
-    return cuda_err(e, "queue D2H");
+    return fail_after_queue(st, cuda_err(e, "queue D2H"));
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_err(e, "pm_invert_batch_noalloc");
   if (qread.err || qread.next < (unsigned long long)npix)
     return pmh_fail(PM_EIO, "pm_invert_batch_noalloc: the inversion kernel stopped early");

@@ -162,11 +162,25 @@ const char* pmk_last_cuda_error();
 // Makes dev the calling thread's current device for the guard's scope and puts
 // the caller's back afterwards: every entry point that works on a context or a
 // server runs on that object's GPU whatever the caller's thread has selected.
+// err is the result of selecting dev; an entry point returns PM_ENODEV when it
+// is not cudaSuccess rather than work on whatever device is current.
 struct PmDeviceGuard {
   int prev = -1;
+  cudaError_t err = cudaSuccess;
   explicit PmDeviceGuard(int dev) {
-    if (cudaGetDevice(&prev) != cudaSuccess || prev == dev || cudaSetDevice(dev) != cudaSuccess) prev = -1;
+    err = cudaGetDevice(&prev);
+    if (err != cudaSuccess) {
+      prev = -1;
+      return;
+    }
+    if (prev == dev) {
+      prev = -1;
+      return;
+    }
+    err = cudaSetDevice(dev);
+    if (err != cudaSuccess) prev = -1;
   }
+  bool ok() const { return err == cudaSuccess; }
   ~PmDeviceGuard() {
     if (prev >= 0) cudaSetDevice(prev);
   }

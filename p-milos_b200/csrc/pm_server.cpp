@@ -394,8 +394,14 @@ void finish(pm_server* s, Scan* sc) {
 }
 
 void serve(pm_server* s) {
-  cudaSetDevice(s->device);  // a new thread starts on device 0: work on the server's GPU
+  // a new thread starts on device 0: work on the server's GPU, or end every scan
+  const cudaError_t dev_err = cudaSetDevice(s->device);
   std::unique_lock<std::mutex> lk(s->mu);
+  if (dev_err != cudaSuccess) {
+    char msg[200];
+    std::snprintf(msg, sizeof msg, "scheduler: selecting the server's device: %s", cudaGetErrorString(dev_err));
+    fail_all_code(s, PM_ENODEV, msg);
+  }
   while (true) {
     bool progress = false;
     if (s->error == PM_OK) {
@@ -715,6 +721,7 @@ extern "C" int pm_server_set_slight(pm_server* s, int grid, const float* slight,
   std::lock_guard<std::mutex> lk(s->mu);
   if (s->next_id != 1) return sfail(PM_EINVAL, "pm_server_set_slight: scans were submitted already");
   PmDeviceGuard dg(s->device);
+  if (!dg.ok()) return sfail(PM_ENODEV, "pm_server_set_slight: selecting the server's device: %s", cudaGetErrorString(dg.err));
   PmParams& P = s->gs->g[grid];
   if (slight_mode == PM_SLIGHT_PER_PIXEL && (!slight || npix < 1))
     return sfail(PM_EINVAL, "pm_server_set_slight: a per-pixel cube needs slight and npix >= 1");

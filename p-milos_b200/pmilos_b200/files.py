@@ -21,6 +21,8 @@ import re
 
 import numpy as np
 
+from .specs import grid_from_malla  # noqa: F401  (the .grid rules, milos.c:176-196)
+
 # readFileCuanticLines' letters (readConfig.c:46-95, J for L = 6 as it has it),
 # and the spectroscopic I and K it leaves undecoded (L unset there)
 _LEVELS = {"S": 0, "P": 1, "D": 2, "F": 3, "G": 4, "H": 5, "J": 6, "I": 6, "K": 7}
@@ -76,22 +78,6 @@ def read_grid_file(path: str):
             if line.startswith("------"):
                 found = True
     raise ValueError(f"no grid definition in {path}")
-
-
-def grid_from_malla(initial_ma: float, step_ma: float, final_ma: float, lambda0: float):
-    """Wavelength grid as milos.c:176-196 builds it: nl = (final - initial)/step + 1
-    (truncated), offsets and wavelengths accumulated sample by sample.
-    Returns (offsets [mA], wavelengths [A])."""
-    nl = int((final_ma - initial_ma) / step_ma) + 1
-    offs = np.zeros(nl)
-    offs[0] = initial_ma
-    for i in range(1, nl):
-        offs[i] = offs[i - 1] + step_ma
-    lam = np.zeros(nl)
-    lam[0] = lambda0 + initial_ma / 1000.0
-    for i in range(1, nl):
-        lam[i] = lam[i - 1] + step_ma / 1000.0
-    return offs, lam
 
 
 def read_psf_file(path: str):

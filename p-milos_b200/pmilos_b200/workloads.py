@@ -15,15 +15,10 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import LineData, grid_from_malla, psf_from_table, psf_gaussian
-
-FE6173 = 6173.3354
-FE6302 = 6302.4936
-TRIPLET = (2.0, 1.0, 1.0, 2.0, 2.0, 0.0)  # 5P1.0 - 5D0.0 after readFileCuanticLines' decoding
-GUESS = np.array([8.0, 400.0, 0.0, 0.03, 0.1, 30.0, 30.0, 0.25, 0.75, 0.0, 1.0])
-QUIET_SUN_B0 = np.array([13.0, 0.0, 0.2, 0.035, 0.19, 30.0, 30.0, 0.26, 0.74, 0.0, 1.0])
-NOISE_SIGMA = 1e-3
-SN = 1000
+from . import LineData, psf_from_table, psf_gaussian
+from .specs import (DEFAULT_NPIX, FE6173, FE6302, GUESS, NOISE_SIGMA, QUIET_SUN_B0, SN, TRIPLET,  # noqa: F401
+                    gaussian_psf_table, grid_from_malla, grid_spec, nterms_fix_guess, psf_route)
+from .specs import truth_models as _truth_models
 
 
 @dataclass
@@ -48,71 +43,26 @@ class Workload:
         return int(self.lam.size)
 
 
-def gaussian_psf_table(fwhm_ma: float, half_range_ma: float = 1500.0, step_ma: float = 1.0):
-    """A zero-mean, unit-area Gaussian sampled like run/CRISP_6173_1mA.psf."""
-    x = np.arange(-half_range_ma, half_range_ma + step_ma / 2, step_ma)
-    sig = fwhm_ma / (2.0 * np.sqrt(2.0 * np.log(2.0)))
-    y = np.exp(-0.5 * (x / sig) ** 2)
-    y /= y.sum() * step_ma
-    return x, y
-
-
-def _grid(cfg: int, which: int = 2):
-    if cfg == 4:
-        return -1204.0, 21.5, 1182.5, FE6302
-    if cfg == 3:
-        return [(-172.5, 69.0, 172.5), (-350.0, 50.0, 350.0), (-350.0, 25.0, 375.0)][which] + (FE6173,)
-    return -350.0, 25.0, 375.0, FE6173
-
-
 def config(cfg: int, npix: int | None = None, grid: int = 2) -> Workload:
     """Workload spec of benchmark configuration ``cfg`` (0..4)."""
-    ini, step, fin, l0 = _grid(cfg, grid)
+    ini, step, fin, l0 = grid_spec(cfg, grid)
     offs, lam = grid_from_malla(ini, step, fin, l0)
     line = LineData(l0, TRIPLET)
-    default_npix = {0: 64 * 64, 1: 256 * 256, 2: 1024 * 1024, 3: 256 * 256, 4: 4096 * 4096}[cfg]
     psf = None
-    if cfg in (1, 2):
-        x, y = gaussian_psf_table(60.0)
+    route = psf_route(cfg)
+    if route is not None and route[0] == "table":
+        x, y = gaussian_psf_table(route[1])
         psf = psf_from_table(x, y, offs)
-    elif cfg == 3:
-        psf = psf_gaussian(60.0, lam)  # the 6-point grid has no zero sample: numeric-FWHM route
-    elif cfg == 4:
-        x, y = gaussian_psf_table(25.0)
-        psf = psf_from_table(x, y, offs)
-    w = Workload(f"config{cfg}", cfg, line, offs, lam, psf, npix or default_npix, seed=cfg)
-    if cfg == 2:
-        w.nterms = 10
-        w.fix = [1] * 9 + [0, 1]
-        w.guess = GUESS.copy()
-        w.guess[10] = 0.9
+    elif route is not None:
+        psf = psf_gaussian(route[1], lam)
+    w = Workload(f"config{cfg}", cfg, line, offs, lam, psf, npix or DEFAULT_NPIX[cfg], seed=cfg)
+    w.nterms, w.fix, w.guess = nterms_fix_guess(cfg)
     return w
 
 
 def truth_models(w: Workload, rng: np.random.Generator | None = None) -> np.ndarray:
     """Seeded per-pixel atmospheres [npix][11]."""
-    rng = rng or np.random.default_rng(w.seed)
-    n = w.npix
-    m = np.zeros((n, 11))
-    m[:, 0] = rng.uniform(1, 20, n)
-    m[:, 1] = rng.uniform(0, 3000, n)
-    m[:, 2] = rng.uniform(-3, 3, n)
-    m[:, 3] = rng.uniform(0.02, 0.05, n)
-    m[:, 4] = rng.uniform(0.01, 0.5, n)
-    m[:, 5] = rng.uniform(0, 180, n)
-    m[:, 6] = rng.uniform(0, 180, n)
-    m[:, 7] = rng.uniform(0.1, 0.4, n)
-    m[:, 8] = rng.uniform(0.4, 0.9, n)
-    m[:, 9] = 0.0
-    m[:, 10] = 1.0
-    if w.cfg in (2, 3):
-        weak = rng.uniform(0, 1, n) < 0.7
-        m[weak, 1] = rng.uniform(0, 200, int(weak.sum()))
-        m[weak, 0] = rng.uniform(1, 5, int(weak.sum()))
-        m[~weak, 1] = rng.uniform(1500, 3500, int((~weak).sum()))
-    if w.cfg == 2:
-        m[:, 10] = 1.0 - rng.uniform(0, 0.3, n)
-    return m
+    return _truth_models(w.cfg, w.npix, rng or np.random.default_rng(w.seed))
 
 
 def synthesize(w: Workload, inv_fp64=None, rng: np.random.Generator | None = None, truth: np.ndarray | None = None,

@@ -3,7 +3,9 @@
 Run in a container where the reference tree exists (its sources are compiled by
 oracle/Makefile into oracle/_ref/):
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <the reference tree>
+
+(or with PM_REFERENCE_SRC set to its src/ directory)
 
 Writes
   kat_synthesis.npz   the reference's own known-answer test (test/synthesis.mtrol:
@@ -456,9 +458,14 @@ def classical_only_cases():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=None, help="the reference tree (default: the parent of $PM_REFERENCE_SRC)")
     ap.add_argument("--only", choices=("all", "wide", "mac", "fits", "zeeman", "classical", "lines"), default="all")
     a = ap.parse_args()
+    if a.reference is None:
+        src = os.environ.get("PM_REFERENCE_SRC")
+        if not src:
+            ap.error("give --reference <the reference tree> or set PM_REFERENCE_SRC to its src/ directory")
+        a.reference = os.path.dirname(os.path.abspath(src))
     os.environ["PM_REFERENCE_SRC"] = os.path.join(a.reference, "src")
     po.build()
     if a.only in ("all", "lines"):
