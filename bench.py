@@ -400,8 +400,10 @@ def bench_served(args, rank: int, world: int, metric: str):
         pool[(si, g)] = h.numpy()
     torch.cuda.empty_cache()
 
-    def run(precision, count):
-        lat, pix, infos = [], 0, []
+    def run(precision, count, rate_scale=1.0):
+        """Replay scans warmup..warmup+count of the schedule, arrival times
+        scaled by 1/rate_scale (rate_scale < 1: a lighter load than 20 scans/s)."""
+        infos = []
         with pm.Server(line, grids(precision), hbm_budget_bytes=int(args.budget_gb * (1 << 30)), max_inflight=64,
                        linger_ms=5.0) as srv:
             for i in range(min(args.warmup, count)):  # warm-up scans (untimed): smallest cube of each grid
@@ -410,7 +412,7 @@ def bench_served(args, rank: int, world: int, metric: str):
             t0 = time.perf_counter()
             ids = []
             for i in range(args.warmup, args.warmup + count):
-                dt = t0 + (arrivals[i] - arrivals[args.warmup]) - time.perf_counter()
+                dt = t0 + (arrivals[i] - arrivals[args.warmup]) / rate_scale - time.perf_counter()
                 if dt > 0:
                     time.sleep(dt)
                 ids.append(srv.submit(int(which[i]), pool[(int(sizes[i]), int(which[i]))], want_status=False))
@@ -421,17 +423,30 @@ def bench_served(args, rank: int, world: int, metric: str):
         first = min(x["submit_ms"] for x in infos)
         last = max(x["done_ms"] for x in infos)
         lat = np.array([x["done_ms"] - x["submit_ms"] for x in infos])
+        svc = np.array([x["done_ms"] - x["admit_ms"] for x in infos])
+        queue = np.array([x["admit_ms"] - x["submit_ms"] for x in infos])
         pix = sum(x["npix"] for x in infos)
         its = sum(x["iterations"] for x in infos)
+        span = (arrivals[args.warmup + count - 1] - arrivals[args.warmup]) / rate_scale
         return {"pixels_per_s": pix / ((last - first) / 1000.0), "pixels": int(pix), "scans": len(infos),
+                "offered_pixels_per_s": pix / span if span > 0 else None,
+                "arrival_rate_scans_per_s": 20.0 * rate_scale,
                 "wall_ms": last - first, "latency_p50_ms": float(np.percentile(lat, 50)),
                 "latency_p99_ms": float(np.percentile(lat, 99)), "latency_max_ms": float(lat.max()),
+                "service_p50_ms": float(np.percentile(svc, 50)), "service_p99_ms": float(np.percentile(svc, 99)),
+                "queue_p50_ms": float(np.percentile(queue, 50)), "queue_p99_ms": float(np.percentile(queue, 99)),
                 "kernel_launches": st["kernel_launches"], "prepass_launches": st["prepass_launches"],
                 "arena_peak_gib": st["arena_peak_bytes"] / 2**30,
                 "iterations_per_pixel": its / pix}
 
     with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
         fp32 = run(pm.PREC_FP32, args.requests)
+    # the same scans offered below capacity (arrivals slowed to half the rate the
+    # first run served): latency without a backlog
+    light = None
+    if args.light_load:
+        scale = 0.5 * fp32["pixels_per_s"] / fp32["offered_pixels_per_s"]
+        light = run(pm.PREC_FP32, args.requests, rate_scale=min(1.0, scale))
     plain = run(pm.PREC_FP64, min(args.plain_requests, args.requests)) if args.plain_requests > 0 else None
     h2d = sum(pool[(int(sizes[i]), int(which[i]))].nbytes for i in range(args.warmup, n)) / args.requests
     d2h = sum(SIZES[int(sizes[i])] for i in range(args.warmup, n)) * (11 * 8 + 4 + 4) / args.requests
@@ -449,8 +464,11 @@ def bench_served(args, rank: int, world: int, metric: str):
                     "d2h_bytes_per_step": d2h,
                     "note": "host clock from each scan's submit (host buffers) to its results in host memory"},
             "latency_ms": {"p50": fp32["latency_p50_ms"], "p99": fp32["latency_p99_ms"],
-                           "max": fp32["latency_max_ms"]},
-            "served_fp32": fp32, "plain_fp64": plain, "clocks": clk.summary(),
+                           "max": fp32["latency_max_ms"], "service_p50": fp32["service_p50_ms"],
+                           "service_p99": fp32["service_p99_ms"],
+                           "note": "latency: submit -> results in host memory; service: admit -> results"},
+            "offered_pixels_per_s": fp32["offered_pixels_per_s"],
+            "served_fp32": fp32, "served_fp32_light_load": light, "plain_fp64": plain, "clocks": clk.summary(),
             "gpu_launches": fp32["kernel_launches"] + fp32["prepass_launches"]}), flush=True)
 
 
@@ -531,6 +549,8 @@ def main():
     ap.add_argument("--plain-requests", type=int, default=12,
                     help="served stream: scans of the same schedule timed on the plain FP64 server")
     ap.add_argument("--budget-gb", type=float, default=24.0, help="served stream: device arena of the server")
+    ap.add_argument("--light-load", type=int, default=1,
+                    help="served stream: also replay the scans at half the served rate (1) or not (0)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch tuning")
     ap.add_argument("--tuning", default=None, help="variant,warps_per_block: this launch tuning, no autotuning")
     ap.add_argument("--ingest", action="store_true",

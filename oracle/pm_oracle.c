@@ -846,7 +846,7 @@ void pmo_classical_only(const pmo_ctx *c, const float *spectro, double *m) { cla
 /* ------------------------------------------------------------------ */
 static int lm(pmo_ctx *c, const float *obs, double *model, float *chisqrf, const real *slight, double toplim,
               int miter, const real *w, const int *fix, real sigma, real ilambda, int *iter, real ah,
-              int logclambda, int *accepted) {
+              int logclambda, int *accepted, int *why) {
   const int n = c->nl, K = c->K;
   const real better = 5.0, worse = 10.0;
   real factor = 1.0, flambda, chi, ochi, chi0;
@@ -854,6 +854,7 @@ static int lm(pmo_ctx *c, const float *obs, double *model, float *chisqrf, const
   double covar[11 * 11], delta[11], trial[11];
   int i, ghosts = 0, nfree, stop = 0;
   *accepted = 0;
+  *why = 2; /* the iteration cap, unless a stopping test ends the loop */
   for (i = 0; i < 4 * n; i++) {
     if (obs[i] <= -1) { c->vsigma[i] = (real)PMO_GHOST_SIGMA; ghosts++; }
     else c->vsigma[i] = sigma;
@@ -878,7 +879,10 @@ static int lm(pmo_ctx *c, const float *obs, double *model, float *chisqrf, const
     clamp_model(trial);
     if (synthesis(c, trial, ah, slight) != 0) return -3;
     chi = chisq(c, obs, w, c->vsigma, (real)nfree);
-    if ((RFABS((ochi - chi) * 100 / chi) < toplim) || (chi < 0.0001)) stop = 1;
+    if ((RFABS((ochi - chi) * 100 / chi) < toplim) || (chi < 0.0001)) {
+      stop = 1;
+      *why = 0;
+    }
     if (chi - ochi < 0.) {
       flambda = flambda / (better * factor);
       for (i = 0; i < 11; i++) model[i] = trial[i];
@@ -892,7 +896,10 @@ static int lm(pmo_ctx *c, const float *obs, double *model, float *chisqrf, const
       for (i = 0; i < K * K; i++) covar[i] = alpha[i];
       flambda = flambda * worse * factor;
     }
-    if ((flambda > 1e+7) || (flambda < 1e-25)) stop = 1;
+    if ((flambda > 1e+7) || (flambda < 1e-25)) {
+      if (!stop) *why = 1;
+      stop = 1;
+    }
     (*iter)++;
     if (logclambda) factor = (real)(log10f((float)chi) / log10f((float)chi0));
   } while (*iter < miter && !stop);
@@ -928,7 +935,7 @@ int pmo_invert_pixel(pmo_ctx *c, const float *spectro, const double *guess, cons
                      float *chisq_out, int *iters, double *spectra_out, pmo_stats *stats) {
   double m[11];
   real ww[4];
-  int i, it = -1, acc = 0, rc;
+  int i, it = -1, acc = 0, why = 2, rc;
   float chi = 0.0f;
   real *sl = stage_slight(c, slight);
   for (i = 0; i < 4; i++) ww[i] = (real)w[i];
@@ -942,13 +949,13 @@ int pmo_invert_pixel(pmo_ctx *c, const float *spectro, const double *guess, cons
     if (isnan(m[I_AZ])) m[I_AZ] = 1;
   }
   rc = lm(c, spectro, m, &chi, sl, toplim, miter, ww, fix, (real)noise, (real)ilambda, &it, (real)mu, logclambda,
-          &acc);
+          &acc, &why);
   for (i = 0; i < 11; i++) model_out[i] = m[i];
   if (chisq_out) *chisq_out = chi;
   if (iters) *iters = it;
   if (spectra_out)
     for (i = 0; i < 4 * c->nl; i++) spectra_out[i] = c->spectra[i];
-  if (stats) { stats->iterations = it; stats->accepted = acc; stats->status = rc == 1 ? 0 : rc; }
+  if (stats) { stats->iterations = it; stats->accepted = acc; stats->status = rc == 1 ? why : rc; }
   return rc;
 }
 
@@ -956,7 +963,7 @@ int pmo_invert_batch(pmo_ctx *c, int npix, const float *spectro, const double *g
                      int slight_per_pixel, int use_classical, int miter, const double *w, double noise,
                      double ilambda, int logclambda, double toplim, double mu, const int *fix,
                      double *models_out, float *chisq_out, int *iters_out, float *spectra_out,
-                     int *accepted_out) {
+                     int *accepted_out, int *status_out) {
   const size_t n4 = (size_t)4 * c->nl;
   double *sp = spectra_out ? (double *)malloc(sizeof(double) * n4) : NULL;
   int p;
@@ -967,6 +974,7 @@ int pmo_invert_batch(pmo_ctx *c, int npix, const float *spectro, const double *g
     pmo_invert_pixel(c, spectro + (size_t)p * n4, guess, slp, use_classical, miter, w, noise, ilambda, logclambda,
                      toplim, mu, fix, models_out + (size_t)p * 11, chisq_out + p, iters_out + p, sp, &st);
     if (accepted_out) accepted_out[p] = st.accepted;
+    if (status_out) status_out[p] = st.status;
     if (sp)
       for (i = 0; i < n4; i++) spectra_out[(size_t)p * n4 + i] = (float)sp[i];
   }

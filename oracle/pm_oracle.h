@@ -28,7 +28,9 @@ typedef struct pmo_ctx pmo_ctx;
 typedef struct {
   int iterations;   /* same value as lm_mils' *iter */
   int accepted;     /* LM steps that lowered chi^2 (each one re-ran me_der) */
-  int status;       /* 0 ok, -1 nfree == 0 (lm_mils returns -1) */
+  int status;       /* how lm_mils' loop ended: 0 the toplim test (or chi^2 < 1e-4),
+                       1 the lambda bound, 2 the iteration cap; -1 nfree == 0
+                       (lm_mils returns -1) -- the codes of pmilos.h's PM_PIX_* */
 } pmo_stats;
 
 int pmo_sizeof_real(void);
@@ -65,7 +67,7 @@ int pmo_invert_batch(pmo_ctx *c, int npix, const float *spectro, const double *g
                      int slight_per_pixel, int use_classical, int miter, const double *w, double noise,
                      double ilambda, int logclambda, double toplim, double mu, const int *fix,
                      double *models_out, float *chisq_out, int *iters_out, float *spectra_out,
-                     int *accepted_out);
+                     int *accepted_out, int *status_out);
 
 /* Unit-level pieces. */
 int pmo_fvoigt(double damp, const double *v, int n, double *h, double *f);

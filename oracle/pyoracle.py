@@ -114,10 +114,13 @@ class _Lib:
         chi = np.zeros(npix, dtype=np.float32)
         its = np.zeros(npix, dtype=np.int32)
         acc = np.zeros(npix, dtype=np.int32)
+        st = np.full(npix, -9, dtype=np.int32)
         sp = np.zeros((npix, 4 * nl), dtype=np.float32) if want_spectra else None
         self._batch(npix, obs, g, sl, int(slight_per_pixel), int(classical), miter, w, noise, ilambda,
-                    logclambda, toplim, mu, fx, models, chi, its, sp, acc)
+                    logclambda, toplim, mu, fx, models, chi, its, sp, acc, st)
         out = {"models": models, "chisq": chi, "iters": its, "accepted": acc}
+        if (st != -9).all():  # the restatement reports how each pixel's loop ended (PM_PIX_* codes)
+            out["status"] = st
         if sp is not None:
             out["spectra"] = sp.reshape(npix, 4, nl)
         return out
@@ -137,7 +140,7 @@ class Restatement(_Lib):
         L.pmo_classical_only.argtypes = [ctypes.c_void_p, _F, _D]
         L.pmo_invert_batch.argtypes = [ctypes.c_void_p, ctypes.c_int, _F, _D, _D, ctypes.c_int, ctypes.c_int,
                                        ctypes.c_int, _D, ctypes.c_double, ctypes.c_double, ctypes.c_int,
-                                       ctypes.c_double, ctypes.c_double, _I, _D, _F, _I, _F, _I]
+                                       ctypes.c_double, ctypes.c_double, _I, _D, _F, _I, _F, _I, _I]
         L.pmo_fvoigt.argtypes = [ctypes.c_double, _D, ctypes.c_int, _D, _D]
         L.pmo_conv.argtypes = [ctypes.c_void_p, _D, ctypes.c_int, ctypes.c_double]
         L.pmo_svd_solve.argtypes = [ctypes.c_int, _D, _D, _D]
@@ -164,9 +167,9 @@ class Restatement(_Lib):
         (self.L.pmo_classical if initial_use else self.L.pmo_classical_only)(self.ctx, _f(obs), _d(m))
 
     def _batch(self, npix, obs, g, sl, slpp, cl, miter, w, noise, ilam, logc, toplim, mu, fx, models, chi, its,
-               sp, acc):
+               sp, acc, st):
         self.L.pmo_invert_batch(self.ctx, npix, _f(obs), _d(g), _d(sl), slpp, cl, miter, _d(w), noise, ilam, logc,
-                                toplim, mu, _i(fx), _d(models), _f(chi), _i(its), _f(sp), _i(acc))
+                                toplim, mu, _i(fx), _d(models), _f(chi), _i(its), _f(sp), _i(acc), _i(st))
 
     def fvoigt(self, damp, v):
         v = np.ascontiguousarray(v, dtype=np.float64)
@@ -233,8 +236,8 @@ class Reference(_Lib):
         (self.L.pmref_classical if initial_use else self.L.pmref_classical_only)(_f(obs), _d(m))
 
     def _batch(self, npix, obs, g, sl, slpp, cl, miter, w, noise, ilam, logc, toplim, mu, fx, models, chi, its,
-               sp, acc):
-        acc[:] = -1  # the reference does not count accepted steps
+               sp, acc, st):
+        acc[:] = -1  # the reference does not count accepted steps nor report how its loop ended
         self.L.pmref_invert_batch(npix, _f(obs), _d(g), _d(sl), slpp, cl, miter, _d(w), noise, ilam, logc, toplim,
                                   mu, _i(fx), _d(models), _f(chi), _i(its), _f(sp))
 

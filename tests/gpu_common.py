@@ -48,3 +48,25 @@ def within_tolerance(a, b, params=(0, 1, 2, 3, 4, 5, 6, 7, 8, 10)):
         else:
             ok &= np.abs(a[:, p] - b[:, p]) <= REL_TOL[p] * np.maximum(np.abs(b[:, p]), 1e-12)
     return ok
+
+
+# lm_mils' loop ended by one of its own tests (toplim or the damping bound),
+# not at the iteration cap: "where both codes converge"
+STOPPED = (pm.PIX_CONVERGED, pm.PIX_LAMBDA)
+
+
+def both_converged(gpu_status, oracle_status):
+    """Boolean [npix] mask of the pixels whose LM loop converged in both codes."""
+    return np.isin(gpu_status, STOPPED) & np.isin(oracle_status, STOPPED)
+
+
+def param_error(a, b, p):
+    """|a - b| of parameter p per pixel: absolute for the parameters with an
+    absolute tolerance (B, v_los, the angles, v_mac; the azimuth modulo 180 deg),
+    relative to |b| for the others."""
+    d = np.abs(a[:, p] - b[:, p])
+    if p == 6:
+        d = np.minimum(d, 180.0 - d)
+    if p in ABS_TOL:
+        return d
+    return d / np.maximum(np.abs(b[:, p]), 1e-12)
