@@ -1443,6 +1443,204 @@ __device__ __forceinline__ void invert_pixel(const PmParams& P, const BlockSmem<
   __syncwarp();
 }
 
+// ---------------------------------------------------------------------------
+// lm_mils in phases, for kernels whose warps advance in lock-step: the state of
+// one pixel's LM loop lives in registers (PixelLM) between three phases that a
+// block runs together, separated by block barriers -- the damped solve, the
+// synthesis with chi^2 and the acceptance test, the response functions with the
+// normal equations (accepted steps) -- so that at any time every warp of the
+// block executes the same phase's code.  Per pixel the arithmetic and its order
+// are those of invert_pixel.
+// ---------------------------------------------------------------------------
+template <typename R>
+struct PixelLM {
+  float O[4];
+  R isig[4];
+  R S[4], Su[4];
+  const float* sl_pix;
+  double dlp;
+  double ochi, chi0, chi, flambda, factor;
+  int nfree, status, iter, accepted, fallbacks;
+  bool stop, first, accept, finished;
+};
+
+// Before the loop (invert_pixel up to its first pass): the pixel's profiles,
+// ghosts, starting model; finished at once when nfree == 0.
+template <typename R, bool PIXGRID>
+__device__ __forceinline__ void lm_begin(const PmParams& P, WarpSmem<R>& sm, int lane, PixelLM<R>& L) {
+  const bool valid = lane < P.nl;
+  double* m = sm.model;
+  const PmJob* jp = sm.job;
+  const size_t p = sm.pix;
+  const size_t base = p * 4 * P.nl;
+  L.sl_pix = nullptr;
+  if (P.slight_mode == PM_SLIGHT_PER_PIXEL) {
+    const float* sl = ld_ptr(&jp->slight);
+    if (sl) L.sl_pix = sl + base;
+  }
+  const float* obs = ld_ptr(&jp->spectro) + base;
+  const double* model_in = ld_ptr(&jp->model_in);
+  L.dlp = 0.0;
+  if constexpr (PIXGRID) L.dlp = valid ? __ldcg(ld_ptr(&jp->lambda) + p * P.nl + lane) - P.lambda0 : 0.0;
+  const double dl = PIXGRID ? L.dlp : P.dl[valid ? lane : 0];
+  int ghosts = 0;
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    L.O[s] = valid ? __ldcg(obs + s * P.nl + lane) : 0.0f;
+    const bool g = valid && L.O[s] <= -1.0f;
+    ghosts += __popc(__ballot_sync(kFull, g));
+    L.isig[s] = R(1.0 / (g ? kGhostSigma : P.noise));
+  }
+  if (model_in) {
+    if (lane < 11) m[lane] = __ldcg(model_in + p * 11 + lane);
+  } else {
+    double g[11];
+#pragma unroll
+    for (int i = 0; i < 11; ++i) g[i] = P.guess[i];
+    if (P.classical) classical(P, L.O, lane, valid, dl, g);
+    double mine = g[0];
+#pragma unroll
+    for (int i = 1; i < 11; ++i)
+      if (lane == i) mine = g[i];
+    if (lane < 11) m[lane] = mine;
+  }
+  __syncwarp();
+  L.nfree = P.nfree_base - ghosts;
+  L.status = PM_PIX_MAXITER;
+  L.iter = 0;
+  L.accepted = 0;
+  L.fallbacks = 0;
+  L.ochi = 0;
+  L.chi0 = 0;
+  L.chi = 0;
+  L.flambda = P.ilambda;
+  L.factor = 1.0;
+  L.stop = false;
+  L.first = true;
+  L.accept = false;
+  L.finished = false;
+  if (L.nfree == 0) {
+    L.status = PM_PIX_NFREE;
+    L.iter = -1;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) L.S[s] = 0;
+    L.finished = true;
+  } else {
+    if (lane < 11) sm.trial[lane] = m[lane];
+    __syncwarp();
+  }
+}
+
+// Phase 1: the damped solve and the trial model (every pass but the first).
+template <typename R, int KT>
+__device__ __forceinline__ void lm_solve(const PmParams& P, WarpSmem<R>& sm, int lane, PixelLM<R>& L) {
+  if (L.first) return;
+  double dlt[KT];
+  bool ok = true;
+  double* scratch = reinterpret_cast<double*>(sm.tr);
+  if (P.solver == PM_SOLVE_CHOLESKY) ok = solve_cholesky<KT>(sm.sv, scratch, lane, L.flambda, dlt);
+  if (P.solver != PM_SOLVE_CHOLESKY || !ok) {
+    if (P.solver == PM_SOLVE_CHOLESKY) ++L.fallbacks;
+    solve_eigen<KT>(sm.sv, scratch, lane, L.flambda);
+#pragma unroll
+    for (int i = 0; i < KT; ++i) dlt[i] = sm.sv.delta[i];
+    __syncwarp();
+  }
+  double t[11];
+#pragma unroll
+  for (int i = 0; i < 11; ++i) t[i] = sm.trial[i];
+  apply_delta<KT>(P, sm.model, dlt, t);
+  check_model(t);
+  __syncwarp();
+#pragma unroll
+  for (int i = 0; i < 11; ++i)
+    if (lane == i) sm.trial[i] = t[i];
+  __syncwarp();
+}
+
+// Phase 2: synthesis of the trial model, chi^2, the stopping and acceptance tests.
+template <typename R, bool MAC, bool PIXGRID, bool ZM>
+__device__ __forceinline__ void lm_synth(const PmParams& P, WarpSmem<R>& sm, int lane, PixelLM<R>& L) {
+  const bool valid = lane < P.nl;
+  const double dl = PIXGRID ? L.dlp : P.dl[valid ? lane : 0];
+  synthesize<R, MAC, ZM>(P, sm, sm.trial, L.sl_pix, lane, valid, dl, L.S, L.Su);
+  L.chi = chisq<R>(P, L.S, L.O, L.isig, valid, double(L.nfree));
+  L.accept = true;
+  if (!L.first) {
+    if ((fabs((L.ochi - L.chi) * 100 / L.chi) < P.toplim) || (L.chi < 0.0001)) {
+      L.stop = true;
+      L.status = PM_PIX_CONVERGED;
+    }
+    L.accept = L.chi - L.ochi < 0.;
+  }
+}
+
+// Phase 3: on acceptance the response functions and normal equations at the
+// new model; the damping update and the loop's end test.
+template <typename R, int KT, bool MAC, bool PIXGRID, bool ZM>
+__device__ __forceinline__ void lm_update(const PmParams& P, const BlockSmem<R>& bs, WarpSmem<R>& sm, int lane,
+                                          PixelLM<R>& L) {
+  const bool valid = lane < P.nl;
+  const double dl = PIXGRID ? L.dlp : P.dl[valid ? lane : 0];
+  if (L.accept) {
+    if (!L.first) L.flambda = L.flambda / (5.0 * L.factor);
+    if (lane < 11) sm.model[lane] = sm.trial[lane];
+    __syncwarp();
+    R Sff[4];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) Sff[s] = L.first ? L.Su[s] : L.S[s];
+    rf_and_normal_eq<R, KT, MAC, ZM>(P, bs, sm, lane, valid, dl, L.S, Sff, L.O, L.isig, L.sl_pix);
+    L.ochi = L.chi;
+    if (L.first) L.chi0 = L.chi;
+    else ++L.accepted;
+  } else {
+    L.flambda = L.flambda * 10.0 * L.factor;
+  }
+  if (!L.first) {
+    if ((L.flambda > 1e+7) || (L.flambda < 1e-25)) {
+      if (!L.stop) L.status = PM_PIX_LAMBDA;
+      L.stop = true;
+    }
+    ++L.iter;
+    if (P.logclambda) L.factor = double(log10f(float(L.chi)) / log10f(float(L.chi0)));
+    if (!(L.iter < P.miter && !L.stop)) L.finished = true;
+  }
+  L.first = false;
+}
+
+// After the loop: the finite check and the pixel's results (invert_pixel's outputs).
+template <typename R>
+__device__ __forceinline__ void lm_end(const PmParams& P, WarpSmem<R>& sm, int lane, PixelLM<R>& L,
+                                       unsigned long long* ctr) {
+  const bool valid = lane < P.nl;
+  double* m = sm.model;
+  if (L.nfree != 0) {
+    bool finite = isfinite(L.ochi);
+#pragma unroll
+    for (int i = 0; i < 11; ++i) finite = finite && isfinite(m[i]);
+    if (!finite) L.status = PM_PIX_NONFINITE;
+  }
+  const PmJob* jp = *reinterpret_cast<const PmJob* const volatile*>(&sm.job);
+  const size_t p = *reinterpret_cast<const volatile unsigned long long*>(&sm.pix);
+  const size_t base = p * 4 * P.nl;
+  if (lane < 11) ld_ptr(&jp->models)[p * 11 + lane] = m[lane];
+  if (lane == 0) {
+    ld_ptr(&jp->chisq)[p] = float(L.ochi);
+    ld_ptr(&jp->iters)[p] = L.iter;
+    int* st = ld_ptr(&jp->status);
+    if (st) st[p] = L.status;
+    atomicAdd(&ctr[PMC_ITERS], (unsigned long long)(L.iter > 0 ? L.iter : 0));
+    atomicAdd(&ctr[PMC_ACCEPTED], (unsigned long long)L.accepted);
+    if (L.fallbacks) atomicAdd(&ctr[PMC_FALLBACK], (unsigned long long)L.fallbacks);
+  }
+  float* spectra = ld_ptr(&jp->spectra);
+  if (spectra && valid) {
+#pragma unroll
+    for (int s = 0; s < 4; ++s) spectra[base + s * P.nl + lane] = float(L.S[s]);
+  }
+  __syncwarp();
+}
+
 }  // namespace
 
 // Text of the last launch error (defined in pm_kernels.cu).

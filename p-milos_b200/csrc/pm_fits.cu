@@ -75,11 +75,13 @@ bool card_string(const char* card, char* out, size_t cap) {
 // Three forms, all reading and writing coalesced, HBM-bound:
 //  * identity (the reference's default order: wavelength, Stokes, rows,
 //    columns): a flat byte swap, 16 bytes per thread and step;
-//  * wavelength contiguous in the input: one warp per output row (pixel, Stokes);
-//  * otherwise 32 x 32 tiles of (the input's contiguous axis, wavelength)
-//    through shared memory; every index inside a tile is a linear function of
-//    the tile's corner, and consecutive tiles of a block differ by constant
-//    offsets, so there is no division per element or per tile.
+//  * wavelength contiguous in the input: one warp per pixel, whose four Stokes
+//    rows are four contiguous runs of the input and one contiguous run of the
+//    output (16-byte accesses when nl is a multiple of 4); the pixel's input
+//    offset advances by additions from one pixel to the next;
+//  * otherwise 32 x 32 tiles of (the input's contiguous axis, wavelength), each
+//    transposed by one warp through its own shared-memory tile: 32 loads in
+//    flight per lane, then 32 stores, with no block barrier.
 struct Reorder {
   long long n[4];    // axis sizes
   long long st[4];   // element strides of the axes in the input
@@ -90,60 +92,98 @@ struct Reorder {
 
 __device__ __forceinline__ unsigned int swap32(unsigned int u) { return __byte_perm(u, 0, 0x0123); }
 __device__ __forceinline__ float swap_be(unsigned int u) { return __uint_as_float(swap32(u)); }
+__device__ __forceinline__ uint4 swap_be4(uint4 v) {
+  v.x = swap32(v.x);
+  v.y = swap32(v.y);
+  v.z = swap32(v.z);
+  v.w = swap32(v.w);
+  return v;
+}
 
 __global__ void __launch_bounds__(256) reorder_identity(const uint4* __restrict__ in, uint4* __restrict__ out,
                                                        long long n4) {
   const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride) {
-    uint4 v = __ldg(in + i);
-    v.x = swap32(v.x);
-    v.y = swap32(v.y);
-    v.z = swap32(v.z);
-    v.w = swap32(v.w);
-    out[i] = v;
-  }
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride)
+    out[i] = swap_be4(__ldg(in + i));
 }
 
+// Wavelength contiguous in the input.  Each warp takes a run of `per` pixels
+// (pixel = col * rows + row); within the run the pixel's input offset advances
+// by st_row, and by st_col - (rows - 1) * st_row when the row wraps.  VEC: nl is
+// a multiple of 4 and both arrays start on 16-byte boundaries.
+template <bool VEC>
 __global__ void __launch_bounds__(256) reorder_rows(const Reorder R, const unsigned int* __restrict__ in,
-                                                   float* __restrict__ out) {
+                                                   float* __restrict__ out, long long per) {
   const int lane = threadIdx.x & 31;
-  const long long nrows_out = R.total / R.nl;
+  const long long npix = R.total / (4 * R.nl);
   const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
-  for (long long r = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < nrows_out; r += nwarps) {
-    const long long s = r & 3, pixel = r >> 2;
-    const long long row = pixel % R.rows, col = pixel / R.rows;
-    const long long ib = s * R.st[R.ax_s] + row * R.st[R.ax_row] + col * R.st[R.ax_col];
-    for (long long l = lane; l < R.nl; l += 32) out[r * R.nl + l] = swap_be(__ldg(in + ib + l));
+  const long long st_s = R.st[R.ax_s], st_row = R.st[R.ax_row], st_col = R.st[R.ax_col];
+  const long long nl = R.nl;
+  for (long long p0 = ((long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * per; p0 < npix;
+       p0 += nwarps * per) {
+    const long long p1 = p0 + per < npix ? p0 + per : npix;
+    long long row = p0 % R.rows;
+    long long ib = row * st_row + (p0 / R.rows) * st_col;
+    for (long long p = p0; p < p1; ++p) {
+      float* o = out + p * 4 * nl;
+      if constexpr (VEC) {
+        const long long n4 = nl >> 2;
+        for (long long q = lane; q < n4; q += 32) {
+          uint4 v[4];
+#pragma unroll
+          for (int s = 0; s < 4; ++s) v[s] = __ldg(reinterpret_cast<const uint4*>(in + ib + s * st_s) + q);
+#pragma unroll
+          for (int s = 0; s < 4; ++s) reinterpret_cast<uint4*>(o + s * nl)[q] = swap_be4(v[s]);
+        }
+      } else {
+        for (long long l = lane; l < nl; l += 32) {
+          unsigned int v[4];
+#pragma unroll
+          for (int s = 0; s < 4; ++s) v[s] = __ldg(in + ib + s * st_s + l);
+#pragma unroll
+          for (int s = 0; s < 4; ++s) o[s * nl + l] = swap_be(v[s]);
+        }
+      }
+      if (++row == R.rows) {
+        row = 0;
+        ib += st_col - (R.rows - 1) * st_row;
+      } else {
+        ib += st_row;
+      }
+    }
   }
 }
 
-// Work item = (wavelength tile, g, h); a block walks the item's tiles along f in
-// order, so the only per-tile index arithmetic is two additions.
+// Work item = (f tile, wavelength tile, g, h), items along f consecutive; one
+// warp per item: lane = f while loading (the input's contiguous axis), lane =
+// wavelength while storing (the output's contiguous axis).
 __global__ void __launch_bounds__(256) reorder_tiled(const Reorder R, int f, int g, int h,
                                                     const unsigned int* __restrict__ in, float* __restrict__ out) {
-  __shared__ float tile[32][33];
-  const long long tl = (R.nl + 31) / 32;
-  const long long items = tl * R.n[g] * R.n[h];
-  const int x = threadIdx.x & 31;
-  const long long st_l = R.st[R.ax_l], ost_f = R.ost[f], nf = R.n[f];
-  for (long long it = blockIdx.x; it < items; it += gridDim.x) {
-    const long long lt = it % tl, rest = it / tl;
-    const long long cg = rest % R.n[g], ch = rest / R.n[g];
-    const long long l0 = lt * 32;
+  __shared__ float tile[8][32][33];
+  const int x = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const long long tf = (R.n[f] + 31) / 32, tl = (R.nl + 31) / 32;
+  const long long items = tf * tl * R.n[g] * R.n[h];
+  const long long nwarps = (long long)gridDim.x * 8;
+  const long long st_l = R.st[R.ax_l], ost_f = R.ost[f];
+  for (long long it = (long long)blockIdx.x * 8 + w; it < items; it += nwarps) {
+    const long long ft = it % tf, r1 = it / tf;
+    const long long lt = r1 % tl, r2 = r1 / tl;
+    const long long cg = r2 % R.n[g], ch = r2 / R.n[g];
+    const long long f0 = ft * 32, l0 = lt * 32;
+    const int fx = int(R.n[f] - f0 < 32 ? R.n[f] - f0 : 32);
     const int lx = int(R.nl - l0 < 32 ? R.nl - l0 : 32);
-    long long ib = cg * R.st[g] + ch * R.st[h] + l0 * st_l;
-    long long ob = cg * R.ost[g] + ch * R.ost[h] + l0;
-    for (long long f0 = 0; f0 < nf; f0 += 32, ib += 32, ob += 32 * ost_f) {
-      const int fx = int(nf - f0 < 32 ? nf - f0 : 32);
-      // load: lanes along f, the input's contiguous axis
-      for (int k = threadIdx.x >> 5; k < lx; k += blockDim.x >> 5)
-        if (x < fx) tile[k][x] = swap_be(__ldg(in + ib + x + k * st_l));
-      __syncthreads();
-      // store: lanes along wavelength, the output's contiguous axis
-      for (int k = threadIdx.x >> 5; k < fx; k += blockDim.x >> 5)
-        if (x < lx) out[ob + k * ost_f + x] = tile[x][k];
-      __syncthreads();
-    }
+    const long long ib = cg * R.st[g] + ch * R.st[h] + l0 * st_l + f0;
+    const long long ob = cg * R.ost[g] + ch * R.ost[h] + l0 + f0 * ost_f;
+    float v[32];
+#pragma unroll
+    for (int k = 0; k < 32; ++k) v[k] = (k < lx && x < fx) ? swap_be(__ldg(in + ib + x + k * st_l)) : 0.0f;
+#pragma unroll
+    for (int k = 0; k < 32; ++k) tile[w][k][x] = v[k];
+    __syncwarp();
+#pragma unroll 8
+    for (int k = 0; k < 32; ++k)
+      if (k < fx && x < lx) out[ob + k * ost_f + x] = tile[w][x][k];
+    __syncwarp();
   }
 }
 
@@ -269,8 +309,15 @@ extern "C" int pm_fits_reorder(const pm_fits_cube* info, const void* data_dev, f
     reorder_identity<<<unsigned(std::max(1LL, blocks)), 256, 0, s>>>(reinterpret_cast<const uint4*>(data_dev),
                                                                    reinterpret_cast<uint4*>(cube_dev), n4);
   } else if (R.ax_l == 0) {
-    const long long blocks = std::min(cap, (R.total / R.nl + 7) / 8);
-    reorder_rows<<<unsigned(std::max(1LL, blocks)), 256, 0, s>>>(R, in, cube_dev);
+    // pixels per warp: every warp of a full grid gets a few runs
+    const long long npix = R.total / (4 * R.nl);
+    const long long warps = cap * 8;
+    const long long per = std::max(1LL, std::min(64LL, npix / (4 * warps)));
+    const long long blocks = std::min(cap, (npix + 8 * per - 1) / (8 * per));
+    if (R.nl % 4 == 0 && aligned)
+      reorder_rows<true><<<unsigned(std::max(1LL, blocks)), 256, 0, s>>>(R, in, cube_dev, per);
+    else
+      reorder_rows<false><<<unsigned(std::max(1LL, blocks)), 256, 0, s>>>(R, in, cube_dev, per);
   } else {
     // f: the input's contiguous axis (axis 0); g, h: the two other non-wavelength axes
     const int f = 0;
@@ -280,8 +327,9 @@ extern "C" int pm_fits_reorder(const pm_fits_cube* info, const void* data_dev, f
         if (g < 0) g = a;
         else h = a;
       }
-    const long long work = ((R.nl + 31) / 32) * R.n[g] * R.n[h];
-    reorder_tiled<<<unsigned(std::max(1LL, std::min(cap, work))), 256, 0, s>>>(R, f, g, h, in, cube_dev);
+    const long long work = ((R.n[f] + 31) / 32) * ((R.nl + 31) / 32) * R.n[g] * R.n[h];
+    const long long blocks = std::min(cap, (work + 7) / 8);
+    reorder_tiled<<<unsigned(std::max(1LL, blocks)), 256, 0, s>>>(R, f, g, h, in, cube_dev);
   }
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {

@@ -82,9 +82,7 @@ struct HostCtl {
   PmJob job;
   PmStreamQ qinit;                           // queue state before a fully published launch
   PmStreamQ qread;                           // queue state after the kernel (counters, err)
-  PmJob piece_job[PM_STAGING_MAX];           // pipelined host-buffer calls: one launch per piece
-  PmStreamQ piece_qinit[PM_STAGING_MAX];
-  PmStreamQ piece_qread[PM_STAGING_MAX];
+  unsigned long long piece_avail[PM_STAGING_MAX];  // tickets published once piece i of a streamed call is in
   unsigned long long wide_ctr[2][PMC_COUNT];  // counters of the two buffer sets of a wide-grid call
 };
 
@@ -503,6 +501,14 @@ int stream_resources(pm_ctx* c) {
 int run_streamed(pm_ctx* c, int64_t n, const float* spectro, const float* slight, int slight_mode,
                  pm_model* models_out, float* chisq_out, int* iters_out, float* best_fit_out, int* status_out,
                  float* kernel_ms, float* total_ms) {
+  // One persistent launch fed while it runs.  The cube goes to the device in
+  // `pieces` copies on the copy stream; after each copy the copy stream writes
+  // the running pixel count into the queue's avail word, which publishes that
+  // piece's tickets to the kernel already running on the kernel stream (a warp
+  // holding a ticket beyond avail waits, bounded, for its publication).  The
+  // kernel computes each pixel's classical estimates itself (a pre-pass launch
+  // could not find SM slots beside the persistent kernel).  The results come
+  // back in one copy after the kernel.
   int rc = stream_resources(c);
   if (rc != PM_OK) return rc;
   const int nl = c->P.nl;
@@ -523,11 +529,36 @@ int run_streamed(pm_ctx* c, int64_t n, const float* spectro, const float* slight
   per = std::max<int64_t>(32, (per + 31) / 32 * 32);
   const int np = int((n + per - 1) / per);
 
+  PmJob& job = hc->job;
+  std::memset(&job, 0, sizeof job);
+  job.npix = n;
+  job.spectro = static_cast<const float*>(c->spectro.p);
+  job.slight = slight_mode == PM_SLIGHT_PER_PIXEL ? static_cast<const float*>(c->slight.p) : nullptr;
+  job.models = static_cast<double*>(c->models.p);
+  job.chisq = static_cast<float*>(c->chisq.p);
+  job.iters = static_cast<int*>(c->iters.p);
+  job.status = status_out ? static_cast<int*>(c->status.p) : nullptr;
+  job.spectra = best_fit_out ? static_cast<float*>(c->spectra.p) : nullptr;
+  job.model_in = nullptr;  // classical estimates in the kernel
+  std::memset(&hc->qinit, 0, sizeof hc->qinit);  // nothing published, queue open
+
   // order after the caller's earlier work on its stream
   PM_CUDA(cudaEventRecord(c->ev_start, c->stream), "event");
   PM_CUDA(cudaStreamWaitEvent(c->s_copy, c->ev_start, 0), "wait");
   PM_CUDA(cudaStreamWaitEvent(c->s_kern, c->ev_start, 0), "wait");
-  PM_CUDA(cudaEventRecord(c->t0, c->s_copy), "event");
+  PM_CUDA(cudaEventRecord(c->t0, c->s_kern), "event");
+  PM_CUDA(cudaMemcpyAsync(c->jobs.p, &job, sizeof job, cudaMemcpyHostToDevice, c->s_kern), "job H2D");
+  PM_CUDA(cudaMemcpyAsync(q, &hc->qinit, sizeof(PmStreamQ), cudaMemcpyHostToDevice, c->s_kern), "queue H2D");
+  PM_CUDA(cudaEventRecord(c->ev_q, c->s_kern), "event");  // the queue is reset: publications may follow
+  PM_CUDA(cudaEventRecord(c->k0, c->s_kern), "event");
+  rc = pmk_invert_stream(*c->gs, sio, c->precision, c->tuning.variant, c->tuning.warps_per_block, false, c->s_kern,
+                         c->num_sms, nullptr);
+  if (rc != PM_OK) {
+    // the kernel did not start: nothing waits for the publications below
+    cudaStreamSynchronize(c->s_kern);
+    return fail(rc, "%s", pmk_last_cuda_error());
+  }
+  PM_CUDA(cudaEventRecord(c->k1, c->s_kern), "event");
   for (int i = 0; i < np; ++i) {
     const int64_t p0 = i * per, m = std::min(per, n - p0);
     PM_CUDA(cudaMemcpyAsync(static_cast<char*>(c->spectro.p) + prof * p0, spectro + p0 * 4 * nl, prof * m,
@@ -537,66 +568,38 @@ int run_streamed(pm_ctx* c, int64_t n, const float* spectro, const float* slight
       PM_CUDA(cudaMemcpyAsync(static_cast<char*>(c->slight.p) + prof * p0, slight + p0 * 4 * nl, prof * m,
                               cudaMemcpyHostToDevice, c->s_copy),
               "slight H2D");
-    PM_CUDA(cudaEventRecord(c->ev_piece[i], c->s_copy), "event");
+    if (i == 0) PM_CUDA(cudaStreamWaitEvent(c->s_copy, c->ev_q, 0), "wait");
+    hc->piece_avail[i] = (unsigned long long)(p0 + m);
+    PM_CUDA(cudaMemcpyAsync(&q->avail, &hc->piece_avail[i], sizeof(unsigned long long), cudaMemcpyHostToDevice,
+                            c->s_copy),
+            "publish");
   }
-  for (int i = 0; i < np; ++i) {
-    const int64_t p0 = i * per, m = std::min(per, n - p0);
-    PmJob& job = hc->piece_job[i];
-    std::memset(&job, 0, sizeof job);
-    job.npix = m;
-    job.spectro = static_cast<const float*>(c->spectro.p) + p0 * 4 * nl;
-    job.slight = slight_mode == PM_SLIGHT_PER_PIXEL ? static_cast<const float*>(c->slight.p) + p0 * 4 * nl : nullptr;
-    job.models = static_cast<double*>(c->models.p) + p0 * 11;
-    job.chisq = static_cast<float*>(c->chisq.p) + p0;
-    job.iters = static_cast<int*>(c->iters.p) + p0;
-    job.status = status_out ? static_cast<int*>(c->status.p) + p0 : nullptr;
-    job.spectra = best_fit_out ? static_cast<float*>(c->spectra.p) + p0 * 4 * nl : nullptr;
-    job.model_in = c->P.classical ? job.models : nullptr;  // written by the pre-pass below
-    std::memset(&hc->piece_qinit[i], 0, sizeof(PmStreamQ));
-    hc->piece_qinit[i].avail = (unsigned long long)m;
-    hc->piece_qinit[i].closed = 1;
-    PM_CUDA(cudaStreamWaitEvent(c->s_kern, c->ev_piece[i], 0), "wait");
-    PM_CUDA(cudaMemcpyAsync(c->jobs.p, &job, sizeof job, cudaMemcpyHostToDevice, c->s_kern), "job H2D");
-    PM_CUDA(cudaMemcpyAsync(q, &hc->piece_qinit[i], sizeof(PmStreamQ), cudaMemcpyHostToDevice, c->s_kern),
-            "queue H2D");
-    if (i == 0) PM_CUDA(cudaEventRecord(c->k0, c->s_kern), "event");
-    if (c->P.classical) {
-      rc = pmk_classical_prepass(c->P, job.spectro, job.models, m, c->s_kern, c->num_sms);
-      if (rc != PM_OK) return fail(rc, "%s", pmk_last_cuda_error());
-    }
-    rc = pmk_invert_stream(*c->gs, sio, c->precision, c->tuning.variant, c->tuning.warps_per_block, false, c->s_kern,
-                           c->num_sms, nullptr);
-    if (rc != PM_OK) return fail(rc, "%s", pmk_last_cuda_error());
-    if (i == np - 1) PM_CUDA(cudaEventRecord(c->k1, c->s_kern), "event");
-    PM_CUDA(cudaMemcpyAsync(models_out + p0, job.models, sizeof(pm_model) * m, cudaMemcpyDeviceToHost, c->s_kern),
-            "models D2H");
-    PM_CUDA(cudaMemcpyAsync(chisq_out + p0, job.chisq, sizeof(float) * m, cudaMemcpyDeviceToHost, c->s_kern),
-            "chisq D2H");
-    PM_CUDA(cudaMemcpyAsync(iters_out + p0, job.iters, sizeof(int) * m, cudaMemcpyDeviceToHost, c->s_kern),
-            "iters D2H");
-    if (best_fit_out)
-      PM_CUDA(cudaMemcpyAsync(best_fit_out + p0 * 4 * nl, job.spectra, prof * m, cudaMemcpyDeviceToHost, c->s_kern),
-              "best fit D2H");
-    if (status_out)
-      PM_CUDA(cudaMemcpyAsync(status_out + p0, job.status, sizeof(int) * m, cudaMemcpyDeviceToHost, c->s_kern),
-              "status D2H");
-    PM_CUDA(cudaMemcpyAsync(&hc->piece_qread[i], q, sizeof(PmStreamQ), cudaMemcpyDeviceToHost, c->s_kern),
-            "queue D2H");
-  }
+  // closed after the last publication: warps holding tickets beyond n exit
+  PM_CUDA(cudaMemcpyAsync(&q->closed, &hc->one, sizeof(unsigned long long), cudaMemcpyHostToDevice, c->s_copy),
+          "close");
+  PM_CUDA(cudaMemcpyAsync(models_out, job.models, sizeof(pm_model) * n, cudaMemcpyDeviceToHost, c->s_kern),
+          "models D2H");
+  PM_CUDA(cudaMemcpyAsync(chisq_out, job.chisq, sizeof(float) * n, cudaMemcpyDeviceToHost, c->s_kern), "chisq D2H");
+  PM_CUDA(cudaMemcpyAsync(iters_out, job.iters, sizeof(int) * n, cudaMemcpyDeviceToHost, c->s_kern), "iters D2H");
+  if (best_fit_out)
+    PM_CUDA(cudaMemcpyAsync(best_fit_out, job.spectra, prof * n, cudaMemcpyDeviceToHost, c->s_kern), "best fit D2H");
+  if (status_out)
+    PM_CUDA(cudaMemcpyAsync(status_out, job.status, sizeof(int) * n, cudaMemcpyDeviceToHost, c->s_kern),
+            "status D2H");
+  PM_CUDA(cudaMemcpyAsync(&hc->qread, q, sizeof(PmStreamQ), cudaMemcpyDeviceToHost, c->s_kern), "queue D2H");
   PM_CUDA(cudaEventRecord(c->t1, c->s_kern), "event");
   PM_CUDA(cudaEventRecord(c->ev_done, c->s_kern), "event");
   PM_CUDA(cudaStreamWaitEvent(c->stream, c->ev_done, 0), "wait");
-  PM_CUDA(cudaEventSynchronize(c->t1), "pipelined inversion");
-  for (int i = 0; i < np; ++i) {
-    const PmStreamQ& r = hc->piece_qread[i];
-    const int64_t m = std::min(per, n - int64_t(i) * per);
-    if (r.err || r.next < (unsigned long long)m)
-      return fail(PM_EIO, "pipelined inversion, piece %d: queue error %llu, %llu of %lld pixels handed out", i, r.err,
-                  r.next, (long long)m);
-    c->stats.iterations += int64_t(r.ctr[PMC_ITERS]);
-    c->stats.accepted += int64_t(r.ctr[PMC_ACCEPTED]);
-    c->stats.eigen_fallbacks += int64_t(r.ctr[PMC_FALLBACK]);
-  }
+  // the copy stream's last publication is done once the kernel has ended
+  PM_CUDA(cudaStreamWaitEvent(c->s_copy, c->ev_done, 0), "wait");
+  PM_CUDA(cudaEventSynchronize(c->t1), "streamed inversion");
+  const PmStreamQ& r = hc->qread;
+  if (r.err || r.next < (unsigned long long)n)
+    return fail(PM_EIO, "streamed inversion: queue error %llu, %llu of %lld pixels handed out", r.err, r.next,
+                (long long)n);
+  c->stats.iterations += int64_t(r.ctr[PMC_ITERS]);
+  c->stats.accepted += int64_t(r.ctr[PMC_ACCEPTED]);
+  c->stats.eigen_fallbacks += int64_t(r.ctr[PMC_FALLBACK]);
   cudaEventElapsedTime(kernel_ms, c->k0, c->k1);
   cudaEventElapsedTime(total_ms, c->t0, c->t1);
   c->stats.pixels += n;
@@ -734,7 +737,7 @@ int run_graph_small(pm_ctx* c, int64_t n, const float* spectro, const float* sli
   job.iters = static_cast<int*>(c->iters.p);
   job.status = want_status ? static_cast<int*>(c->status.p) : nullptr;
   job.spectra = want_spectra ? static_cast<float*>(c->spectra.p) : nullptr;
-  job.model_in = c->P.classical ? static_cast<const double*>(c->models.p) : nullptr;
+  job.model_in = nullptr;  // classical estimates in the kernel
   std::memset(&hc->qinit, 0, sizeof hc->qinit);
   hc->qinit.avail = (unsigned long long)n;
   hc->qinit.closed = 1;
@@ -766,10 +769,7 @@ int run_graph_small(pm_ctx* c, int64_t n, const float* spectro, const float* sli
     if (e == cudaSuccess) e = cudaMemcpyAsync(c->jobs.p, &hc->job, sizeof(PmJob), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(q, &hc->qinit, sizeof(PmStreamQ), cudaMemcpyHostToDevice, s);
     int krc = PM_OK;
-    if (e == cudaSuccess && c->P.classical)
-      krc = pmk_classical_prepass(c->P, static_cast<const float*>(c->spectro.p), static_cast<double*>(c->models.p), n,
-                                  s, c->num_sms);
-    if (e == cudaSuccess && krc == PM_OK) {
+    if (e == cudaSuccess) {
       PmStreamIO sio{};
       sio.q = q;
       sio.jobs = static_cast<const PmJob*>(c->jobs.p);
@@ -902,7 +902,7 @@ int run_invert(pm_ctx* c, PmIO io, float* kernel_ms) {
   job.iters = io.iters_out;
   job.status = io.status_out;
   job.spectra = io.spectra_out;
-  job.model_in = c->P.classical ? io.models_out : nullptr;  // written by the pre-pass below
+  job.model_in = nullptr;  // classical estimates in the kernel, as on every one-warp batch path
   job.lambda = io.lambda_pix;
   std::memset(&hc->qinit, 0, sizeof hc->qinit);
   hc->qinit.avail = (unsigned long long)io.npix;
@@ -919,10 +919,6 @@ int run_invert(pm_ctx* c, PmIO io, float* kernel_ms) {
   sio.first_job = 0;
   sio.wait_limit_ns = 20000000000LL;
   PM_CUDA(cudaEventRecord(c->k0, c->stream), "event");
-  if (c->P.classical) {
-    rc = pmk_classical_prepass(c->P, io.spectro, io.models_out, io.npix, c->stream, c->num_sms, io.lambda_pix);
-    if (rc != PM_OK) return fail(rc, "%s", pmk_last_cuda_error());
-  }
   rc = pmk_invert_stream(*c->gs, sio, c->precision, c->tuning.variant, c->tuning.warps_per_block, false, c->stream,
                          c->num_sms, nullptr, 0, io.lambda_pix != nullptr);
   if (rc != PM_OK) return fail(rc, "%s", pmk_last_cuda_error());
@@ -1189,11 +1185,12 @@ extern "C" int pm_get_tuning(const pm_ctx* c, pm_tuning* out) {
 
 extern "C" int pm_set_tuning(pm_ctx* c, const pm_tuning* in) {
   if (!c || !in) return fail(PM_EINVAL, "pm_set_tuning: NULL argument");
-  if (in->variant != 0 && in->variant != 1) return fail(PM_EINVAL, "pm_set_tuning: variant=%d", in->variant);
+  if (in->variant < 0 || in->variant > 2) return fail(PM_EINVAL, "pm_set_tuning: variant=%d", in->variant);
   if (in->staging_depth < 0 || in->staging_depth > PM_STAGING_MAX)
     return fail(PM_EINVAL, "pm_set_tuning: staging_depth=%d (0..%d)", in->staging_depth, PM_STAGING_MAX);
-  if (in->warps_per_block != 1 && in->warps_per_block != 2 && in->warps_per_block != 4)
-    return fail(PM_EINVAL, "pm_set_tuning: warps_per_block=%d (1, 2 or 4)", in->warps_per_block);
+  const int w = in->warps_per_block;
+  if (in->variant == 2 ? (w != 4 && w != 8 && w != 16) : (w != 1 && w != 2 && w != 4))
+    return fail(PM_EINVAL, "pm_set_tuning: warps_per_block=%d (1, 2 or 4; 4, 8 or 16 with variant 2)", w);
   if (in->graphs != 0 && in->graphs != 1) return fail(PM_EINVAL, "pm_set_tuning: graphs=%d (0 or 1)", in->graphs);
   c->tuning = *in;
   return PM_OK;

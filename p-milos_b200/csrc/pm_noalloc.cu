@@ -178,7 +178,7 @@ extern "C" int pm_invert_batch_noalloc(const pm_line* line, const pm_config* cfg
   job.iters = io.iters_out;
   job.status = io.status_out;
   job.spectra = io.spectra_out;
-  job.model_in = P.classical ? io.models_out : nullptr;  // written by the pre-pass below
+  job.model_in = nullptr;  // classical estimates in the kernel, as on every one-warp batch path
   PmStreamQ qinit{};
   qinit.avail = (unsigned long long)npix;
   qinit.closed = 1;
@@ -196,11 +196,8 @@ extern "C" int pm_invert_batch_noalloc(const pm_line* line, const pm_config* cfg
   sio.jobs_cap = 1;
   sio.first_job = 0;
   sio.wait_limit_ns = 20000000000LL;
-  if (P.classical) {
-    rc = pmk_classical_prepass(P, job.spectro, io.models_out, npix, st, sms);
-    if (rc != PM_OK) return fail_after_queue(st, pmh_fail(rc, pmk_last_cuda_error()));
-  }
-  rc = pmk_invert_stream(gs, sio, cfg->precision, 0, 4, false, st, sms, nullptr);
+  // the launch tuning a context starts with (128-register FP32 budget, 4 pixels per block)
+  rc = pmk_invert_stream(gs, sio, cfg->precision, 1, 4, false, st, sms, nullptr);
   if (rc != PM_OK) return fail_after_queue(st, pmh_fail(rc, pmk_last_cuda_error()));
   if ((e = cudaMemcpyAsync(models_out, io.models_out, sizeof(pm_model) * npix, cudaMemcpyDeviceToHost, st)) !=
       cudaSuccess)

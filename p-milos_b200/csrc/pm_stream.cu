@@ -49,6 +49,13 @@ int launch_stream_any(const PmGridSet& GS, const PmStreamIO& sio, cudaStream_t s
   }
   if constexpr (sizeof(R) == 4) {
     if (multi) return launch_invert_stream<float, KT, 4, true, MAC>(GS, sio, st, num_sms, smem_out, wpb, reserve);
+    if constexpr (!MAC && KT <= 10) {
+      if (variant == 2) {  // lock-step blocks of wpb warps
+        if (wpb == 16) return launch_invert_lockstep<float, KT, 16, MAC>(GS, sio, st, num_sms, smem_out, reserve);
+        if (wpb == 8) return launch_invert_lockstep<float, KT, 8, MAC>(GS, sio, st, num_sms, smem_out, reserve);
+        return launch_invert_lockstep<float, KT, 4, MAC>(GS, sio, st, num_sms, smem_out, reserve);
+      }
+    }
     return variant == 1 ? launch_invert_stream<float, KT, 4, false, MAC>(GS, sio, st, num_sms, smem_out, wpb, reserve)
                         : launch_invert_stream<float, KT, 3, false, MAC>(GS, sio, st, num_sms, smem_out, wpb, reserve);
   } else {
@@ -76,7 +83,10 @@ int launch_stream_k(const PmGridSet& GS, const PmStreamIO& sio, cudaStream_t st,
 int pmk_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, int precision, int variant, int warps_per_block,
                       bool multi, void* stream, int num_sms, size_t* smem_out, int reserve_blocks, bool pixgrid) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const int wpb = (warps_per_block == 1 || warps_per_block == 2) ? warps_per_block : 4;
+  const int wpb = (warps_per_block == 1 || warps_per_block == 2 ||
+                   (variant == 2 && (warps_per_block == 8 || warps_per_block == 16)))
+                      ? warps_per_block
+                      : 4;
   if (GS.ngrids < 1 || GS.ngrids > PMK_MAX_GRIDS || (!multi && GS.ngrids != 1)) {
     snprintf(pmk_g_err, sizeof pmk_g_err, "stream: %d grids", GS.ngrids);
     return PM_EINVAL;

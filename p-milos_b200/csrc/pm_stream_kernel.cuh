@@ -62,6 +62,27 @@ struct GridParams {
   PmParams g[NG];
 };
 
+// The warp's pixel is finished: count it on its job and, when it was the job's
+// last pixel, raise the job's host flag (the server's completion signal).
+template <typename R>
+__device__ __forceinline__ void job_pixel_done(WarpSmem<R>& sm, int lane) {
+  const PmJob* jp = *reinterpret_cast<const PmJob* const volatile*>(&sm.job);
+  unsigned long long* done = ld_ptr(&jp->done);
+  if (done) {
+    __threadfence();  // every lane: its part of this pixel's results before the count
+    __syncwarp();
+    if (lane == 0) {
+      int* flag = ld_ptr(&jp->host_flag);
+      const unsigned long long np = __ldcg(reinterpret_cast<const unsigned long long*>(&jp->npix));
+      if (atomicAdd(done, 1ull) + 1 == np && flag) {
+        __threadfence_system();
+        *reinterpret_cast<volatile int*>(flag) = 1;
+      }
+    }
+  }
+  __syncwarp();
+}
+
 template <typename R, int KT, int MINB, bool MULTI, bool MAC, bool PIXGRID, bool ZM = false>
 __global__ void __launch_bounds__(128, MINB) invert_stream_kernel(
     const __grid_constant__ GridParams<MULTI ? PMK_MAX_GRIDS : 1> GS, const PmStreamIO sio) {
@@ -119,24 +140,114 @@ __global__ void __launch_bounds__(128, MINB) invert_stream_kernel(
     }
     __syncwarp();
     invert_pixel<R, KT, MAC, PIXGRID, ZM>(P, bs[gi], sm, lane, sio.q->ctr);
-    jp = *reinterpret_cast<const PmJob* const volatile*>(&sm.job);
-    unsigned long long* done = ld_ptr(&jp->done);
-    if (done) {
-      __threadfence();  // every lane: its part of this pixel's results before the count
-      __syncwarp();
-      if (lane == 0) {
-        int* flag = ld_ptr(&jp->host_flag);
-        const unsigned long long np = __ldcg(reinterpret_cast<const unsigned long long*>(&jp->npix));
-        if (atomicAdd(done, 1ull) + 1 == np && flag) {
-          __threadfence_system();
-          *reinterpret_cast<volatile int*>(flag) = 1;
-        }
-      }
-    }
-    __syncwarp();
+    job_pixel_done(sm, lane);
   }
 }
 
+
+// Lock-step form of the streamed kernel (one grid): the W warps of a block
+// advance through the LM loop together, one phase at a time (lm_solve,
+// lm_synth, lm_update, with block barriers between them), so that at any time
+// the block executes one phase's code.  A warp whose pixel is finished takes
+// the next ticket before the next pass; warps without one (the queue is
+// drained) keep taking part in the barriers until every warp of the block is
+// done.  Per pixel the arithmetic is invert_pixel's.
+template <typename R, int KT, int W, bool MAC, bool PIXGRID, bool ZM = false>
+__global__ void __launch_bounds__(32 * W, 16 / W) invert_lockstep_kernel(const __grid_constant__ GridParams<1> GS,
+                                                                        const PmStreamIO sio) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  BlockSmem<R>* bs = reinterpret_cast<BlockSmem<R>*>(smem_raw);
+  WarpSmem<R>& sm = reinterpret_cast<WarpSmem<R>*>(smem_raw + sizeof(BlockSmem<R>))[warp];
+  const PmParams& P = GS.g[0];
+  load_taps<R>(P, bs[0]);
+  for (int e = lane; e < 4 * XSR; e += 32) (&sm.xs[0][0])[e] = R(0);
+  if (lane == 0) {
+    sm.job_k = sio.first_job;
+    sm.grid_cur = 0;
+    sm.xs_dirty = 0;
+  }
+  __syncthreads();
+  PixelLM<R> L;
+  bool have = false, drained = false;
+  while (true) {
+    while (!have && !drained) {
+      long long t = 0;
+      if (lane == 0) t = next_ticket(sio.q, sio.wait_limit_ns);
+      t = __shfl_sync(kFull, t, 0);
+      if (t < 0) {
+        drained = true;
+        break;
+      }
+      const PmJob* jp = nullptr;
+      unsigned long long t0 = 0;
+      long long k = sm.job_k;
+      for (int guard = 0; guard <= sio.jobs_cap; ++guard, ++k) {
+        const PmJob* c = sio.jobs + (k % sio.jobs_cap);
+        const unsigned long long c0 = __ldcg(&c->t0);
+        const unsigned long long cn = __ldcg(reinterpret_cast<const unsigned long long*>(&c->npix));
+        if ((unsigned long long)t >= c0 && (unsigned long long)t < c0 + cn) {
+          jp = c;
+          t0 = c0;
+          break;
+        }
+      }
+      if (!jp) {
+        if (lane == 0) atomicExch(&sio.q->err, (unsigned long long)PMQ_ERR_JOB);
+        drained = true;
+        break;
+      }
+      if (lane == 0) {
+        sm.job_k = k;
+        sm.job = jp;
+        sm.pix = (unsigned long long)t - t0;
+      }
+      __syncwarp();
+      lm_begin<R, PIXGRID>(P, sm, lane, L);
+      if (L.finished) {
+        lm_end<R>(P, sm, lane, L, sio.q->ctr);
+        job_pixel_done(sm, lane);
+      } else {
+        have = true;
+      }
+    }
+    if (!__syncthreads_or(have)) break;
+    if (have) lm_solve<R, KT>(P, sm, lane, L);
+    __syncthreads();
+    if (have) lm_synth<R, MAC, PIXGRID, ZM>(P, sm, lane, L);
+    __syncthreads();
+    if (have) {
+      lm_update<R, KT, MAC, PIXGRID, ZM>(P, bs[0], sm, lane, L);
+      if (L.finished) {
+        lm_end<R>(P, sm, lane, L, sio.q->ctr);
+        job_pixel_done(sm, lane);
+        have = false;
+      }
+    }
+  }
+}
+
+template <typename R, int KT, int W, bool MAC, bool PIXGRID = false, bool ZM = false>
+int launch_invert_lockstep(const PmGridSet& GS, const PmStreamIO& sio, cudaStream_t st, int num_sms,
+                           size_t* smem_out, int reserve) {
+  constexpr int threads = 32 * W;
+  const size_t smem = sizeof(BlockSmem<R>) + sizeof(WarpSmem<R>) * W;
+  if (smem_out) *smem_out = smem;
+  auto kern = invert_lockstep_kernel<R, KT, W, MAC, PIXGRID, ZM>;
+  GridParams<1> gp;
+  gp.ngrids = 1;
+  gp.g[0] = GS.g[0];
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return snprintf(pmk_g_err, sizeof pmk_g_err, "%s", cudaGetErrorString(e)), PM_EIO;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+  if (e != cudaSuccess || per_sm < 1) return snprintf(pmk_g_err, sizeof pmk_g_err, "occupancy: %s", cudaGetErrorString(e)), PM_EIO;
+  const int blocks = per_sm * num_sms - reserve > 1 ? per_sm * num_sms - reserve : 1;
+  kern<<<unsigned(blocks), threads, smem, st>>>(gp, sio);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return snprintf(pmk_g_err, sizeof pmk_g_err, "lock-step launch: %s", cudaGetErrorString(e)), PM_EIO;
+  return PM_OK;
+}
 
 template <typename R, int KT, int MINB, bool MULTI, bool MAC, bool PIXGRID = false, bool ZM = false>
 int launch_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, cudaStream_t st, int num_sms,

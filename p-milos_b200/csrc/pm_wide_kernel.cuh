@@ -721,19 +721,22 @@ int launch_invert_wide_inst(const PmParams& P, const PmIO& io, cudaStream_t st, 
     cudaEventCreate(&b);
     cudaEventRecord(a, st);
   }
-  if (P.classical) {
-    const int rc = launch_classical_wide<G>(P, io, st, num_sms);
-    if (rc != PM_OK) return rc;
+  int rc = PM_OK;
+  if (P.classical) rc = launch_classical_wide<G>(P, io, st, num_sms);
+  if (rc == PM_OK) {
+    kern<<<unsigned(blocks), threads, smem, st>>>(P, io);
+    e = cudaGetLastError();
   }
-  kern<<<unsigned(blocks), threads, smem, st>>>(P, io);
-  e = cudaGetLastError();
   if (kernel_ms) {
-    cudaEventRecord(b, st);
-    cudaEventSynchronize(b);
-    cudaEventElapsedTime(kernel_ms, a, b);
+    if (rc == PM_OK) {
+      cudaEventRecord(b, st);
+      cudaEventSynchronize(b);
+      cudaEventElapsedTime(kernel_ms, a, b);
+    }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
   }
+  if (rc != PM_OK) return rc;
   if (e != cudaSuccess) return snprintf(pmk_g_err, sizeof pmk_g_err, "invert launch: %s", cudaGetErrorString(e)), PM_EIO;
   return PM_OK;
 }

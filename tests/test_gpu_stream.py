@@ -81,7 +81,8 @@ def test_autotune_picks_a_valid_tuning_and_keeps_results():
 def test_bad_tuning_is_rejected():
     c = case(1)
     with inverter(c, pm.PREC_FP32) as inv:
-        for bad in ({"warps_per_block": 3}, {"staging_depth": 65}, {"variant": 2}):
+        for bad in ({"warps_per_block": 3}, {"staging_depth": 65}, {"variant": 3},
+                    {"variant": 1, "warps_per_block": 8}, {"variant": 2, "warps_per_block": 2}):
             with pytest.raises(pm.PmError) as e:
                 inv.tuning = bad
             assert e.value.code == -22

@@ -33,10 +33,18 @@ def _same(a, b):
         assert np.array_equal(a[k], b[k]), k
 
 
+def _regular(c, precision):
+    """A context with the launch tuning the no-alloc entry uses (the contexts'
+    default: the 128-register FP32 kernel, 4 pixels per block)."""
+    inv = inverter(c, precision)
+    inv.tuning = {"variant": 1, "warps_per_block": 4}
+    return inv
+
+
 @pytest.mark.parametrize("cfg,precision", [(1, pm.PREC_FP32), (1, pm.PREC_FP64), (2, pm.PREC_FP32)])
 def test_noalloc_matches_regular_entry_twice(cfg, precision):
     c = case(cfg)
-    with inverter(c, precision) as inv:
+    with _regular(c, precision) as inv:
         ref = inv.invert(c["obs"], c["guess"], slight=c["slight"])
         first = inv.invert_noalloc(c["obs"], c["guess"], slight=c["slight"])
         second = inv.invert_noalloc(c["obs"], c["guess"], slight=c["slight"])
@@ -47,7 +55,7 @@ def test_noalloc_matches_regular_entry_twice(cfg, precision):
 def test_noalloc_per_pixel_stray_light_and_a_smaller_second_call():
     c = case(2)
     sl = np.ascontiguousarray(np.broadcast_to(c["slight"].astype(np.float32), (c["obs"].shape[0], 4, c["lam"].size)))
-    with inverter(c, pm.PREC_FP32) as inv:
+    with _regular(c, pm.PREC_FP32) as inv:
         ref = inv.invert(c["obs"], c["guess"], slight=sl, slight_mode=pm.SLIGHT_PER_PIXEL)
         big = inv.invert_noalloc(c["obs"], c["guess"], slight=sl, slight_mode=pm.SLIGHT_PER_PIXEL)
         small = inv.invert_noalloc(c["obs"][:5], c["guess"], slight=sl[:5], slight_mode=pm.SLIGHT_PER_PIXEL)
