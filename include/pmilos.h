@@ -332,7 +332,9 @@ typedef struct pm_server_stats {
   double latency_p50_ms, latency_p99_ms, latency_max_ms;  /* submit -> results in host memory */
   double busy_ms;           /* first submit -> last completion */
   size_t arena_peak_bytes;
-  int64_t prepass_launches; /* classical pre-pass launches, one per admitted scan on a grid with classical estimates */
+  int64_t prepass_launches; /* classical-estimate launches apart from the inversion kernel: one per admitted scan
+                               on grids wider than 32 wavelengths; 0 on one-warp grids, whose persistent kernel
+                               computes the estimates of each pixel it takes */
 } pm_server_stats;
 
 /* grids[g], guesses[g]: the settings and initial model of grid g (g < ngrids). */

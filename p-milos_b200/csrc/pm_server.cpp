@@ -47,9 +47,6 @@ namespace {
 using Clock = std::chrono::steady_clock;
 
 constexpr int kRing = 4096;  // job descriptor ring: job k lives in slot k % kRing
-// Block slots the persistent kernel leaves free (about 2% of a B200's) so that
-// the classical pre-pass of each newly admitted scan can run beside it.
-constexpr int kReservedBlocks = 12;
 constexpr size_t kAlign = 256;
 
 size_t round_up(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
@@ -275,18 +272,9 @@ bool admit(pm_server* s, Scan* sc) {
   cudaError_t e = cudaMemsetAsync(s->done_dev + slot, 0, sizeof(unsigned long long), s->s_copy);
   if (e == cudaSuccess && !sc->device_input)
     e = cudaMemcpyAsync(base, sc->spectro, prof * size_t(sc->npix), cudaMemcpyHostToDevice, s->s_copy);
-  // the classical estimates of the scan, on the copy stream before its tickets
-  // are published, in the block slots the persistent kernel leaves free
-  const PmParams& P = s->gs->g[sc->grid];
-  if (e == cudaSuccess && P.classical) {
-    J.model_in = J.models;
-    // blocks of the persistent kernel's size (4 warps): one fits the slot a
-    // reserved block leaves free, whatever the pre-pass's register count
-    if (pmk_classical_prepass(P, J.spectro, J.models, sc->npix, s->s_copy, s->num_sms, nullptr, 128) != PM_OK)
-      e = cudaErrorLaunchFailure;
-    else
-      ++s->prepass_launches;
-  }
+  // the classical estimates: computed by the persistent kernel for each pixel
+  // it takes (J.model_in stays null), so it fills every block slot and no
+  // pre-pass launch has to find room beside it
   if (e == cudaSuccess) e = cudaMemcpyAsync(s->jobs_dev + slot, &J, sizeof J, cudaMemcpyHostToDevice, s->s_copy);
   s->avail_host[slot] = s->t_next + (unsigned long long)sc->npix;
   if (e == cudaSuccess)
@@ -331,7 +319,7 @@ bool launch(pm_server* s) {
   sio.first_job = s->oldest_job();
   sio.wait_limit_ns = (long long)(std::max(1000.0, 2 * s->sc.linger_ms) * 1e6) + 30000000000LL;
   const int rc = pmk_invert_stream(*s->gs, sio, s->precision, s->variant, 4, s->ngrids > 1, s->s_kern, s->num_sms,
-                                   nullptr, kReservedBlocks);
+                                   nullptr, 0);
   if (rc != PM_OK) {
     s->error = rc;
     std::snprintf(s->error_msg, sizeof s->error_msg, "%s", pmk_last_cuda_error());

@@ -118,8 +118,8 @@ def test_many_small_scans_share_a_kernel(cubes):
     for r in res[1:]:
         _eq(r, res[0])
     assert st["kernel_launches"] <= 5, st
-    # the grids estimate classically: one pre-pass launch per admitted scan
-    assert st["prepass_launches"] == 41, st
+    # the persistent kernel computes the classical estimates itself: no pre-pass launches
+    assert st["prepass_launches"] == 0, st
     assert st["latency_p99_ms"] >= st["latency_p50_ms"] > 0
 
 
