@@ -156,13 +156,16 @@ typedef struct pm_ctx pm_ctx;
  * reference, which has no device launches to tune. */
 #define PM_STAGING_MAX 64
 typedef struct pm_tuning {
-  int variant;          /* FP32 register budget per thread: 0 = 168 (3 blocks of 4 warps per SM),
-                           1 = 128 (4 blocks per SM, a few spills) */
+  int variant;          /* FP32 kernel of the one-warp grids: 0 = 168 registers per thread (3 blocks of 4
+                           warps per SM), 1 = 128 (4 blocks per SM, a few spills), 2 = lock-step blocks
+                           (128 registers; the warps of a block run each LM phase together, so they share
+                           the phase's instruction-cache lines; nine or ten free parameters without a
+                           v_mac row, one-warp grids; elsewhere 2 runs as 1) */
   int staging_depth;    /* host-buffer calls on grids of <= 32 wavelengths: the cube goes in this many
-                           pieces, each inverted by its own launch while the next one is copied in
-                           and the previous one's results are copied out (1..PM_STAGING_MAX);
-                           0 = copy everything, then launch once */
-  int warps_per_block;  /* pixels (one warp each) per block of the one-warp kernels: 1, 2 or 4 */
+                           pieces; one persistent launch inverts them as the copy stream publishes each
+                           piece (1..PM_STAGING_MAX); 0 = copy everything, then launch */
+  int warps_per_block;  /* pixels (one warp each) per block of the one-warp kernels: 1, 2 or 4; with
+                           variant 2: 4, 8 or 16 */
   int graphs;           /* 1: host-buffer calls of at most PM_GRAPH_MAX_PIXELS pixels on grids of <= 32
                            wavelengths (pm_lm_mils among them) stage through pinned memory and replay a
                            CUDA graph of the whole call, captured once per size; 0: no graphs */
@@ -374,9 +377,9 @@ int pm_set_tuning(pm_ctx *ctx, const pm_tuning *in);
 /* Autotuner: inverts npix sample pixels (host buffers, the same call path as
  * pm_invert_batch with PM_MEM_HOST, so copies and kernel are both timed) once per
  * candidate tuning and repetition, and keeps the fastest tuning in the context.
- * Candidates: variant {0, 1} x warps_per_block {1, 2, 4} x staging_depth
- * {0, 2, 4}.  *out (nullable) receives the choice.  No counterpart in the
- * reference. */
+ * Candidates: variants 0 and 1 with warps_per_block {1, 2, 4}, variant 2 with
+ * {8, 16}, each with staging_depth {0, 2, 4}.  *out (nullable) receives the
+ * choice.  No counterpart in the reference. */
 int pm_autotune(pm_ctx *ctx, int64_t npix, const float *spectro, const float *slight, int slight_mode,
                 const pm_model *guess, int reps, pm_tuning *out);
 

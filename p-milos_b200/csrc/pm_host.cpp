@@ -1210,13 +1210,15 @@ extern "C" int pm_autotune(pm_ctx* c, int64_t npix, const float* spectro, const 
   std::vector<int> its(static_cast<size_t>(npix));
   std::vector<pm_tuning> cands;
   const bool fp32 = c->precision == PM_PREC_FP32;
-  for (int variant : {0, 1}) {
+  for (int variant : {0, 1, 2}) {
     if (!fp32 && variant != c->tuning.variant) continue;  // the FP64 kernel has one register budget
-    for (int wpb : {1, 2, 4})
+    for (int wpb : {1, 2, 4, 8, 16}) {
+      if ((variant == 2) != (wpb >= 8)) continue;  // lock-step blocks of 8 or 16 warps; 1, 2, 4 otherwise
       for (int depth : {0, 2, 4}) {
         if (c->P.G != 1 && depth != 0) continue;  // multi-warp grids are not streamed
         cands.push_back(pm_tuning{variant, depth, wpb, c->tuning.graphs});
       }
+    }
   }
   const pm_tuning saved = c->tuning;
   pm_tuning best = saved;

@@ -40,7 +40,7 @@ int launch_stream_any(const PmGridSet& GS, const PmStreamIO& sio, cudaStream_t s
   if (pixgrid) {
     if (multi) return snprintf(pmk_g_err, sizeof pmk_g_err, "pixel grids: single-grid launches only"), PM_EINVAL;
     if constexpr (sizeof(R) == 4) {
-      return variant == 1
+      return variant != 0  // 1, or 2 where no lock-step instance exists: the 128-register kernel
                  ? launch_invert_stream<float, KT, 4, false, MAC, true>(GS, sio, st, num_sms, smem_out, wpb, reserve)
                  : launch_invert_stream<float, KT, 3, false, MAC, true>(GS, sio, st, num_sms, smem_out, wpb, reserve);
     } else {
@@ -48,15 +48,20 @@ int launch_stream_any(const PmGridSet& GS, const PmStreamIO& sio, cudaStream_t s
     }
   }
   if constexpr (sizeof(R) == 4) {
-    if (multi) return launch_invert_stream<float, KT, 4, true, MAC>(GS, sio, st, num_sms, smem_out, wpb, reserve);
     if constexpr (!MAC && KT <= 10) {
       if (variant == 2) {  // lock-step blocks of wpb warps
-        if (wpb == 16) return launch_invert_lockstep<float, KT, 16, MAC>(GS, sio, st, num_sms, smem_out, reserve);
-        if (wpb == 8) return launch_invert_lockstep<float, KT, 8, MAC>(GS, sio, st, num_sms, smem_out, reserve);
-        return launch_invert_lockstep<float, KT, 4, MAC>(GS, sio, st, num_sms, smem_out, reserve);
+        if (multi) {
+          if (wpb == 16) return launch_invert_lockstep<float, KT, 16, true, MAC>(GS, sio, st, num_sms, smem_out, reserve);
+          if (wpb == 4) return launch_invert_lockstep<float, KT, 4, true, MAC>(GS, sio, st, num_sms, smem_out, reserve);
+          return launch_invert_lockstep<float, KT, 8, true, MAC>(GS, sio, st, num_sms, smem_out, reserve);
+        }
+        if (wpb == 16) return launch_invert_lockstep<float, KT, 16, false, MAC>(GS, sio, st, num_sms, smem_out, reserve);
+        if (wpb == 4) return launch_invert_lockstep<float, KT, 4, false, MAC>(GS, sio, st, num_sms, smem_out, reserve);
+        return launch_invert_lockstep<float, KT, 8, false, MAC>(GS, sio, st, num_sms, smem_out, reserve);
       }
     }
-    return variant == 1 ? launch_invert_stream<float, KT, 4, false, MAC>(GS, sio, st, num_sms, smem_out, wpb, reserve)
+    if (multi) return launch_invert_stream<float, KT, 4, true, MAC>(GS, sio, st, num_sms, smem_out, wpb, reserve);
+    return variant != 0 ? launch_invert_stream<float, KT, 4, false, MAC>(GS, sio, st, num_sms, smem_out, wpb, reserve)
                         : launch_invert_stream<float, KT, 3, false, MAC>(GS, sio, st, num_sms, smem_out, wpb, reserve);
   } else {
     return multi ? launch_invert_stream<double, KT, 1, true, MAC>(GS, sio, st, num_sms, smem_out, wpb, reserve)

@@ -145,30 +145,32 @@ __global__ void __launch_bounds__(128, MINB) invert_stream_kernel(
 }
 
 
-// Lock-step form of the streamed kernel (one grid): the W warps of a block
-// advance through the LM loop together, one phase at a time (lm_solve,
-// lm_synth, lm_update, with block barriers between them), so that at any time
-// the block executes one phase's code.  A warp whose pixel is finished takes
-// the next ticket before the next pass; warps without one (the queue is
-// drained) keep taking part in the barriers until every warp of the block is
-// done.  Per pixel the arithmetic is invert_pixel's.
-template <typename R, int KT, int W, bool MAC, bool PIXGRID, bool ZM = false>
-__global__ void __launch_bounds__(32 * W, 16 / W) invert_lockstep_kernel(const __grid_constant__ GridParams<1> GS,
-                                                                        const PmStreamIO sio) {
+// Lock-step form of the streamed kernel: the W warps of a block advance through
+// the LM loop together, one phase at a time (lm_solve, lm_synth, lm_update,
+// with block barriers between them), so that at any time the block executes
+// one phase's code and the warps of an SM sub-partition share its instruction
+// cache lines.  A warp whose pixel is finished takes the next ticket before
+// the next pass; warps without one (the queue is drained) keep taking part in
+// the barriers until every warp of the block is done.  MULTI: the launch serves
+// up to PMK_MAX_GRIDS grids (a server's), each warp on its pixel's grid.  Per
+// pixel the arithmetic is invert_pixel's.
+template <typename R, int KT, int W, bool MULTI, bool MAC, bool PIXGRID, bool ZM = false>
+__global__ void __launch_bounds__(32 * W, 16 / W) invert_lockstep_kernel(
+    const __grid_constant__ GridParams<MULTI ? PMK_MAX_GRIDS : 1> GS, const PmStreamIO sio) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int NG = MULTI ? PMK_MAX_GRIDS : 1;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   BlockSmem<R>* bs = reinterpret_cast<BlockSmem<R>*>(smem_raw);
-  WarpSmem<R>& sm = reinterpret_cast<WarpSmem<R>*>(smem_raw + sizeof(BlockSmem<R>))[warp];
-  const PmParams& P = GS.g[0];
-  load_taps<R>(P, bs[0]);
-  for (int e = lane; e < 4 * XSR; e += 32) (&sm.xs[0][0])[e] = R(0);
+  WarpSmem<R>& sm = reinterpret_cast<WarpSmem<R>*>(smem_raw + NG * sizeof(BlockSmem<R>))[warp];
+#pragma unroll 1
+  for (int g = 0; g < NG && g < GS.ngrids; ++g) load_taps<R>(GS.g[g], bs[g]);
   if (lane == 0) {
     sm.job_k = sio.first_job;
-    sm.grid_cur = 0;
-    sm.xs_dirty = 0;
+    sm.grid_cur = -1;  // grid of the previous pixel: the padded rows are re-zeroed on a change
   }
   __syncthreads();
   PixelLM<R> L;
+  int gi = 0;
   bool have = false, drained = false;
   while (true) {
     while (!have && !drained) {
@@ -197,27 +199,37 @@ __global__ void __launch_bounds__(32 * W, 16 / W) invert_lockstep_kernel(const _
         drained = true;
         break;
       }
+      gi = MULTI ? __ldcg(&jp->grid) : 0;
+      if (gi != sm.grid_cur) {
+        for (int e = lane; e < 4 * XSR; e += 32) (&sm.xs[0][0])[e] = R(0);
+        __syncwarp();
+        if (lane == 0) {
+          sm.grid_cur = gi;
+          sm.xs_dirty = 0;
+        }
+      }
       if (lane == 0) {
         sm.job_k = k;
         sm.job = jp;
         sm.pix = (unsigned long long)t - t0;
       }
       __syncwarp();
-      lm_begin<R, PIXGRID>(P, sm, lane, L);
+      lm_begin<R, PIXGRID>(GS.g[gi], sm, lane, L);
       if (L.finished) {
-        lm_end<R>(P, sm, lane, L, sio.q->ctr);
+        lm_end<R>(GS.g[gi], sm, lane, L, sio.q->ctr);
         job_pixel_done(sm, lane);
       } else {
         have = true;
       }
     }
     if (!__syncthreads_or(have)) break;
+    const PmParams& P = GS.g[gi];
     if (have) lm_solve<R, KT>(P, sm, lane, L);
     __syncthreads();
     if (have) lm_synth<R, MAC, PIXGRID, ZM>(P, sm, lane, L);
     __syncthreads();
     if (have) {
-      lm_update<R, KT, MAC, PIXGRID, ZM>(P, bs[0], sm, lane, L);
+      lm_update<R, KT, MAC, PIXGRID, ZM>(P, bs[gi], sm, lane, L);
       if (L.finished) {
         lm_end<R>(P, sm, lane, L, sio.q->ctr);
         job_pixel_done(sm, lane);
@@ -227,16 +239,17 @@ __global__ void __launch_bounds__(32 * W, 16 / W) invert_lockstep_kernel(const _
   }
 }
 
-template <typename R, int KT, int W, bool MAC, bool PIXGRID = false, bool ZM = false>
+template <typename R, int KT, int W, bool MULTI, bool MAC, bool PIXGRID = false, bool ZM = false>
 int launch_invert_lockstep(const PmGridSet& GS, const PmStreamIO& sio, cudaStream_t st, int num_sms,
                            size_t* smem_out, int reserve) {
   constexpr int threads = 32 * W;
-  const size_t smem = sizeof(BlockSmem<R>) + sizeof(WarpSmem<R>) * W;
+  constexpr int NG = MULTI ? PMK_MAX_GRIDS : 1;
+  const size_t smem = NG * sizeof(BlockSmem<R>) + sizeof(WarpSmem<R>) * W;
   if (smem_out) *smem_out = smem;
-  auto kern = invert_lockstep_kernel<R, KT, W, MAC, PIXGRID, ZM>;
-  GridParams<1> gp;
-  gp.ngrids = 1;
-  gp.g[0] = GS.g[0];
+  auto kern = invert_lockstep_kernel<R, KT, W, MULTI, MAC, PIXGRID, ZM>;
+  GridParams<NG> gp;  // copied into the launch
+  gp.ngrids = GS.ngrids < NG ? GS.ngrids : NG;
+  for (int g = 0; g < gp.ngrids; ++g) gp.g[g] = GS.g[g];
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return snprintf(pmk_g_err, sizeof pmk_g_err, "%s", cudaGetErrorString(e)), PM_EIO;
   int per_sm = 0;
@@ -252,6 +265,7 @@ int launch_invert_lockstep(const PmGridSet& GS, const PmStreamIO& sio, cudaStrea
 template <typename R, int KT, int MINB, bool MULTI, bool MAC, bool PIXGRID = false, bool ZM = false>
 int launch_invert_stream(const PmGridSet& GS, const PmStreamIO& sio, cudaStream_t st, int num_sms,
                          size_t* smem_out, int wpb, int reserve) {
+  if (wpb > 4) wpb = 4;  // the lock-step tunings' block sizes: this kernel takes at most 4 warps per block
   const int threads = 32 * wpb;
   const size_t smem = (MULTI ? PMK_MAX_GRIDS : 1) * sizeof(BlockSmem<R>) + sizeof(WarpSmem<R>) * (threads / 32);
   if (smem_out) *smem_out = smem;

@@ -16,7 +16,7 @@ import pytest
 import pmilos_b200 as pm
 import pyoracle as po
 from conftest import GOLDEN
-from gpu_common import LINE_6173, NOISE64, case, within_tolerance
+from gpu_common import LINE_6173, NOISE64, assert_plain_parity, case, within_tolerance
 
 pytestmark = pytest.mark.gpu
 
@@ -49,6 +49,20 @@ def truths(n, seed, mac=False):
 
 def oracles(lam, psf, nterms):
     return [po.Restatement(po.LineSetup(l, LINE_6173[0], CUANTIC, psf, nterms), "f64") for l in lam]
+
+
+def fast_models(oras, obs, guess, fix):
+    """The reference's own optimised FP64 build on each pixel's grid (None when
+    it was not built): the yardstick of gpu_common.assert_plain_parity."""
+    if not po.reference_available("f64_fast"):
+        return None
+    models = [po.Reference(o.setup, "f64_fast").invert(obs[i:i + 1], guess, fix=fix, noise=NOISE64,
+                                                        want_spectra=False)["models"] for i, o in enumerate(oras)]
+    return {"models": np.concatenate(models)}
+
+
+def stacked(results):
+    return {k: np.concatenate([r[k] for r in results]) for k in ("models", "spectra", "status")}
 
 
 def observed(oras, models, fix, seed):
@@ -86,10 +100,8 @@ def test_fp64_inversion_on_each_pixels_grid():
                      precision=pm.PREC_FP64, solver=pm.SOLVE_EIGEN) as inv:
         r = inv.invert(obs, c["guess"], lam=lam)
         shared = inv.invert(obs, c["guess"])
-    ok = within_tolerance(r["models"], ref_models)
-    assert ok.mean() >= 0.9, f"only {ok.mean():.2%} of pixels within tolerance"
-    ref_spectra = np.concatenate([x["spectra"] for x in ref])
-    assert np.abs(r["spectra"][ok] - ref_spectra[ok]).max() < 1e-5
+    assert_plain_parity(r, stacked(ref), params=tuple(i for i in range(11) if c["fix"][i]),
+                        fast=fast_models(oras, obs, c["guess"], c["fix"]))
     # the shifts matter: on the shared grid the same profiles give other models
     assert within_tolerance(shared["models"], ref_models).mean() < 0.5
 
@@ -192,13 +204,14 @@ def test_wide_inversion_on_each_pixels_grid(prec):
     lam = grids(c["lam"], n, 23, c["l0"])
     oras = wide_oracles(c, lam)
     obs = observed(oras, truths(n, 24), c["fix"], 25)
-    ref = np.concatenate([o.invert(obs[i:i + 1], c["guess"], fix=c["fix"], noise=NOISE64)["models"]
-                          for i, o in enumerate(oras)])
+    refs = stacked([o.invert(obs[i:i + 1], c["guess"], fix=c["fix"], noise=NOISE64) for i, o in enumerate(oras)])
+    ref = refs["models"]
     with wide_inverter(c, prec, pm.SOLVE_EIGEN if prec == pm.PREC_FP64 else pm.SOLVE_DEFAULT) as inv:
         r = inv.invert(obs, c["guess"], lam=lam)
         shared = inv.invert(obs, c["guess"])
     if prec == pm.PREC_FP64:
-        assert within_tolerance(r["models"], ref).mean() >= 0.9
+        assert_plain_parity(r, refs, params=tuple(i for i in range(11) if c["fix"][i]),
+                            fast=fast_models(oras, obs, c["guess"], c["fix"]))
     else:
         dB = np.abs(r["models"][:, 1] - ref[:, 1])
         assert np.median(dB) < 1.0 and (dB < 5.0).mean() >= 0.9

@@ -46,6 +46,13 @@ def test_every_tuning_gives_the_device_call_result(cfg, precision):
                     inv.tuning = {"variant": variant, "staging_depth": depth, "warps_per_block": wpb}
                     r = inv.invert(c["obs"], c["guess"], slight=c["slight"])
                     _same(r, ref)
+        if precision == pm.PREC_FP32:
+            # the lock-step kernel: the 128-register kernel's arithmetic, phase by phase
+            for wpb in (4, 8, 16):
+                inv.tuning = {"variant": 2, "staging_depth": 0, "warps_per_block": wpb}
+                _same(_device_reference(inv, c), refs[1])
+                inv.tuning = {"variant": 2, "staging_depth": 3, "warps_per_block": wpb}
+                _same(inv.invert(c["obs"], c["guess"], slight=c["slight"]), refs[1])
     for other in refs[1:]:
         # the stated FP32 tolerance: |dB| < 5 G for 90% of pixels, median below 1 G
         dB = np.abs(other["models"][:, 1] - refs[0]["models"][:, 1])
@@ -73,7 +80,8 @@ def test_autotune_picks_a_valid_tuning_and_keeps_results():
     with inverter(c, pm.PREC_FP32) as inv:
         t = inv.autotune(np.tile(c["obs"], (64, 1, 1)), c["guess"], reps=1)
         assert t == inv.tuning
-        assert t["variant"] in (0, 1) and t["warps_per_block"] in (1, 2, 4) and t["staging_depth"] in (0, 2, 4)
+        assert (t["variant"], t["warps_per_block"]) in {(v, w) for v in (0, 1) for w in (1, 2, 4)} | {(2, 8), (2, 16)}
+        assert t["staging_depth"] in (0, 2, 4)
         # the chosen register budget's own device-buffer result
         _same(inv.invert(c["obs"], c["guess"]), _device_reference(inv, c))
 

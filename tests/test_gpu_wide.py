@@ -15,7 +15,7 @@ import pytest
 import pmilos_b200 as pm
 import pyoracle as po
 from conftest import GOLDEN
-from gpu_common import NOISE64, within_tolerance
+from gpu_common import NOISE64, assert_plain_parity, reference_fast, within_tolerance
 
 pytestmark = pytest.mark.gpu
 
@@ -141,10 +141,12 @@ def test_plain_fp64_wide_matches_oracle(name):
     c, obs, ref = _case_results(name)
     with winverter(c, pm.PREC_FP64, pm.SOLVE_EIGEN) as inv:
         r = inv.invert(obs, c["guess"], slight=c["slight"])
-    ok = within_tolerance(r["models"], ref["models"])
-    assert ok.mean() >= 0.9, f"only {ok.mean():.2%} of pixels within tolerance"
+    fast = reference_fast(po.LineSetup(c["lam"], c["lambda0"], np.array([1.0, *CUANTIC]), c["psf"], c["nterms"]))
+    fast_r = None if fast is None else fast.invert(obs, c["guess"], slight=c["slight"], fix=c["fix"],
+                                                   noise=NOISE64, want_spectra=False)
+    ok = assert_plain_parity(r, ref, params=tuple(i for i in range(11) if c["fix"][i]), fast=fast_r,
+                             min_converged=0.2)
     assert ok[:6].all()  # the ghost pixels
-    assert np.abs(r["spectra"][ok] - ref["spectra"][ok]).max() < 1e-5
     assert np.allclose(np.sort(r["chisq"][ok]), np.sort(ref["chisq"][ok]), rtol=1e-3)
     assert abs(np.median(r["iters"]) - np.median(ref["iters"])) <= 2
 
