@@ -699,31 +699,49 @@ __device__ __forceinline__ void rf_correlate(const PmParams& P, const BlockSmem<
   const bool isI = (lane & 3) == 0;
   const R e0 = row[0], en = row[P.nl - 1];
   const R ic = isI ? ((e0 > en) ? e0 : en) : R(0);
-  R acc[NL];
+  if constexpr (VEC == 4) {
+    // FP32: the products in pairs, one packed FMA (sm_100 f32x2) per two outputs;
+    // each half of a pair rounds exactly as a scalar fma would
+    float2 acc[NL / 2];
 #pragma unroll
-  for (int k = 0; k < NL; ++k) acc[k] = 0;
+    for (int k = 0; k < NL / 2; ++k) acc[k] = make_float2(0.0f, 0.0f);
 #pragma unroll 1
-  for (int m = 0; m < P.nl; ++m) {
-    const R xm = isI ? ic - row[m] : row[m];
-    const int c = (31 - m) & (VEC - 1), b = (31 - m) - c;
-    const R* g = bs.rv[c] + b;
+    for (int m = 0; m < P.nl; ++m) {
+      const float xm = isI ? ic - row[m] : row[m];
+      const float2 x2 = make_float2(xm, xm);
+      const int c = (31 - m) & (VEC - 1), b = (31 - m) - c;
+      const R* g = bs.rv[c] + b;
 #pragma unroll
-    for (int k = 0; k < NL; k += VEC) {
-      if constexpr (VEC == 4) {
+      for (int k = 0; k < NL; k += VEC) {
         const float4 q = *reinterpret_cast<const float4*>(g + k);
-        acc[k] = fma(xm, q.x, acc[k]);
-        acc[k + 1] = fma(xm, q.y, acc[k + 1]);
-        acc[k + 2] = fma(xm, q.z, acc[k + 2]);
-        acc[k + 3] = fma(xm, q.w, acc[k + 3]);
-      } else {
+        acc[k / 2] = __ffma2_rn(x2, make_float2(q.x, q.y), acc[k / 2]);
+        acc[k / 2 + 1] = __ffma2_rn(x2, make_float2(q.z, q.w), acc[k / 2 + 1]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < NL / 2; ++k) {
+      row[2 * k] = isI ? ic - acc[k].x : acc[k].x;
+      row[2 * k + 1] = isI ? ic - acc[k].y : acc[k].y;
+    }
+  } else {
+    R acc[NL];
+#pragma unroll
+    for (int k = 0; k < NL; ++k) acc[k] = 0;
+#pragma unroll 1
+    for (int m = 0; m < P.nl; ++m) {
+      const R xm = isI ? ic - row[m] : row[m];
+      const int c = (31 - m) & (VEC - 1), b = (31 - m) - c;
+      const R* g = bs.rv[c] + b;
+#pragma unroll
+      for (int k = 0; k < NL; k += VEC) {
         const double2 q = *reinterpret_cast<const double2*>(g + k);
         acc[k] = fma(xm, q.x, acc[k]);
         acc[k + 1] = fma(xm, q.y, acc[k + 1]);
       }
     }
-  }
 #pragma unroll
-  for (int k = 0; k < NL; ++k) row[k] = isI ? ic - acc[k] : acc[k];
+    for (int k = 0; k < NL; ++k) row[k] = isI ? ic - acc[k] : acc[k];
+  }
   __syncwarp();
 }
 
@@ -809,15 +827,29 @@ __device__ __forceinline__ R ne_entry(const R (&d)[KT][4], const R (&cw)[4], con
     return R(0);
   } else {
     constexpr int a = ne_row(E, KT), b = ne_col(E, KT);
-    R acc = 0;
-    if constexpr (a < KT) {
-#pragma unroll
-      for (int s = 0; s < 4; ++s) acc = fma(d[a][s] * d[b][s], cw[s], acc);
+    if constexpr (sizeof(R) == 4) {
+      // FP32: Stokes pairs in packed f32x2 operations; dw = d * cw (row a's
+      // weighted RFs, a common subexpression of the row's entries) or rw
+      const float2 w01 = a < KT ? __fmul2_rn(make_float2(d[a < KT ? a : 0][0], d[a < KT ? a : 0][1]),
+                                             make_float2(cw[0], cw[1]))
+                                : make_float2(rw[0], rw[1]);
+      const float2 w23 = a < KT ? __fmul2_rn(make_float2(d[a < KT ? a : 0][2], d[a < KT ? a : 0][3]),
+                                             make_float2(cw[2], cw[3]))
+                                : make_float2(rw[2], rw[3]);
+      float2 p = __fmul2_rn(w01, make_float2(d[b][0], d[b][1]));
+      p = __ffma2_rn(w23, make_float2(d[b][2], d[b][3]), p);
+      return p.x + p.y;
     } else {
+      R acc = 0;
+      if constexpr (a < KT) {
 #pragma unroll
-      for (int s = 0; s < 4; ++s) acc = fma(rw[s], d[b][s], acc);
+        for (int s = 0; s < 4; ++s) acc = fma(d[a][s] * d[b][s], cw[s], acc);
+      } else {
+#pragma unroll
+        for (int s = 0; s < 4; ++s) acc = fma(rw[s], d[b][s], acc);
+      }
+      return acc;
     }
-    return acc;
   }
 }
 

@@ -115,7 +115,7 @@ struct SmallStage {
 struct pm_ctx {
   PmParams P;
   int precision = PM_PREC_FP32;
-  pm_tuning tuning{1, 8, 4, 1};
+  pm_tuning tuning{2, 8, 8, 1};  // lock-step blocks of 8 warps (FP32 one-warp grids), fed in 8 pieces
   int device = 0;
   int num_sms = 148;
   cudaStream_t stream = nullptr;
@@ -429,7 +429,11 @@ extern "C" int pm_ctx_create(const pm_line* line, const pm_config* cfg, void* st
                 prop.minor);
   }
   c->num_sms = prop.multiProcessorCount;
-  if (const char* v = std::getenv("PMILOS_VARIANT")) c->tuning.variant = std::atoi(v);
+  if (const char* v = std::getenv("PMILOS_VARIANT")) {
+    const int var = std::atoi(v);
+    if (var >= 0 && var <= 2) c->tuning.variant = var;
+    if (c->tuning.variant != 2) c->tuning.warps_per_block = 4;
+  }
   if (const char* v = std::getenv("PMILOS_RESIDENT_MB"))
     if (std::atoll(v) > 0) c->resident_bytes = size_t(std::atoll(v)) << 20;
   if (const char* v = std::getenv("PMILOS_STAGING")) c->tuning.staging_depth = std::atoi(v);

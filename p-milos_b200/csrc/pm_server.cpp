@@ -120,7 +120,7 @@ thread_local char g_err[256];
 }  // namespace
 
 struct pm_server {
-  int device = 0, num_sms = 148, precision = PM_PREC_FP32, variant = 1, ngrids = 0;
+  int device = 0, num_sms = 148, precision = PM_PREC_FP32, variant = 2, ngrids = 0;
   PmGridSet* gs = nullptr;
   pm_server_config sc{};
   size_t prof[PM_SERVER_MAX_GRIDS] = {};
@@ -318,8 +318,8 @@ bool launch(pm_server* s) {
   sio.jobs_cap = kRing;
   sio.first_job = s->oldest_job();
   sio.wait_limit_ns = (long long)(std::max(1000.0, 2 * s->sc.linger_ms) * 1e6) + 30000000000LL;
-  const int rc = pmk_invert_stream(*s->gs, sio, s->precision, s->variant, 4, s->ngrids > 1, s->s_kern, s->num_sms,
-                                   nullptr, 0);
+  const int rc = pmk_invert_stream(*s->gs, sio, s->precision, s->variant, s->variant == 2 ? 8 : 4, s->ngrids > 1,
+                                   s->s_kern, s->num_sms, nullptr, 0);
   if (rc != PM_OK) {
     s->error = rc;
     std::snprintf(s->error_msg, sizeof s->error_msg, "%s", pmk_last_cuda_error());
@@ -579,7 +579,7 @@ extern "C" int pm_server_create(const pm_line* line, const pm_config* const* gri
   }
   s->precision = grids[0]->precision;
   s->wide = s->gs->g[0].G != 1;
-  if (const char* v = std::getenv("PMILOS_VARIANT")) s->variant = std::atoi(v) == 1 ? 1 : 0;
+  if (const char* v = std::getenv("PMILOS_VARIANT")) s->variant = std::atoi(v) >= 0 && std::atoi(v) <= 2 ? std::atoi(v) : 2;
   cudaDeviceProp prop;
   cudaError_t e = cudaGetDevice(&s->device);
   if (e == cudaSuccess) e = cudaGetDeviceProperties(&prop, s->device);

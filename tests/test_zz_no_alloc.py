@@ -35,9 +35,9 @@ def _same(a, b):
 
 def _regular(c, precision):
     """A context with the launch tuning the no-alloc entry uses (the contexts'
-    default: the 128-register FP32 kernel, 4 pixels per block)."""
+    default: lock-step blocks of 8 pixels)."""
     inv = inverter(c, precision)
-    inv.tuning = {"variant": 1, "warps_per_block": 4}
+    inv.tuning = {"variant": 2, "warps_per_block": 8}
     return inv
 
 
