@@ -298,9 +298,8 @@ int pm_fits_reorder(const pm_fits_cube *info, const void *data_dev, float *cube_
  *
  * No counterpart in the reference, whose drivers invert one cube per process
  * run.  A server holds up to PM_SERVER_MAX_GRIDS wavelength grids (line, grid,
- * PSF and settings resident on the device; all share nterms and precision, and
- * either every grid has <= 32 wavelengths or every grid has more, else
- * PM_ENOTSUP) and a device arena of hbm_budget_bytes.  A scheduler thread admits
+ * PSF and settings resident on the device; all share nterms and precision) and
+ * a device arena of hbm_budget_bytes.  A scheduler thread admits
  * submitted scans in arrival order as arena space and in-flight slots free up:
  * it copies each admitted scan to the device and publishes its pixels to one
  * persistent inversion kernel that is already running, so scans that arrive
@@ -308,8 +307,11 @@ int pm_fits_reorder(const pm_fits_cube *info, const void *data_dev, float *cube_
  * back as soon as its last pixel is done.  Scans on different grids share the
  * launch.  On grids of more than 32 wavelengths each scan is one launch of the
  * wide kernel instead, queued after its copy-in (copies still overlap the
- * inversions of other scans).  Each pixel's arithmetic is the same whatever else
- * is in flight. */
+ * inversions of other scans); a server may hold grids of both kinds, and a scan
+ * on a wide grid is admitted once the persistent kernel has ended (the scheduler
+ * closes it when such a scan is next), then the persistent kernel is launched
+ * again for the scans behind it.  Each pixel's arithmetic is the same whatever
+ * else is in flight. */
 #define PM_SERVER_MAX_GRIDS 4
 #define PM_SERVER_MAX_INFLIGHT 256
 #define PM_ETIMEDOUT (-110)   /* pm_server_wait: the scan did not finish in time */

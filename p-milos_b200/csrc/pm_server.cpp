@@ -21,10 +21,14 @@
 //     published ticket; the next launch reopens the queue at the first
 //     unpublished ticket).
 // Scans thus join a kernel that is already running, and results leave while
-// other scans are still on the GPU.  Grids of more than 32 wavelengths (all of
-// a server's grids, or none) have no persistent kernel: each admitted scan is
-// one launch of the wide kernel after its copy-in, and an event on the kernel
-// stream takes the place of the completion flag.
+// other scans are still on the GPU.  Grids of more than 32 wavelengths are not
+// in the persistent kernel: each admitted scan on one is a launch of the wide
+// kernel after its copy-in, and an event on the kernel stream takes the place of
+// the completion flag.  A server may hold both kinds of grid; a wide scan is
+// admitted only while the persistent kernel is stopped (when one is next in the
+// queue the scheduler closes the queue, the kernel ends once its published
+// tickets are inverted, and the wide launch follows it on the kernel stream),
+// and the persistent kernel is relaunched behind it for the next narrow scans.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -128,10 +132,15 @@ struct pm_server {
   int64_t slight_npix[PM_SERVER_MAX_GRIDS] = {};  // and its pixel count (every scan on the grid has it)
   cudaStream_t s_kern = nullptr, s_copy = nullptr, s_out = nullptr;
   cudaEvent_t ev_kernel = nullptr, ev_reset = nullptr;
-  // grids of more than 32 wavelengths: no persistent kernel; each admitted scan
-  // is one launch of the wide kernel, after its copy-in (ev_copied), with its
-  // pixel and iteration counters in ctr_dev
-  bool wide = false;
+  // grids of more than 32 wavelengths: not in the persistent kernel; each
+  // admitted scan is one launch of the wide kernel on the kernel stream, after
+  // its copy-in (ev_copied), with its pixel and iteration counters in ctr_dev.
+  // The persistent kernel serves the other grids (narrow_index: a grid's slot in
+  // gs_narrow, the parameter blocks it takes)
+  bool wide_grid[PM_SERVER_MAX_GRIDS] = {};
+  int narrow_index[PM_SERVER_MAX_GRIDS] = {};
+  int nnarrow = 0;
+  PmGridSet* gs_narrow = nullptr;
   cudaEvent_t ev_copied = nullptr;
   unsigned long long* ctr_dev = nullptr;
   enum { K_STOPPED, K_RUNNING, K_CLOSING } kstate = K_STOPPED;
@@ -250,7 +259,7 @@ bool admit_wide(pm_server* s, Scan* sc) {
 }
 
 bool admit(pm_server* s, Scan* sc) {
-  if (s->wide) return admit_wide(s, sc);
+  if (s->wide_grid[sc->grid]) return admit_wide(s, sc);
   const size_t prof = s->prof[sc->grid];
   const long long k = s->next_job;
   const int slot = int(k % kRing);
@@ -259,7 +268,7 @@ bool admit(pm_server* s, Scan* sc) {
   std::memset(&J, 0, sizeof J);
   J.t0 = s->t_next;
   J.npix = sc->npix;
-  J.grid = sc->grid;
+  J.grid = s->narrow_index[sc->grid];
   J.spectro = sc->device_input ? sc->spectro : reinterpret_cast<const float*>(base);
   J.slight = s->slight_dev[sc->grid];
   J.models = reinterpret_cast<double*>(base + sc->o_models);
@@ -318,8 +327,12 @@ bool launch(pm_server* s) {
   sio.jobs_cap = kRing;
   sio.first_job = s->oldest_job();
   sio.wait_limit_ns = (long long)(std::max(1000.0, 2 * s->sc.linger_ms) * 1e6) + 30000000000LL;
-  const int rc = pmk_invert_stream(*s->gs, sio, s->precision, s->variant, s->variant == 2 ? 8 : 4, s->ngrids > 1,
-                                   s->s_kern, s->num_sms, nullptr, 0);
+  // the grids of at most 32 wavelengths, as they are now (stray light may have been set)
+  s->gs_narrow->ngrids = s->nnarrow;
+  for (int g = 0; g < s->ngrids; ++g)
+    if (!s->wide_grid[g]) s->gs_narrow->g[s->narrow_index[g]] = s->gs->g[g];
+  const int rc = pmk_invert_stream(*s->gs_narrow, sio, s->precision, s->variant, s->variant == 2 ? 8 : 4,
+                                   s->nnarrow > 1, s->s_kern, s->num_sms, nullptr, 0);
   if (rc != PM_OK) {
     s->error = rc;
     std::snprintf(s->error_msg, sizeof s->error_msg, "%s", pmk_last_cuda_error());
@@ -397,6 +410,9 @@ void serve(pm_server* s) {
       while (s->kstate != pm_server::K_CLOSING && !s->queued.empty() &&
              int(s->active.size()) < s->sc.max_inflight && s->next_job - s->oldest_job() < kRing) {
         Scan* sc = s->queued.front();
+        // a wide scan's launch follows the persistent kernel on the kernel
+        // stream: admitted only while that kernel is stopped (step 3 closes it)
+        if (s->wide_grid[sc->grid] && s->kstate != pm_server::K_STOPPED) break;
         size_t off = 0;
         if (!s->arena->alloc(sc->bytes, &off)) break;
         s->queued.pop_front();
@@ -409,7 +425,7 @@ void serve(pm_server* s) {
         Scan* sc = s->active[i];
         const int slot = int(sc->job % kRing);
         bool inverted = false;
-        if (sc->state == Scan::ADMITTED && s->wide) {
+        if (sc->state == Scan::ADMITTED && s->wide_grid[sc->grid]) {
           const cudaError_t e = cudaEventQuery(sc->ev_kernel);
           if (e == cudaSuccess) inverted = true;
           else if (e != cudaErrorNotReady) fail_all(s, "inversion kernel", e);
@@ -460,12 +476,18 @@ void serve(pm_server* s) {
           fail_all(s, "inversion kernel", e);
         }
       }
-      if (s->error == PM_OK && s->kstate == pm_server::K_STOPPED && !s->wide) {
-        bool pending = false;
-        for (const Scan* sc : s->active) pending = pending || sc->state == Scan::ADMITTED;
-        if (pending && launch(s)) progress = true;
+      bool narrow_pending = false;  // admitted scans of the persistent kernel's grids not yet inverted
+      for (const Scan* sc : s->active)
+        narrow_pending = narrow_pending || (sc->state == Scan::ADMITTED && !s->wide_grid[sc->grid]);
+      if (s->error == PM_OK && s->kstate == pm_server::K_STOPPED) {
+        if (narrow_pending && launch(s)) progress = true;
       } else if (s->error == PM_OK && s->kstate == pm_server::K_RUNNING) {
-        if (s->active.empty() && s->queued.empty()) {
+        const bool wide_next = !s->queued.empty() && s->wide_grid[s->queued.front()->grid];
+        if (wide_next) {
+          // the next scan is on a wide grid: close now, the kernel ends once its
+          // published tickets are inverted and the wide launch follows it
+          if (close_queue(s)) progress = true;
+        } else if (!narrow_pending && s->queued.empty()) {
           const double now = s->now_ms();
           if (s->idle_since < 0) s->idle_since = now;
           else if (now - s->idle_since >= s->sc.linger_ms || s->stop) {
@@ -521,6 +543,7 @@ void release(pm_server* s) {
     if (p) cudaFreeHost(p);
   delete s->arena;
   delete s->gs;
+  delete s->gs_narrow;
   delete s;
 }
 
@@ -566,11 +589,8 @@ extern "C" int pm_server_create(const pm_line* line, const pm_config* const* gri
       release(s);
       return sfail(PM_EINVAL, "pm_server_create: miter < 0 (classical estimates only) is not served");
     }
-    if ((P.G != 1) != (s->gs->g[0].G != 1)) {
-      release(s);
-      return sfail(PM_ENOTSUP, "pm_server_create: grids of at most 32 wavelengths and wider ones are served by "
-                               "separate servers");
-    }
+    s->wide_grid[g] = P.G != 1;
+    if (!s->wide_grid[g]) s->narrow_index[g] = s->nnarrow++;
     if (grids[g]->precision != grids[0]->precision || P.K != s->gs->g[0].K) {
       release(s);
       return sfail(PM_EINVAL, "pm_server_create: grids differ in precision or nterms");
@@ -578,7 +598,11 @@ extern "C" int pm_server_create(const pm_line* line, const pm_config* const* gri
     s->prof[g] = sizeof(float) * 4 * size_t(P.nl);
   }
   s->precision = grids[0]->precision;
-  s->wide = s->gs->g[0].G != 1;
+  s->gs_narrow = new (std::nothrow) PmGridSet();
+  if (!s->gs_narrow) {
+    release(s);
+    return sfail(PM_ENOMEM, "pm_server_create: out of host memory");
+  }
   if (const char* v = std::getenv("PMILOS_VARIANT")) s->variant = std::atoi(v) >= 0 && std::atoi(v) <= 2 ? std::atoi(v) : 2;
   cudaDeviceProp prop;
   cudaError_t e = cudaGetDevice(&s->device);

@@ -190,11 +190,28 @@ def test_wide_grid_scans_equal_the_batch_entry_point():
     assert st["pixels_done"] == 3000 + 2000 + 500 + 2000
 
 
-def test_one_warp_and_wide_grids_are_served_apart():
+def test_one_warp_and_wide_grids_in_one_server():
+    """A server holding a 30-point grid (the persistent kernel) and the 112-point
+    grid (one wide launch per scan): scans of both kinds, interleaved in the
+    queue, each equal to pm_invert_batch's result on its grid bit for bit; the
+    persistent kernel is closed before each wide scan and relaunched after it."""
     G = wide_grids()
-    with pytest.raises(pm.PmError) as e:
-        pm.Server(WIDE_LINE, [G[0], grids()[2]], hbm_budget_bytes=1 << 28)
-    assert e.value.code == -95  # PM_ENOTSUP
+    lam30 = G[0].lam[41:71].copy()
+    g30 = pm.Grid(lam=lam30, psf=pm.psf_gaussian(25.0, lam30), guess=G[0].guess, noise=NOISE64, fix=FIX9, nterms=9)
+    both = [g30, G[0]]
+    cubes_ = {"a": wide_cube(g30, 4000, 81), "b": wide_cube(g30, 700, 82), "w": wide_cube(G[0], 1500, 83)}
+    order = [(0, "a"), (1, "w"), (0, "b"), (1, "w"), (0, "a")]
+    with pm.Server(WIDE_LINE, both, hbm_budget_bytes=1 << 30, max_inflight=8, linger_ms=20.0) as srv:
+        ids = [srv.submit(g, cubes_[c]) for g, c in order]
+        res = [srv.wait(i) for i in ids]
+        st = srv.stats()
+    for (g, c), r in zip(order, res):
+        with pm.Inverter(WIDE_LINE, both[g].lam, both[g].psf, noise=NOISE64, fix=FIX9, nterms=9,
+                         precision=pm.PREC_FP32) as inv:
+            b = inv.invert(cubes_[c], both[g].guess)
+        _eq(r, b)
+    assert st["scans_done"] == 5 and st["pixels_done"] == 4000 + 1500 + 700 + 1500 + 4000
+    assert st["kernel_launches"] >= 4  # two wide launches, and the persistent kernel around them
 
 
 # ---- stray light, as the reference's real-time loop applies its StrayLightFile ----
