@@ -53,6 +53,22 @@ __device__ long long next_ticket(PmStreamQ* q, long long limit_ns) {
 }
 
 
+// A published ticket if one is free now, else -1 (without waiting; *drained:
+// the queue is closed and every published ticket is taken).  The counter never
+// passes the published count, so a ticket taken here is always published.
+__device__ __forceinline__ long long try_ticket(PmStreamQ* q, bool* drained) {
+  unsigned long long n = *reinterpret_cast<volatile unsigned long long*>(&q->next);
+  unsigned long long avail = ld_acquire(&q->avail);
+  while (n < avail) {
+    const unsigned long long prev = atomicCAS(&q->next, n, n + 1);
+    if (prev == n) return (long long)n;
+    n = prev;
+  }
+  // closed is written after the last publication: closed and nothing left means drained
+  *drained = ld_acquire(&q->closed) && n >= ld_acquire(&q->avail);
+  return -1;
+}
+
 // The grids a launch serves, by value: all PMK_MAX_GRIDS slots for a server's
 // mixed launch, one slot otherwise (a 7 KB rather than 28 KB parameter block).
 template <int NG>
@@ -150,10 +166,13 @@ __global__ void __launch_bounds__(128, MINB) invert_stream_kernel(
 // with block barriers between them), so that at any time the block executes
 // one phase's code and the warps of an SM sub-partition share its instruction
 // cache lines.  A warp whose pixel is finished takes the next ticket before
-// the next pass; warps without one (the queue is drained) keep taking part in
-// the barriers until every warp of the block is done.  MULTI: the launch serves
-// up to PMK_MAX_GRIDS grids (a server's), each warp on its pixel's grid.  Per
-// pixel the arithmetic is invert_pixel's.
+// the next pass if one is published; it never waits for one while other warps
+// of its block hold pixels (they would wait for it at the barrier, and in a
+// server the publication it waits for may depend on their pixels finishing).
+// A block none of whose warps holds a pixel sleeps between attempts, up to the
+// wait limit (then PMQ_ERR_WAIT), and ends once the queue is closed and
+// drained.  MULTI: the launch serves up to PMK_MAX_GRIDS grids (a server's),
+// each warp on its pixel's grid.  Per pixel the arithmetic is invert_pixel's.
 template <typename R, int KT, int W, bool MULTI, bool MAC, bool PIXGRID, bool ZM = false>
 __global__ void __launch_bounds__(32 * W, 16 / W) invert_lockstep_kernel(
     const __grid_constant__ GridParams<MULTI ? PMK_MAX_GRIDS : 1> GS, const PmStreamIO sio) {
@@ -169,16 +188,20 @@ __global__ void __launch_bounds__(32 * W, 16 / W) invert_lockstep_kernel(
     sm.grid_cur = -1;  // grid of the previous pixel: the padded rows are re-zeroed on a change
   }
   __syncthreads();
+  __shared__ int s_stop;
   PixelLM<R> L;
   int gi = 0;
   bool have = false, drained = false;
+  long long idle_since = -1;
+  unsigned sleep_ns = 32;
   while (true) {
     while (!have && !drained) {
       long long t = 0;
-      if (lane == 0) t = next_ticket(sio.q, sio.wait_limit_ns);
+      bool dr = false;
+      if (lane == 0) t = try_ticket(sio.q, &dr);
       t = __shfl_sync(kFull, t, 0);
       if (t < 0) {
-        drained = true;
+        drained = __shfl_sync(kFull, dr ? 1 : 0, 0) != 0;
         break;
       }
       const PmJob* jp = nullptr;
@@ -222,7 +245,24 @@ __global__ void __launch_bounds__(32 * W, 16 / W) invert_lockstep_kernel(
         have = true;
       }
     }
-    if (!__syncthreads_or(have)) break;
+    if (!__syncthreads_or(have)) {
+      // no warp of the block holds a pixel: done once every warp has seen the
+      // queue closed and drained, else wait for a publication (bounded)
+      if (__syncthreads_and(drained)) break;
+      if (threadIdx.x == 0) {
+        const long long now = global_ns();
+        if (idle_since < 0) idle_since = now;
+        s_stop = now - idle_since > sio.wait_limit_ns;
+        if (s_stop) atomicExch(&sio.q->err, (unsigned long long)PMQ_ERR_WAIT);
+      }
+      __nanosleep(sleep_ns);
+      sleep_ns = sleep_ns < 2048 ? 2 * sleep_ns : 2048;
+      __syncthreads();
+      if (s_stop) break;
+      continue;
+    }
+    idle_since = -1;
+    sleep_ns = 32;
     const PmParams& P = GS.g[gi];
     if (have) lm_solve<R, KT>(P, sm, lane, L);
     __syncthreads();
