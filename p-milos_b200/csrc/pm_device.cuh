@@ -827,29 +827,15 @@ __device__ __forceinline__ R ne_entry(const R (&d)[KT][4], const R (&cw)[4], con
     return R(0);
   } else {
     constexpr int a = ne_row(E, KT), b = ne_col(E, KT);
-    if constexpr (sizeof(R) == 4) {
-      // FP32: Stokes pairs in packed f32x2 operations; dw = d * cw (row a's
-      // weighted RFs, a common subexpression of the row's entries) or rw
-      const float2 w01 = a < KT ? __fmul2_rn(make_float2(d[a < KT ? a : 0][0], d[a < KT ? a : 0][1]),
-                                             make_float2(cw[0], cw[1]))
-                                : make_float2(rw[0], rw[1]);
-      const float2 w23 = a < KT ? __fmul2_rn(make_float2(d[a < KT ? a : 0][2], d[a < KT ? a : 0][3]),
-                                             make_float2(cw[2], cw[3]))
-                                : make_float2(rw[2], rw[3]);
-      float2 p = __fmul2_rn(w01, make_float2(d[b][0], d[b][1]));
-      p = __ffma2_rn(w23, make_float2(d[b][2], d[b][3]), p);
-      return p.x + p.y;
+    R acc = 0;
+    if constexpr (a < KT) {
+#pragma unroll
+      for (int s = 0; s < 4; ++s) acc = fma(d[a][s] * d[b][s], cw[s], acc);
     } else {
-      R acc = 0;
-      if constexpr (a < KT) {
 #pragma unroll
-        for (int s = 0; s < 4; ++s) acc = fma(d[a][s] * d[b][s], cw[s], acc);
-      } else {
-#pragma unroll
-        for (int s = 0; s < 4; ++s) acc = fma(rw[s], d[b][s], acc);
-      }
-      return acc;
+      for (int s = 0; s < 4; ++s) acc = fma(rw[s], d[b][s], acc);
     }
+    return acc;
   }
 }
 

@@ -53,19 +53,20 @@ __device__ long long next_ticket(PmStreamQ* q, long long limit_ns) {
 }
 
 
-// A published ticket if one is free now, else -1 (without waiting; *drained:
-// the queue is closed and every published ticket is taken).  The counter never
-// passes the published count, so a ticket taken here is always published.
-__device__ __forceinline__ long long try_ticket(PmStreamQ* q, bool* drained) {
-  unsigned long long n = *reinterpret_cast<volatile unsigned long long*>(&q->next);
-  unsigned long long avail = ld_acquire(&q->avail);
-  while (n < avail) {
-    const unsigned long long prev = atomicCAS(&q->next, n, n + 1);
-    if (prev == n) return (long long)n;
-    n = prev;
+// The lock-step kernel's ticket, without waiting.  A warp draws its next ticket
+// with one atomicAdd (as next_ticket does: the counter may run past the
+// published count, so draws never contend beyond one atomic each) and holds it
+// in *held until it is published: returns it then, else -1, and *drained once
+// the queue is closed with the held ticket beyond the last publication (closed
+// is written after the last publication, so that ticket is never published).
+__device__ __forceinline__ long long poll_ticket(PmStreamQ* q, long long* held, bool* drained) {
+  if (*held < 0) *held = (long long)atomicAdd(&q->next, 1ull);
+  const unsigned long long t = (unsigned long long)*held;
+  if (t < ld_acquire(&q->avail)) {
+    *held = -1;
+    return (long long)t;
   }
-  // closed is written after the last publication: closed and nothing left means drained
-  *drained = ld_acquire(&q->closed) && n >= ld_acquire(&q->avail);
+  *drained = ld_acquire(&q->closed) && t >= ld_acquire(&q->avail);
   return -1;
 }
 
@@ -165,10 +166,11 @@ __global__ void __launch_bounds__(128, MINB) invert_stream_kernel(
 // the LM loop together, one phase at a time (lm_solve, lm_synth, lm_update,
 // with block barriers between them), so that at any time the block executes
 // one phase's code and the warps of an SM sub-partition share its instruction
-// cache lines.  A warp whose pixel is finished takes the next ticket before
-// the next pass if one is published; it never waits for one while other warps
-// of its block hold pixels (they would wait for it at the barrier, and in a
-// server the publication it waits for may depend on their pixels finishing).
+// cache lines.  A warp whose pixel is finished draws the next ticket before
+// the next pass and starts on it once it is published; it never waits for a
+// publication while other warps of its block hold pixels (they would wait for
+// it at the barrier, and in a server the publication it waits for may depend on
+// their pixels finishing).
 // A block none of whose warps holds a pixel sleeps between attempts, up to the
 // wait limit (then PMQ_ERR_WAIT), and ends once the queue is closed and
 // drained.  MULTI: the launch serves up to PMK_MAX_GRIDS grids (a server's),
@@ -192,13 +194,13 @@ __global__ void __launch_bounds__(32 * W, 16 / W) invert_lockstep_kernel(
   PixelLM<R> L;
   int gi = 0;
   bool have = false, drained = false;
-  long long idle_since = -1;
+  long long idle_since = -1, held = -1;  // held: lane 0's drawn, not yet published ticket
   unsigned sleep_ns = 32;
   while (true) {
     while (!have && !drained) {
       long long t = 0;
       bool dr = false;
-      if (lane == 0) t = try_ticket(sio.q, &dr);
+      if (lane == 0) t = poll_ticket(sio.q, &held, &dr);
       t = __shfl_sync(kFull, t, 0);
       if (t < 0) {
         drained = __shfl_sync(kFull, dr ? 1 : 0, 0) != 0;

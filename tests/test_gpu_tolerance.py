@@ -55,7 +55,7 @@ IDS = ["c1", "c2", "c3-6pt", "c3-15pt", "c3-30pt", "c4-112pt"]
 # table for the grids that sample the line (15 to 112 points), one for the
 # 6-point grid, which has no sample at the line centre and 24 data for 9
 # parameters.
-_SAMPLED = {0: 3e-2, 1: 0.5, 2: 2e-4, 3: 5e-3, 4: 1e-2, 5: 0.1, 6: 1.0, 7: 3e-2, 8: 1e-2, 10: 1e-4}
+_SAMPLED = {0: 5e-2, 1: 0.5, 2: 2e-4, 3: 5e-3, 4: 1e-2, 5: 0.1, 6: 1.0, 7: 5e-2, 8: 2e-2, 10: 1e-4}
 _SIX = {0: 0.3, 1: 200.0, 2: 0.3, 3: 0.6, 4: 0.05, 5: 1.0, 6: 40.0, 7: 0.06, 8: 0.02}
 FP32_TOL = {"c1": _SAMPLED, "c2": _SAMPLED, "c3-6pt": _SIX, "c3-15pt": _SAMPLED, "c3-30pt": _SAMPLED,
             "c4-112pt": _SAMPLED}
