@@ -341,6 +341,10 @@ struct alignas(16) WarpSmem {
   long long job_k;
   int grid_cur;
   int xs_dirty;  // xs holds macroturbulence data: restore its zero padding before psf_rows
+  // the lock-step kernel's ticket state: the last published count seen and the
+  // first ticket and pixel count of `job`
+  unsigned long long avail_seen, job_t0, job_n;
+  unsigned long long pad_;
 };
 
 // The 16-byte vector loads of psf_rows and rf_correlate need every per-warp

@@ -906,7 +906,10 @@ int run_invert(pm_ctx* c, PmIO io, float* kernel_ms) {
   job.iters = io.iters_out;
   job.status = io.status_out;
   job.spectra = io.spectra_out;
-  job.model_in = nullptr;  // classical estimates in the kernel, as on every one-warp batch path
+  // every pixel is on the device before the launch: the classical estimates come
+  // from a pre-pass launch (the LM kernel reads them through model_in), which
+  // keeps their FP64 code out of the LM kernel's instruction stream
+  job.model_in = c->P.classical ? io.models_out : nullptr;
   job.lambda = io.lambda_pix;
   std::memset(&hc->qinit, 0, sizeof hc->qinit);
   hc->qinit.avail = (unsigned long long)io.npix;
@@ -923,6 +926,10 @@ int run_invert(pm_ctx* c, PmIO io, float* kernel_ms) {
   sio.first_job = 0;
   sio.wait_limit_ns = 20000000000LL;
   PM_CUDA(cudaEventRecord(c->k0, c->stream), "event");
+  if (c->P.classical) {
+    rc = pmk_classical_prepass(c->P, io.spectro, io.models_out, io.npix, c->stream, c->num_sms, io.lambda_pix);
+    if (rc != PM_OK) return fail(rc, "%s", pmk_last_cuda_error());
+  }
   rc = pmk_invert_stream(*c->gs, sio, c->precision, c->tuning.variant, c->tuning.warps_per_block, false, c->stream,
                          c->num_sms, nullptr, 0, io.lambda_pix != nullptr);
   if (rc != PM_OK) return fail(rc, "%s", pmk_last_cuda_error());

@@ -23,7 +23,10 @@ __global__ void __launch_bounds__(256) classical_prepass_kernel(const __grid_con
     double g[11];
 #pragma unroll
     for (int i = 0; i < 11; ++i) g[i] = P.guess[i];
-    classical<true>(P, O, lane, valid, dl, g);
+    // the LM kernels' own instance when they follow (the same code as their
+    // in-kernel estimates); the estimates-only branch otherwise
+    if (P.miter < 0) classical<true>(P, O, lane, valid, dl, g);
+    else classical<false>(P, O, lane, valid, dl, g);
     double mine = g[0];
 #pragma unroll
     for (int i = 1; i < 11; ++i)

@@ -53,23 +53,6 @@ __device__ long long next_ticket(PmStreamQ* q, long long limit_ns) {
 }
 
 
-// The lock-step kernel's ticket, without waiting.  A warp draws its next ticket
-// with one atomicAdd (as next_ticket does: the counter may run past the
-// published count, so draws never contend beyond one atomic each) and holds it
-// in *held until it is published: returns it then, else -1, and *drained once
-// the queue is closed with the held ticket beyond the last publication (closed
-// is written after the last publication, so that ticket is never published).
-__device__ __forceinline__ long long poll_ticket(PmStreamQ* q, long long* held, bool* drained) {
-  if (*held < 0) *held = (long long)atomicAdd(&q->next, 1ull);
-  const unsigned long long t = (unsigned long long)*held;
-  if (t < ld_acquire(&q->avail)) {
-    *held = -1;
-    return (long long)t;
-  }
-  *drained = ld_acquire(&q->closed) && t >= ld_acquire(&q->avail);
-  return -1;
-}
-
 // The grids a launch serves, by value: all PMK_MAX_GRIDS slots for a server's
 // mixed launch, one slot otherwise (a 7 KB rather than 28 KB parameter block).
 template <int NG>
@@ -166,11 +149,14 @@ __global__ void __launch_bounds__(128, MINB) invert_stream_kernel(
 // the LM loop together, one phase at a time (lm_solve, lm_synth, lm_update,
 // with block barriers between them), so that at any time the block executes
 // one phase's code and the warps of an SM sub-partition share its instruction
-// cache lines.  A warp whose pixel is finished draws the next ticket before
-// the next pass and starts on it once it is published; it never waits for a
-// publication while other warps of its block hold pixels (they would wait for
-// it at the barrier, and in a server the publication it waits for may depend on
-// their pixels finishing).
+// cache lines.  A warp draws its next ticket (one atomicAdd) as soon as it
+// starts a pixel and starts on that ticket, once it is published, when the pixel
+// is finished; it never waits for a publication while other warps of its block
+// hold pixels (they would wait for it at the barrier, and in a server the
+// publication it waits for may depend on their pixels finishing).  Drawing
+// ahead and remembering the last published count and the previous ticket's job
+// keep the global-memory round trips of taking a ticket off the block's
+// critical path.
 // A block none of whose warps holds a pixel sleeps between attempts, up to the
 // wait limit (then PMQ_ERR_WAIT), and ends once the queue is closed and
 // drained.  MULTI: the launch serves up to PMK_MAX_GRIDS grids (a server's),
@@ -194,36 +180,70 @@ __global__ void __launch_bounds__(32 * W, 16 / W) invert_lockstep_kernel(
   PixelLM<R> L;
   int gi = 0;
   bool have = false, drained = false;
-  long long idle_since = -1, held = -1;  // held: lane 0's drawn, not yet published ticket
+  long long idle_since = -1;
   unsigned sleep_ns = 32;
+  // lane 0's drawn, not yet started ticket (drawn as soon as the previous one is
+  // taken, so the atomic's round trip overlaps a pixel's work); the last
+  // published count seen and the previous ticket's job live in shared memory
+  long long held = -1;
+  if (lane == 0) {
+    sm.avail_seen = 0;
+    sm.job = nullptr;
+  }
+  __syncwarp();
   while (true) {
     while (!have && !drained) {
-      long long t = 0;
+      long long t = -1;
       bool dr = false;
-      if (lane == 0) t = poll_ticket(sio.q, &held, &dr);
+      if (lane == 0) {
+        if (held < 0) held = (long long)atomicAdd(&sio.q->next, 1ull);
+        if ((unsigned long long)held >= sm.avail_seen) sm.avail_seen = ld_acquire(&sio.q->avail);
+        if ((unsigned long long)held < sm.avail_seen) {
+          t = held;
+          held = (long long)atomicAdd(&sio.q->next, 1ull);  // the next one, for the next refill
+        } else {
+          // closed is written after the last publication: the held ticket is then never published
+          dr = ld_acquire(&sio.q->closed) && (unsigned long long)held >= ld_acquire(&sio.q->avail);
+        }
+      }
       t = __shfl_sync(kFull, t, 0);
       if (t < 0) {
         drained = __shfl_sync(kFull, dr ? 1 : 0, 0) != 0;
         break;
       }
-      const PmJob* jp = nullptr;
-      unsigned long long t0 = 0;
-      long long k = sm.job_k;
-      for (int guard = 0; guard <= sio.jobs_cap; ++guard, ++k) {
-        const PmJob* c = sio.jobs + (k % sio.jobs_cap);
-        const unsigned long long c0 = __ldcg(&c->t0);
-        const unsigned long long cn = __ldcg(reinterpret_cast<const unsigned long long*>(&c->npix));
-        if ((unsigned long long)t >= c0 && (unsigned long long)t < c0 + cn) {
-          jp = c;
-          t0 = c0;
-          break;
+      // the ticket's job: usually the previous ticket's, else walk the ring forward
+      int found = 0;
+      if (lane == 0) {
+        if (sm.job && (unsigned long long)t >= sm.job_t0 && (unsigned long long)t < sm.job_t0 + sm.job_n) {
+          found = 1;
+        } else {
+          long long k = sm.job_k;
+          for (int guard = 0; guard <= sio.jobs_cap; ++guard, ++k) {
+            const PmJob* c = sio.jobs + (k % sio.jobs_cap);
+            const unsigned long long c0 = __ldcg(&c->t0);
+            const unsigned long long cn = __ldcg(reinterpret_cast<const unsigned long long*>(&c->npix));
+            if ((unsigned long long)t >= c0 && (unsigned long long)t < c0 + cn) {
+              sm.job = c;
+              sm.job_t0 = c0;
+              sm.job_n = cn;
+              sm.job_k = k;
+              found = 1;
+              break;
+            }
+          }
+        }
+        if (found) {
+          sm.pix = (unsigned long long)t - sm.job_t0;
+        } else {
+          atomicExch(&sio.q->err, (unsigned long long)PMQ_ERR_JOB);
         }
       }
-      if (!jp) {
-        if (lane == 0) atomicExch(&sio.q->err, (unsigned long long)PMQ_ERR_JOB);
+      if (!__shfl_sync(kFull, found, 0)) {
         drained = true;
         break;
       }
+      __syncwarp();
+      const PmJob* jp = sm.job;
       gi = MULTI ? __ldcg(&jp->grid) : 0;
       if (gi != sm.grid_cur) {
         for (int e = lane; e < 4 * XSR; e += 32) (&sm.xs[0][0])[e] = R(0);
@@ -232,11 +252,6 @@ __global__ void __launch_bounds__(32 * W, 16 / W) invert_lockstep_kernel(
           sm.grid_cur = gi;
           sm.xs_dirty = 0;
         }
-      }
-      if (lane == 0) {
-        sm.job_k = k;
-        sm.job = jp;
-        sm.pix = (unsigned long long)t - t0;
       }
       __syncwarp();
       lm_begin<R, PIXGRID>(GS.g[gi], sm, lane, L);
