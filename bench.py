@@ -14,9 +14,11 @@ this library's FP64 path instead.
 JSON line (rank 0):
   value    pixels/s with the cube resident in HBM (CUDA-event time of the
            inversion kernel; L2 flushed between steps)
-  e2e      pixels/s through the public C ABI with pinned host buffers: the
-           host->device copy of the cube and the device->host copy of models,
-           chi^2 and iterations are inside the timed region
+  e2e      pixels/s through the public call (Inverter.invert -> pm_invert_batch)
+           with the cube and the result arrays in pinned host memory, timed by the
+           wall clock around the call: the host->device copy of the cube and the
+           device->host transfer of models, chi^2 and iterations (stored by the
+           kernel into the pinned arrays, or copied back) are inside it
   plain    the FP64 plain form on the same cube (eigen solve, and Cholesky)
   roofline FP32-pipe fraction from the frozen flop model (below: add/sub/mul/div 1,
            FMA 2, transcendentals 0, per pixel and iteration)
@@ -610,9 +612,11 @@ def main():
         v, wpb = (int(x) for x in args.tuning.split(","))
         inv32.tuning = {"variant": v, "warps_per_block": wpb}
     elif not args.no_autotune:
-        ns = min(w.npix, 32768)
-        sample = obs[:ns] if obs is not None else obs_d[:ns].cpu().numpy()
-        inv32.autotune(sample, w.guess, slight=sl_h, reps=2)
+        ns = min(w.npix, 65536)  # configurations 0-2: the whole cube (a smaller one has a different tail)
+        sample = torch.from_numpy(np.ascontiguousarray(obs[:ns])) if obs is not None else obs_d[:ns].cpu()
+        sample = sample.pin_memory()  # pinned, as e2e's input
+        inv32.autotune(sample.numpy(), w.guess, slight=sl_h, reps=3)
+        del sample
     tuning = inv32.tuning
 
     def barrier():
@@ -658,16 +662,25 @@ def main():
         else:
             pinned = torch.from_numpy(obs).pin_memory()
         obs_pinned = pinned.numpy()
+        # result arrays in pinned host memory, allocated once (as a host's scan loop would)
+        res = {"models": torch.empty((w.npix, 11), dtype=torch.float64, pin_memory=True).numpy(),
+               "chisq": torch.empty(w.npix, dtype=torch.float32, pin_memory=True).numpy(),
+               "iters": torch.empty(w.npix, dtype=torch.int32, pin_memory=True).numpy()}
         for _ in range(max(1, args.warmup)):
-            inv32.invert(obs_pinned, w.guess, slight=sl_h, want_spectra=False, want_status=False)
+            inv32.invert(obs_pinned, w.guess, slight=sl_h, want_spectra=False, want_status=False, out=res)
         e2e_ms = []
         for _ in range(args.steps):
             flush.fill_(1)
             torch.cuda.synchronize()
-            inv32.invert(obs_pinned, w.guess, slight=sl_h, want_spectra=False, want_status=False)
-            e2e_ms.append(inv32.stats()["total_ms"])
+            t0 = time.perf_counter()  # wall clock around the public call: copies, kernel, results in host memory
+            inv32.invert(obs_pinned, w.guess, slight=sl_h, want_spectra=False, want_status=False, out=res)
+            e2e_ms.append((time.perf_counter() - t0) * 1000.0)
+        if dist is not None:
+            t = torch.tensor([float(np.mean(e2e_ms))], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = [float(t.item())]
         e2e_v = world * w.npix / (float(np.mean(e2e_ms)) / 1000.0)
-        del obs_pinned, pinned
+        del obs_pinned, pinned, res
     h2d = cube_bytes
     d2h = w.npix * (11 * 8 + 4 + 4)
 
@@ -700,10 +713,10 @@ def main():
     hbm_peak = json.load(open(peaks_path))["hbm_gbs"] if os.path.exists(peaks_path) else 6650.0
     hbm_bytes = w.npix * args.steps * (16 * w.nl + 11 * 8 + 8)
     # DRAM bytes per pixel of the FP32 inversion kernel from one ncu capture of a
-    # smaller cube of the same workload, scaled to this launch by its pixel count:
-    # 355.2 MB for 524,288 pixels of the 30-point grid (dram__bytes_read.sum +
-    # dram__bytes_write.sum), 132.7 MB for 65,536 pixels of the 112-point grid
-    traffic = {1: 677.5, 4: 2025.0}.get(args.config) if w.nl in (30, 112) else None
+    # cube of the same workload, scaled to this launch by its pixel count: 356.9 MB
+    # for 524,288 pixels of the 30-point grid (lock-step kernel, dram__bytes_read.sum
+    # + dram__bytes_write.sum), 132.7 MB for 65,536 pixels of the 112-point grid
+    traffic = {1: 680.7, 4: 2025.0}.get(args.config) if w.nl in (30, 112) else None
     traffic = traffic * w.npix if traffic else None
     roofline = {"bound": "fp32", "achieved": round(achieved, 3), "peak": round(peak_fp32, 2), "unit": "TFLOP/s",
                 "frac": round(achieved / peak_fp32, 4), "traffic": traffic,

@@ -161,9 +161,11 @@ typedef struct pm_tuning {
                            (128 registers; the warps of a block run each LM phase together, so they share
                            the phase's instruction-cache lines; nine or ten free parameters without a
                            v_mac row, one-warp grids; elsewhere 2 runs as 1) */
-  int staging_depth;    /* host-buffer calls on grids of <= 32 wavelengths: the cube goes in this many
-                           pieces; one persistent launch inverts them as the copy stream publishes each
-                           piece (1..PM_STAGING_MAX); 0 = copy everything, then launch */
+  int staging_depth;    /* host-buffer calls on grids of <= 32 wavelengths: the cube goes in at most
+                           this many pieces, each twice the one before; one persistent launch inverts
+                           them as the copy stream publishes each piece (1..PM_STAGING_MAX); 0 = copy
+                           everything, then launch.  Output buffers in pinned, mapped host memory
+                           (cudaHostAlloc) receive each pixel's results from the kernel directly */
   int warps_per_block;  /* pixels (one warp each) per block of the one-warp kernels: 1, 2 or 4; with
                            variant 2: 4, 8 or 16 */
   int graphs;           /* 1: host-buffer calls of at most PM_GRAPH_MAX_PIXELS pixels on grids of <= 32

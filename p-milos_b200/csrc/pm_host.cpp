@@ -495,24 +495,39 @@ int stream_resources(pm_ctx* c) {
   return PM_OK;
 }
 
-// One resident chunk of a host-buffer inversion, pipelined in `staging_depth`
-// pieces (multiples of 32 pixels, so no 128-byte line of the cube spans two):
-// the copy stream brings piece k + 1 in while the kernel stream inverts piece k
-// (classical pre-pass, then the streamed kernel with the piece fully published)
-// and copies piece k's results back.  Each piece is its own launch because a
-// pre-pass cannot run beside a persistent kernel that holds the SMs, and making
-// the estimates inside the LM kernel costs more than the copies this hides.
+// The device address of host range [p, p + bytes) when the whole range is
+// pinned, mapped memory (cudaHostAlloc, or cudaHostRegister with mapping), else
+// nullptr: a kernel can then store results into it directly.
+void* mapped_host_range(const void* p, size_t bytes) {
+  if (!p || bytes == 0) return nullptr;
+  cudaPointerAttributes a{}, b{};
+  const char* last = static_cast<const char*>(p) + bytes - 1;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess || cudaPointerGetAttributes(&b, last) != cudaSuccess) {
+    cudaGetLastError();  // not a pointer CUDA knows: pageable
+    return nullptr;
+  }
+  if (a.type != cudaMemoryTypeHost || b.type != cudaMemoryTypeHost || !a.devicePointer || !b.devicePointer)
+    return nullptr;
+  if (static_cast<const char*>(b.devicePointer) - static_cast<const char*>(a.devicePointer) != ptrdiff_t(bytes - 1))
+    return nullptr;
+  return a.devicePointer;
+}
+
+// One resident chunk of a host-buffer inversion: one persistent launch fed while
+// it runs.  The cube goes to the device in up to `staging_depth` copies on the
+// copy stream, each twice the size of the one before (multiples of 32 pixels,
+// so no 128-byte line of the cube spans two), so the first publication follows
+// a copy of a few hundred pixels; after each copy the copy stream writes the
+// running pixel count into the queue's avail word, which publishes that piece's
+// tickets to the kernel already running on the kernel stream.  The kernel
+// computes each pixel's classical estimates itself (a pre-pass launch could not
+// find SM slots beside the persistent kernel).  Results go straight into the
+// caller's buffers when those are pinned and mapped (each pixel's stores cross
+// the bus as the pixel ends, nothing is left to copy after the kernel), else
+// they come back in one copy after the kernel.
 int run_streamed(pm_ctx* c, int64_t n, const float* spectro, const float* slight, int slight_mode,
                  pm_model* models_out, float* chisq_out, int* iters_out, float* best_fit_out, int* status_out,
                  float* kernel_ms, float* total_ms) {
-  // One persistent launch fed while it runs.  The cube goes to the device in
-  // `pieces` copies on the copy stream; after each copy the copy stream writes
-  // the running pixel count into the queue's avail word, which publishes that
-  // piece's tickets to the kernel already running on the kernel stream (a warp
-  // holding a ticket beyond avail waits, bounded, for its publication).  The
-  // kernel computes each pixel's classical estimates itself (a pre-pass launch
-  // could not find SM slots beside the persistent kernel).  The results come
-  // back in one copy after the kernel.
   int rc = stream_resources(c);
   if (rc != PM_OK) return rc;
   const int nl = c->P.nl;
@@ -528,21 +543,28 @@ int run_streamed(pm_ctx* c, int64_t n, const float* spectro, const float* slight
   sio.first_job = 0;
   sio.wait_limit_ns = 20000000000LL;
 
-  const int pieces = std::max(1, std::min(c->tuning.staging_depth, PM_STAGING_MAX));
-  int64_t per = (n + pieces - 1) / pieces;
-  per = std::max<int64_t>(32, (per + 31) / 32 * 32);
-  const int np = int((n + per - 1) / per);
+  // piece i holds first << i pixels (the last one the rest): at most `depth` pieces
+  const int depth = std::max(1, std::min(c->tuning.staging_depth, PM_STAGING_MAX));
+  const double units = std::ldexp(1.0, std::min(depth, 40)) - 1.0;
+  const int64_t first = std::max<int64_t>(32, (int64_t(std::ceil(double(n) / units)) + 31) / 32 * 32);
+
+  // outputs the kernel can store into directly
+  double* models_dev = static_cast<double*>(mapped_host_range(models_out, sizeof(pm_model) * n));
+  float* chisq_dev = static_cast<float*>(mapped_host_range(chisq_out, sizeof(float) * n));
+  int* iters_dev = static_cast<int*>(mapped_host_range(iters_out, sizeof(int) * n));
+  int* status_dev = status_out ? static_cast<int*>(mapped_host_range(status_out, sizeof(int) * n)) : nullptr;
+  float* spectra_dev = best_fit_out ? static_cast<float*>(mapped_host_range(best_fit_out, prof * n)) : nullptr;
 
   PmJob& job = hc->job;
   std::memset(&job, 0, sizeof job);
   job.npix = n;
   job.spectro = static_cast<const float*>(c->spectro.p);
   job.slight = slight_mode == PM_SLIGHT_PER_PIXEL ? static_cast<const float*>(c->slight.p) : nullptr;
-  job.models = static_cast<double*>(c->models.p);
-  job.chisq = static_cast<float*>(c->chisq.p);
-  job.iters = static_cast<int*>(c->iters.p);
-  job.status = status_out ? static_cast<int*>(c->status.p) : nullptr;
-  job.spectra = best_fit_out ? static_cast<float*>(c->spectra.p) : nullptr;
+  job.models = models_dev ? models_dev : static_cast<double*>(c->models.p);
+  job.chisq = chisq_dev ? chisq_dev : static_cast<float*>(c->chisq.p);
+  job.iters = iters_dev ? iters_dev : static_cast<int*>(c->iters.p);
+  job.status = status_out ? (status_dev ? status_dev : static_cast<int*>(c->status.p)) : nullptr;
+  job.spectra = best_fit_out ? (spectra_dev ? spectra_dev : static_cast<float*>(c->spectra.p)) : nullptr;
   job.model_in = nullptr;  // classical estimates in the kernel
   std::memset(&hc->qinit, 0, sizeof hc->qinit);  // nothing published, queue open
 
@@ -563,8 +585,9 @@ int run_streamed(pm_ctx* c, int64_t n, const float* spectro, const float* slight
     return fail(rc, "%s", pmk_last_cuda_error());
   }
   PM_CUDA(cudaEventRecord(c->k1, c->s_kern), "event");
-  for (int i = 0; i < np; ++i) {
-    const int64_t p0 = i * per, m = std::min(per, n - p0);
+  int64_t p0 = 0;
+  for (int i = 0; p0 < n; ++i) {
+    const int64_t m = i + 1 < PM_STAGING_MAX ? std::min(first << std::min(i, 40), n - p0) : n - p0;
     PM_CUDA(cudaMemcpyAsync(static_cast<char*>(c->spectro.p) + prof * p0, spectro + p0 * 4 * nl, prof * m,
                             cudaMemcpyHostToDevice, c->s_copy),
             "spectro H2D");
@@ -577,17 +600,21 @@ int run_streamed(pm_ctx* c, int64_t n, const float* spectro, const float* slight
     PM_CUDA(cudaMemcpyAsync(&q->avail, &hc->piece_avail[i], sizeof(unsigned long long), cudaMemcpyHostToDevice,
                             c->s_copy),
             "publish");
+    p0 += m;
   }
   // closed after the last publication: warps holding tickets beyond n exit
   PM_CUDA(cudaMemcpyAsync(&q->closed, &hc->one, sizeof(unsigned long long), cudaMemcpyHostToDevice, c->s_copy),
           "close");
-  PM_CUDA(cudaMemcpyAsync(models_out, job.models, sizeof(pm_model) * n, cudaMemcpyDeviceToHost, c->s_kern),
-          "models D2H");
-  PM_CUDA(cudaMemcpyAsync(chisq_out, job.chisq, sizeof(float) * n, cudaMemcpyDeviceToHost, c->s_kern), "chisq D2H");
-  PM_CUDA(cudaMemcpyAsync(iters_out, job.iters, sizeof(int) * n, cudaMemcpyDeviceToHost, c->s_kern), "iters D2H");
-  if (best_fit_out)
+  if (!models_dev)
+    PM_CUDA(cudaMemcpyAsync(models_out, job.models, sizeof(pm_model) * n, cudaMemcpyDeviceToHost, c->s_kern),
+            "models D2H");
+  if (!chisq_dev)
+    PM_CUDA(cudaMemcpyAsync(chisq_out, job.chisq, sizeof(float) * n, cudaMemcpyDeviceToHost, c->s_kern), "chisq D2H");
+  if (!iters_dev)
+    PM_CUDA(cudaMemcpyAsync(iters_out, job.iters, sizeof(int) * n, cudaMemcpyDeviceToHost, c->s_kern), "iters D2H");
+  if (best_fit_out && !spectra_dev)
     PM_CUDA(cudaMemcpyAsync(best_fit_out, job.spectra, prof * n, cudaMemcpyDeviceToHost, c->s_kern), "best fit D2H");
-  if (status_out)
+  if (status_out && !status_dev)
     PM_CUDA(cudaMemcpyAsync(status_out, job.status, sizeof(int) * n, cudaMemcpyDeviceToHost, c->s_kern),
             "status D2H");
   PM_CUDA(cudaMemcpyAsync(&hc->qread, q, sizeof(PmStreamQ), cudaMemcpyDeviceToHost, c->s_kern), "queue D2H");
@@ -1216,9 +1243,18 @@ extern "C" int pm_autotune(pm_ctx* c, int64_t npix, const float* spectro, const 
   if (!dg.ok()) return cuda_fail(dg.err, "pm_autotune: selecting the context's device", PM_ENODEV);
   if (npix < 1) return fail(PM_EINVAL, "pm_autotune: npix=%lld", (long long)npix);
   reps = std::max(1, std::min(reps, 16));
-  std::vector<pm_model> models(static_cast<size_t>(npix));
-  std::vector<float> chi(static_cast<size_t>(npix));
-  std::vector<int> its(static_cast<size_t>(npix));
+  // results in pinned host memory, so that the candidates differ only in what they tune
+  struct PinnedOut {
+    void* p = nullptr;
+    ~PinnedOut() {
+      if (p) cudaFreeHost(p);
+    }
+  } out_buf;
+  const size_t out_bytes = (sizeof(pm_model) + sizeof(float) + sizeof(int)) * size_t(npix);
+  PM_CUDA(cudaHostAlloc(&out_buf.p, out_bytes, cudaHostAllocDefault), "pm_autotune: pinned results");
+  pm_model* models = static_cast<pm_model*>(out_buf.p);
+  float* chi = reinterpret_cast<float*>(models + npix);
+  int* its = reinterpret_cast<int*>(chi + npix);
   std::vector<pm_tuning> cands;
   const bool fp32 = c->precision == PM_PREC_FP32;
   for (int variant : {0, 1, 2}) {
@@ -1238,8 +1274,8 @@ extern "C" int pm_autotune(pm_ctx* c, int64_t npix, const float* spectro, const 
     c->tuning = t;
     std::vector<double> ms;
     for (int r = 0; r <= reps; ++r) {
-      const int rc = pm_invert_batch(c, npix, spectro, slight, slight_mode, guess, models.data(), chi.data(),
-                                     its.data(), nullptr, nullptr, PM_MEM_HOST);
+      const int rc = pm_invert_batch(c, npix, spectro, slight, slight_mode, guess, models, chi, its, nullptr,
+                                     nullptr, PM_MEM_HOST);
       if (rc != PM_OK) {
         c->tuning = saved;
         return rc;

@@ -308,11 +308,18 @@ class Inverter:
 
     # ---- batched inversion ----
     def invert(self, spectro, guess, *, slight=None, slight_mode=None, want_spectra=True, want_status=True,
-               lam=None):
+               lam=None, out=None):
         """Invert [npix][4][nl] float32 profiles.  numpy in -> numpy out (host staging);
         torch CUDA in -> torch CUDA out (no copies).  lam: [npix][nl] absolute
-        wavelengths of each pixel (pm_invert_batch_grids) instead of the grid."""
+        wavelengths of each pixel (pm_invert_batch_grids) instead of the grid.
+        out (numpy input only): preallocated C-contiguous result arrays, a dict
+        with "models" [npix][11] float64, "chisq" [npix] float32, "iters" [npix]
+        int32 and, when wanted, "spectra" [npix][4][nl] float32 and "status" [npix]
+        int32; in pinned, mapped host memory (e.g. torch's pin_memory) the kernel
+        stores the results into them directly."""
         if _is_torch(spectro):
+            if out is not None:
+                raise ValueError("out= takes host arrays; device inputs return device tensors")
             return self._invert_device(spectro, guess, slight, slight_mode, want_spectra, want_status, lam)
         obs = np.ascontiguousarray(spectro, dtype=np.float32).reshape(-1, 4, self.nl)
         npix = obs.shape[0]
@@ -322,11 +329,23 @@ class Inverter:
             if lamp.size != npix * self.nl:
                 raise ValueError("per-pixel wavelengths must be [npix][nl]")
         sl, mode = self._slight_host(slight, slight_mode, npix)
-        models = np.zeros((npix, 11), dtype=np.float64)
-        chi = np.zeros(npix, dtype=np.float32)
-        its = np.zeros(npix, dtype=np.int32)
-        sp = np.zeros((npix, 4, self.nl), dtype=np.float32) if want_spectra else None
-        stt = np.zeros(npix, dtype=np.int32) if want_status else None
+        shapes = {"models": ((npix, 11), np.float64), "chisq": ((npix,), np.float32), "iters": ((npix,), np.int32),
+                  "spectra": ((npix, 4, self.nl), np.float32), "status": ((npix,), np.int32)}
+        wanted = {"models": True, "chisq": True, "iters": True, "spectra": want_spectra, "status": want_status}
+        arr = {}
+        for k, (shape, dt) in shapes.items():
+            if not wanted[k]:
+                arr[k] = None
+            elif out is not None and k in out:
+                a = out[k]
+                if not (isinstance(a, np.ndarray) and a.dtype == dt and a.shape == shape and a.flags.c_contiguous
+                        and a.flags.writeable):
+                    raise ValueError(f"out[{k!r}] must be a writeable C-contiguous {np.dtype(dt).name} array of "
+                                     f"shape {shape}")
+                arr[k] = a
+            else:
+                arr[k] = np.zeros(shape, dtype=dt)
+        models, chi, its, sp, stt = (arr[k] for k in ("models", "chisq", "iters", "spectra", "status"))
         g = _model_struct(guess)
         outs = (ctypes.byref(g), models.ctypes.data, chi.ctypes.data, its.ctypes.data,
                 None if sp is None else sp.ctypes.data, None if stt is None else stt.ctypes.data, MEM_HOST)

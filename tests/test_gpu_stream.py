@@ -1,11 +1,12 @@
 """Host-buffer pipelining, the launch tunings and graph replay.
 
 Every one-warp inversion runs the streamed kernel.  Device-buffer calls publish
-all pixels before one launch; host-buffer calls split the cube into
-pm_tuning.staging_depth pieces, each inverted by its own launch while the next
-one is copied in.  Staging depth and pixels per block do not change the compiled
-code, so results are bit-identical across them and equal to the device-buffer
-call.  The two register budgets (pm_tuning.variant) are separately compiled
+all pixels before one launch; host-buffer calls send the cube in up to
+pm_tuning.staging_depth pieces of doubling size to one launch that inverts each
+piece once the copy stream has published it.  Staging depth, pixels per block
+and where the results are stored (device buffers copied back, or pinned host
+arrays written by the kernel) do not change the compiled code, so results are
+bit-identical across them and equal to the device-buffer call.  The two register budgets (pm_tuning.variant) are separately compiled
 kernels whose floating-point contractions may differ in the last bits: between
 them the stated FP32 tolerance applies.
 """
@@ -73,6 +74,43 @@ def test_streamed_many_pieces_large_cube():
         s = inv.stats()
     _same(a, b)
     assert s["pixels"] == obs.shape[0] and s["iterations"] == int(np.maximum(b["iters"], 0).sum())
+
+
+def test_pinned_result_arrays_are_written_by_the_kernel():
+    """Result arrays in pinned host memory (out=) receive the kernel's stores
+    directly; the results equal those of pageable arrays and of the device call bit
+    for bit, in one piece and in doubling pieces, with and without status and
+    best-fit profiles, on both kernels."""
+    c = case(1)
+    n = 3333  # above the graph path's limit: the streamed host-buffer call
+    obs = np.ascontiguousarray(np.tile(c["obs"], (n // c["obs"].shape[0] + 1, 1, 1))[:n])
+    pin = lambda shape, dt: torch.empty(shape, dtype=dt, pin_memory=True).numpy()
+    with inverter(c, pm.PREC_FP32) as inv:
+        for variant, wpb in ((1, 4), (2, 8)):
+            inv.tuning = {"variant": variant, "warps_per_block": wpb, "staging_depth": 1}
+            ref = _device_reference(inv, {**c, "obs": obs})
+            for depth in (1, 5, 64):
+                inv.tuning = {"variant": variant, "warps_per_block": wpb, "staging_depth": depth}
+                out = {"models": pin((n, 11), torch.float64), "chisq": pin((n,), torch.float32),
+                       "iters": pin((n,), torch.int32), "status": pin((n,), torch.int32),
+                       "spectra": pin((n, 4, inv.nl), torch.float32)}
+                for a in out.values():
+                    a.fill(-7)
+                r = inv.invert(obs, c["guess"], slight=c["slight"], out=out)
+                assert all(r[k] is out[k] for k in out)
+                _same(r, ref)
+                # without status and profiles: only the arrays asked for are written
+                out2 = {k: out[k] for k in ("models", "chisq", "iters")}
+                for a in out2.values():
+                    a.fill(-7)
+                r2 = inv.invert(obs, c["guess"], slight=c["slight"], want_spectra=False, want_status=False, out=out2)
+                for k in out2:
+                    assert np.array_equal(r2[k], ref[k]), k
+                # pageable arrays of the caller's own
+                r3 = inv.invert(obs, c["guess"], slight=c["slight"], out={"models": np.empty((n, 11))})
+                _same(r3, ref)
+        with pytest.raises(ValueError):
+            inv.invert(obs, c["guess"], out={"models": np.empty((n, 10))})
 
 
 def test_autotune_picks_a_valid_tuning_and_keeps_results():
