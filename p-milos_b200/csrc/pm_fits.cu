@@ -154,36 +154,53 @@ __global__ void __launch_bounds__(256) reorder_rows(const Reorder R, const unsig
   }
 }
 
-// Work item = (f tile, wavelength tile, g, h), items along f consecutive; one
-// warp per item: lane = f while loading (the input's contiguous axis), lane =
-// wavelength while storing (the output's contiguous axis).
+// Work item = (f segment, wavelength tile, g, h), segments consecutive: a run of
+// kSegTiles 32 x 32 tiles along f, the input's contiguous axis; one warp per item
+// (the item's offsets are decomposed once, not per tile; four tiles per item keep
+// enough items for every warp of the grid): lane = f while loading, lane =
+// wavelength while storing (the output's contiguous axis).  The 32 loads of a
+// tile are unconditional, so all of them are in flight at once: a partial tile
+// clamps its indices to its last row and column (those loads hit lines the tile
+// reads anyway and are never stored).
+constexpr int kSegTiles = 4;
+
 __global__ void __launch_bounds__(256) reorder_tiled(const Reorder R, int f, int g, int h,
                                                     const unsigned int* __restrict__ in, float* __restrict__ out) {
   __shared__ float tile[8][32][33];
   const int x = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const long long tf = (R.n[f] + 31) / 32, tl = (R.nl + 31) / 32;
-  const long long items = tf * tl * R.n[g] * R.n[h];
+  const long long nf = R.n[f], tl = (R.nl + 31) / 32;
+  const long long segs = (nf + 32 * kSegTiles - 1) / (32 * kSegTiles);
+  const long long items = segs * tl * R.n[g] * R.n[h];
   const long long nwarps = (long long)gridDim.x * 8;
   const long long st_l = R.st[R.ax_l], ost_f = R.ost[f];
   for (long long it = (long long)blockIdx.x * 8 + w; it < items; it += nwarps) {
-    const long long ft = it % tf, r1 = it / tf;
+    const long long sg = it % segs, r1 = it / segs;
     const long long lt = r1 % tl, r2 = r1 / tl;
     const long long cg = r2 % R.n[g], ch = r2 / R.n[g];
-    const long long f0 = ft * 32, l0 = lt * 32;
-    const int fx = int(R.n[f] - f0 < 32 ? R.n[f] - f0 : 32);
+    const long long l0 = lt * 32;
     const int lx = int(R.nl - l0 < 32 ? R.nl - l0 : 32);
-    const long long ib = cg * R.st[g] + ch * R.st[h] + l0 * st_l + f0;
-    const long long ob = cg * R.ost[g] + ch * R.ost[h] + l0 + f0 * ost_f;
-    float v[32];
+    const unsigned int* src_run = in + cg * R.st[g] + ch * R.st[h] + l0 * st_l;
+    float* dst_run = out + cg * R.ost[g] + ch * R.ost[h] + l0;
+    const long long f_end = (sg + 1) * 32 * kSegTiles < nf ? (sg + 1) * 32 * kSegTiles : nf;
+#pragma unroll 1
+    for (long long f0 = sg * 32 * kSegTiles; f0 < f_end; f0 += 32) {
+      const int fx = int(nf - f0 < 32 ? nf - f0 : 32);
+      const unsigned int* src = src_run + f0 + (x < fx ? x : fx - 1);
+      unsigned int u[32];
 #pragma unroll
-    for (int k = 0; k < 32; ++k) v[k] = (k < lx && x < fx) ? swap_be(__ldg(in + ib + x + k * st_l)) : 0.0f;
+      for (int k = 0; k < 32; ++k) {
+        u[k] = __ldg(src);
+        if (k + 1 < lx) src += st_l;
+      }
 #pragma unroll
-    for (int k = 0; k < 32; ++k) tile[w][k][x] = v[k];
-    __syncwarp();
+      for (int k = 0; k < 32; ++k) tile[w][k][x] = swap_be(u[k]);
+      __syncwarp();
+      float* dst = dst_run + f0 * ost_f + x;
 #pragma unroll 8
-    for (int k = 0; k < 32; ++k)
-      if (k < fx && x < lx) out[ob + k * ost_f + x] = tile[w][x][k];
-    __syncwarp();
+      for (int k = 0; k < 32; ++k)
+        if (k < fx && x < lx) dst[k * ost_f] = tile[w][x][k];
+      __syncwarp();
+    }
   }
 }
 
@@ -327,7 +344,8 @@ extern "C" int pm_fits_reorder(const pm_fits_cube* info, const void* data_dev, f
         if (g < 0) g = a;
         else h = a;
       }
-    const long long work = ((R.n[f] + 31) / 32) * ((R.nl + 31) / 32) * R.n[g] * R.n[h];
+    // segments of kSegTiles tiles along f, one per warp
+    const long long work = ((R.n[f] + 32 * kSegTiles - 1) / (32 * kSegTiles)) * ((R.nl + 31) / 32) * R.n[g] * R.n[h];
     const long long blocks = std::min(cap, (work + 7) / 8);
     reorder_tiled<<<unsigned(std::max(1LL, blocks)), 256, 0, s>>>(R, f, g, h, in, cube_dev);
   }
