@@ -653,7 +653,12 @@ def main():
     # e2e: host buffers (pinned) through the C ABI; copies inside the timed region
     e2e_v, e2e_note = None, None
     cube_bytes = obs_d.numel() * 4
-    if not args.no_e2e and obs is None and _mem_available() < 3 * cube_bytes:
+    room = obs is not None or _mem_available() >= 3 * cube_bytes
+    if dist is not None:  # every rank takes the same branch (the e2e leg has a collective)
+        f = torch.tensor([1 if room else 0], device="cuda", dtype=torch.int32)
+        dist.all_reduce(f, op=dist.ReduceOp.MIN)
+        room = bool(f.item())
+    if not args.no_e2e and not room:
         e2e_note = f"not measured: {cube_bytes / 2**30:.1f} GiB cube, host memory available {_mem_available() / 2**30:.1f} GiB"
     elif not args.no_e2e:
         if obs is None:
