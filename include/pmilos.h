@@ -20,7 +20,9 @@
  *  - Return codes: 0 on success, negative errno-style values on failure (PM_E*).
  *    Nothing in the library calls exit().
  *  - Buffers are owned by the caller.  Each call says where its buffers live:
- *    PM_MEM_HOST (the library copies through its own device staging buffers) or
+ *    PM_MEM_HOST (the library copies through its own device staging buffers;
+ *    result arrays in pinned, mapped host memory are written by the kernel
+ *    directly where the call streams its cube, see pm_tuning.staging_depth) or
  *    PM_MEM_DEVICE (pointers into this GPU's memory; nothing is copied).
  *  - A context may be used by one host thread at a time; separate contexts are
  *    independent.  All work of a context is ordered on the stream it was created

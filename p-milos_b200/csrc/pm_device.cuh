@@ -1506,9 +1506,22 @@ __device__ __forceinline__ void lm_begin(const PmParams& P, WarpSmem<R>& sm, int
   if constexpr (PIXGRID) L.dlp = valid ? __ldcg(ld_ptr(&jp->lambda) + p * P.nl + lane) - P.lambda0 : 0.0;
   const double dl = PIXGRID ? L.dlp : P.dl[valid ? lane : 0];
   int ghosts = 0;
+  if ((reinterpret_cast<uintptr_t>(obs) & 15) == 0) {
+    // the pixel's 4 x nl floats as nl 16-byte loads (one per lane, one
+    // instruction for the warp), redistributed to lane = wavelength through the
+    // warp's transpose buffer (idle while a pixel starts)
+    float* stage = reinterpret_cast<float*>(sm.tr);
+    if (lane < P.nl) reinterpret_cast<float4*>(stage)[lane] = __ldcg(reinterpret_cast<const float4*>(obs) + lane);
+    __syncwarp();
+#pragma unroll
+    for (int s = 0; s < 4; ++s) L.O[s] = valid ? stage[s * P.nl + lane] : 0.0f;
+    __syncwarp();
+  } else {
+#pragma unroll
+    for (int s = 0; s < 4; ++s) L.O[s] = valid ? __ldcg(obs + s * P.nl + lane) : 0.0f;
+  }
 #pragma unroll
   for (int s = 0; s < 4; ++s) {
-    L.O[s] = valid ? __ldcg(obs + s * P.nl + lane) : 0.0f;
     const bool g = valid && L.O[s] <= -1.0f;
     ghosts += __popc(__ballot_sync(kFull, g));
     L.isig[s] = R(1.0 / (g ? kGhostSigma : P.noise));
