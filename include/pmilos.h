@@ -154,14 +154,15 @@ typedef struct pm_stats {
 
 typedef struct pm_ctx pm_ctx;
 
-/* Launch choices of a context (what pm_autotune picks).  No counterpart in the
- * reference, which has no device launches to tune. */
+/* Launch choices of a context (what pm_autotune picks; a new context starts with
+ * {2, 8, 16, 1}).  No counterpart in the reference, which has no device launches
+ * to tune. */
 #define PM_STAGING_MAX 64
 typedef struct pm_tuning {
   int variant;          /* FP32 kernel of the one-warp grids: 0 = 168 registers per thread (3 blocks of 4
                            warps per SM), 1 = 128 (4 blocks per SM, a few spills), 2 = lock-step blocks
-                           (128 registers; the warps of a block run each LM phase together, so they share
-                           the phase's instruction-cache lines; nine or ten free parameters without a
+                           (128 registers; the warps of a block run each LM pass together, so they share
+                           the instruction-cache lines of its parts; nine or ten free parameters without a
                            v_mac row, one-warp grids; elsewhere 2 runs as 1) */
   int staging_depth;    /* host-buffer calls on grids of <= 32 wavelengths: the cube goes in at most
                            this many pieces, each twice the one before; one persistent launch inverts

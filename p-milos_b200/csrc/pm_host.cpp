@@ -115,7 +115,7 @@ struct SmallStage {
 struct pm_ctx {
   PmParams P;
   int precision = PM_PREC_FP32;
-  pm_tuning tuning{2, 8, 8, 1};  // lock-step blocks of 8 warps (FP32 one-warp grids), fed in 8 pieces
+  pm_tuning tuning{2, 8, 16, 1};  // lock-step blocks of 16 warps (FP32 one-warp grids), fed in up to 8 pieces
   int device = 0;
   int num_sms = 148;
   cudaStream_t stream = nullptr;

@@ -196,8 +196,8 @@ extern "C" int pm_invert_batch_noalloc(const pm_line* line, const pm_config* cfg
   sio.jobs_cap = 1;
   sio.first_job = 0;
   sio.wait_limit_ns = 20000000000LL;
-  // the launch tuning a context starts with (lock-step blocks of 8 pixels)
-  rc = pmk_invert_stream(gs, sio, cfg->precision, 2, 8, false, st, sms, nullptr);
+  // the launch tuning a context starts with (lock-step blocks of 16 pixels)
+  rc = pmk_invert_stream(gs, sio, cfg->precision, 2, 16, false, st, sms, nullptr);
   if (rc != PM_OK) return fail_after_queue(st, pmh_fail(rc, pmk_last_cuda_error()));
   if ((e = cudaMemcpyAsync(models_out, io.models_out, sizeof(pm_model) * npix, cudaMemcpyDeviceToHost, st)) !=
       cudaSuccess)

@@ -146,10 +146,12 @@ __global__ void __launch_bounds__(128, MINB) invert_stream_kernel(
 
 
 // Lock-step form of the streamed kernel: the W warps of a block advance through
-// the LM loop together, one phase at a time (lm_solve, lm_synth, lm_update,
-// with block barriers between them), so that at any time the block executes
-// one phase's code and the warps of an SM sub-partition share its instruction
-// cache lines.  A warp draws its next ticket (one atomicAdd) as soon as it
+// the LM loop together, one pass at a time, with a block barrier before the
+// damped solve (lm_solve; where finished warps take new pixels) and one before
+// the synthesis and acceptance test (lm_synth), which the update of an accepted
+// step (lm_update) follows directly, so that the block executes one part of the
+// loop's code at a time and the warps of an SM sub-partition share its
+// instruction cache lines.  A warp draws its next ticket (one atomicAdd) as soon as it
 // starts a pixel and starts on that ticket, once it is published, when the pixel
 // is finished; it never waits for a publication while other warps of its block
 // hold pixels (they would wait for it at the barrier, and in a server the
@@ -283,8 +285,10 @@ __global__ void __launch_bounds__(32 * W, 16 / W) invert_lockstep_kernel(
     const PmParams& P = GS.g[gi];
     if (have) lm_solve<R, KT>(P, sm, lane, L);
     __syncthreads();
+    // no barrier between the synthesis and the update: a warp whose step was
+    // accepted starts its response functions while slower warps finish their
+    // synthesis (a barrier here cost 2-5%)
     if (have) lm_synth<R, MAC, PIXGRID, ZM>(P, sm, lane, L);
-    __syncthreads();
     if (have) {
       lm_update<R, KT, MAC, PIXGRID, ZM>(P, bs[gi], sm, lane, L);
       if (L.finished) {

@@ -113,6 +113,25 @@ def test_pinned_result_arrays_are_written_by_the_kernel():
             inv.invert(obs, c["guess"], out={"models": np.empty((n, 10))})
 
 
+def test_unaligned_device_cube_gives_the_aligned_result():
+    """The lock-step kernel reads a pixel's profiles with 16-byte loads when the
+    cube starts on a 16-byte boundary and with 4-byte loads otherwise: a device
+    cube one float into its buffer gives the aligned copy's results bit for bit."""
+    c = case(1)
+    obs = torch.as_tensor(c["obs"], device="cuda")
+    buf = torch.empty(obs.numel() + 1, dtype=torch.float32, device="cuda")
+    buf[1:].copy_(obs.reshape(-1))
+    shifted = buf[1:].view(obs.shape)
+    assert shifted.data_ptr() % 16 != 0 and obs.data_ptr() % 16 == 0
+    with inverter(c, pm.PREC_FP32) as inv:
+        for wpb in (8, 16):
+            inv.tuning = {"variant": 2, "warps_per_block": wpb}
+            a = inv.invert(obs, c["guess"])
+            b = inv.invert(shifted, c["guess"])
+            for k in ("models", "chisq", "iters", "spectra", "status"):
+                assert torch.equal(a[k], b[k]), k
+
+
 def test_autotune_picks_a_valid_tuning_and_keeps_results():
     c = case(1)
     with inverter(c, pm.PREC_FP32) as inv:
