@@ -692,8 +692,14 @@ __device__ __forceinline__ void rf_lane(const PmParams& P, const ModelTerms<R>& 
 // PSF correlation of the 32 response-function profiles, one profile per lane
 // (me_der.c:471-496): out[k] = sum_m x[m] G[m - k + nl/2].  A runtime loop over
 // the inputs m keeps the code small: per m one load of x[m] from the lane's own
-// row and the 32 taps of all outputs as aligned broadcast vector loads.  Stokes-I
-// rows correlate Ic - x with Ic = max of the row's end points.
+// row and the 32 taps of all outputs as aligned broadcast vector loads.  FP32
+// takes the inputs four at a time: their taps are one window of 35 consecutive
+// entries of a reversed tap row (9 vector loads for 128 products instead of 32),
+// which matters because all warps of a lock-step block run this loop together and
+// the broadcast loads were bound by shared-memory bandwidth; every output still
+// adds its products in the order of m, so the results are those of the one-input
+// loop bit for bit.  Stokes-I rows correlate Ic - x with Ic = max of the row's end
+// points.
 template <typename R>
 __device__ __forceinline__ void rf_correlate(const PmParams& P, const BlockSmem<R>& bs, WarpSmem<R>& sm,
                                              int lane) {
@@ -709,8 +715,48 @@ __device__ __forceinline__ void rf_correlate(const PmParams& P, const BlockSmem<
     float2 acc[NL / 2];
 #pragma unroll
     for (int k = 0; k < NL / 2; ++k) acc[k] = make_float2(0.0f, 0.0f);
+    constexpr int BLK = 4;                           // inputs per pass of the loop
+    constexpr int TW = (NL + BLK - 1 + 3) & ~3;      // their taps window, whole float4s
+    int m = 0;
 #pragma unroll 1
-    for (int m = 0; m < P.nl; ++m) {
+    for (; m + BLK <= P.nl; m += BLK) {
+      float xb[BLK];
+#pragma unroll
+      for (int i = 0; i < BLK; ++i) {
+        const float r = row[m + i];
+        xb[i] = isI ? ic - r : r;
+      }
+      // input m + i, output k: tap rv[c][b + k] with c + b = 31 - (m + i), i.e.
+      // t[(BLK - 1 - i) + k] of the window starting at rv[c0][b0]
+      const int base = 31 - m - (BLK - 1);
+      const int c0 = base & (VEC - 1), b0 = base - c0;
+      const float* g = bs.rv[c0] + b0;
+      float t[TW];
+#pragma unroll
+      for (int j = 0; j < TW; j += 4) {
+        const float4 q = *reinterpret_cast<const float4*>(g + j);
+        t[j] = q.x;
+        t[j + 1] = q.y;
+        t[j + 2] = q.z;
+        t[j + 3] = q.w;
+      }
+#pragma unroll
+      for (int i = 0; i < BLK; ++i) {
+        const int sh = BLK - 1 - i;
+        const float2 x2 = make_float2(xb[i], xb[i]);
+#pragma unroll
+        for (int k = 0; k < NL; k += 2) {
+          if ((sh & 1) == 0) {
+            acc[k / 2] = __ffma2_rn(x2, make_float2(t[sh + k], t[sh + k + 1]), acc[k / 2]);
+          } else {
+            acc[k / 2].x = fmaf(xb[i], t[sh + k], acc[k / 2].x);
+            acc[k / 2].y = fmaf(xb[i], t[sh + k + 1], acc[k / 2].y);
+          }
+        }
+      }
+    }
+#pragma unroll 1
+    for (; m < P.nl; ++m) {
       const float xm = isI ? ic - row[m] : row[m];
       const float2 x2 = make_float2(xm, xm);
       const int c = (31 - m) & (VEC - 1), b = (31 - m) - c;
