@@ -718,11 +718,11 @@ def main():
     hbm_peak = json.load(open(peaks_path))["hbm_gbs"] if os.path.exists(peaks_path) else 6650.0
     hbm_bytes = w.npix * args.steps * (16 * w.nl + 11 * 8 + 8)
     # DRAM bytes per pixel of the FP32 inversion kernel from one ncu capture of a
-    # cube of the same workload, scaled to this launch by its pixel count: 351.6 MB
+    # cube of the same workload, scaled to this launch by its pixel count: 353.9 MB
     # for 524,288 pixels of the 30-point grid (lock-step kernel, 16-warp blocks,
     # dram__bytes_read.sum + dram__bytes_write.sum), 132.7 MB for 65,536 pixels of
     # the 112-point grid
-    traffic = {1: 670.6, 4: 2025.0}.get(args.config) if w.nl in (30, 112) else None
+    traffic = {1: 675.0, 4: 2025.0}.get(args.config) if w.nl in (30, 112) else None
     traffic = traffic * w.npix if traffic else None
     roofline = {"bound": "fp32", "achieved": round(achieved, 3), "peak": round(peak_fp32, 2), "unit": "TFLOP/s",
                 "frac": round(achieved / peak_fp32, 4), "traffic": traffic,
