@@ -331,7 +331,7 @@ bool launch(pm_server* s) {
   s->gs_narrow->ngrids = s->nnarrow;
   for (int g = 0; g < s->ngrids; ++g)
     if (!s->wide_grid[g]) s->gs_narrow->g[s->narrow_index[g]] = s->gs->g[g];
-  const int rc = pmk_invert_stream(*s->gs_narrow, sio, s->precision, s->variant, s->variant == 2 ? 8 : 4,
+  const int rc = pmk_invert_stream(*s->gs_narrow, sio, s->precision, s->variant, s->variant == 2 ? 16 : 4,
                                    s->nnarrow > 1, s->s_kern, s->num_sms, nullptr, 0);
   if (rc != PM_OK) {
     s->error = rc;
