@@ -74,12 +74,6 @@ template <>
 __device__ __forceinline__ float omw<float>(const PmParams& P, int k) { return P.omw_f[k]; }
 template <>
 __device__ __forceinline__ double omw<double>(const PmParams& P, int k) { return P.omw_d[k]; }
-template <typename R>
-__device__ __forceinline__ R slshared(const PmParams& P, int i);
-template <>
-__device__ __forceinline__ float slshared<float>(const PmParams& P, int i) { return P.sl_f[i]; }
-template <>
-__device__ __forceinline__ double slshared<double>(const PmParams& P, int i) { return double(P.sl_f[i]); }
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -316,6 +310,11 @@ struct alignas(16) BlockSmem {
   // rv[c][u] = G[31 - (u + c) + half] (0 outside [0, nl)): for input m the
   // taps of outputs k = 0..31 are rv[c][b + k] with b + c = 31 - m, b % VEC == 0
   R rv[VEC][64 + VEC];
+  // the grid's offsets lambda - lambda0 per lane (dl[0] beyond nl) and the shared
+  // stray-light profile [4][nl] (PM_SLIGHT_SHARED): lane-indexed reads of the
+  // parameter block would be serialised by the constant cache
+  double dl[NL];
+  float sl[4 * NL];
 };
 
 // State of the damped solve: the normal equations and the Jacobi rotation tables.
@@ -368,6 +367,19 @@ __device__ __forceinline__ void load_taps(const PmParams& P, BlockSmem<R>& bs) {
     const int j = 31 - (u + c) + P.half;
     bs.rv[c][u] = (j >= 0 && j < P.nl) ? taps<R>(P, j) : R(0);
   }
+  for (int e = threadIdx.x; e < NL; e += blockDim.x) bs.dl[e] = P.dl[e < P.nl ? e : 0];
+  if (P.slight_mode == PM_SLIGHT_SHARED)
+    for (int e = threadIdx.x; e < 4 * NL; e += blockDim.x) bs.sl[e] = e < 4 * P.nl ? P.sl_f[e] : 0.0f;
+}
+
+// The stray-light profile a pixel mixes in: the block's copy of the shared one,
+// the pixel's own row of a per-pixel cube, or none.
+template <typename R>
+__device__ __forceinline__ const float* slight_of(const PmParams& P, const BlockSmem<R>& bs, const float* cube,
+                                                  size_t base) {
+  if (P.slight_mode == PM_SLIGHT_SHARED) return bs.sl;
+  if (P.slight_mode == PM_SLIGHT_PER_PIXEL && cube) return cube + base;
+  return nullptr;
 }
 
 // PSF correlation of the four synthesized profiles (mil_sinrf.c:387-402,
@@ -577,7 +589,7 @@ __device__ __forceinline__ void synthesize(const PmParams& P, WarpSmem<R>& sm, c
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
       const int idx = s * P.nl + (valid ? lane : 0);
-      const R slv = P.slight_mode == PM_SLIGHT_SHARED ? slshared<R>(P, idx) : R(sl_pix[idx]);
+      const R slv = R(sl_pix[idx]);  // shared profile (block copy) or the pixel's own
       S[s] = S[s] * T.alf + slv * T.oma;
     }
   }
@@ -848,7 +860,7 @@ __device__ __forceinline__ void gather_rf(const PmParams& P, const WarpSmem<R>& 
         d[r][s] = d[r][s] * alf;
         if (r == P.ff_row) {
           const int idx = s * P.nl + (valid ? lane : 0);
-          const R slv = P.slight_mode == PM_SLIGHT_SHARED ? slshared<R>(P, idx) : R(sl_pix[idx]);
+          const R slv = R(sl_pix[idx]);
           d[r][s] = valid ? Sff[s] - slv : R(0);
         }
       }
@@ -1363,18 +1375,15 @@ __device__ __forceinline__ void invert_pixel(const PmParams& P, const BlockSmem<
   const PmJob* jp = sm.job;
   size_t p = sm.pix;
   size_t base = p * 4 * P.nl;
-  const float* sl_pix = nullptr;
-  if (P.slight_mode == PM_SLIGHT_PER_PIXEL) {
-    const float* sl = ld_ptr(&jp->slight);
-    if (sl) sl_pix = sl + base;
-  }
+  const float* sl_pix =
+      slight_of<R>(P, bs, P.slight_mode == PM_SLIGHT_PER_PIXEL ? ld_ptr(&jp->slight) : nullptr, base);
   const float* obs = ld_ptr(&jp->spectro) + base;
   const double* model_in = ld_ptr(&jp->model_in);
   double dlp = 0.0;
   if constexpr (PIXGRID) dlp = valid ? __ldcg(ld_ptr(&jp->lambda) + p * P.nl + lane) - P.lambda0 : 0.0;
   auto dl = [&]() -> double {
     if constexpr (PIXGRID) return dlp;
-    else return P.dl[valid ? lane : 0];
+    else return bs.dl[lane];
   };
 
   float O[4];
@@ -1535,22 +1544,19 @@ struct PixelLM {
 // Before the loop (invert_pixel up to its first pass): the pixel's profiles,
 // ghosts, starting model; finished at once when nfree == 0.
 template <typename R, bool PIXGRID>
-__device__ __forceinline__ void lm_begin(const PmParams& P, WarpSmem<R>& sm, int lane, PixelLM<R>& L) {
+__device__ __forceinline__ void lm_begin(const PmParams& P, const BlockSmem<R>& bs, WarpSmem<R>& sm, int lane,
+                                         PixelLM<R>& L) {
   const bool valid = lane < P.nl;
   double* m = sm.model;
   const PmJob* jp = sm.job;
   const size_t p = sm.pix;
   const size_t base = p * 4 * P.nl;
-  L.sl_pix = nullptr;
-  if (P.slight_mode == PM_SLIGHT_PER_PIXEL) {
-    const float* sl = ld_ptr(&jp->slight);
-    if (sl) L.sl_pix = sl + base;
-  }
+  L.sl_pix = slight_of<R>(P, bs, P.slight_mode == PM_SLIGHT_PER_PIXEL ? ld_ptr(&jp->slight) : nullptr, base);
   const float* obs = ld_ptr(&jp->spectro) + base;
   const double* model_in = ld_ptr(&jp->model_in);
   L.dlp = 0.0;
   if constexpr (PIXGRID) L.dlp = valid ? __ldcg(ld_ptr(&jp->lambda) + p * P.nl + lane) - P.lambda0 : 0.0;
-  const double dl = PIXGRID ? L.dlp : P.dl[valid ? lane : 0];
+  const double dl = PIXGRID ? L.dlp : bs.dl[lane];
   int ghosts = 0;
   if ((reinterpret_cast<uintptr_t>(obs) & 15) == 0) {
     // the pixel's 4 x nl floats as nl 16-byte loads (one per lane, one
@@ -1641,9 +1647,10 @@ __device__ __forceinline__ void lm_solve(const PmParams& P, WarpSmem<R>& sm, int
 
 // Phase 2: synthesis of the trial model, chi^2, the stopping and acceptance tests.
 template <typename R, bool MAC, bool PIXGRID, bool ZM>
-__device__ __forceinline__ void lm_synth(const PmParams& P, WarpSmem<R>& sm, int lane, PixelLM<R>& L) {
+__device__ __forceinline__ void lm_synth(const PmParams& P, const BlockSmem<R>& bs, WarpSmem<R>& sm, int lane,
+                                         PixelLM<R>& L) {
   const bool valid = lane < P.nl;
-  const double dl = PIXGRID ? L.dlp : P.dl[valid ? lane : 0];
+  const double dl = PIXGRID ? L.dlp : bs.dl[lane];
   synthesize<R, MAC, ZM>(P, sm, sm.trial, L.sl_pix, lane, valid, dl, L.S, L.Su);
   L.chi = chisq<R>(P, L.S, L.O, L.isig, valid, double(L.nfree));
   L.accept = true;
@@ -1662,7 +1669,7 @@ template <typename R, int KT, bool MAC, bool PIXGRID, bool ZM>
 __device__ __forceinline__ void lm_update(const PmParams& P, const BlockSmem<R>& bs, WarpSmem<R>& sm, int lane,
                                           PixelLM<R>& L) {
   const bool valid = lane < P.nl;
-  const double dl = PIXGRID ? L.dlp : P.dl[valid ? lane : 0];
+  const double dl = PIXGRID ? L.dlp : bs.dl[lane];
   if (L.accept) {
     if (!L.first) L.flambda = L.flambda / (5.0 * L.factor);
     if (lane < 11) sm.model[lane] = sm.trial[lane];

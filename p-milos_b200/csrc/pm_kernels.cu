@@ -21,7 +21,7 @@ __global__ void __launch_bounds__(128) synth_kernel(const __grid_constant__ PmPa
   const int64_t nwarps = int64_t(gridDim.x) * (blockDim.x >> 5);
   for (int64_t pix = int64_t(blockIdx.x) * (blockDim.x >> 5) + warp; pix < io.npix; pix += nwarps) {
     const size_t base = size_t(pix) * 4 * P.nl;
-    const float* sl_pix = (P.slight_mode == PM_SLIGHT_PER_PIXEL) ? io.slight + base : nullptr;
+    const float* sl_pix = slight_of<R>(P, bs, io.slight, base);
     if (lane < 11) sm.model[lane] = io.models_in[size_t(pix) * 11 + lane];
     __syncwarp();
     const double dl = !valid ? 0.0 : (io.lambda_pix ? io.lambda_pix[size_t(pix) * P.nl + lane] - P.lambda0 : P.dl[lane]);

@@ -256,7 +256,7 @@ __global__ void __launch_bounds__(32 * W, 16 / W) invert_lockstep_kernel(
         }
       }
       __syncwarp();
-      lm_begin<R, PIXGRID>(GS.g[gi], sm, lane, L);
+      lm_begin<R, PIXGRID>(GS.g[gi], bs[gi], sm, lane, L);
       if (L.finished) {
         lm_end<R>(GS.g[gi], sm, lane, L, sio.q->ctr);
         job_pixel_done(sm, lane);
@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(32 * W, 16 / W) invert_lockstep_kernel(
     // no barrier between the synthesis and the update: a warp whose step was
     // accepted starts its response functions while slower warps finish their
     // synthesis (a barrier here cost 2-5%)
-    if (have) lm_synth<R, MAC, PIXGRID, ZM>(P, sm, lane, L);
+    if (have) lm_synth<R, MAC, PIXGRID, ZM>(P, bs[gi], sm, lane, L);
     if (have) {
       lm_update<R, KT, MAC, PIXGRID, ZM>(P, bs[gi], sm, lane, L);
       if (L.finished) {

@@ -31,8 +31,26 @@ struct alignas(16) WideSmem {
   SolveSmem sv;
   double red[2][G][RED];       // per-warp partial sums, double-buffered
   double model[11], trial[11];
+  // the shared stray-light profile [4][nl] (PM_SLIGHT_SHARED): thread-indexed
+  // reads of the parameter block would be serialised by the constant cache
+  float sl[4 * NT];
   unsigned long long pix;
 };
+
+// The block's copy of the shared stray-light profile (every thread calls it; the
+// caller's next barrier publishes it) and the profile a pixel mixes in.
+template <typename R, int G>
+__device__ __forceinline__ void load_slight_wide(const PmParams& P, WideSmem<R, G>& sm) {
+  if (P.slight_mode == PM_SLIGHT_SHARED)
+    for (int e = threadIdx.x; e < 4 * WideSmem<R, G>::NT; e += 32 * G) sm.sl[e] = e < 4 * P.nl ? P.sl_f[e] : 0.0f;
+}
+template <typename R, int G>
+__device__ __forceinline__ const float* slight_of_wide(const PmParams& P, const WideSmem<R, G>& sm,
+                                                       const float* cube, size_t base) {
+  if (P.slight_mode == PM_SLIGHT_SHARED) return sm.sl;
+  if (P.slight_mode == PM_SLIGHT_PER_PIXEL && cube) return cube + base;
+  return nullptr;
+}
 
 template <typename R, int G>
 constexpr bool wide_layout_ok() {
@@ -271,7 +289,7 @@ __device__ __forceinline__ void synthesize_wide(const PmParams& P, WideSmem<R, G
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
       const int idx = s * P.nl + (valid ? t : 0);
-      const R slv = P.slight_mode == PM_SLIGHT_SHARED ? slshared<R>(P, idx) : R(sl_pix[idx]);
+      const R slv = R(sl_pix[idx]);  // shared profile (block copy) or the pixel's own
       S[s] = S[s] * T.alf + slv * T.oma;
     }
   }
@@ -371,7 +389,7 @@ __device__ __forceinline__ void rf_wide(const PmParams& P, WideSmem<R, G>& sm, i
         d[r][s] = d[r][s] * alf;
         if (r == P.ff_row) {
           const int idx = s * P.nl + (valid ? t : 0);
-          const R slv = P.slight_mode == PM_SLIGHT_SHARED ? slshared<R>(P, idx) : R(sl_pix[idx]);
+          const R slv = R(sl_pix[idx]);
           d[r][s] = valid ? Sff[s] - slv : R(0);
         }
       }
@@ -467,6 +485,7 @@ __global__ void __launch_bounds__(32 * G, MINB) invert_wide_kernel(const __grid_
   double* m = sm.model;
   double* trial = sm.trial;
   int slot = 0;
+  load_slight_wide<R, G>(P, sm);  // published by the loop's first barrier
 
   while (true) {
     if (t == 0) sm.pix = atomicAdd(&io.ctr[PMC_NEXT], 1ull);
@@ -477,7 +496,7 @@ __global__ void __launch_bounds__(32 * G, MINB) invert_wide_kernel(const __grid_
     const double* lp = PIXGRID ? io.lambda_pix + size_t(pix) * P.nl : nullptr;
     if constexpr (PIXGRID) dl_t = lp[valid ? t : 0] - P.lambda0;
     const size_t base = size_t(pix) * 4 * P.nl;
-    const float* sl_pix = (P.slight_mode == PM_SLIGHT_PER_PIXEL) ? io.slight + base : nullptr;
+    const float* sl_pix = slight_of_wide<R, G>(P, sm, io.slight, base);
 
     float O[4];
     R isig[4];
@@ -656,9 +675,10 @@ __global__ void __launch_bounds__(32 * G) synth_wide_kernel(const __grid_constan
   const bool valid = t < P.nl;
   double dl_t = P.dl[valid ? t : 0];
   const R omw_t = valid ? omw<R>(P, t) : R(0);
+  load_slight_wide<R, G>(P, sm);  // published by the loop's first barrier
   for (int64_t pix = blockIdx.x; pix < io.npix; pix += gridDim.x) {
     const size_t base = size_t(pix) * 4 * P.nl;
-    const float* sl_pix = (P.slight_mode == PM_SLIGHT_PER_PIXEL) ? io.slight + base : nullptr;
+    const float* sl_pix = slight_of_wide<R, G>(P, sm, io.slight, base);
     const double* lp = io.lambda_pix ? io.lambda_pix + size_t(pix) * P.nl : nullptr;  // the pixel's own wavelengths
     if (lp) dl_t = lp[valid ? t : 0] - P.lambda0;
     if (t < 11) sm.model[t] = io.models_in[size_t(pix) * 11 + t];
