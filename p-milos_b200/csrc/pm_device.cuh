@@ -310,10 +310,8 @@ struct alignas(16) BlockSmem {
   // rv[c][u] = G[31 - (u + c) + half] (0 outside [0, nl)): for input m the
   // taps of outputs k = 0..31 are rv[c][b + k] with b + c = 31 - m, b % VEC == 0
   R rv[VEC][64 + VEC];
-  // the grid's offsets lambda - lambda0 per lane (dl[0] beyond nl) and the shared
-  // stray-light profile [4][nl] (PM_SLIGHT_SHARED): lane-indexed reads of the
-  // parameter block would be serialised by the constant cache
-  double dl[NL];
+  // the shared stray-light profile [4][nl] (PM_SLIGHT_SHARED): lane-indexed
+  // reads of the parameter block would be serialised by the constant cache
   float sl[4 * NL];
 };
 
@@ -367,7 +365,6 @@ __device__ __forceinline__ void load_taps(const PmParams& P, BlockSmem<R>& bs) {
     const int j = 31 - (u + c) + P.half;
     bs.rv[c][u] = (j >= 0 && j < P.nl) ? taps<R>(P, j) : R(0);
   }
-  for (int e = threadIdx.x; e < NL; e += blockDim.x) bs.dl[e] = P.dl[e < P.nl ? e : 0];
   if (P.slight_mode == PM_SLIGHT_SHARED)
     for (int e = threadIdx.x; e < 4 * NL; e += blockDim.x) bs.sl[e] = e < 4 * P.nl ? P.sl_f[e] : 0.0f;
 }
@@ -1383,7 +1380,7 @@ __device__ __forceinline__ void invert_pixel(const PmParams& P, const BlockSmem<
   if constexpr (PIXGRID) dlp = valid ? __ldcg(ld_ptr(&jp->lambda) + p * P.nl + lane) - P.lambda0 : 0.0;
   auto dl = [&]() -> double {
     if constexpr (PIXGRID) return dlp;
-    else return bs.dl[lane];
+    else return P.dl[valid ? lane : 0];
   };
 
   float O[4];
@@ -1556,7 +1553,7 @@ __device__ __forceinline__ void lm_begin(const PmParams& P, const BlockSmem<R>& 
   const double* model_in = ld_ptr(&jp->model_in);
   L.dlp = 0.0;
   if constexpr (PIXGRID) L.dlp = valid ? __ldcg(ld_ptr(&jp->lambda) + p * P.nl + lane) - P.lambda0 : 0.0;
-  const double dl = PIXGRID ? L.dlp : bs.dl[lane];
+  const double dl = PIXGRID ? L.dlp : P.dl[valid ? lane : 0];
   int ghosts = 0;
   if ((reinterpret_cast<uintptr_t>(obs) & 15) == 0) {
     // the pixel's 4 x nl floats as nl 16-byte loads (one per lane, one
@@ -1647,10 +1644,9 @@ __device__ __forceinline__ void lm_solve(const PmParams& P, WarpSmem<R>& sm, int
 
 // Phase 2: synthesis of the trial model, chi^2, the stopping and acceptance tests.
 template <typename R, bool MAC, bool PIXGRID, bool ZM>
-__device__ __forceinline__ void lm_synth(const PmParams& P, const BlockSmem<R>& bs, WarpSmem<R>& sm, int lane,
-                                         PixelLM<R>& L) {
+__device__ __forceinline__ void lm_synth(const PmParams& P, WarpSmem<R>& sm, int lane, PixelLM<R>& L) {
   const bool valid = lane < P.nl;
-  const double dl = PIXGRID ? L.dlp : bs.dl[lane];
+  const double dl = PIXGRID ? L.dlp : P.dl[valid ? lane : 0];
   synthesize<R, MAC, ZM>(P, sm, sm.trial, L.sl_pix, lane, valid, dl, L.S, L.Su);
   L.chi = chisq<R>(P, L.S, L.O, L.isig, valid, double(L.nfree));
   L.accept = true;
@@ -1669,7 +1665,7 @@ template <typename R, int KT, bool MAC, bool PIXGRID, bool ZM>
 __device__ __forceinline__ void lm_update(const PmParams& P, const BlockSmem<R>& bs, WarpSmem<R>& sm, int lane,
                                           PixelLM<R>& L) {
   const bool valid = lane < P.nl;
-  const double dl = PIXGRID ? L.dlp : bs.dl[lane];
+  const double dl = PIXGRID ? L.dlp : P.dl[valid ? lane : 0];
   if (L.accept) {
     if (!L.first) L.flambda = L.flambda / (5.0 * L.factor);
     if (lane < 11) sm.model[lane] = sm.trial[lane];

@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(32 * W, 16 / W) invert_lockstep_kernel(
     // no barrier between the synthesis and the update: a warp whose step was
     // accepted starts its response functions while slower warps finish their
     // synthesis (a barrier here cost 2-5%)
-    if (have) lm_synth<R, MAC, PIXGRID, ZM>(P, bs[gi], sm, lane, L);
+    if (have) lm_synth<R, MAC, PIXGRID, ZM>(P, sm, lane, L);
     if (have) {
       lm_update<R, KT, MAC, PIXGRID, ZM>(P, bs[gi], sm, lane, L);
       if (L.finished) {
